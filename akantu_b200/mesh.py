@@ -1,0 +1,219 @@
+"""Mesh container, Gmsh v2 reader and structured mesh generators.
+
+Mirrors the subset of akantu::Mesh the explicit path uses (mesh.hh:100):
+nodal coordinates (getNodes, mesh.hh:293), one connectivity array of the
+spatial dimension's element type (getConnectivity, mesh.hh:353) and node
+groups for boundary conditions (GroupManager, group_manager.hh:63).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _abi
+
+# element type properties: (name, dimension, nodes per element, quadrature points)
+ELEMENT_TYPES = {
+    _abi.SEGMENT_2: ("_segment_2", 1, 2, 1),
+    _abi.TRIANGLE_3: ("_triangle_3", 2, 3, 1),
+    _abi.TETRAHEDRON_4: ("_tetrahedron_4", 3, 4, 1),
+    _abi.HEXAHEDRON_8: ("_hexahedron_8", 3, 8, 8),
+}
+NAME_TO_TYPE = {v[0]: k for k, v in ELEMENT_TYPES.items()}
+
+# gmsh element type -> akantu type (mesh_io_msh.cc: _msh_to_akantu_element_types);
+# no node permutation for these types (mesh_io_msh.cc:224-276).
+_MSH_TYPES = {1: _abi.SEGMENT_2, 2: _abi.TRIANGLE_3, 4: _abi.TETRAHEDRON_4,
+              5: _abi.HEXAHEDRON_8}
+
+# boundary facets of each element type (local node indices)
+_FACETS = {
+    _abi.SEGMENT_2: [(0,), (1,)],
+    _abi.TRIANGLE_3: [(0, 1), (1, 2), (2, 0)],
+    _abi.TETRAHEDRON_4: [(0, 2, 1), (1, 2, 3), (2, 0, 3), (0, 1, 3)],
+    _abi.HEXAHEDRON_8: [(0, 1, 2, 3), (4, 5, 6, 7), (0, 1, 5, 4),
+                        (1, 2, 6, 5), (2, 3, 7, 6), (3, 0, 4, 7)],
+}
+
+
+def element_properties(element_type):
+    name, dim, nnpe, nqp = ELEMENT_TYPES[element_type]
+    return dim, nnpe, nqp
+
+
+class Mesh:
+    """Nodes (N x d, float64) + connectivity (E x n, uint32) + node groups."""
+
+    def __init__(self, spatial_dimension, element_type=None, nodes=None,
+                 connectivity=None):
+        self.spatial_dimension = int(spatial_dimension)
+        self.element_type = element_type
+        self.nodes = np.zeros((0, self.spatial_dimension)) if nodes is None \
+            else np.ascontiguousarray(nodes, dtype=np.float64)
+        self.connectivity = np.zeros((0, 0), dtype=np.uint32) if connectivity is None \
+            else np.ascontiguousarray(connectivity, dtype=np.uint32)
+        self.node_groups: dict[str, np.ndarray] = {}
+
+    # --- reference-style accessors -------------------------------------
+    def getNodes(self):
+        return self.nodes
+
+    def getConnectivity(self, element_type=None):
+        return self.connectivity
+
+    def getNbNodes(self):
+        return self.nodes.shape[0]
+
+    def getNbElement(self, element_type=None):
+        return self.connectivity.shape[0]
+
+    def getSpatialDimension(self):
+        return self.spatial_dimension
+
+    def getNodeGroup(self, name):
+        return self.node_groups[name]
+
+    def createNodeGroup(self, name, nodes):
+        self.node_groups[name] = np.unique(np.asarray(nodes, dtype=np.int64))
+        return self.node_groups[name]
+
+    # --- Gmsh reader (MeshIOMSH::read, mesh_io_msh.cc) ------------------
+    def read(self, filename):
+        with open(filename) as fh:
+            text = fh.read()
+        self.read_msh_text(text)
+
+    def read_msh_text(self, text):
+        """Gmsh ASCII v2 reader: nodes in file order, elements of this mesh's
+        spatial dimension; lower-dimension elements are kept by physical tag
+        as node groups named 'physical_<tag>'."""
+        lines = [ln.strip() for ln in text.splitlines()]
+        i = 0
+        tag_to_index = {}
+        nodes = []
+        blocks: dict[int, list] = {}
+        groups: dict[str, set] = {}
+        while i < len(lines):
+            ln = lines[i]
+            if ln == "$Nodes":
+                n = int(lines[i + 1])
+                for k in range(n):
+                    parts = lines[i + 2 + k].split()
+                    tag_to_index[int(parts[0])] = k
+                    nodes.append([float(x) for x in parts[1:1 + self.spatial_dimension]])
+                i += n + 2
+                continue
+            if ln == "$Elements":
+                n = int(lines[i + 1])
+                for k in range(n):
+                    parts = [int(x) for x in lines[i + 2 + k].split()]
+                    etype, ntags = parts[1], parts[2]
+                    tags = parts[3:3 + ntags]
+                    conn = [tag_to_index[t] for t in parts[3 + ntags:]]
+                    akt = _MSH_TYPES.get(etype)
+                    if akt is not None and ELEMENT_TYPES[akt][1] == self.spatial_dimension:
+                        blocks.setdefault(akt, []).append(conn)
+                    elif tags:
+                        groups.setdefault("physical_%d" % tags[0], set()).update(conn)
+                i += n + 2
+                continue
+            i += 1
+        if len(blocks) != 1:
+            raise ValueError("expected one element type of dimension %d, found %s"
+                             % (self.spatial_dimension, list(blocks)))
+        (akt, conn), = blocks.items()
+        self.element_type = akt
+        self.nodes = np.asarray(nodes, dtype=np.float64).reshape(-1, self.spatial_dimension)
+        self.connectivity = np.asarray(conn, dtype=np.uint32)
+        for name, s in groups.items():
+            self.node_groups[name] = np.array(sorted(s), dtype=np.int64)
+
+    # --- boundary groups (Mesh::createBoundaryGroupFromGeometry) ---------
+    def boundary_nodes(self):
+        """Nodes of facets that belong to exactly one element."""
+        counts = {}
+        for elem in self.connectivity:
+            for f in _FACETS[self.element_type]:
+                key = tuple(sorted(int(elem[k]) for k in f))
+                counts[key] = counts.get(key, 0) + 1
+        nodes = set()
+        for key, c in counts.items():
+            if c == 1:
+                nodes.update(key)
+        return np.array(sorted(nodes), dtype=np.int64)
+
+    def createBoundaryGroupFromGeometry(self):
+        """One node group 'boundary' with every node on a boundary facet
+        (the reference splits it into connected surfaces; the explicit path
+        only uses the union)."""
+        return self.createNodeGroup("boundary", self.boundary_nodes())
+
+    def iterateNodeGroups(self):
+        return self.node_groups.items()
+
+
+# --------------------------------------------------------------------------
+# structured generators (seeded synthetic workloads)
+# --------------------------------------------------------------------------
+def bar_segment2(nb_nodes, length=1.0):
+    """1D bar of nb_nodes-1 segment_2 elements on [0, length]."""
+    x = np.arange(nb_nodes, dtype=np.float64) * (length / (nb_nodes - 1))
+    conn = np.stack([np.arange(nb_nodes - 1), np.arange(1, nb_nodes)], 1)
+    return Mesh(1, _abi.SEGMENT_2, x.reshape(-1, 1), conn)
+
+
+def plate_triangle3(nx, ny, lx, ly, origin=(0.0, 0.0)):
+    """nx x ny squares over lx x ly, each split along the (i,j)-(i+1,j+1)
+    diagonal into two counter-clockwise triangle_3; nodes numbered x-fastest,
+    elements cell by cell (x-fastest), two per cell."""
+    xs = origin[0] + np.arange(nx + 1, dtype=np.float64) * (lx / nx)
+    ys = origin[1] + np.arange(ny + 1, dtype=np.float64) * (ly / ny)
+    X, Y = np.meshgrid(xs, ys, indexing="xy")
+    nodes = np.stack([X.ravel(), Y.ravel()], 1)
+    j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    n00 = (j * (nx + 1) + i).ravel()
+    n10 = n00 + 1
+    n01 = n00 + (nx + 1)
+    n11 = n01 + 1
+    t1 = np.stack([n00, n10, n11], 1)
+    t2 = np.stack([n00, n11, n01], 1)
+    conn = np.stack([t1, t2], 1).reshape(-1, 3)
+    return Mesh(2, _abi.TRIANGLE_3, nodes, conn)
+
+
+def _grid_nodes_3d(n, length):
+    xs = np.arange(n + 1, dtype=np.float64) * (length / n)
+    Z, Y, X = np.meshgrid(xs, xs, xs, indexing="ij")
+    return np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+
+
+def cube_tetrahedron4(n, length=1.0):
+    """n^3 cubes, each split into 6 tetrahedra around the (0,0,0)-(1,1,1)
+    diagonal (Kuhn split), all positively oriented; nodes x-fastest."""
+    nodes = _grid_nodes_3d(n, length)
+    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    base = (k * (n + 1) * (n + 1) + j * (n + 1) + i).ravel()
+    off = {"x": 1, "y": n + 1, "z": (n + 1) * (n + 1)}
+    tets = []
+    for perm in ("xyz", "xzy", "yxz", "yzx", "zxy", "zyx"):
+        a = off[perm[0]]
+        b = a + off[perm[1]]
+        c = b + off[perm[2]]
+        # even permutations are positively oriented; odd ones swap two nodes
+        even = perm in ("xyz", "yzx", "zxy")
+        t = (base, base + a, base + b, base + c) if even else \
+            (base, base + b, base + a, base + c)
+        tets.append(np.stack(t, 1))
+    conn = np.stack(tets, 1).reshape(-1, 4)
+    return Mesh(3, _abi.TETRAHEDRON_4, nodes, conn)
+
+
+def block_hexahedron8(n, length=1.0):
+    """n^3 hexahedron_8 (reference node order: bottom face counter-clockwise,
+    then top face); nodes x-fastest, elements x-fastest."""
+    nodes = _grid_nodes_3d(n, length)
+    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    p = n + 1
+    b = (k * p * p + j * p + i).ravel()
+    conn = np.stack([b, b + 1, b + 1 + p, b + p,
+                     b + p * p, b + 1 + p * p, b + 1 + p + p * p, b + p + p * p], 1)
+    return Mesh(3, _abi.HEXAHEDRON_8, nodes, conn)

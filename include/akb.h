@@ -1,0 +1,201 @@
+/*
+ * akb.h -- C ABI of the B200-native explicit-dynamics library (libakb.so).
+ *
+ * This is the drop-in boundary for Akantu's explicit central-difference path
+ * with lumped mass. The reference exposes that path only as a C++ class API
+ * (no C ABI); every entry point below names the reference member function it
+ * replaces, cited as file:line within the Akantu 3.1.0 source tree.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only; no CUDA or torch types in any signature
+ *    (streams are passed as void*, holding a cudaStream_t).
+ *  - Host arrays use the reference Array<T> layout: one row per node (or per
+ *    element, or per quadrature point), components contiguous, row-major.
+ *  - Every call returns an akb_status; AKB_OK is 0. On failure a message is
+ *    stored per host thread and returned by akb_last_error().
+ *  - A model handle may be used by one host thread at a time.
+ */
+#ifndef AKB_H
+#define AKB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AKB_ABI_VERSION 1
+
+typedef int32_t akb_status;
+enum {
+  AKB_OK = 0,
+  AKB_ERR_INVALID_ARGUMENT = 1,
+  AKB_ERR_BAD_MESH = 2,
+  AKB_ERR_NEGATIVE_JACOBIAN = 3, /* integrator_gauss_inline_impl.hh:183-205 */
+  AKB_ERR_NON_FINITE = 4,
+  AKB_ERR_CUDA = 5,
+  AKB_ERR_TIMEOUT = 6,
+  AKB_ERR_STATE = 7,
+  AKB_ERR_UNSUPPORTED = 8,
+  AKB_ERR_OUT_OF_MEMORY = 9
+};
+
+/* Element types on the path (reference ElementType, aka_element_classes_info). */
+enum {
+  AKB_SEGMENT_2 = 1,
+  AKB_TRIANGLE_3 = 2,
+  AKB_TETRAHEDRON_4 = 3,
+  AKB_HEXAHEDRON_8 = 4
+};
+
+/* Constitutive laws on the path. */
+enum {
+  AKB_MATERIAL_ELASTIC = 0,    /* materials/material_elastic.cc */
+  AKB_MATERIAL_NEOHOOKEAN = 1  /* material_finite_deformation/material_neohookean.cc */
+};
+
+/* Arithmetic modes.
+ * AKB_MODE_FP64_REFERENCE: FP64, the reference's own operation order (stored
+ *   shape derivatives, B^T sigma, Gauss integration, element-order scatter),
+ *   compiled without FMA contraction.
+ * AKB_MODE_FP64: FP64 element and nodal arithmetic, fused kernels.
+ * AKB_MODE_FP32_BULK: element gradient, stress and B^T sigma in FP32 with
+ *   FP32 accumulation; nodal state, inverse lumped mass and energies FP64. */
+enum {
+  AKB_MODE_FP64_REFERENCE = 0,
+  AKB_MODE_FP64 = 1,
+  AKB_MODE_FP32_BULK = 2
+};
+
+/* Fields (reference getters, solid_mechanics_model.hh:364-397). */
+enum {
+  AKB_FIELD_DISPLACEMENT = 0,   /* N x d, read/write */
+  AKB_FIELD_VELOCITY = 1,       /* N x d, read/write */
+  AKB_FIELD_ACCELERATION = 2,   /* N x d, read/write */
+  AKB_FIELD_EXTERNAL_FORCE = 3, /* N x d, read/write */
+  AKB_FIELD_INTERNAL_FORCE = 4, /* N x d, read only */
+  AKB_FIELD_MASS = 5,           /* N x d, read only (after mass assembly) */
+  AKB_FIELD_NODES = 6,          /* N x d, read only */
+  AKB_FIELD_GRAD_U = 7,         /* (E*q) x d*d column-major, read only */
+  AKB_FIELD_STRESS = 8          /* (E*q) x d*d: Cauchy (small strain) or PK2 */
+};
+
+/* Energies (SolidMechanicsModel::getEnergy, solid_mechanics_model.cc:536-683). */
+enum {
+  AKB_ENERGY_KINETIC = 0,
+  AKB_ENERGY_POTENTIAL = 1,
+  AKB_ENERGY_EXTERNAL_WORK = 2
+};
+
+typedef struct {
+  int32_t spatial_dimension;   /* 1, 2 or 3 */
+  int32_t element_type;        /* AKB_SEGMENT_2 ... AKB_HEXAHEDRON_8 */
+  int64_t nb_nodes;
+  int64_t nb_elements;
+  const double* nodes;          /* [nb_nodes][spatial_dimension] */
+  const uint32_t* connectivity; /* [nb_elements][nodes_per_element] */
+} akb_mesh_desc;
+
+/* Parameters of one material section of the reference input file
+ * (material elastic [ rho, E, nu, Plane_Stress, finite_deformation ]). */
+typedef struct {
+  int32_t kind;               /* AKB_MATERIAL_* */
+  int32_t plane_stress;       /* 2D only; 0 = plane strain (reference default) */
+  int32_t finite_deformation; /* elastic only; neo-Hookean is always finite */
+  int32_t reserved;
+  double rho;
+  double E;
+  double nu;
+} akb_material_desc;
+
+typedef struct {
+  int32_t precision_mode; /* AKB_MODE_* */
+  int32_t device;         /* CUDA device ordinal */
+  void* stream;           /* cudaStream_t to run on; NULL = library-owned stream */
+} akb_model_options;
+
+typedef struct {
+  int32_t spatial_dimension;
+  int32_t element_type;
+  int32_t nodes_per_element;
+  int32_t quadrature_points_per_element;
+  int64_t nb_nodes;
+  int64_t nb_elements;
+  int32_t precision_mode;
+  int32_t nb_materials;
+  int64_t device_bytes; /* bytes of device memory the model holds */
+} akb_model_info;
+
+typedef struct akb_model akb_model;
+
+/* Library version and the message of the last failed call on this thread. */
+int32_t akb_abi_version(void);
+const char* akb_last_error(void);
+
+/* SolidMechanicsModel(mesh) + initFull(_analysis_method = _explicit_lumped_mass)
+ * (solid_mechanics_model.hh:85-88, model.hh:78-99, solid_mechanics_model.cc:132-147).
+ * element_material may be NULL (every element uses material 0); otherwise one
+ * material index per element (the reference's material_index). */
+akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
+                            const akb_material_desc* materials,
+                            const uint32_t* element_material,
+                            const akb_model_options* options,
+                            akb_model** model);
+akb_status akb_model_destroy(akb_model* model);
+akb_status akb_model_get_info(const akb_model* model, akb_model_info* info);
+
+/* getDisplacement()/getVelocity()/... copies (solid_mechanics_model.hh:364-397).
+ * count is the number of doubles in the host array. */
+akb_status akb_set_field(akb_model* model, int32_t field, const double* values,
+                         int64_t count);
+akb_status akb_get_field(akb_model* model, int32_t field, double* values,
+                         int64_t count);
+/* Device address of a field (N x d doubles), valid until akb_model_destroy. */
+akb_status akb_field_device_pointer(akb_model* model, int32_t field,
+                                    void** device_pointer);
+
+/* getBlockedDOFs() (solid_mechanics_model.hh:397): N x d bytes, 0 or 1. */
+akb_status akb_set_blocked_dofs(akb_model* model, const uint8_t* blocked,
+                                int64_t count);
+akb_status akb_get_blocked_dofs(akb_model* model, uint8_t* blocked,
+                                int64_t count);
+
+/* SolidMechanicsModel::assembleMassLumped (solid_mechanics_model_mass.cc:58-133). */
+akb_status akb_assemble_mass_lumped(akb_model* model);
+
+/* SolidMechanicsModel::getStableTimeStep (solid_mechanics_model.cc:482-533). */
+akb_status akb_get_stable_time_step(akb_model* model, double* time_step);
+
+/* setTimeStep / getTimeStep (solid_mechanics_model.cc:109-115, model_solver.cc:321-325). */
+akb_status akb_set_time_step(akb_model* model, double time_step);
+akb_status akb_get_time_step(const akb_model* model, double* time_step);
+
+/* ModelSolver::solveStep (model_solver.cc:265-278) for the explicit lumped
+ * solver: NonLinearSolverLumped::solve (non_linear_solver_lumped.cc:58-82). */
+akb_status akb_solve_step(akb_model* model);
+/* nb_steps consecutive solveStep() calls, replayed from a CUDA graph. */
+akb_status akb_solve_steps(akb_model* model, int64_t nb_steps);
+/* akb_solve_steps timed with CUDA events on the model's stream; *elapsed_ms
+ * is the device time of the whole sequence. */
+akb_status akb_time_solve_steps(akb_model* model, int64_t nb_steps,
+                                double* elapsed_ms);
+
+/* SolidMechanicsModel::assembleInternalForces (solid_mechanics_model.cc:375-414)
+ * at the current displacement. */
+akb_status akb_assemble_internal_forces(akb_model* model);
+/* Material::computeAllStresses (material.cc:254-279) at the current
+ * displacement; fills AKB_FIELD_GRAD_U and AKB_FIELD_STRESS. */
+akb_status akb_compute_stresses(akb_model* model);
+
+/* SolidMechanicsModel::getEnergy (solid_mechanics_model.cc:665-683). */
+akb_status akb_get_energy(akb_model* model, int32_t kind, double* value);
+
+/* Waits for all work queued on the model's stream. */
+akb_status akb_synchronize(akb_model* model);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AKB_H */

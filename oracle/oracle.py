@@ -1,0 +1,161 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
+the checker and by bench.py's CPU-baseline leg. The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from akantu_b200 import _abi
+from akantu_b200.mesh import element_properties
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS = {}
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _lib(fast=False):
+    name = "liboracle_fast.so" if fast else "liboracle.so"
+    if name in _LIBS:
+        return _LIBS[name]
+    path = os.path.join(_HERE, "_build", name)
+    if not os.path.exists(path):
+        build()
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.oracle_create.restype = P
+    lib.oracle_create.argtypes = [C.POINTER(_abi.MeshDesc), C.c_int32,
+                                  C.POINTER(_abi.MaterialDesc), C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_int32)]
+    lib.oracle_destroy.argtypes = [P]
+    lib.oracle_field.restype = C.POINTER(C.c_double)
+    lib.oracle_field.argtypes = [P, C.c_int32]
+    lib.oracle_field_size.restype = C.c_int64
+    lib.oracle_field_size.argtypes = [P, C.c_int32]
+    lib.oracle_blocked.restype = C.POINTER(C.c_uint8)
+    lib.oracle_blocked.argtypes = [P]
+    for fn in ("oracle_assemble_mass_lumped", "oracle_solve_step",
+               "oracle_assemble_internal_forces", "oracle_compute_stresses"):
+        getattr(lib, fn).argtypes = [P]
+    lib.oracle_stable_time_step.restype = C.c_double
+    lib.oracle_stable_time_step.argtypes = [P]
+    lib.oracle_set_time_step.argtypes = [P, C.c_double]
+    lib.oracle_solve_steps.argtypes = [P, C.c_int64]
+    lib.oracle_energy.restype = C.c_double
+    lib.oracle_energy.argtypes = [P, C.c_int32]
+    lib.oracle_time_steps.restype = C.c_double
+    lib.oracle_time_steps.argtypes = [P, C.c_int64]
+    _LIBS[name] = lib
+    return lib
+
+
+def material_desc(kind=_abi.MATERIAL_ELASTIC, rho=1.0, E=1.0, nu=0.0,
+                  plane_stress=False, finite_deformation=False):
+    return _abi.MaterialDesc(kind, int(plane_stress), int(finite_deformation), 0,
+                             float(rho), float(E), float(nu))
+
+
+class OracleModel:
+    """FP64 CPU restatement of SolidMechanicsModel on the explicit path."""
+
+    def __init__(self, mesh, materials, element_material=None, fast=False):
+        self.lib = _lib(fast)
+        self.mesh = mesh
+        self.dim, self.nnpe, self.nqp = element_properties(mesh.element_type)
+        self._nodes = np.ascontiguousarray(mesh.nodes, dtype=np.float64)
+        self._conn = np.ascontiguousarray(mesh.connectivity, dtype=np.uint32)
+        desc = _abi.MeshDesc(mesh.spatial_dimension, mesh.element_type,
+                             self._nodes.shape[0], self._conn.shape[0],
+                             self._nodes.ctypes.data_as(C.POINTER(C.c_double)),
+                             self._conn.ctypes.data_as(C.POINTER(C.c_uint32)))
+        if isinstance(materials, _abi.MaterialDesc):
+            materials = [materials]
+        mats = (_abi.MaterialDesc * len(materials))(*materials)
+        em = None
+        if element_material is not None:
+            self._em = np.ascontiguousarray(element_material, dtype=np.uint32)
+            em = self._em.ctypes.data_as(C.POINTER(C.c_uint32))
+        status = C.c_int32(0)
+        self.h = self.lib.oracle_create(C.byref(desc), len(materials), mats, em,
+                                        C.byref(status))
+        if not self.h:
+            raise RuntimeError("oracle_create failed: %s" % _abi.STATUS_NAMES[status.value])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_destroy(self.h)
+            self.h = None
+
+    def field(self, field):
+        """numpy view on the model-owned array (writable)."""
+        n = self.lib.oracle_field_size(self.h, field)
+        p = self.lib.oracle_field(self.h, field)
+        arr = np.ctypeslib.as_array(p, shape=(n,))
+        if field in (_abi.FIELD_GRAD_U, _abi.FIELD_STRESS):
+            return arr.reshape(-1, self.dim * self.dim)
+        return arr.reshape(-1, self.dim)
+
+    @property
+    def displacement(self):
+        return self.field(_abi.FIELD_DISPLACEMENT)
+
+    @property
+    def velocity(self):
+        return self.field(_abi.FIELD_VELOCITY)
+
+    @property
+    def acceleration(self):
+        return self.field(_abi.FIELD_ACCELERATION)
+
+    @property
+    def internal_force(self):
+        return self.field(_abi.FIELD_INTERNAL_FORCE)
+
+    @property
+    def external_force(self):
+        return self.field(_abi.FIELD_EXTERNAL_FORCE)
+
+    @property
+    def mass(self):
+        return self.field(_abi.FIELD_MASS)
+
+    @property
+    def blocked(self):
+        n = self._nodes.shape[0] * self.dim
+        return np.ctypeslib.as_array(self.lib.oracle_blocked(self.h),
+                                     shape=(n,)).reshape(-1, self.dim)
+
+    def assemble_mass_lumped(self):
+        self.lib.oracle_assemble_mass_lumped(self.h)
+
+    def stable_time_step(self):
+        return self.lib.oracle_stable_time_step(self.h)
+
+    def set_time_step(self, dt):
+        self.lib.oracle_set_time_step(self.h, dt)
+
+    def solve_step(self):
+        self.lib.oracle_solve_step(self.h)
+
+    def solve_steps(self, n):
+        self.lib.oracle_solve_steps(self.h, n)
+
+    def assemble_internal_forces(self):
+        self.lib.oracle_assemble_internal_forces(self.h)
+
+    def compute_stresses(self):
+        self.lib.oracle_compute_stresses(self.h)
+
+    def energy(self, kind):
+        return self.lib.oracle_energy(self.h, kind)
+
+    def time_steps(self, n):
+        return self.lib.oracle_time_steps(self.h, n)
