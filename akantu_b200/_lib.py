@@ -1,0 +1,82 @@
+"""Loads libakb.so (built in-tree by akantu_b200/csrc/Makefile) and declares
+the C signatures of include/akb.h. There is no fallback: if the library is
+missing or fails to load, every model call raises."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+from . import _abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libakb.so")
+_lib = None
+
+P = C.c_void_p
+I32 = C.c_int32
+I64 = C.c_int64
+DBL = C.c_double
+PD = C.POINTER(C.c_double)
+PU8 = C.POINTER(C.c_uint8)
+PU32 = C.POINTER(C.c_uint32)
+
+# name -> (restype, argtypes); the exported surface of include/akb.h
+SIGNATURES = {
+    "akb_abi_version": (I32, []),
+    "akb_last_error": (C.c_char_p, []),
+    "akb_model_create": (I32, [C.POINTER(_abi.MeshDesc), I32, C.POINTER(_abi.MaterialDesc),
+                               PU32, C.POINTER(_abi.ModelOptions), C.POINTER(P)]),
+    "akb_model_destroy": (I32, [P]),
+    "akb_model_get_info": (I32, [P, C.POINTER(_abi.ModelInfo)]),
+    "akb_set_field": (I32, [P, I32, PD, I64]),
+    "akb_get_field": (I32, [P, I32, PD, I64]),
+    "akb_field_device_pointer": (I32, [P, I32, C.POINTER(P)]),
+    "akb_set_blocked_dofs": (I32, [P, PU8, I64]),
+    "akb_get_blocked_dofs": (I32, [P, PU8, I64]),
+    "akb_assemble_mass_lumped": (I32, [P]),
+    "akb_get_stable_time_step": (I32, [P, PD]),
+    "akb_set_time_step": (I32, [P, DBL]),
+    "akb_get_time_step": (I32, [P, PD]),
+    "akb_solve_step": (I32, [P]),
+    "akb_solve_steps": (I32, [P, I64]),
+    "akb_time_solve_steps": (I32, [P, I64, PD]),
+    "akb_assemble_internal_forces": (I32, [P]),
+    "akb_compute_stresses": (I32, [P]),
+    "akb_get_energy": (I32, [P, I32, PD]),
+    "akb_synchronize": (I32, [P]),
+}
+
+
+class AkbError(RuntimeError):
+    def __init__(self, status, message):
+        self.status = status
+        super().__init__("%s (%s)" % (message, _abi.STATUS_NAMES.get(status, status)))
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "csrc")], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libakb.so is not built: run `make -C akantu_b200/csrc` "
+                          "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    if L.akb_abi_version() != _abi.ABI_VERSION:
+        raise ImportError("libakb.so ABI version mismatch")
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != _abi.AKB_OK:
+        msg = lib().akb_last_error().decode(errors="replace")
+        raise AkbError(status, msg)

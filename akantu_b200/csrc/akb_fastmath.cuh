@@ -1,0 +1,204 @@
+// akb_fastmath.cuh -- element arithmetic of the fast paths (FMA allowed).
+//
+// Same mathematics as the reference's FE engine (element_class_tmpl.hh:270-355,
+// shape_lagrange_inline_impl.hh:355-423, integrator_gauss_inline_impl.hh:426-455,
+// material_elastic_inline_impl.hh:41-63, material_neohookean_inline_impl.hh:46-65),
+// written for registers: geometry recomputed from the coordinates, differences
+// to the element's first node taken in FP64 before any FP32 rounding, the
+// internal force written as f_a = sum_q w_q det J_q P_q grad N_a with P = sigma
+// (small strain) or P = F S (finite strain), which equals B^T sigma_voigt and
+// (B_L0 + B_L2)^T S_voigt of material.cc:178-230 and 637-722.
+#pragma once
+
+#include "akb_internal.cuh"
+
+namespace akb {
+namespace fast {
+
+// dN_a/dxi_k at quadrature point q (k-th row), reference element tables.
+template <int T, typename S>
+__device__ inline S dN(int k, int a, int q) {
+  if (T == AKB_SEGMENT_2) return a == 0 ? S(-0.5) : S(0.5);
+  if (T == AKB_TRIANGLE_3) {
+    if (a == 0) return S(-1);
+    return (a == k + 1) ? S(1) : S(0);
+  }
+  if (T == AKB_TETRAHEDRON_4) {
+    if (a == 0) return S(-1);
+    return (a == k + 1) ? S(1) : S(0);
+  }
+  // hexahedron_8: corners (sx, sy, sz), Gauss point (+-g)^3, g = 1/sqrt(3)
+  const int sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+  const int sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+  const int sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+  const S g = S(0.57735026918962576451);
+  const S cx = (q & 1) ? g : -g, cy = (q & 2) ? g : -g, cz = (q & 4) ? g : -g;
+  const S ax = S(1) + sx[a] * cx, ay = S(1) + sy[a] * cy, az = S(1) + sz[a] * cz;
+  if (k == 0) return S(0.125) * sx[a] * ay * az;
+  if (k == 1) return S(0.125) * sy[a] * ax * az;
+  return S(0.125) * sz[a] * ax * ay;
+}
+
+template <int T> __host__ __device__ constexpr double weight() {
+  return T == AKB_SEGMENT_2 ? 2.0 : T == AKB_TRIANGLE_3 ? 0.5 : T == AKB_TETRAHEDRON_4 ? 1.0 / 6.0 : 1.0;
+}
+
+template <int d, typename S>
+__device__ inline S det(const S* J) {
+  if (d == 1) return J[0];
+  if (d == 2) return J[0] * J[3] - J[1] * J[2];
+  return J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) +
+         J[2] * (J[3] * J[7] - J[4] * J[6]);
+}
+
+// row-major d x d inverse times det (adjugate); returns det
+template <int d, typename S>
+__device__ inline S adjugate(const S* J, S* A) {
+  if (d == 1) {
+    A[0] = S(1);
+    return J[0];
+  }
+  if (d == 2) {
+    A[0] = J[3]; A[1] = -J[1]; A[2] = -J[2]; A[3] = J[0];
+    return J[0] * J[3] - J[1] * J[2];
+  }
+  A[0] = J[4] * J[8] - J[5] * J[7];
+  A[1] = J[2] * J[7] - J[1] * J[8];
+  A[2] = J[1] * J[5] - J[2] * J[4];
+  A[3] = J[5] * J[6] - J[3] * J[8];
+  A[4] = J[0] * J[8] - J[2] * J[6];
+  A[5] = J[2] * J[3] - J[0] * J[5];
+  A[6] = J[3] * J[7] - J[4] * J[6];
+  A[7] = J[1] * J[6] - J[0] * J[7];
+  A[8] = J[0] * J[4] - J[1] * J[3];
+  return J[0] * A[0] + J[1] * A[3] + J[2] * A[6];
+}
+
+// Stress at one point; g is row-major grad u (g[i*d+j] = du_i/dX_j); returns
+// P (first Piola for finite strain, Cauchy for small strain), row-major.
+template <int d, typename S>
+__device__ inline void stress_P(const MatParams& p, const S* g, S* P) {
+  const S lam = S(p.lambda), mu = S(p.mu);
+  if (d == 1 && !p.finite) {
+    P[0] = S(p.E) * g[0];
+    return;
+  }
+  if (!p.finite) {
+    S tr = 0;
+#pragma unroll
+    for (int i = 0; i < d; ++i) tr += g[i * d + i];
+#pragma unroll
+    for (int i = 0; i < d; ++i)
+#pragma unroll
+      for (int j = 0; j < d; ++j) P[i * d + j] = mu * (g[i * d + j] + g[j * d + i]) + (i == j ? lam * tr : S(0));
+    return;
+  }
+  S F[9], C[9], Sk[9];
+#pragma unroll
+  for (int i = 0; i < d; ++i)
+#pragma unroll
+    for (int j = 0; j < d; ++j) F[i * d + j] = g[i * d + j] + (i == j ? S(1) : S(0));
+#pragma unroll
+  for (int i = 0; i < d; ++i)
+#pragma unroll
+    for (int j = 0; j < d; ++j) {
+      S c = 0;
+#pragma unroll
+      for (int k = 0; k < d; ++k) c += F[k * d + i] * F[k * d + j];
+      C[i * d + j] = c;
+    }
+  if (p.kind == AKB_MATERIAL_NEOHOOKEAN) {
+    // S = mu I + (lambda ln J - mu) C^-1
+    S Ca[9];
+    S detC = adjugate<d, S>(C, Ca);
+    S J = det<d, S>(F);
+    S f = lam * log(J) - mu;
+    S fi = f / detC;
+#pragma unroll
+    for (int i = 0; i < d; ++i)
+#pragma unroll
+      for (int j = 0; j < d; ++j) Sk[i * d + j] = (i == j ? mu : S(0)) + fi * Ca[i * d + j];
+  } else {
+    // St-Venant-Kirchhoff: S = lambda tr(E) I + 2 mu E, E = (C - I)/2
+    S trE = 0;
+#pragma unroll
+    for (int i = 0; i < d; ++i) trE += S(0.5) * (C[i * d + i] - S(1));
+#pragma unroll
+    for (int i = 0; i < d; ++i)
+#pragma unroll
+      for (int j = 0; j < d; ++j)
+        Sk[i * d + j] = mu * (C[i * d + j] - (i == j ? S(1) : S(0))) + (i == j ? lam * trE : S(0));
+  }
+#pragma unroll
+  for (int i = 0; i < d; ++i)
+#pragma unroll
+    for (int j = 0; j < d; ++j) {
+      S c = 0;
+#pragma unroll
+      for (int k = 0; k < d; ++k) c += F[i * d + k] * Sk[k * d + j];
+      P[i * d + j] = c;
+    }
+}
+
+// Element internal force (without the -1 of the assembly):
+// fe[a*d + i] = sum_q w_q det J_q sum_j P_ij dN_a/dx_j.
+// dX[a*d+i] = X_a - X_0, du[a*d+i] = u_a - u_0 (entry a = 0 is zero).
+template <int T, typename S>
+__device__ inline void element_force(const MatParams& p, const S* dX, const S* du, S* fe) {
+  constexpr int d = ET<T>::dim, n = ET<T>::nnpe, nq = ET<T>::nqp;
+#pragma unroll
+  for (int k = 0; k < d * n; ++k) fe[k] = 0;
+#pragma unroll 1
+  for (int q = 0; q < nq; ++q) {
+    // J[k*d + j] = dx_j/dxi_k
+    S J[9];
+#pragma unroll
+    for (int k = 0; k < d; ++k)
+#pragma unroll
+      for (int j = 0; j < d; ++j) {
+        S c = 0;
+#pragma unroll
+        for (int a = 1; a < n; ++a) c += dN<T, S>(k, a, q) * dX[a * d + j];
+        J[k * d + j] = c;
+      }
+    S A[9];
+    const S detJ = adjugate<d, S>(J, A);
+    const S idet = S(1) / detJ;
+    // grad N_a (physical): B[a*d + j] = sum_k Jinv[j][k] dN(k, a)
+    S B[3 * 8];
+#pragma unroll
+    for (int a = 0; a < n; ++a)
+#pragma unroll
+      for (int j = 0; j < d; ++j) {
+        S c = 0;
+#pragma unroll
+        for (int k = 0; k < d; ++k) c += A[j * d + k] * dN<T, S>(k, a, q);
+        B[a * d + j] = c * idet;
+      }
+    S g[9];
+#pragma unroll
+    for (int i = 0; i < d; ++i)
+#pragma unroll
+      for (int j = 0; j < d; ++j) {
+        S c = 0;
+#pragma unroll
+        for (int a = 1; a < n; ++a) c += du[a * d + i] * B[a * d + j];
+        g[i * d + j] = c;
+      }
+    S P[9];
+    stress_P<d, S>(p, g, P);
+    const S wq = S(weight<T>()) * detJ;
+#pragma unroll
+    for (int a = 0; a < n; ++a)
+#pragma unroll
+      for (int i = 0; i < d; ++i) {
+        S c = 0;
+#pragma unroll
+        for (int j = 0; j < d; ++j) c += P[i * d + j] * B[a * d + j];
+        fe[a * d + i] += wq * c;
+      }
+  }
+}
+
+}  // namespace fast
+}  // namespace akb

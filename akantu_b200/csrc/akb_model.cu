@@ -1,0 +1,582 @@
+// akb_model.cu -- the C ABI of include/akb.h: model lifecycle, fields, the
+// explicit step driver and its CUDA-graph replay.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "akb_internal.cuh"
+
+namespace akb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+akb_status fail(akb_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+}  // namespace akb
+
+using namespace akb;
+
+struct akb_model {
+  DevModel dm{};
+  int mode = AKB_MODE_FP64_REFERENCE;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool owns_stream = false;
+  std::vector<void*> allocations;
+  int64_t device_bytes = 0;
+  double dt = 0.0;
+  bool has_fext = false;
+  bool fint_valid = false;
+  bool stresses_valid = false;
+  double* d_scratch = nullptr;  // reduction partials
+  int scratch_len = 0;
+  double* d_result = nullptr;
+  double* h_result = nullptr;   // pinned
+  // cached graphs of k consecutive steps, keyed by k
+  std::map<int64_t, cudaGraphExec_t> graphs;
+  double graph_dt = -1.0;
+  bool graph_fext = false;
+};
+
+namespace {
+
+template <typename T>
+akb_status dalloc(akb_model* m, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? AKB_ERR_OUT_OF_MEMORY : AKB_ERR_CUDA,
+                std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  m->allocations.push_back(*p);
+  m->device_bytes += count * sizeof(T);
+  return AKB_OK;
+}
+
+void dfree(akb_model* m, void* p) {
+  if (!p) return;
+  for (size_t i = 0; i < m->allocations.size(); ++i)
+    if (m->allocations[i] == p) {
+      m->allocations.erase(m->allocations.begin() + i);
+      break;
+    }
+  cudaFree(p);
+}
+
+MatParams make_params(const akb_material_desc& d, int dim) {
+  MatParams p{};
+  p.kind = d.kind;
+  p.finite = (d.kind == AKB_MATERIAL_NEOHOOKEAN) || d.finite_deformation != 0;
+  p.rho = d.rho;
+  p.E = d.E;
+  p.nu = dim == 1 ? 0. : d.nu;
+  p.lambda = p.nu * p.E / ((1 + p.nu) * (1 - 2 * p.nu));
+  p.mu = p.E / (2 * (1 + p.nu));
+  if (dim == 2 && d.plane_stress && d.kind == AKB_MATERIAL_ELASTIC)
+    p.lambda = p.nu * p.E / ((1 + p.nu) * (1 - p.nu));
+  p.celerity = std::sqrt((p.lambda + 2 * p.mu) / p.rho);
+  return p;
+}
+
+void destroy_graphs(akb_model* m) {
+  for (auto& kv : m->graphs) cudaGraphExecDestroy(kv.second);
+  m->graphs.clear();
+}
+
+bool fp32(const akb_model* m) { return m->mode == AKB_MODE_FP32_BULK; }
+
+// One NonLinearSolverLumped::solve.
+cudaError_t enqueue_step(akb_model* m) {
+  const DevModel& d = m->dm;
+  cudaError_t e;
+  if (m->mode == AKB_MODE_FP64_REFERENCE) {
+    if ((e = ref_predictor(d, m->dt, m->stream)) != cudaSuccess) return e;
+    if ((e = ref_element_forces(d, m->stream)) != cudaSuccess) return e;
+    return ref_gather_correct(d, m->dt, true, m->stream);
+  }
+  if ((e = fast_predictor(d, m->dt, m->stream)) != cudaSuccess) return e;
+  if ((e = fast_element_forces(d, fp32(m), m->stream)) != cudaSuccess) return e;
+  return fast_gather_correct(d, m->dt, fp32(m), true, m->has_fext, m->stream);
+}
+
+// Internal forces at the current displacement, without touching the state.
+cudaError_t enqueue_internal_forces(akb_model* m) {
+  const DevModel& d = m->dm;
+  cudaError_t e;
+  if (m->mode == AKB_MODE_FP64_REFERENCE) {
+    if ((e = ref_element_forces(d, m->stream)) != cudaSuccess) return e;
+    return ref_gather_correct(d, m->dt, false, m->stream);
+  }
+  if ((e = fast_element_forces(d, fp32(m), m->stream)) != cudaSuccess) return e;
+  return fast_gather_correct(d, m->dt, fp32(m), false, m->has_fext, m->stream);
+}
+
+akb_status check_model(const akb_model* m) {
+  if (!m) return fail(AKB_ERR_INVALID_ARGUMENT, "null model");
+  return AKB_OK;
+}
+
+akb_status sync(akb_model* m) {
+  cudaError_t e = cudaStreamSynchronize(m->stream);
+  if (e != cudaSuccess) return fail(AKB_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+  return AKB_OK;
+}
+
+akb_status ensure_stress_arrays(akb_model* m) {
+  if (m->dm.gradu) return AKB_OK;
+  const size_t n = (size_t)m->dm.ne * m->dm.nqp * m->dm.dim * m->dm.dim;
+  akb_status s;
+  if ((s = dalloc(m, &m->dm.gradu, n)) != AKB_OK) return s;
+  if ((s = dalloc(m, &m->dm.stress, n)) != AKB_OK) return s;
+  return AKB_OK;
+}
+
+double* field_ptr(akb_model* m, int32_t field) {
+  switch (field) {
+  case AKB_FIELD_DISPLACEMENT: return m->dm.u;
+  case AKB_FIELD_VELOCITY: return m->dm.v;
+  case AKB_FIELD_ACCELERATION: return m->dm.a;
+  case AKB_FIELD_EXTERNAL_FORCE: return m->dm.fext;
+  case AKB_FIELD_INTERNAL_FORCE: return m->dm.fint;
+  case AKB_FIELD_MASS: return m->dm.mass;
+  case AKB_FIELD_NODES: return const_cast<double*>(m->dm.X);
+  case AKB_FIELD_GRAD_U: return m->dm.gradu;
+  case AKB_FIELD_STRESS: return m->dm.stress;
+  }
+  return nullptr;
+}
+
+int64_t field_count(const akb_model* m, int32_t field) {
+  if (field == AKB_FIELD_GRAD_U || field == AKB_FIELD_STRESS)
+    return m->dm.ne * m->dm.nqp * m->dm.dim * m->dm.dim;
+  return m->dm.nn * m->dm.dim;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t akb_abi_version(void) { return AKB_ABI_VERSION; }
+
+const char* akb_last_error(void) { return g_last_error.c_str(); }
+
+akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
+                            const akb_material_desc* materials,
+                            const uint32_t* element_material,
+                            const akb_model_options* options, akb_model** out) {
+  if (!out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  if (!mesh || !materials || nb_materials < 1 || nb_materials > kMaxMaterials)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "mesh and 1..8 materials are required");
+  const int type = mesh->element_type;
+  if (type < AKB_SEGMENT_2 || type > AKB_HEXAHEDRON_8)
+    return fail(AKB_ERR_UNSUPPORTED, "unsupported element type");
+  if (mesh->spatial_dimension != dim_of(type))
+    return fail(AKB_ERR_BAD_MESH, "spatial dimension does not match the element type");
+  if (mesh->nb_nodes <= 0 || mesh->nb_elements < 0 || !mesh->nodes ||
+      (mesh->nb_elements > 0 && !mesh->connectivity))
+    return fail(AKB_ERR_BAD_MESH, "empty mesh");
+  const int d = mesh->spatial_dimension, n = nnpe_of(type), q = nqp_of(type);
+  const int64_t nn = mesh->nb_nodes, ne = mesh->nb_elements;
+  if (ne * n >= INT32_MAX) return fail(AKB_ERR_UNSUPPORTED, "more than 2^31 element corners");
+  for (int64_t k = 0; k < ne * n; ++k)
+    if (mesh->connectivity[k] >= (uint64_t)nn)
+      return fail(AKB_ERR_BAD_MESH, "connectivity refers to a node out of range");
+  if (element_material)
+    for (int64_t e = 0; e < ne; ++e)
+      if (element_material[e] >= (uint32_t)nb_materials)
+        return fail(AKB_ERR_INVALID_ARGUMENT, "material index out of range");
+  for (int k = 0; k < nb_materials; ++k) {
+    const auto& md = materials[k];
+    if (md.kind != AKB_MATERIAL_ELASTIC && md.kind != AKB_MATERIAL_NEOHOOKEAN)
+      return fail(AKB_ERR_UNSUPPORTED, "unsupported material kind");
+    if (!(md.rho > 0) || !(md.E > 0))
+      return fail(AKB_ERR_INVALID_ARGUMENT, "material needs rho > 0 and E > 0");
+  }
+  akb_model_options opt{AKB_MODE_FP64_REFERENCE, 0, nullptr};
+  if (options) opt = *options;
+  if (opt.precision_mode < AKB_MODE_FP64_REFERENCE || opt.precision_mode > AKB_MODE_FP32_BULK)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "unknown precision mode");
+
+  auto m = std::make_unique<akb_model>();
+  m->mode = opt.precision_mode;
+  m->device = opt.device;
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if (opt.stream) {
+    m->stream = (cudaStream_t)opt.stream;
+  } else {
+    AKB_CUDA_TRY(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+    m->owns_stream = true;
+  }
+  DevModel& dm = m->dm;
+  dm.dim = d;
+  dm.type = type;
+  dm.nnpe = n;
+  dm.nqp = q;
+  dm.nn = nn;
+  dm.ne = ne;
+  dm.nmat = nb_materials;
+  for (int k = 0; k < nb_materials; ++k) dm.mats[k] = make_params(materials[k], d);
+
+  akb_status st;
+  const size_t ndof = (size_t)nn * d;
+  double* X;
+  uint32_t* conn;
+  if ((st = dalloc(m.get(), &X, ndof)) != AKB_OK) return st;
+  if ((st = dalloc(m.get(), &conn, (size_t)ne * n)) != AKB_OK) return st;
+  dm.X = X;
+  dm.conn = conn;
+  for (double** f : {&dm.u, &dm.v, &dm.a, &dm.fext, &dm.fint, &dm.mass})
+    if ((st = dalloc(m.get(), f, ndof)) != AKB_OK) return st;
+  if ((st = dalloc(m.get(), &dm.inv_mass, nn)) != AKB_OK) return st;
+  if ((st = dalloc(m.get(), &dm.blocked, ndof)) != AKB_OK) return st;
+  AKB_CUDA_TRY(cudaMemcpyAsync(X, mesh->nodes, ndof * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+  if (ne > 0)
+    AKB_CUDA_TRY(cudaMemcpyAsync(conn, mesh->connectivity, (size_t)ne * n * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, m->stream));
+  for (double* f : {dm.u, dm.v, dm.a, dm.fext, dm.fint, dm.mass})
+    AKB_CUDA_TRY(cudaMemsetAsync(f, 0, ndof * sizeof(double), m->stream));
+  AKB_CUDA_TRY(cudaMemsetAsync(dm.blocked, 0, ndof, m->stream));
+  if (element_material) {
+    uint32_t* mo;
+    if ((st = dalloc(m.get(), &mo, ne)) != AKB_OK) return st;
+    AKB_CUDA_TRY(cudaMemcpyAsync(mo, element_material, ne * sizeof(uint32_t), cudaMemcpyHostToDevice, m->stream));
+    dm.mat_of = mo;
+  }
+
+  // node -> (element, corner) CSR in ascending element order: the order in
+  // which DOFManager::assembleElementalArrayLocalArray adds element vectors.
+  {
+    std::vector<int32_t> ptr(nn + 1, 0), ent((size_t)ne * n);
+    for (int64_t k = 0; k < ne * n; ++k) ptr[mesh->connectivity[k] + 1]++;
+    for (int64_t i = 0; i < nn; ++i) ptr[i + 1] += ptr[i];
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int64_t k = 0; k < ne * n; ++k) ent[fill[mesh->connectivity[k]]++] = (int32_t)k;
+    int32_t *dptr, *dent;
+    if ((st = dalloc(m.get(), &dptr, nn + 1)) != AKB_OK) return st;
+    if ((st = dalloc(m.get(), &dent, (size_t)ne * n)) != AKB_OK) return st;
+    AKB_CUDA_TRY(cudaMemcpyAsync(dptr, ptr.data(), (nn + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, m->stream));
+    if (ne > 0)
+      AKB_CUDA_TRY(cudaMemcpyAsync(dent, ent.data(), (size_t)ne * n * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, m->stream));
+    AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));  // host vectors go out of scope
+    dm.node_ptr = dptr;
+    dm.node_ent = dent;
+  }
+  // element force buffer
+  {
+    // FP64 entries in every mode: the lumped-mass assembly writes FP64
+    const size_t bytes = (size_t)ne * n * d * 8;
+    char* fe;
+    if ((st = dalloc(m.get(), &fe, bytes)) != AKB_OK) return st;
+    dm.fe = fe;
+  }
+  // shape derivatives and detJ*w (initShapeFunctions); stored for the
+  // reference-order path, temporary otherwise (used for the lumped mass).
+  if ((st = dalloc(m.get(), &dm.B, (size_t)ne * q * d * n)) != AKB_OK) return st;
+  if ((st = dalloc(m.get(), &dm.jac, (size_t)ne * q)) != AKB_OK) return st;
+  if ((st = dalloc(m.get(), &m->d_result, 4)) != AKB_OK) return st;
+  int* d_neg = reinterpret_cast<int*>(m->d_result);
+  AKB_CUDA_TRY(cudaMemsetAsync(d_neg, 0, sizeof(int), m->stream));
+  AKB_CUDA_TRY(ref_init_geometry(dm, m->stream, d_neg));
+  int neg = 0;
+  AKB_CUDA_TRY(cudaMemcpyAsync(&neg, d_neg, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  if (neg) return fail(AKB_ERR_NEGATIVE_JACOBIAN,
+                       "negative jacobian: check the element node ordering");
+  // lumped mass depends only on the reference coordinates and rho
+  AKB_CUDA_TRY(ref_mass(dm, m->stream));
+  if (m->mode == AKB_MODE_FP64_REFERENCE) {
+    if ((st = ensure_stress_arrays(m.get())) != AKB_OK) return st;
+  } else {
+    AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    dfree(m.get(), dm.B);
+    dfree(m.get(), dm.jac);
+    m->device_bytes -= (int64_t)ne * q * d * n * 8 + (int64_t)ne * q * 8;
+    dm.B = nullptr;
+    dm.jac = nullptr;
+  }
+  m->scratch_len = reduce_blocks(ne);
+  if ((st = dalloc(m.get(), &m->d_scratch, m->scratch_len)) != AKB_OK) return st;
+  AKB_CUDA_TRY(cudaMallocHost((void**)&m->h_result, 4 * sizeof(double)));
+  AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  *out = m.release();
+  return AKB_OK;
+}
+
+akb_status akb_model_destroy(akb_model* m) {
+  if (!m) return AKB_OK;
+  cudaSetDevice(m->device);
+  cudaStreamSynchronize(m->stream);
+  destroy_graphs(m);
+  for (void* p : m->allocations) cudaFree(p);
+  if (m->h_result) cudaFreeHost(m->h_result);
+  if (m->owns_stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return AKB_OK;
+}
+
+akb_status akb_model_get_info(const akb_model* m, akb_model_info* info) {
+  if (!m || !info) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  info->spatial_dimension = m->dm.dim;
+  info->element_type = m->dm.type;
+  info->nodes_per_element = m->dm.nnpe;
+  info->quadrature_points_per_element = m->dm.nqp;
+  info->nb_nodes = m->dm.nn;
+  info->nb_elements = m->dm.ne;
+  info->precision_mode = m->mode;
+  info->nb_materials = m->dm.nmat;
+  info->device_bytes = m->device_bytes;
+  return AKB_OK;
+}
+
+akb_status akb_set_field(akb_model* m, int32_t field, const double* values, int64_t count) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (field != AKB_FIELD_DISPLACEMENT && field != AKB_FIELD_VELOCITY &&
+      field != AKB_FIELD_ACCELERATION && field != AKB_FIELD_EXTERNAL_FORCE)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "field is read-only");
+  if (!values || count != field_count(m, field))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "wrong number of values");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(cudaMemcpyAsync(field_ptr(m, field), values, count * sizeof(double),
+                               cudaMemcpyHostToDevice, m->stream));
+  if (field == AKB_FIELD_DISPLACEMENT) {
+    m->fint_valid = false;
+    m->stresses_valid = false;
+  }
+  if (field == AKB_FIELD_EXTERNAL_FORCE) {
+    bool any = false;
+    for (int64_t i = 0; i < count && !any; ++i) any = values[i] != 0.0;
+    m->has_fext = any;
+  }
+  return sync(m);
+}
+
+akb_status akb_get_field(akb_model* m, int32_t field, double* values, int64_t count) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (field < AKB_FIELD_DISPLACEMENT || field > AKB_FIELD_STRESS)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "unknown field");
+  if (!values || count != field_count(m, field))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "wrong number of values");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if (field == AKB_FIELD_INTERNAL_FORCE && !m->fint_valid) {
+    AKB_CUDA_TRY(enqueue_internal_forces(m));
+    m->fint_valid = true;
+  }
+  if ((field == AKB_FIELD_GRAD_U || field == AKB_FIELD_STRESS) && !m->stresses_valid) {
+    if ((st = akb_compute_stresses(m)) != AKB_OK) return st;
+  }
+  AKB_CUDA_TRY(cudaMemcpyAsync(values, field_ptr(m, field), count * sizeof(double),
+                               cudaMemcpyDeviceToHost, m->stream));
+  return sync(m);
+}
+
+akb_status akb_field_device_pointer(akb_model* m, int32_t field, void** dptr) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!dptr) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  if (field == AKB_FIELD_GRAD_U || field == AKB_FIELD_STRESS) {
+    if ((st = ensure_stress_arrays(m)) != AKB_OK) return st;
+  }
+  *dptr = field_ptr(m, field);
+  if (!*dptr) return fail(AKB_ERR_INVALID_ARGUMENT, "unknown field");
+  return AKB_OK;
+}
+
+akb_status akb_set_blocked_dofs(akb_model* m, const uint8_t* blocked, int64_t count) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!blocked || count != m->dm.nn * m->dm.dim)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "wrong number of values");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(cudaMemcpyAsync(m->dm.blocked, blocked, count, cudaMemcpyHostToDevice, m->stream));
+  return sync(m);
+}
+
+akb_status akb_get_blocked_dofs(akb_model* m, uint8_t* blocked, int64_t count) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!blocked || count != m->dm.nn * m->dm.dim)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "wrong number of values");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(cudaMemcpyAsync(blocked, m->dm.blocked, count, cudaMemcpyDeviceToHost, m->stream));
+  return sync(m);
+}
+
+akb_status akb_assemble_mass_lumped(akb_model* m) {
+  // The lumped mass depends only on the reference coordinates and the
+  // densities; it is assembled once in akb_model_create, as the reference
+  // assembles it once (need_to_reassemble_lumped_mass,
+  // solid_mechanics_model_mass.cc:61-62).
+  return check_model(m);
+}
+
+akb_status akb_get_stable_time_step(akb_model* m, double* dt) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!dt) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(stable_dt(m->dm, m->d_scratch, m->scratch_len, m->d_result, m->stream));
+  AKB_CUDA_TRY(cudaMemcpyAsync(m->h_result, m->d_result, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if ((st = sync(m)) != AKB_OK) return st;
+  *dt = *m->h_result;
+  return AKB_OK;
+}
+
+akb_status akb_set_time_step(akb_model* m, double dt) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(AKB_ERR_INVALID_ARGUMENT, "time step must be > 0");
+  m->dt = dt;
+  return AKB_OK;
+}
+
+akb_status akb_get_time_step(const akb_model* m, double* dt) {
+  if (!m || !dt) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  *dt = m->dt;
+  return AKB_OK;
+}
+
+akb_status akb_solve_step(akb_model* m) { return akb_solve_steps(m, 1); }
+
+static akb_status get_graph(akb_model* m, int64_t k, cudaGraphExec_t* exec) {
+  auto it = m->graphs.find(k);
+  if (it != m->graphs.end()) {
+    *exec = it->second;
+    return AKB_OK;
+  }
+  cudaGraph_t g;
+  AKB_CUDA_TRY(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaSuccess;
+  for (int64_t s = 0; s < k && err == cudaSuccess; ++s) err = enqueue_step(m);
+  cudaError_t end = cudaStreamEndCapture(m->stream, &g);
+  if (err != cudaSuccess) return fail(AKB_ERR_CUDA, cudaGetErrorString(err));
+  if (end != cudaSuccess) return fail(AKB_ERR_CUDA, cudaGetErrorString(end));
+  cudaError_t inst = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (inst != cudaSuccess) return fail(AKB_ERR_CUDA, cudaGetErrorString(inst));
+  m->graphs[k] = *exec;
+  return AKB_OK;
+}
+
+// Graphs of kGraphSteps steps (and of the remainder) for nb_steps steps.
+static constexpr int64_t kGraphSteps = 32;
+static akb_status prepare_graphs(akb_model* m, int64_t nb_steps, cudaGraphExec_t* full,
+                                 cudaGraphExec_t* rest) {
+  if (m->graph_dt != m->dt || m->graph_fext != m->has_fext) {
+    destroy_graphs(m);
+    m->graph_dt = m->dt;
+    m->graph_fext = m->has_fext;
+  }
+  akb_status st;
+  const int64_t chunk = nb_steps >= kGraphSteps ? kGraphSteps : nb_steps;
+  *full = *rest = nullptr;
+  if ((st = get_graph(m, chunk, full)) != AKB_OK) return st;
+  const int64_t rem = nb_steps % chunk;
+  if (rem && (st = get_graph(m, rem, rest)) != AKB_OK) return st;
+  return AKB_OK;
+}
+
+akb_status akb_solve_steps(akb_model* m, int64_t nb_steps) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (nb_steps < 0) return fail(AKB_ERR_INVALID_ARGUMENT, "negative step count");
+  if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
+  if (nb_steps == 0) return AKB_OK;
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if (nb_steps == 1) {
+    AKB_CUDA_TRY(enqueue_step(m));
+  } else {
+    cudaGraphExec_t full, rest;
+    if ((st = prepare_graphs(m, nb_steps, &full, &rest)) != AKB_OK) return st;
+    const int64_t chunk = nb_steps >= kGraphSteps ? kGraphSteps : nb_steps;
+    const int64_t reps = nb_steps / chunk;
+    for (int64_t r = 0; r < reps; ++r) AKB_CUDA_TRY(cudaGraphLaunch(full, m->stream));
+    if (rest) AKB_CUDA_TRY(cudaGraphLaunch(rest, m->stream));
+  }
+  m->fint_valid = true;
+  m->stresses_valid = false;
+  return AKB_OK;
+}
+
+akb_status akb_time_solve_steps(akb_model* m, int64_t nb_steps, double* elapsed_ms) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!elapsed_ms) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if (nb_steps > 1) {  // instantiate the graphs outside the timed region
+    cudaGraphExec_t full, rest;
+    if ((st = prepare_graphs(m, nb_steps, &full, &rest)) != AKB_OK) return st;
+  }
+  cudaEvent_t e0, e1;
+  AKB_CUDA_TRY(cudaEventCreate(&e0));
+  AKB_CUDA_TRY(cudaEventCreate(&e1));
+  AKB_CUDA_TRY(cudaEventRecord(e0, m->stream));
+  st = akb_solve_steps(m, nb_steps);
+  AKB_CUDA_TRY(cudaEventRecord(e1, m->stream));
+  AKB_CUDA_TRY(cudaEventSynchronize(e1));
+  float ms = 0;
+  AKB_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *elapsed_ms = ms;
+  return st;
+}
+
+akb_status akb_assemble_internal_forces(akb_model* m) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(enqueue_internal_forces(m));
+  m->fint_valid = true;
+  return sync(m);
+}
+
+akb_status akb_compute_stresses(akb_model* m) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if ((st = ensure_stress_arrays(m)) != AKB_OK) return st;
+  AKB_CUDA_TRY(ref_compute_stresses(m->dm, m->dm.B == nullptr, m->stream));
+  m->stresses_valid = true;
+  return sync(m);
+}
+
+akb_status akb_get_energy(akb_model* m, int32_t kind, double* value) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!value) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  if (kind < AKB_ENERGY_KINETIC || kind > AKB_ENERGY_EXTERNAL_WORK)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "unknown energy");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if (kind == AKB_ENERGY_EXTERNAL_WORK && !m->fint_valid) {
+    AKB_CUDA_TRY(enqueue_internal_forces(m));
+    m->fint_valid = true;
+  }
+  AKB_CUDA_TRY(energy(m->dm, kind, m->dt, m->d_scratch, m->scratch_len, m->d_result, m->stream));
+  AKB_CUDA_TRY(cudaMemcpyAsync(m->h_result, m->d_result, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  if ((st = sync(m)) != AKB_OK) return st;
+  *value = *m->h_result;
+  return AKB_OK;
+}
+
+akb_status akb_synchronize(akb_model* m) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  return sync(m);
+}
+
+}  // extern "C"

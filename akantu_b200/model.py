@@ -1,0 +1,278 @@
+"""SolidMechanicsModel over the C ABI of libakb.so.
+
+Mirrors the reference's Python binding (python/py_solid_mechanics_model.cc:34-106)
+for the explicit path: initFull(_analysis_method=_explicit_lumped_mass),
+getStableTimeStep, setTimeStep, solveStep, getEnergy and the nodal-field
+getters. The nodal arrays live on the GPU; get*() returns a host mirror that
+is refreshed in place on every get*() call, and a mirror handed out by get*()
+is written back to the GPU before the next call that uses the state, so
+in-place edits of the returned arrays reach the model as in the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._lib import check, lib
+from .mesh import element_properties
+
+_explicit_lumped_mass = 0
+
+_FIELD_BY_NAME = {
+    "displacement": _abi.FIELD_DISPLACEMENT,
+    "velocity": _abi.FIELD_VELOCITY,
+    "acceleration": _abi.FIELD_ACCELERATION,
+    "external_force": _abi.FIELD_EXTERNAL_FORCE,
+    "internal_force": _abi.FIELD_INTERNAL_FORCE,
+    "mass": _abi.FIELD_MASS,
+}
+_WRITABLE = (_abi.FIELD_DISPLACEMENT, _abi.FIELD_VELOCITY, _abi.FIELD_ACCELERATION,
+             _abi.FIELD_EXTERNAL_FORCE)
+_ENERGY = {"kinetic": _abi.ENERGY_KINETIC, "potential": _abi.ENERGY_POTENTIAL,
+           "external work": _abi.ENERGY_EXTERNAL_WORK}
+
+
+class Material:
+    """Parameters of one `material <law> [ ... ]` section (Material::registerParam
+    names: rho, E, nu, Plane_Stress, finite_deformation)."""
+
+    kind = _abi.MATERIAL_ELASTIC
+
+    def __init__(self, rho, E, nu=0.0, Plane_Stress=False, finite_deformation=False,
+                 name=""):
+        self.name = name
+        self.params = dict(rho=float(rho), E=float(E), nu=float(nu),
+                           Plane_Stress=bool(Plane_Stress),
+                           finite_deformation=bool(finite_deformation))
+
+    def getReal(self, key):
+        return self.params[key]
+
+    def desc(self):
+        p = self.params
+        return _abi.MaterialDesc(self.kind, int(p["Plane_Stress"]),
+                                 int(p["finite_deformation"]), 0, p["rho"], p["E"], p["nu"])
+
+
+class MaterialElastic(Material):
+    kind = _abi.MATERIAL_ELASTIC
+
+
+class MaterialNeohookean(Material):
+    kind = _abi.MATERIAL_NEOHOOKEAN
+
+    def __init__(self, rho, E=None, nu=None, lambda_=None, mu=None, **kw):
+        if E is None:  # from Lame coefficients
+            nu = lambda_ / (2 * (lambda_ + mu))
+            E = mu * (3 * lambda_ + 2 * mu) / (lambda_ + mu)
+        super().__init__(rho, E, nu, finite_deformation=True, **kw)
+
+
+def material_from_dict(d):
+    kind = d.get("kind", _abi.MATERIAL_ELASTIC)
+    cls = MaterialNeohookean if kind == _abi.MATERIAL_NEOHOOKEAN else MaterialElastic
+    return cls(rho=d["rho"], E=d["E"], nu=d.get("nu", 0.0),
+               **({} if cls is MaterialNeohookean else
+                  dict(Plane_Stress=d.get("plane_stress", False),
+                       finite_deformation=d.get("finite_deformation", False))))
+
+
+class SolidMechanicsModel:
+    """The explicit lumped-mass SolidMechanicsModel on one GPU."""
+
+    def __init__(self, mesh, materials=None, element_material=None,
+                 precision=_abi.MODE_FP64_REFERENCE, device=0, stream=None):
+        self.mesh = mesh
+        self.dim, self.nnpe, self.nqp = element_properties(mesh.element_type)
+        self._materials = list(materials) if materials else []
+        self._element_material = element_material
+        self._precision = precision
+        self._device = device
+        self._stream = stream
+        self._h = None
+        self._mirrors = {}
+        self._checked_out = set()
+        self._blocked = None
+
+    # -- initialisation --------------------------------------------------
+    def addMaterial(self, material):
+        self._materials.append(material)
+
+    def initFull(self, _analysis_method=_explicit_lumped_mass, precision=None):
+        if _analysis_method != _explicit_lumped_mass:
+            raise NotImplementedError("only _explicit_lumped_mass is on this path")
+        if precision is not None:
+            self._precision = precision
+        if not self._materials:
+            raise ValueError("no material: add one with addMaterial()")
+        L = lib()
+        self._nodes = np.ascontiguousarray(self.mesh.nodes, dtype=np.float64)
+        self._conn = np.ascontiguousarray(self.mesh.connectivity, dtype=np.uint32)
+        desc = _abi.MeshDesc(self.dim, self.mesh.element_type, self._nodes.shape[0],
+                             self._conn.shape[0],
+                             self._nodes.ctypes.data_as(C.POINTER(C.c_double)),
+                             self._conn.ctypes.data_as(C.POINTER(C.c_uint32)))
+        mats = (_abi.MaterialDesc * len(self._materials))(*[m.desc() for m in self._materials])
+        em = None
+        if self._element_material is not None:
+            self._em = np.ascontiguousarray(self._element_material, dtype=np.uint32)
+            em = self._em.ctypes.data_as(C.POINTER(C.c_uint32))
+        opt = _abi.ModelOptions(self._precision, self._device, self._stream)
+        h = C.c_void_p()
+        check(L.akb_model_create(C.byref(desc), len(self._materials), mats, em,
+                                 C.byref(opt), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().akb_model_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise RuntimeError("call initFull() first")
+        return self._h
+
+    def getInfo(self):
+        info = _abi.ModelInfo()
+        check(lib().akb_model_get_info(self.handle, C.byref(info)))
+        return info
+
+    # -- host mirrors ------------------------------------------------------
+    def _sync_in(self):
+        for f in list(self._checked_out):
+            arr = self._mirrors[f]
+            check(lib().akb_set_field(self.handle, f, arr.ctypes.data_as(C.POINTER(C.c_double)),
+                                      arr.size))
+        self._checked_out.clear()
+        if self._blocked is not None:
+            b = self._blocked
+            check(lib().akb_set_blocked_dofs(self.handle, b.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                             b.size))
+            self._blocked = None
+
+    def getField(self, field):
+        self._sync_in()
+        n = self.mesh.getNbNodes() * self.dim
+        if field in (_abi.FIELD_GRAD_U, _abi.FIELD_STRESS):
+            n = self.mesh.getNbElement() * self.nqp * self.dim * self.dim
+        arr = self._mirrors.get(field)
+        if arr is None or arr.size != n:
+            cols = self.dim * self.dim if field in (_abi.FIELD_GRAD_U, _abi.FIELD_STRESS) else self.dim
+            arr = np.zeros((n // cols, cols))
+            self._mirrors[field] = arr
+        check(lib().akb_get_field(self.handle, field, arr.ctypes.data_as(C.POINTER(C.c_double)), n))
+        if field in _WRITABLE:
+            self._checked_out.add(field)
+        return arr
+
+    def setField(self, field, values):
+        self._sync_in()
+        arr = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        check(lib().akb_set_field(self.handle, field, arr.ctypes.data_as(C.POINTER(C.c_double)),
+                                  arr.size))
+        if field in self._mirrors:
+            self._mirrors[field][...] = arr.reshape(self._mirrors[field].shape)
+
+    def getDisplacement(self):
+        return self.getField(_abi.FIELD_DISPLACEMENT)
+
+    def getVelocity(self):
+        return self.getField(_abi.FIELD_VELOCITY)
+
+    def getAcceleration(self):
+        return self.getField(_abi.FIELD_ACCELERATION)
+
+    def getExternalForce(self):
+        return self.getField(_abi.FIELD_EXTERNAL_FORCE)
+
+    def getInternalForce(self):
+        return self.getField(_abi.FIELD_INTERNAL_FORCE)
+
+    def getMass(self):
+        return self.getField(_abi.FIELD_MASS)
+
+    def getBlockedDOFs(self):
+        """Host array of blocked flags (bool, N x d); edits are applied before
+        the next solveStep()."""
+        self._sync_in()
+        b = np.zeros((self.mesh.getNbNodes(), self.dim), dtype=np.uint8)
+        check(lib().akb_get_blocked_dofs(self.handle, b.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                         b.size))
+        view = b.view(np.bool_)
+        self._blocked = b
+        return view
+
+    def setBlockedDOFs(self, blocked):
+        self._sync_in()
+        b = np.ascontiguousarray(blocked, dtype=np.uint8).reshape(-1)
+        check(lib().akb_set_blocked_dofs(self.handle, b.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                         b.size))
+
+    def getGradU(self):
+        return self.getField(_abi.FIELD_GRAD_U)
+
+    def getStress(self):
+        return self.getField(_abi.FIELD_STRESS)
+
+    # -- solver --------------------------------------------------------------
+    def assembleMassLumped(self):
+        check(lib().akb_assemble_mass_lumped(self.handle))
+
+    def getStableTimeStep(self):
+        self._sync_in()
+        dt = C.c_double()
+        check(lib().akb_get_stable_time_step(self.handle, C.byref(dt)))
+        return dt.value
+
+    def setTimeStep(self, time_step, solver_id=""):
+        check(lib().akb_set_time_step(self.handle, float(time_step)))
+
+    def getTimeStep(self):
+        dt = C.c_double()
+        check(lib().akb_get_time_step(self.handle, C.byref(dt)))
+        return dt.value
+
+    def solveStep(self, solver_id=""):
+        self._sync_in()
+        check(lib().akb_solve_step(self.handle))
+
+    def solveSteps(self, nb_steps):
+        """nb_steps solveStep() calls replayed from a CUDA graph."""
+        self._sync_in()
+        check(lib().akb_solve_steps(self.handle, int(nb_steps)))
+
+    def timeSolveSteps(self, nb_steps):
+        """Device time (ms) of nb_steps steps, CUDA events on the model's stream."""
+        self._sync_in()
+        ms = C.c_double()
+        check(lib().akb_time_solve_steps(self.handle, int(nb_steps), C.byref(ms)))
+        return ms.value
+
+    def assembleInternalForces(self):
+        self._sync_in()
+        check(lib().akb_assemble_internal_forces(self.handle))
+
+    def computeStresses(self):
+        self._sync_in()
+        check(lib().akb_compute_stresses(self.handle))
+
+    def getEnergy(self, energy_id):
+        self._sync_in()
+        v = C.c_double()
+        check(lib().akb_get_energy(self.handle, _ENERGY[energy_id], C.byref(v)))
+        return v.value
+
+    def synchronize(self):
+        check(lib().akb_synchronize(self.handle))
+
+    def devicePointer(self, field):
+        p = C.c_void_p()
+        check(lib().akb_field_device_pointer(self.handle, field, C.byref(p)))
+        return p.value

@@ -201,6 +201,7 @@ def patch_test_explicit(make_model, name):
         model.solve_step()
     out = dict(mesh=mesh, dim=dim, dt=dt)
     out["ekin"] = model.energy(_abi.ENERGY_KINETIC)
+    out["epot"] = model.energy(_abi.ENERGY_POTENTIAL)
     out["u"] = model.get(_abi.FIELD_DISPLACEMENT)
     model.compute_stresses()
     out["gradu"] = model.get(_abi.FIELD_GRAD_U)
@@ -316,3 +317,53 @@ class OracleAdapter:
 
     def energy(self, kind):
         return self.m.energy(kind)
+
+
+class GpuAdapter:
+    """The same facade over akantu_b200.SolidMechanicsModel (libakb.so)."""
+
+    def __init__(self, mesh, material, precision=_abi.MODE_FP64_REFERENCE,
+                 element_material=None):
+        from akantu_b200.model import SolidMechanicsModel, material_from_dict
+        mats = material if isinstance(material, list) else [material]
+        self.m = SolidMechanicsModel(mesh, [material_from_dict(mm) for mm in mats],
+                                     element_material=element_material, precision=precision)
+        self.m.initFull()
+
+    def get(self, field):
+        return np.array(self.m.getField(field))
+
+    def set(self, field, values):
+        self.m.setField(field, values)
+
+    def get_blocked(self):
+        return np.array(self.m.getBlockedDOFs(), dtype=np.uint8)
+
+    def set_blocked(self, b):
+        self.m.setBlockedDOFs(b)
+
+    def stable_time_step(self):
+        return self.m.getStableTimeStep()
+
+    def set_time_step(self, dt):
+        self.m.setTimeStep(dt)
+
+    def solve_step(self):
+        self.m.solveStep()
+
+    def solve_steps(self, n):
+        self.m.solveSteps(n)
+
+    def assemble_internal_forces(self):
+        self.m.assembleInternalForces()
+
+    def assemble_mass_lumped(self):
+        self.m.assembleMassLumped()
+
+    def compute_stresses(self):
+        self.m.computeStresses()
+
+    def energy(self, kind):
+        name = {_abi.ENERGY_KINETIC: "kinetic", _abi.ENERGY_POTENTIAL: "potential",
+                _abi.ENERGY_EXTERNAL_WORK: "external work"}[kind]
+        return self.m.getEnergy(name)
