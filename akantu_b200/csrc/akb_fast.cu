@@ -62,18 +62,19 @@ __global__ void k_gather_correct(DevModel m, double dt, bool correct, bool has_f
   int64_t node = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (node >= m.nn) return;
   const int d = m.dim;
+  // element vectors are S; their assembly into the nodal force is FP64
   const S* fe = static_cast<const S*>(m.fe);
-  S f[3] = {0, 0, 0};
+  double f[3] = {0, 0, 0};
   const int beg = m.node_ptr[node], end = m.node_ptr[node + 1];
   for (int k = beg; k < end; ++k) {
     const int32_t ent = m.node_ent[k];
     const int64_t base = (int64_t)ent * d;  // (e*n + a)*d
-    for (int i = 0; i < d; ++i) f[i] -= fe[base + i];
+    for (int i = 0; i < d; ++i) f[i] -= double(fe[base + i]);
   }
   const double im = m.inv_mass[node];
   for (int i = 0; i < d; ++i) {
     const int64_t idx = node * d + i;
-    const double fi = double(f[i]);
+    const double fi = f[i];
     m.fint[idx] = fi;
     if (!correct || m.blocked[idx]) continue;
     double r = fi;
@@ -97,7 +98,24 @@ cudaError_t launch_elements(const DevModel& m, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+__global__ void k_apply_dirichlet(DevModel m, const uint32_t* nodes, int64_t n, int comp,
+                                  const double* values) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t node = nodes[k];
+  if (node >= m.nn) return;  // out-of-range node ids are ignored
+  const int64_t i = (int64_t)node * m.dim + comp;
+  m.blocked[i] = 1;
+  m.u[i] = values[k];
+}
+
 }  // namespace
+
+cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n, int comp,
+                            const double* values, cudaStream_t s) {
+  k_apply_dirichlet<<<blocks_for(n), kThreads, 0, s>>>(m, nodes, n, comp, values);
+  return cudaGetLastError();
+}
 
 cudaError_t fast_predictor(const DevModel& m, double dt, cudaStream_t s) {
   k_predictor<<<blocks_for(m.nn * m.dim), kThreads, 0, s>>>(m, dt);

@@ -93,42 +93,72 @@ __device__ inline void stress_P(const MatParams& p, const S* g, S* P) {
       for (int j = 0; j < d; ++j) P[i * d + j] = mu * (g[i * d + j] + g[j * d + i]) + (i == j ? lam * tr : S(0));
     return;
   }
-  S F[9], C[9], Sk[9];
-#pragma unroll
-  for (int i = 0; i < d; ++i)
-#pragma unroll
-    for (int j = 0; j < d; ++j) F[i * d + j] = g[i * d + j] + (i == j ? S(1) : S(0));
+  // Written in terms of grad u so that no O(1) quantity cancels near F = I
+  // (in FP32, C - I computed as C minus the identity loses eps/strain):
+  //   E2 = C - I = g + g^T + g^T g
+  //   neo-Hookean S = mu I + (lambda ln J - mu) C^-1 = C^-1 (mu E2 + lambda ln J I)
+  //   with J - 1 = I1 + I2 + I3 of g and ln J = log1p(J - 1);
+  //   St-Venant-Kirchhoff S = lambda tr(E2)/2 I + mu E2.
+  S E2[9], Sk[9];
 #pragma unroll
   for (int i = 0; i < d; ++i)
 #pragma unroll
     for (int j = 0; j < d; ++j) {
-      S c = 0;
+      S c = g[i * d + j] + g[j * d + i];
 #pragma unroll
-      for (int k = 0; k < d; ++k) c += F[k * d + i] * F[k * d + j];
-      C[i * d + j] = c;
+      for (int k = 0; k < d; ++k) c += g[k * d + i] * g[k * d + j];
+      E2[i * d + j] = c;
     }
   if (p.kind == AKB_MATERIAL_NEOHOOKEAN) {
-    // S = mu I + (lambda ln J - mu) C^-1
-    S Ca[9];
-    S detC = adjugate<d, S>(C, Ca);
-    S J = det<d, S>(F);
-    S f = lam * log(J) - mu;
-    S fi = f / detC;
+    S tr = 0;
+#pragma unroll
+    for (int i = 0; i < d; ++i) tr += g[i * d + i];
+    S Jm1 = tr;
+    if (d == 2) Jm1 += g[0] * g[3] - g[1] * g[2];
+    if (d == 3) {
+      S tr2 = 0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) tr2 += g[i * 3 + k] * g[k * 3 + i];
+      Jm1 += S(0.5) * (tr * tr - tr2) + det<3, S>(g);
+    }
+    const S lnJ = log1p(Jm1);
+    const S J = S(1) + Jm1;
+    S C[9], Ca[9], M[9];
+#pragma unroll
+    for (int k = 0; k < d * d; ++k) C[k] = E2[k];
+#pragma unroll
+    for (int i = 0; i < d; ++i) C[i * d + i] += S(1);
+    adjugate<d, S>(C, Ca);
+    const S idetC = S(1) / (J * J);
+#pragma unroll
+    for (int k = 0; k < d * d; ++k) M[k] = mu * E2[k];
+#pragma unroll
+    for (int i = 0; i < d; ++i) M[i * d + i] += lam * lnJ;
 #pragma unroll
     for (int i = 0; i < d; ++i)
 #pragma unroll
-      for (int j = 0; j < d; ++j) Sk[i * d + j] = (i == j ? mu : S(0)) + fi * Ca[i * d + j];
+      for (int j = 0; j < d; ++j) {
+        S c = 0;
+#pragma unroll
+        for (int k = 0; k < d; ++k) c += Ca[i * d + k] * M[k * d + j];
+        Sk[i * d + j] = c * idetC;
+      }
   } else {
-    // St-Venant-Kirchhoff: S = lambda tr(E) I + 2 mu E, E = (C - I)/2
     S trE = 0;
 #pragma unroll
-    for (int i = 0; i < d; ++i) trE += S(0.5) * (C[i * d + i] - S(1));
+    for (int i = 0; i < d; ++i) trE += S(0.5) * E2[i * d + i];
 #pragma unroll
     for (int i = 0; i < d; ++i)
 #pragma unroll
-      for (int j = 0; j < d; ++j)
-        Sk[i * d + j] = mu * (C[i * d + j] - (i == j ? S(1) : S(0))) + (i == j ? lam * trE : S(0));
+      for (int j = 0; j < d; ++j) Sk[i * d + j] = mu * E2[i * d + j] + (i == j ? lam * trE : S(0));
   }
+  S F[9];
+#pragma unroll
+  for (int i = 0; i < d; ++i)
+#pragma unroll
+    for (int j = 0; j < d; ++j) F[i * d + j] = g[i * d + j] + (i == j ? S(1) : S(0));
 #pragma unroll
   for (int i = 0; i < d; ++i)
 #pragma unroll

@@ -77,6 +77,10 @@ cudaError_t fast_element_forces(const DevModel& m, bool fp32, cudaStream_t s);
 cudaError_t fast_gather_correct(const DevModel& m, double dt, bool fp32, bool correct,
                                 bool has_fext, cudaStream_t s);
 
+// Dirichlet values (akb_fast.cu): blocked[node][comp] = 1, u[node][comp] = value.
+cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n, int comp,
+                            const double* values, cudaStream_t s);
+
 // Reductions (akb_reduce.cu). Scratch holds per-block partial results.
 cudaError_t stable_dt(const DevModel& m, double* d_scratch, int scratch_len,
                       double* d_out, cudaStream_t s);

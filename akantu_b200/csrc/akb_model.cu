@@ -43,6 +43,10 @@ struct akb_model {
   std::map<int64_t, cudaGraphExec_t> graphs;
   double graph_dt = -1.0;
   bool graph_fext = false;
+  // staging of akb_apply_dirichlet
+  uint32_t* d_bc_nodes = nullptr;
+  double* d_bc_values = nullptr;
+  int64_t bc_capacity = 0;
 };
 
 namespace {
@@ -94,18 +98,46 @@ void destroy_graphs(akb_model* m) {
 
 bool fp32(const akb_model* m) { return m->mode == AKB_MODE_FP32_BULK; }
 
+// Optional CUDA events recorded before each kernel of a step (and after the
+// last one), for akb_time_kernels.
+struct StepTimer {
+  cudaEvent_t ev[AKB_MAX_KERNEL_SLOTS + 1];
+  int n = 0;
+};
+inline void mark(StepTimer* t, cudaStream_t s) {
+  if (t && t->n <= AKB_MAX_KERNEL_SLOTS) cudaEventRecord(t->ev[t->n++], s);
+}
+
+const char* const kRefKernels[] = {"ref_predictor", "ref_element_forces", "ref_gather_correct"};
+const char* const kFastKernels[] = {"fast_predictor", "fast_element_forces", "fast_gather_correct"};
+
 // One NonLinearSolverLumped::solve.
-cudaError_t enqueue_step(akb_model* m) {
+cudaError_t enqueue_step(akb_model* m, StepTimer* t = nullptr) {
   const DevModel& d = m->dm;
   cudaError_t e;
   if (m->mode == AKB_MODE_FP64_REFERENCE) {
+    mark(t, m->stream);
     if ((e = ref_predictor(d, m->dt, m->stream)) != cudaSuccess) return e;
+    mark(t, m->stream);
     if ((e = ref_element_forces(d, m->stream)) != cudaSuccess) return e;
-    return ref_gather_correct(d, m->dt, true, m->stream);
+    mark(t, m->stream);
+    e = ref_gather_correct(d, m->dt, true, m->stream);
+    mark(t, m->stream);
+    return e;
   }
+  mark(t, m->stream);
   if ((e = fast_predictor(d, m->dt, m->stream)) != cudaSuccess) return e;
+  mark(t, m->stream);
   if ((e = fast_element_forces(d, fp32(m), m->stream)) != cudaSuccess) return e;
-  return fast_gather_correct(d, m->dt, fp32(m), true, m->has_fext, m->stream);
+  mark(t, m->stream);
+  e = fast_gather_correct(d, m->dt, fp32(m), true, m->has_fext, m->stream);
+  mark(t, m->stream);
+  return e;
+}
+
+const char* kernel_name(const akb_model* m, int slot) {
+  const char* const* names = m->mode == AKB_MODE_FP64_REFERENCE ? kRefKernels : kFastKernels;
+  return (slot >= 0 && slot < 3) ? names[slot] : "";
 }
 
 // Internal forces at the current displacement, without touching the state.
@@ -570,6 +602,74 @@ akb_status akb_get_energy(akb_model* m, int32_t kind, double* value) {
   if ((st = sync(m)) != AKB_OK) return st;
   *value = *m->h_result;
   return AKB_OK;
+}
+
+akb_status akb_apply_dirichlet(akb_model* m, const uint32_t* nodes, int64_t nb_nodes,
+                               int32_t component, const double* values) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (nb_nodes < 0 || (nb_nodes > 0 && (!nodes || !values)))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "null node or value array");
+  if (component < 0 || component >= m->dm.dim)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "component out of range");
+  if (nb_nodes == 0) return AKB_OK;
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if (nb_nodes > m->bc_capacity) {
+    AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+    dfree(m, m->d_bc_nodes);
+    dfree(m, m->d_bc_values);
+    m->d_bc_nodes = nullptr;
+    m->d_bc_values = nullptr;
+    m->bc_capacity = 0;
+    if ((st = dalloc(m, &m->d_bc_nodes, nb_nodes)) != AKB_OK) return st;
+    if ((st = dalloc(m, &m->d_bc_values, nb_nodes)) != AKB_OK) return st;
+    m->bc_capacity = nb_nodes;
+  }
+  AKB_CUDA_TRY(cudaMemcpyAsync(m->d_bc_nodes, nodes, nb_nodes * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice, m->stream));
+  AKB_CUDA_TRY(cudaMemcpyAsync(m->d_bc_values, values, nb_nodes * sizeof(double),
+                               cudaMemcpyHostToDevice, m->stream));
+  AKB_CUDA_TRY(apply_dirichlet(m->dm, m->d_bc_nodes, nb_nodes, component, m->d_bc_values,
+                               m->stream));
+  m->fint_valid = false;
+  m->stresses_valid = false;
+  // the caller's host arrays may be reused as soon as the call returns
+  return sync(m);
+}
+
+akb_status akb_time_kernels(akb_model* m, int64_t nb_steps, double* ms_per_launch,
+                            int32_t nb_slots) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!ms_per_launch || nb_slots < 0 || nb_steps < 1)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "bad timing arguments");
+  if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  StepTimer t;
+  for (auto& e : t.ev) AKB_CUDA_TRY(cudaEventCreate(&e));
+  double acc[AKB_MAX_KERNEL_SLOTS] = {0};
+  int nk = 0;
+  for (int64_t s = 0; s < nb_steps; ++s) {
+    t.n = 0;
+    AKB_CUDA_TRY(enqueue_step(m, &t));
+    AKB_CUDA_TRY(cudaEventSynchronize(t.ev[t.n - 1]));
+    nk = t.n - 1;
+    for (int k = 0; k < nk; ++k) {
+      float ms = 0;
+      AKB_CUDA_TRY(cudaEventElapsedTime(&ms, t.ev[k], t.ev[k + 1]));
+      acc[k] += ms;
+    }
+  }
+  for (auto& e : t.ev) cudaEventDestroy(e);
+  for (int k = 0; k < nb_slots; ++k) ms_per_launch[k] = k < nk ? acc[k] / nb_steps : 0.0;
+  m->fint_valid = true;
+  m->stresses_valid = false;
+  return AKB_OK;
+}
+
+const char* akb_kernel_name(const akb_model* m, int32_t slot) {
+  if (!m) return "";
+  return kernel_name(m, slot);
 }
 
 akb_status akb_synchronize(akb_model* m) {

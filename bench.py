@@ -1,0 +1,393 @@
+#!/usr/bin/env python3
+"""Explicit element-steps/s of the central-difference lumped-mass step.
+
+Workload: the 3D linear-elastic cube of 100^3 cells x 6 tetrahedron_4
+(6 000 000 elements, 1 030 301 nodes), E = 70 GPa, nu = 0.33, rho = 2700,
+bottom face fixed, top face v_z = 1 m/s, dt = 0.8 x stable, FP64 (the
+FP32-bulk form is measured beside it). One step = one solveStep() over the
+whole mesh; the metric counts elements x steps per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); each rank advances its own copy of
+the mesh (the single-mesh path runs as replicas, no data-path collective).
+Device time is measured with CUDA events on the model's stream, max over
+ranks. Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from akantu_b200 import _abi, configs  # noqa: E402
+
+METRIC = "explicit element-steps/s"
+UNIT = "element-steps/s"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def b_alg_bytes(w, fp32):
+    """Compulsory bytes of one step: int32 connectivity, reference
+    coordinates, FP64 u/v/a read + write, FP64 inverse mass per node, one
+    mask byte per node (f_ext is zero in this workload)."""
+    mesh = w["mesh"]
+    E, N, n = mesh.getNbElement(), mesh.getNbNodes(), mesh.connectivity.shape[1]
+    d = mesh.spatial_dimension
+    return E * n * 4 + N * d * (4 if fp32 else 8) + N * d * 8 * 6 + N * 8 + N * 1
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.6)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.1)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        # samples under load: the top half of the SM clocks seen
+        load = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------
+# distributed plumbing (one process per GPU)
+# --------------------------------------------------------------------------
+class Dist:
+    def __init__(self, want_gpus):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local_rank))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def make_model(w, mode, device):
+    from akantu_b200.model import SolidMechanicsModel, material_from_dict
+    m = SolidMechanicsModel(w["mesh"], [material_from_dict(mm) for mm in w["materials"]],
+                            precision=mode, device=device)
+    m.initFull()
+    return m
+
+
+class Facade:
+    def __init__(self, m):
+        self.m = m
+
+    def set(self, f, v):
+        self.m.setField(f, v)
+
+    def set_blocked(self, b):
+        self.m.setBlockedDOFs(b)
+
+    def stable_time_step(self):
+        return self.m.getStableTimeStep()
+
+    def set_time_step(self, dt):
+        self.m.setTimeStep(dt)
+
+
+def reset_state(m, w):
+    m.setField(_abi.FIELD_DISPLACEMENT, w["u0"])
+    m.setField(_abi.FIELD_VELOCITY, w["v0"])
+    m.setField(_abi.FIELD_ACCELERATION, np.zeros_like(w["u0"]))
+
+
+def time_device(m, w, steps, warmup, dist, sampler=None):
+    reset_state(m, w)
+    m.solveSteps(warmup)
+    reset_state(m, w)
+    m.synchronize()
+    dist.barrier()
+    if sampler:
+        sampler.start()
+    ms = m.timeSolveSteps(steps)
+    clocks = sampler.stop() if sampler else None
+    dist.barrier()
+    return dist.max(ms), clocks
+
+
+def time_e2e(m, w, steps, dist):
+    """The reference-facing loop through the C ABI with host buffers: per step
+    applyBC(FixedValue) of the fixed face from pinned host memory, solveStep,
+    and the kinetic energy read back (examples/explicit/explicit_dynamic.cc:87-99)."""
+    import torch
+    from akantu_b200._lib import check, lib
+    L = lib()
+    fixed = np.nonzero(w["blocked"][:, 0])[0].astype(np.uint32)
+    nodes_h = torch.from_numpy(fixed).pin_memory()
+    vals_h = torch.zeros(fixed.size, dtype=torch.float64).pin_memory()
+    pn = C.cast(nodes_h.data_ptr(), C.POINTER(C.c_uint32))
+    pv = C.cast(vals_h.data_ptr(), C.POINTER(C.c_double))
+    d = w["mesh"].spatial_dimension
+    h = m.handle
+    ek = C.c_double()
+    reset_state(m, w)
+    m.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for comp in range(d):
+            check(L.akb_apply_dirichlet(h, pn, fixed.size, comp, pv))
+        check(L.akb_solve_step(h))
+        check(L.akb_get_energy(h, _abi.ENERGY_KINETIC, C.byref(ek)))
+    t1 = time.perf_counter()
+    dist.barrier()
+    h2d = d * fixed.size * (4 + 8)
+    return dist.max(t1 - t0), h2d, 8
+
+
+def kernel_times(m, steps):
+    from akantu_b200._lib import check, lib
+    L = lib()
+    out = (C.c_double * _abi_max_slots())()
+    check(L.akb_time_kernels(m.handle, steps, out, _abi_max_slots()))
+    names = [L.akb_kernel_name(m.handle, k).decode() for k in range(_abi_max_slots())]
+    return [(n, out[k]) for k, n in enumerate(names) if n]
+
+
+def _abi_max_slots():
+    return 8
+
+
+def cpu_baseline(w, seconds_target=15.0):
+    """The oracle (FP64 CPU restatement, OpenMP, bitwise equal to the serial
+    reference order) on this host's cores, bounded sample of the workload."""
+    from oracle.oracle import OracleModel, material_desc
+    threads = os.cpu_count() or 1
+    m = OracleModel(w["mesh"], [material_desc(**mm) for mm in w["materials"]], fast=True)
+    m.set_threads(threads)
+    m.blocked[...] = w["blocked"]
+    m.displacement[...] = w["u0"]
+    m.velocity[...] = w["v0"]
+    m.set_time_step(w["dt_factor"] * m.stable_time_step())
+    t1 = m.time_steps(1)
+    steps = int(max(1, min(50, seconds_target / max(t1, 1e-6))))
+    t = m.time_steps(steps)
+    E = w["mesh"].getNbElement()
+    return dict(value=E * steps / t, unit=UNIT, cores=threads, kind="port",
+                sample="%d steps of the full %d-element mesh after 1 warm-up step "
+                       "(FP64 CPU restatement, OpenMP)" % (steps, E))
+
+
+def run_ours(args, dist):
+    import torch
+    device = dist.local_rank
+    torch.cuda.set_device(device)
+    w = configs.cube_tet4()
+    E = w["mesh"].getNbElement()
+    peak, peak_kind = load_peaks()
+    m = make_model(w, _abi.MODE_FP64, device)
+    dt = configs.setup_model(Facade(m), w)
+    sampler = ClockSampler(device)
+    ms, clocks = time_device(m, w, args.steps, args.warmup, dist, sampler)
+    value = dist.world * E * args.steps / (ms / 1e3)
+    ktimes = kernel_times(m, min(args.steps, 50))
+    step_ms = sum(t for _, t in ktimes)
+    top = max(ktimes, key=lambda kv: kv[1])
+    balg = b_alg_bytes(w, False)
+    e2e_steps = min(args.steps, 200)
+    e2e_s, h2d, d2h = time_e2e(m, w, e2e_steps, dist)
+    e2e_value = dist.world * E * e2e_steps / e2e_s
+    u64 = m.getDisplacement().copy() if dist.rank == 0 else None
+    # FP32-bulk beside it, error vs the FP64 GPU run after the same steps
+    m32 = make_model(w, _abi.MODE_FP32_BULK, device)
+    configs.setup_model(Facade(m32), w)
+    m32.setTimeStep(dt)
+    ms32, _ = time_device(m32, w, args.steps, args.warmup, dist)
+    fp32 = dict(value=dist.world * E * args.steps / (ms32 / 1e3),
+                ms_per_step=ms32 / args.steps,
+                roofline_frac=(b_alg_bytes(w, True) / (ms32 / args.steps / 1e3) / 1e9) / peak)
+    if dist.rank == 0:
+        # same K steps from the same state in both precisions
+        reset_state(m, w)
+        m.solveSteps(args.steps)
+        reset_state(m32, w)
+        m32.solveSteps(args.steps)
+        u64 = m.getDisplacement().copy()
+        u32 = m32.getDisplacement()
+        fp32["rel_err_displacement_vs_fp64"] = float(np.abs(u32 - u64).max() / np.abs(u64).max())
+    m32.close()
+    launches = args.steps * len(ktimes)
+    result = None
+    if dist.rank == 0:
+        achieved = balg / (step_ms / 1e3) / 1e9
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cube_tet4: 100^3 cells x 6 tetrahedron_4 (6,000,000 "
+                                   "elements, 1,030,301 nodes), linear elastic, FP64, "
+                                   "dt = 0.8 x stable", "elements": E,
+                       "nodes": w["mesh"].getNbNodes(), "time_step": dt,
+                       "parallelism": "replicas" if dist.world > 1 else "single GPU",
+                       "l2": "no flush: per-step working set %.0f MB > 126 MB L2" % (balg / 1e6)},
+            "roofline": {"bound": "hbm", "kernel": "whole step (%s)" % ", ".join(n for n, _ in ktimes),
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_step": balg, "traffic": None,
+                         "kernels_ms": {n: t for n, t in ktimes},
+                         "dominant": top[0]},
+            "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "fp32_bulk": fp32,
+        }
+    m.close()
+    return result
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return None
+    w = configs.cube_tet4()
+    from oracle.oracle import OracleModel, material_desc
+    threads = os.cpu_count() or 1
+    m = OracleModel(w["mesh"], [material_desc(**mm) for mm in w["materials"]], fast=True)
+    m.set_threads(threads)
+    m.blocked[...] = w["blocked"]
+    m.velocity[...] = w["v0"]
+    dt = w["dt_factor"] * m.stable_time_step()
+    m.set_time_step(dt)
+    warm = min(args.warmup, 2)
+    m.time_steps(warm)
+    steps = min(args.steps, 40)
+    t = m.time_steps(steps)
+    E = w["mesh"].getNbElement()
+    value = E * steps / t
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+        "steps": steps, "warmup": warm, "ms_per_step": t / steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "cube_tet4: 100^3 cells x 6 tetrahedron_4 (6,000,000 "
+                               "elements, 1,030,301 nodes), linear elastic, FP64",
+                   "elements": E, "time_step": dt},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "%d of the requested %d steps on the full mesh "
+                                   "(the reference cannot be built: Boost is absent)"
+                                   % (steps, args.steps)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+
+        class _D:
+            pass
+        d = _D()
+        d.rank, d.world = rank, world
+        res = run_reference(args, d)
+        print(json.dumps(res), flush=True)
+        return
+    dist = Dist(args.gpus)
+    try:
+        res = run_ours(args, dist)
+        if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline(configs.cube_tet4())
+        if dist.rank == 0:
+            print(json.dumps(res), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

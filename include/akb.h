@@ -191,6 +191,26 @@ akb_status akb_compute_stresses(akb_model* model);
 /* SolidMechanicsModel::getEnergy (solid_mechanics_model.cc:665-683). */
 akb_status akb_get_energy(akb_model* model, int32_t kind, double* value);
 
+/* applyBC(BC::Dirichlet::FixedValue(value, component), group)
+ * (boundary_condition_functor_inline_impl.hh:85-93, boundary_condition_tmpl.hh:63-88):
+ * for each listed node, blocks DOF (node, component) and sets its
+ * displacement to values[k]. nodes and values are host arrays of nb_nodes
+ * entries (pinned memory makes the copy asynchronous-capable). */
+akb_status akb_apply_dirichlet(akb_model* model, const uint32_t* nodes,
+                               int64_t nb_nodes, int32_t component,
+                               const double* values);
+
+/* Kernel slots of one step, for akb_time_kernels. */
+enum { AKB_MAX_KERNEL_SLOTS = 8 };
+/* Runs nb_steps steps one launch at a time, with CUDA events recorded on the
+ * model's stream around every kernel; ms_per_launch[k] receives the mean
+ * device time of the step's k-th kernel (0 past the last one). No reference
+ * counterpart: the reference has no timers (it measures nothing). */
+akb_status akb_time_kernels(akb_model* model, int64_t nb_steps,
+                            double* ms_per_launch, int32_t nb_slots);
+/* Name of the step's k-th kernel, or "" past the last one. */
+const char* akb_kernel_name(const akb_model* model, int32_t slot);
+
 /* Waits for all work queued on the model's stream. */
 akb_status akb_synchronize(akb_model* model);
 

@@ -322,6 +322,11 @@ struct oracle_model {
   std::vector<double> gradu, stress;
   double dt = 0;
   bool mass_assembled = false;
+  // multi-threaded variant: element vectors + node -> (element, corner) CSR
+  int threads = 1;
+  std::vector<double> fe;
+  std::vector<int64_t> node_ptr;
+  std::vector<int64_t> node_ent;
 };
 
 namespace {
@@ -484,14 +489,79 @@ void b_matrix_bl2(int d, int n, const double* B, const double* g, double* Bv, in
 // computeBtD shape_lagrange_inline_impl.hh:383-423, integrate
 // integrator_gauss_inline_impl.hh:426-455, scatter with scale -1
 // dof_manager.cc:83-137) or finite strain (material.cc:637-722).
+void element_vector(oracle_model& m, int64_t e, double* inte);
+
+void assemble_internal_forces_parallel(oracle_model& m);
+
 void assemble_internal_forces(oracle_model& m) {
-  const int d = m.dim, n = m.info.nnpe, q = m.info.nqp;
+  if (m.threads > 1) {
+    assemble_internal_forces_parallel(m);
+    return;
+  }
+  const int d = m.dim, n = m.info.nnpe;
   std::fill(m.fint.begin(), m.fint.end(), 0.);
   compute_all_stresses(m);
-  const int vs = (d == 1) ? 1 : (d == 2 ? 3 : 6);
-  std::vector<double> r(q * d * n), inte(d * n);
-  double Bv[6 * 24], B2[6 * 24];
+  std::vector<double> inte(d * n);
   for (int64_t e = 0; e < m.ne; ++e) {
+    element_vector(m, e, inte.data());
+    for (int aa = 0; aa < n; ++aa) {
+      uint32_t node = m.conn[e * n + aa];
+      for (int i = 0; i < d; ++i) m.fint[node * d + i] += -1. * inte[i + aa * d];
+    }
+  }
+}
+
+// Multi-threaded variant, bitwise equal to the serial one: element vectors in
+// parallel, then each node adds -1 * (its elements' vectors) in ascending
+// element order, the order of the serial element-by-element scatter.
+void assemble_internal_forces_parallel(oracle_model& m) {
+  const int d = m.dim, n = m.info.nnpe, q = m.info.nqp;
+  if (m.fe.size() != (size_t)m.ne * n * d) m.fe.assign((size_t)m.ne * n * d, 0.);
+  if (m.node_ptr.empty()) {
+    m.node_ptr.assign(m.nn + 1, 0);
+    m.node_ent.assign((size_t)m.ne * n, 0);
+    for (int64_t k = 0; k < m.ne * n; ++k) m.node_ptr[m.conn[k] + 1]++;
+    for (int64_t i = 0; i < m.nn; ++i) m.node_ptr[i + 1] += m.node_ptr[i];
+    std::vector<int64_t> fill(m.node_ptr.begin(), m.node_ptr.end() - 1);
+    for (int64_t k = 0; k < m.ne * n; ++k) m.node_ent[fill[m.conn[k]]++] = k;
+  }
+  double* uu = m.u.data();
+  (void)q;
+#pragma omp parallel for schedule(static) num_threads(m.threads)
+  for (int64_t e = 0; e < m.ne; ++e) {
+    double uel[24];
+    for (int aa = 0; aa < n; ++aa)
+      for (int i = 0; i < d; ++i) uel[i + aa * d] = uu[m.conn[e * n + aa] * d + i];
+    const Material& mat = m.mats[m.mat_of[e]];
+    for (int p = 0; p < q; ++p) {
+      double* g = &m.gradu[(e * q + p) * d * d];
+      mmt(d, d, n, uel, &m.B[(e * q + p) * d * n], g);
+      for (int k = 0; k < d * d; ++k) g[k] -= 0.;
+      material_stress(mat, d, g, &m.stress[(e * q + p) * d * d]);
+    }
+    element_vector(m, e, &m.fe[(size_t)e * n * d]);
+  }
+#pragma omp parallel for schedule(static) num_threads(m.threads)
+  for (int64_t node = 0; node < m.nn; ++node) {
+    for (int i = 0; i < d; ++i) {
+      double f = 0.;
+      for (int64_t k = m.node_ptr[node]; k < m.node_ptr[node + 1]; ++k) {
+        const int64_t ent = m.node_ent[k];
+        const int64_t e = ent / n, aa = ent % n;
+        f += -1. * m.fe[(size_t)e * n * d + i + aa * d];
+      }
+      m.fint[node * d + i] = f;
+    }
+  }
+}
+
+// Element vector of Material::assembleInternalForces (before the -1 scatter).
+void element_vector(oracle_model& m, int64_t e, double* inte) {
+  const int d = m.dim, n = m.info.nnpe, q = m.info.nqp;
+  const int vs = (d == 1) ? 1 : (d == 2 ? 3 : 6);
+  double r[8 * 24];
+  double Bv[6 * 24], B2[6 * 24];
+  {
     const Material& mat = m.mats[m.mat_of[e]];
     for (int p = 0; p < q; ++p) {
       const double* s = &m.stress[(e * q + p) * d * d];
@@ -518,13 +588,9 @@ void assemble_internal_forces(oracle_model& m) {
         mtm(d * n, 1, vs, Bv, sv, &r[p * d * n]);
       }
     }
-    std::memset(inte.data(), 0, sizeof(double) * d * n);
+    std::memset(inte, 0, sizeof(double) * d * n);
     for (int p = 0; p < q; ++p)
       for (int k = 0; k < d * n; ++k) inte[k] += r[p * d * n + k] * m.jac[e * q + p];
-    for (int aa = 0; aa < n; ++aa) {
-      uint32_t node = m.conn[e * n + aa];
-      for (int i = 0; i < d; ++i) m.fint[node * d + i] += -1. * inte[i + aa * d];
-    }
   }
 }
 
@@ -533,9 +599,10 @@ void assemble_internal_forces(oracle_model& m) {
 void solve_step(oracle_model& m) {
   const double alpha = 0., beta = 0.5, k = 0., h = 0.;
   const double dt = m.dt;
-  const size_t ndof = m.u.size();
+  const int64_t ndof = (int64_t)m.u.size();
   // NewmarkBeta::predictor (newmark-beta.cc:60-89)
-  for (size_t i = 0; i < ndof; ++i) {
+#pragma omp parallel for schedule(static) num_threads(m.threads) if (m.threads > 1)
+  for (int64_t i = 0; i < ndof; ++i) {
     if (!m.blocked[i]) {
       double dt_a_n = dt * m.a[i];
       m.u[i] += (1 - k * alpha) * dt * m.v[i] + (.5 - h * alpha * beta) * dt * dt_a_n;
@@ -549,21 +616,23 @@ void solve_step(oracle_model& m) {
   assemble_internal_forces(m);
   // SolidMechanicsModel::assembleResidual (solid_mechanics_model.cc:279-293)
   // through DOFManagerDefault::assembleToGlobalArray (dof_manager_default.cc:105-144)
-  for (size_t i = 0; i < ndof; ++i) m.residual[i] += 1. * m.fext[i];
-  for (size_t i = 0; i < ndof; ++i) m.residual[i] += 1. * m.fint[i];
-  // IntegrationScheme2ndOrder::assembleResidual (integration_scheme_2nd_order.cc:79-102)
-  // -> assembleLumpedMatMulVectToResidual (dof_manager_default.cc:271-287)
-  for (size_t i = 0; i < ndof; ++i) {
-    double c = 0.;
-    c += -1. * m.a[i];
-    m.residual[i] += m.lumped[i] * c;
-  }
-  // solveLumped (non_linear_solver_lumped.cc:85-98), b_a2x = 1
-  for (size_t i = 0; i < ndof; ++i)
-    if (!m.blocked[i]) m.solution[i] = 1. * (m.residual[i] / m.lumped[i]);
-  // NewmarkBeta::allCorrector<_acceleration> (newmark-beta.cc:176-210)
+  // (the loops below are element-wise, so fusing them changes no result)
   const double c = 1., dd = beta * dt, ee = alpha * beta * dt * dt;
-  for (size_t i = 0; i < ndof; ++i) {
+#pragma omp parallel for schedule(static) num_threads(m.threads) if (m.threads > 1)
+  for (int64_t i = 0; i < ndof; ++i) {
+    m.residual[i] += 1. * m.fext[i];
+    m.residual[i] += 1. * m.fint[i];
+    // IntegrationScheme2ndOrder::assembleResidual (integration_scheme_2nd_order.cc:79-102)
+    // -> assembleLumpedMatMulVectToResidual (dof_manager_default.cc:271-287)
+    double cache = 0.;
+    cache += -1. * m.a[i];
+    m.residual[i] += m.lumped[i] * cache;
+    // solveLumped (non_linear_solver_lumped.cc:85-98), b_a2x = 1
+    if (!m.blocked[i]) m.solution[i] = 1. * (m.residual[i] / m.lumped[i]);
+  }
+  // NewmarkBeta::allCorrector<_acceleration> (newmark-beta.cc:176-210)
+#pragma omp parallel for schedule(static) num_threads(m.threads) if (m.threads > 1)
+  for (int64_t i = 0; i < ndof; ++i) {
     if (!m.blocked[i]) {
       m.u[i] += ee * m.solution[i];
       m.v[i] += dd * m.solution[i];
@@ -705,6 +774,7 @@ double oracle_stable_time_step(oracle_model* m) {
 }
 
 void oracle_set_time_step(oracle_model* m, double dt) { m->dt = dt; }
+void oracle_set_threads(oracle_model* m, int32_t threads) { m->threads = threads < 1 ? 1 : threads; }
 void oracle_solve_step(oracle_model* m) { solve_step(*m); }
 void oracle_solve_steps(oracle_model* m, int64_t n) {
   for (int64_t s = 0; s < n; ++s) solve_step(*m);

@@ -39,6 +39,9 @@ int64_t oracle_field_size(oracle_model* m, int32_t field);
 void oracle_assemble_mass_lumped(oracle_model* m);
 double oracle_stable_time_step(oracle_model* m);
 void oracle_set_time_step(oracle_model* m, double dt);
+/* Host threads (OpenMP builds only); the multi-threaded path is bitwise
+ * equal to the single-threaded one. */
+void oracle_set_threads(oracle_model* m, int32_t threads);
 void oracle_solve_step(oracle_model* m);
 void oracle_solve_steps(oracle_model* m, int64_t n);
 void oracle_assemble_internal_forces(oracle_model* m);

@@ -48,6 +48,7 @@ def _lib(fast=False):
     lib.oracle_stable_time_step.restype = C.c_double
     lib.oracle_stable_time_step.argtypes = [P]
     lib.oracle_set_time_step.argtypes = [P, C.c_double]
+    lib.oracle_set_threads.argtypes = [P, C.c_int32]
     lib.oracle_solve_steps.argtypes = [P, C.c_int64]
     lib.oracle_energy.restype = C.c_double
     lib.oracle_energy.argtypes = [P, C.c_int32]
@@ -141,6 +142,9 @@ class OracleModel:
 
     def set_time_step(self, dt):
         self.lib.oracle_set_time_step(self.h, dt)
+
+    def set_threads(self, n):
+        self.lib.oracle_set_threads(self.h, n)
 
     def solve_step(self):
         self.lib.oracle_solve_step(self.h)

@@ -89,8 +89,14 @@ def test_plate_tri3_full_run(mode):
         e = rel(dev.get(f), cpu.get(f))
         if mode == _abi.MODE_FP64_REFERENCE:
             assert np.array_equal(dev.get(f), cpu.get(f)), (f, e)
+        elif mode == _abi.MODE_FP64:
+            assert e <= 1e-10, (f, e)
         else:
-            assert e <= (1e-10 if mode == _abi.MODE_FP64 else 1e-5), (f, e)
+            # smooth field (wavelength 400 elements): neighbouring element
+            # forces cancel to ~h k = 1.6e-2 of their size, which amplifies
+            # the FP32 rounding of each; velocity and acceleration carry it
+            assert e <= {_abi.FIELD_DISPLACEMENT: 1e-5, _abi.FIELD_VELOCITY: 3e-5,
+                         _abi.FIELD_ACCELERATION: 2e-4}[f], (f, e)
     for kind in (_abi.ENERGY_KINETIC, _abi.ENERGY_POTENTIAL, _abi.ENERGY_EXTERNAL_WORK):
         ec, eg = cpu.energy(kind), dev.energy(kind)
         tol = 1e-12 if mode != _abi.MODE_FP32_BULK else 1e-5
