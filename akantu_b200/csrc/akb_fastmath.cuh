@@ -15,6 +15,24 @@
 namespace akb {
 namespace fast {
 
+// Central-difference predictor and corrector of one free DOF
+// (newmark-beta.cc:73-81 and 186-200 with alpha = 0, beta = 1/2), with every
+// rounding spelled out so that every kernel computing them agrees bitwise.
+__device__ inline void predict(double dt, double& u, double& v, double a) {
+  const double dta = __dmul_rn(dt, a);
+  u = __dadd_rn(u, __fma_rn(0.5 * dt, dta, __dmul_rn(dt, v)));
+  v = __dadd_rn(v, dta);
+}
+// x = (f_ext + f_int) / M - a; v += dt/2 x; a += x; u += 0 x (only matters
+// when x is not finite).
+__device__ inline void correct(double dt, double r, double inv_m, double& u, double& v,
+                               double& a) {
+  const double x = __fma_rn(r, inv_m, -a);
+  v = __fma_rn(0.5 * dt, x, v);
+  a = __dadd_rn(a, x);
+  if (!isfinite(x)) u += 0.0 * x;
+}
+
 // dN_a/dxi_k at quadrature point q (k-th row), reference element tables.
 template <int T, typename S>
 __device__ inline S dN(int k, int a, int q) {

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "akb_internal.cuh"
+#include "akb_patch.cuh"
 
 namespace akb {
 
@@ -43,6 +44,9 @@ struct akb_model {
   std::map<int64_t, cudaGraphExec_t> graphs;
   double graph_dt = -1.0;
   bool graph_fext = false;
+  // fused patch step of the fast modes
+  DevPatches patches{};
+  bool use_patches = false;
   // staging of akb_apply_dirichlet
   uint32_t* d_bc_nodes = nullptr;
   double* d_bc_values = nullptr;
@@ -110,6 +114,7 @@ inline void mark(StepTimer* t, cudaStream_t s) {
 
 const char* const kRefKernels[] = {"ref_predictor", "ref_element_forces", "ref_gather_correct"};
 const char* const kFastKernels[] = {"fast_predictor", "fast_element_forces", "fast_gather_correct"};
+const char* const kPatchKernels[] = {"patch_step", "patch_shared_nodes"};
 
 // One NonLinearSolverLumped::solve.
 cudaError_t enqueue_step(akb_model* m, StepTimer* t = nullptr) {
@@ -125,6 +130,15 @@ cudaError_t enqueue_step(akb_model* m, StepTimer* t = nullptr) {
     mark(t, m->stream);
     return e;
   }
+  if (m->use_patches) {
+    mark(t, m->stream);
+    if ((e = patch_step(d, m->patches, m->dt, fp32(m), m->has_fext, m->stream)) != cudaSuccess)
+      return e;
+    mark(t, m->stream);
+    e = patch_shared_nodes(d, m->patches, m->dt, m->has_fext, m->stream);
+    mark(t, m->stream);
+    return e;
+  }
   mark(t, m->stream);
   if ((e = fast_predictor(d, m->dt, m->stream)) != cudaSuccess) return e;
   mark(t, m->stream);
@@ -136,8 +150,74 @@ cudaError_t enqueue_step(akb_model* m, StepTimer* t = nullptr) {
 }
 
 const char* kernel_name(const akb_model* m, int slot) {
+  if (m->use_patches) return (slot >= 0 && slot < 2) ? kPatchKernels[slot] : "";
   const char* const* names = m->mode == AKB_MODE_FP64_REFERENCE ? kRefKernels : kFastKernels;
   return (slot >= 0 && slot < 3) ? names[slot] : "";
+}
+
+// Patch sizes per element type: elements per patch and the local node cap,
+// chosen so two 256-thread CTAs fit an SM's shared memory.
+void patch_params(int type, int* target, int* max_nodes) {
+  switch (type) {
+  case AKB_SEGMENT_2: *target = 1024; *max_nodes = 1100; break;
+  case AKB_TRIANGLE_3: *target = 1024; *max_nodes = 640; break;
+  case AKB_TETRAHEDRON_4: *target = 2048; *max_nodes = 640; break;
+  default: *target = 256; *max_nodes = 448; break;
+  }
+}
+
+template <typename T>
+akb_status upload(akb_model* m, const std::vector<T>& v, const T** out);
+
+akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
+                                const uint32_t* element_material) {
+  int target, max_nodes;
+  patch_params(m->dm.type, &target, &max_nodes);
+  PatchHost P = build_patches(mesh->nodes, mesh->connectivity, mesh->nb_nodes,
+                              mesh->nb_elements, m->dm.dim, m->dm.nnpe, target, max_nodes);
+  DevPatches& d = m->patches;
+  d.npatch = P.npatch;
+  d.max_nodes = P.max_nodes;
+  d.max_elems = P.max_elems;
+  d.nshared = (int64_t)P.snodes.size();
+  akb_status st;
+  if ((st = upload(m, P.elem_ptr, &d.elem_ptr)) != AKB_OK) return st;
+  if ((st = upload(m, P.node_ptr, &d.node_ptr)) != AKB_OK) return st;
+  if ((st = upload(m, P.ninterior, &d.ninterior)) != AKB_OK) return st;
+  if ((st = upload(m, P.lnodes, &d.lnodes)) != AKB_OK) return st;
+  if ((st = upload(m, P.lconn, &d.lconn)) != AKB_OK) return st;
+  if ((st = upload(m, P.cbeg, &d.cbeg)) != AKB_OK) return st;
+  if ((st = upload(m, P.centries, &d.centries)) != AKB_OK) return st;
+  if ((st = upload(m, P.slot, &d.slot)) != AKB_OK) return st;
+  if ((st = upload(m, P.snodes, &d.snodes)) != AKB_OK) return st;
+  if ((st = upload(m, P.sptr, &d.sptr)) != AKB_OK) return st;
+  d.emat = nullptr;
+  if (element_material) {
+    std::vector<uint32_t> em(P.elem_order.size());
+    for (size_t i = 0; i < em.size(); ++i) em[i] = element_material[P.elem_order[i]];
+    if ((st = upload(m, em, &d.emat)) != AKB_OK) return st;
+  }
+  if ((st = dalloc(m, &d.partial, (size_t)std::max<int64_t>(P.nslots, 1) * m->dm.dim)) != AKB_OK)
+    return st;
+  AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));  // host vectors go out of scope
+  const size_t smem = patch_smem_bytes(d, m->dm.dim, m->dm.nnpe, fp32(m), 256);
+  if (smem > 227 * 1024)
+    return fail(AKB_ERR_UNSUPPORTED, "patch does not fit in shared memory");
+  AKB_CUDA_TRY(patch_configure(m->dm, d, fp32(m)));
+  m->use_patches = true;
+  return AKB_OK;
+}
+
+template <typename T>
+akb_status upload(akb_model* m, const std::vector<T>& v, const T** out) {
+  T* p;
+  akb_status st;
+  if ((st = dalloc(m, &p, v.size())) != AKB_OK) return st;
+  if (!v.empty())
+    AKB_CUDA_TRY(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice,
+                                 m->stream));
+  *out = p;
+  return AKB_OK;
 }
 
 // Internal forces at the current displacement, without touching the state.
@@ -336,6 +416,9 @@ akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
     m->device_bytes -= (int64_t)ne * q * d * n * 8 + (int64_t)ne * q * 8;
     dm.B = nullptr;
     dm.jac = nullptr;
+  }
+  if (m->mode != AKB_MODE_FP64_REFERENCE && ne > 0) {
+    if ((st = build_device_patches(m.get(), mesh, element_material)) != AKB_OK) return st;
   }
   m->scratch_len = reduce_blocks(ne);
   if ((st = dalloc(m.get(), &m->d_scratch, m->scratch_len)) != AKB_OK) return st;
@@ -537,7 +620,9 @@ akb_status akb_solve_steps(akb_model* m, int64_t nb_steps) {
     for (int64_t r = 0; r < reps; ++r) AKB_CUDA_TRY(cudaGraphLaunch(full, m->stream));
     if (rest) AKB_CUDA_TRY(cudaGraphLaunch(rest, m->stream));
   }
-  m->fint_valid = true;
+  // the fused patch step keeps the internal force on chip; it is recomputed
+  // on demand at the (unchanged) displacement
+  m->fint_valid = !m->use_patches;
   m->stresses_valid = false;
   return AKB_OK;
 }
@@ -662,7 +747,7 @@ akb_status akb_time_kernels(akb_model* m, int64_t nb_steps, double* ms_per_launc
   }
   for (auto& e : t.ev) cudaEventDestroy(e);
   for (int k = 0; k < nb_slots; ++k) ms_per_launch[k] = k < nk ? acc[k] / nb_steps : 0.0;
-  m->fint_valid = true;
+  m->fint_valid = !m->use_patches;
   m->stresses_valid = false;
   return AKB_OK;
 }

@@ -1,0 +1,260 @@
+// akb_patch.cu -- the fused explicit step (AKB_MODE_FP64, AKB_MODE_FP32_BULK).
+//
+// k_patch_step: one CTA per patch.
+//   1. stage the patch's nodes: X, u, v, a, blocked flags; predictor
+//      u+ = u + dt v + dt^2/2 a, v* = v + dt a on free DOFs
+//      (NewmarkBeta::predictor, newmark-beta.cc:60-89);
+//   2. element forces in chunks of blockDim elements from shared memory
+//      (akb_fastmath.cuh), each chunk's vectors added to the node
+//      accumulators in ascending local element order through the patch CSR
+//      (the -1 scatter of dof_manager.cc:83-137, without atomics);
+//   3. nodes of this patch only: residual, lumped solve and corrector
+//      (non_linear_solver_lumped.cc:85-98, newmark-beta.cc:176-210), written
+//      back; nodes shared with other patches: FP64 partial force to its slot.
+// k_shared_nodes: one thread per shared node adds its partials in patch order
+// and applies the same predictor/corrector arithmetic.
+#include "akb_fastmath.cuh"
+#include "akb_patch.cuh"
+
+namespace akb {
+namespace {
+
+constexpr int kThreads = 256;
+
+struct SmemLayout {
+  size_t xs, us, vs, as, fs, contrib, flags, cursor, total;
+};
+
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+__host__ __device__ inline SmemLayout layout(int L, int d, int n, int sbytes, int threads) {
+  SmemLayout s;
+  const size_t nd = (size_t)L * d * sizeof(double);
+  s.xs = 0;
+  s.us = align16(s.xs + nd);
+  s.vs = align16(s.us + nd);
+  s.as = align16(s.vs + nd);
+  s.fs = align16(s.as + nd);
+  s.contrib = align16(s.fs + nd);
+  s.flags = align16(s.contrib + (size_t)threads * n * d * sbytes);
+  s.cursor = align16(s.flags + (size_t)L * d);
+  s.total = align16(s.cursor + (size_t)L * sizeof(uint16_t));
+  return s;
+}
+
+template <int T, typename S, bool FEXT>
+__global__ void __launch_bounds__(kThreads) k_patch_step(DevModel m, DevPatches P, double dt) {
+  constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int p = blockIdx.x;
+  const int nb = P.node_ptr[p];
+  const int L = P.node_ptr[p + 1] - nb;
+  const int eb = P.elem_ptr[p];
+  const int ne = P.elem_ptr[p + 1] - eb;
+  const int nint = P.ninterior[p];
+  const SmemLayout lay = layout(P.max_nodes, d, n, sizeof(S), kThreads);
+  double* xs = reinterpret_cast<double*>(smem + lay.xs);
+  double* us = reinterpret_cast<double*>(smem + lay.us);
+  double* vs = reinterpret_cast<double*>(smem + lay.vs);
+  double* as = reinterpret_cast<double*>(smem + lay.as);
+  double* fs = reinterpret_cast<double*>(smem + lay.fs);
+  S* contrib = reinterpret_cast<S*>(smem + lay.contrib);
+  uint8_t* flags = smem + lay.flags;
+  uint16_t* cursor = reinterpret_cast<uint16_t*>(smem + lay.cursor);
+  const int tid = threadIdx.x;
+
+  // 1. stage nodes + predictor
+  for (int j = tid; j < L; j += kThreads) {
+    const int64_t g = P.lnodes[nb + j];
+#pragma unroll
+    for (int i = 0; i < d; ++i) {
+      const int64_t k = g * d + i;
+      const double x = __ldg(&m.X[k]);
+      double u = m.u[k], v = m.v[k];
+      const double a = m.a[k];
+      const uint8_t b = m.blocked[k];
+      if (!b) fast::predict(dt, u, v, a);
+      xs[j * d + i] = x;
+      us[j * d + i] = u;
+      vs[j * d + i] = v;
+      as[j * d + i] = a;
+      fs[j * d + i] = 0.0;
+      flags[j * d + i] = b;
+    }
+    cursor[j] = P.cbeg[nb + j];
+  }
+  __syncthreads();
+
+  // 2. element forces, chunk by chunk
+  const uint16_t* ent = P.centries + (size_t)eb * n;
+  const int nent = ne * n;
+  for (int c0 = 0; c0 < ne; c0 += kThreads) {
+    const int el = c0 + tid;
+    if (el < ne) {
+      const size_t ge = (size_t)eb + el;
+      int lc[n];
+#pragma unroll
+      for (int a = 0; a < n; ++a) lc[a] = P.lconn[ge * n + a];
+      const MatParams& mp = m.mats[P.emat ? P.emat[ge] : 0];
+      S dX[3 * 8], du[3 * 8];
+#pragma unroll
+      for (int i = 0; i < d; ++i) {
+        dX[i] = 0;
+        du[i] = 0;
+      }
+#pragma unroll
+      for (int a = 1; a < n; ++a)
+#pragma unroll
+        for (int i = 0; i < d; ++i) {
+          dX[a * d + i] = S(xs[lc[a] * d + i] - xs[lc[0] * d + i]);
+          du[a * d + i] = S(us[lc[a] * d + i] - us[lc[0] * d + i]);
+        }
+      S fe[3 * 8];
+      fast::element_force<T, S>(mp, dX, du, fe);
+#pragma unroll
+      for (int k = 0; k < n * d; ++k) contrib[tid * n * d + k] = fe[k];
+    }
+    __syncthreads();
+    const int c1 = c0 + kThreads < ne ? c0 + kThreads : ne;
+    for (int j = tid; j < L; j += kThreads) {
+      int c = cursor[j];
+      const int end = (j + 1 < L) ? P.cbeg[nb + j + 1] : nent;
+      double f[3] = {fs[j * d], d > 1 ? fs[j * d + 1] : 0.0, d > 2 ? fs[j * d + 2] : 0.0};
+      while (c < end) {
+        const int e = ent[c];
+        const int le = e >> 3;
+        if (le >= c1) break;
+        const S* src = contrib + ((le - c0) * n + (e & 7)) * d;
+#pragma unroll
+        for (int i = 0; i < d; ++i) f[i] -= double(src[i]);
+        ++c;
+      }
+      cursor[j] = (uint16_t)c;
+#pragma unroll
+      for (int i = 0; i < d; ++i) fs[j * d + i] = f[i];
+    }
+    __syncthreads();
+  }
+
+  // 3. finish the nodes of this patch, hand out the shared ones
+  for (int j = tid; j < L; j += kThreads) {
+    const int64_t g = P.lnodes[nb + j];
+    if (j < nint) {
+      const double im = m.inv_mass[g];
+#pragma unroll
+      for (int i = 0; i < d; ++i) {
+        if (flags[j * d + i]) continue;  // blocked DOFs keep u, v, a
+        const int64_t k = g * d + i;
+        double r = fs[j * d + i];
+        if (FEXT) r += m.fext[k];
+        double u = us[j * d + i], v = vs[j * d + i], a = as[j * d + i];
+        fast::correct(dt, r, im, u, v, a);
+        m.u[k] = u;
+        m.v[k] = v;
+        m.a[k] = a;
+      }
+    } else {
+      const int64_t s = P.slot[nb + j];
+#pragma unroll
+      for (int i = 0; i < d; ++i) P.partial[s * d + i] = fs[j * d + i];
+    }
+  }
+}
+
+template <int D, bool FEXT>
+__global__ void k_shared_nodes(DevModel m, DevPatches P, double dt) {
+  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= P.nshared) return;
+  const int64_t g = P.snodes[s];
+  const int k0 = P.sptr[s], k1 = P.sptr[s + 1];
+  double f[3] = {0, 0, 0};
+  for (int k = k0; k < k1; ++k)
+#pragma unroll
+    for (int i = 0; i < D; ++i) f[i] += P.partial[(int64_t)k * D + i];
+  const double im = m.inv_mass[g];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    const int64_t k = g * D + i;
+    if (m.blocked[k]) continue;
+    double u = m.u[k], v = m.v[k], a = m.a[k];
+    fast::predict(dt, u, v, a);
+    double r = f[i];
+    if (FEXT) r += m.fext[k];
+    fast::correct(dt, r, im, u, v, a);
+    m.u[k] = u;
+    m.v[k] = v;
+    m.a[k] = a;
+  }
+}
+
+template <int T, typename S>
+cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool fext,
+                         cudaStream_t s) {
+  const SmemLayout lay = layout(p.max_nodes, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
+  if (fext)
+    k_patch_step<T, S, true><<<p.npatch, kThreads, lay.total, s>>>(m, p, dt);
+  else
+    k_patch_step<T, S, false><<<p.npatch, kThreads, lay.total, s>>>(m, p, dt);
+  return cudaGetLastError();
+}
+
+template <int T, typename S>
+cudaError_t configure(const DevPatches& p) {
+  const SmemLayout lay = layout(p.max_nodes, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
+  cudaError_t e = cudaFuncSetAttribute(k_patch_step<T, S, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_patch_step<T, S, false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total);
+}
+
+}  // namespace
+
+size_t patch_smem_bytes(const DevPatches& p, int dim, int nnpe, bool fp32, int threads) {
+  return layout(p.max_nodes, dim, nnpe, fp32 ? 4 : 8, threads).total;
+}
+
+cudaError_t patch_configure(const DevModel& m, const DevPatches& p, bool fp32) {
+  switch (m.type) {
+  case AKB_SEGMENT_2: return fp32 ? configure<AKB_SEGMENT_2, float>(p) : configure<AKB_SEGMENT_2, double>(p);
+  case AKB_TRIANGLE_3: return fp32 ? configure<AKB_TRIANGLE_3, float>(p) : configure<AKB_TRIANGLE_3, double>(p);
+  case AKB_TETRAHEDRON_4: return fp32 ? configure<AKB_TETRAHEDRON_4, float>(p) : configure<AKB_TETRAHEDRON_4, double>(p);
+  default: return fp32 ? configure<AKB_HEXAHEDRON_8, float>(p) : configure<AKB_HEXAHEDRON_8, double>(p);
+  }
+}
+
+cudaError_t patch_step(const DevModel& m, const DevPatches& p, double dt, bool fp32,
+                       bool fext, cudaStream_t s) {
+  if (p.npatch == 0) return cudaSuccess;
+  switch (m.type) {
+  case AKB_SEGMENT_2:
+    return fp32 ? launch_patch<AKB_SEGMENT_2, float>(m, p, dt, fext, s)
+                : launch_patch<AKB_SEGMENT_2, double>(m, p, dt, fext, s);
+  case AKB_TRIANGLE_3:
+    return fp32 ? launch_patch<AKB_TRIANGLE_3, float>(m, p, dt, fext, s)
+                : launch_patch<AKB_TRIANGLE_3, double>(m, p, dt, fext, s);
+  case AKB_TETRAHEDRON_4:
+    return fp32 ? launch_patch<AKB_TETRAHEDRON_4, float>(m, p, dt, fext, s)
+                : launch_patch<AKB_TETRAHEDRON_4, double>(m, p, dt, fext, s);
+  default:
+    return fp32 ? launch_patch<AKB_HEXAHEDRON_8, float>(m, p, dt, fext, s)
+                : launch_patch<AKB_HEXAHEDRON_8, double>(m, p, dt, fext, s);
+  }
+}
+
+cudaError_t patch_shared_nodes(const DevModel& m, const DevPatches& p, double dt, bool fext,
+                               cudaStream_t s) {
+  if (p.nshared == 0) return cudaSuccess;
+  const int blocks = (int)((p.nshared + kThreads - 1) / kThreads);
+  switch (m.dim) {
+  case 1: fext ? k_shared_nodes<1, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
+               : k_shared_nodes<1, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
+  case 2: fext ? k_shared_nodes<2, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
+               : k_shared_nodes<2, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
+  default: fext ? k_shared_nodes<3, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
+                : k_shared_nodes<3, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace akb
