@@ -81,6 +81,8 @@ class ModelOptions(C.Structure):
         ("precision_mode", C.c_int32),
         ("device", C.c_int32),
         ("stream", C.c_void_p),
+        ("patch_elements", C.c_int32),
+        ("patch_nodes", C.c_int32),
     ]
 
 

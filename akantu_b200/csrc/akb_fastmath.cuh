@@ -188,11 +188,59 @@ __device__ inline void stress_P(const MatParams& p, const S* g, S* P) {
     }
 }
 
+// Simplex (triangle_3, tetrahedron_4) internal force. The natural
+// derivatives are constant (dN_a/dxi_k = delta(a, k+1) - delta(a, 0)), so the
+// rows of J are X_a - X_0 (a >= 1) and w det J grad N_a = w adj(J)[:, a-1]:
+//   g = (1/det J) sum_a (u_a - u_0) (x) adj(J)[:, a-1],
+//   fe_a = w P adj(J)[:, a-1] (a >= 1), fe_0 = -(fe_1 + ... + fe_d).
+template <int T, typename S>
+__device__ inline void simplex_force(const MatParams& p, const S* dX, const S* du, S* fe) {
+  constexpr int d = ET<T>::dim;
+  S J[9], A[9];
+#pragma unroll
+  for (int k = 0; k < d; ++k)
+#pragma unroll
+    for (int j = 0; j < d; ++j) J[k * d + j] = dX[(k + 1) * d + j];
+  const S detJ = adjugate<d, S>(J, A);
+  const S idet = S(1) / detJ;
+  S g[9];
+#pragma unroll
+  for (int i = 0; i < d; ++i)
+#pragma unroll
+    for (int j = 0; j < d; ++j) {
+      S c = du[1 * d + i] * A[j * d + 0];
+#pragma unroll
+      for (int a = 2; a <= d; ++a) c += du[a * d + i] * A[j * d + (a - 1)];
+      g[i * d + j] = c * idet;
+    }
+  S P[9];
+  stress_P<d, S>(p, g, P);
+  const S w = S(weight<T>());
+#pragma unroll
+  for (int k = 0; k < d * d; ++k) P[k] *= w;
+#pragma unroll
+  for (int i = 0; i < d; ++i) fe[i] = 0;
+#pragma unroll
+  for (int a = 1; a <= d; ++a)
+#pragma unroll
+    for (int i = 0; i < d; ++i) {
+      S c = P[i * d + 0] * A[0 * d + (a - 1)];
+#pragma unroll
+      for (int j = 1; j < d; ++j) c += P[i * d + j] * A[j * d + (a - 1)];
+      fe[a * d + i] = c;
+      fe[i] -= c;
+    }
+}
+
 // Element internal force (without the -1 of the assembly):
 // fe[a*d + i] = sum_q w_q det J_q sum_j P_ij dN_a/dx_j.
 // dX[a*d+i] = X_a - X_0, du[a*d+i] = u_a - u_0 (entry a = 0 is zero).
 template <int T, typename S>
 __device__ inline void element_force(const MatParams& p, const S* dX, const S* du, S* fe) {
+  if (T == AKB_TRIANGLE_3 || T == AKB_TETRAHEDRON_4) {
+    simplex_force<T, S>(p, dX, du, fe);
+    return;
+  }
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe, nq = ET<T>::nqp;
 #pragma unroll
   for (int k = 0; k < d * n; ++k) fe[k] = 0;

@@ -47,6 +47,7 @@ struct akb_model {
   // fused patch step of the fast modes
   DevPatches patches{};
   bool use_patches = false;
+  int opt_patch_elements = 0, opt_patch_nodes = 0;
   // staging of akb_apply_dirichlet
   uint32_t* d_bc_nodes = nullptr;
   double* d_bc_values = nullptr;
@@ -173,6 +174,8 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
                                 const uint32_t* element_material) {
   int target, max_nodes;
   patch_params(m->dm.type, &target, &max_nodes);
+  if (m->opt_patch_elements > 0) target = std::min(m->opt_patch_elements, 8191);
+  if (m->opt_patch_nodes > 0) max_nodes = std::min(m->opt_patch_nodes, 65535);
   PatchHost P = build_patches(mesh->nodes, mesh->connectivity, mesh->nb_nodes,
                               mesh->nb_elements, m->dm.dim, m->dm.nnpe, target, max_nodes);
   DevPatches& d = m->patches;
@@ -314,13 +317,15 @@ akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
     if (!(md.rho > 0) || !(md.E > 0))
       return fail(AKB_ERR_INVALID_ARGUMENT, "material needs rho > 0 and E > 0");
   }
-  akb_model_options opt{AKB_MODE_FP64_REFERENCE, 0, nullptr};
+  akb_model_options opt{AKB_MODE_FP64_REFERENCE, 0, nullptr, 0, 0};
   if (options) opt = *options;
   if (opt.precision_mode < AKB_MODE_FP64_REFERENCE || opt.precision_mode > AKB_MODE_FP32_BULK)
     return fail(AKB_ERR_INVALID_ARGUMENT, "unknown precision mode");
 
   auto m = std::make_unique<akb_model>();
   m->mode = opt.precision_mode;
+  m->opt_patch_elements = opt.patch_elements;
+  m->opt_patch_nodes = opt.patch_nodes;
   m->device = opt.device;
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   if (opt.stream) {

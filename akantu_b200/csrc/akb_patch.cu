@@ -22,23 +22,24 @@ namespace {
 constexpr int kThreads = 256;
 
 struct SmemLayout {
-  size_t xs, us, vs, as, fs, contrib, flags, cursor, total;
+  size_t xs, us, fs, contrib, ents, cbeg, cursor, flags, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-__host__ __device__ inline SmemLayout layout(int L, int d, int n, int sbytes, int threads) {
+// max_nodes / max_elems: the patch caps; sbytes: element precision
+__host__ __device__ inline SmemLayout layout(int L, int E, int d, int n, int sbytes, int threads) {
   SmemLayout s;
   const size_t nd = (size_t)L * d * sizeof(double);
   s.xs = 0;
   s.us = align16(s.xs + nd);
-  s.vs = align16(s.us + nd);
-  s.as = align16(s.vs + nd);
-  s.fs = align16(s.as + nd);
+  s.fs = align16(s.us + nd);
   s.contrib = align16(s.fs + nd);
-  s.flags = align16(s.contrib + (size_t)threads * n * d * sbytes);
-  s.cursor = align16(s.flags + (size_t)L * d);
-  s.total = align16(s.cursor + (size_t)L * sizeof(uint16_t));
+  s.ents = align16(s.contrib + (size_t)threads * n * d * sbytes);
+  s.cbeg = align16(s.ents + (size_t)E * n * sizeof(uint16_t));
+  s.cursor = align16(s.cbeg + (size_t)(L + 1) * sizeof(uint16_t));
+  s.flags = align16(s.cursor + (size_t)L * sizeof(uint16_t));
+  s.total = align16(s.flags + (size_t)L * d);
   return s;
 }
 
@@ -52,49 +53,62 @@ __global__ void __launch_bounds__(kThreads) k_patch_step(DevModel m, DevPatches 
   const int eb = P.elem_ptr[p];
   const int ne = P.elem_ptr[p + 1] - eb;
   const int nint = P.ninterior[p];
-  const SmemLayout lay = layout(P.max_nodes, d, n, sizeof(S), kThreads);
+  const int nent = ne * n;
+  const SmemLayout lay = layout(P.max_nodes, P.max_elems, d, n, sizeof(S), kThreads);
   double* xs = reinterpret_cast<double*>(smem + lay.xs);
   double* us = reinterpret_cast<double*>(smem + lay.us);
-  double* vs = reinterpret_cast<double*>(smem + lay.vs);
-  double* as = reinterpret_cast<double*>(smem + lay.as);
   double* fs = reinterpret_cast<double*>(smem + lay.fs);
   S* contrib = reinterpret_cast<S*>(smem + lay.contrib);
-  uint8_t* flags = smem + lay.flags;
+  uint16_t* ents = reinterpret_cast<uint16_t*>(smem + lay.ents);
+  uint16_t* cbeg = reinterpret_cast<uint16_t*>(smem + lay.cbeg);
   uint16_t* cursor = reinterpret_cast<uint16_t*>(smem + lay.cursor);
+  uint8_t* flags = smem + lay.flags;
   const int tid = threadIdx.x;
 
-  // 1. stage nodes + predictor
+  // 1. stage the patch: CSR of (local element, corner) entries, node offsets,
+  //    and per (node, component) X, predicted u, blocked flag
+  const uint16_t* gent = P.centries + (size_t)eb * n;
+  for (int k = tid; k < nent; k += kThreads) ents[k] = gent[k];
   for (int j = tid; j < L; j += kThreads) {
-    const int64_t g = P.lnodes[nb + j];
-#pragma unroll
-    for (int i = 0; i < d; ++i) {
-      const int64_t k = g * d + i;
-      const double x = __ldg(&m.X[k]);
-      double u = m.u[k], v = m.v[k];
-      const double a = m.a[k];
-      const uint8_t b = m.blocked[k];
-      if (!b) fast::predict(dt, u, v, a);
-      xs[j * d + i] = x;
-      us[j * d + i] = u;
-      vs[j * d + i] = v;
-      as[j * d + i] = a;
-      fs[j * d + i] = 0.0;
-      flags[j * d + i] = b;
-    }
-    cursor[j] = P.cbeg[nb + j];
+    const uint16_t c = P.cbeg[nb + j];
+    cbeg[j] = c;
+    cursor[j] = c;
+  }
+  if (tid == 0) cbeg[L] = (uint16_t)nent;
+  for (int k = tid; k < L * d; k += kThreads) {
+    const int j = k / d, i = k - j * d;
+    const int64_t idx = (int64_t)P.lnodes[nb + j] * d + i;
+    const double x = __ldg(&m.X[idx]);
+    double u = m.u[idx], v = m.v[idx];
+    const double a = m.a[idx];
+    const uint8_t b = m.blocked[idx];
+    if (!b) fast::predict(dt, u, v, a);
+    xs[k] = x;
+    us[k] = u;
+    fs[k] = 0.0;
+    flags[k] = b;
   }
   __syncthreads();
 
-  // 2. element forces, chunk by chunk
-  const uint16_t* ent = P.centries + (size_t)eb * n;
-  const int nent = ne * n;
+  // 2. element forces, chunk by chunk; each chunk's vectors added per node in
+  //    ascending local element order
   for (int c0 = 0; c0 < ne; c0 += kThreads) {
     const int el = c0 + tid;
     if (el < ne) {
       const size_t ge = (size_t)eb + el;
       int lc[n];
+      if (n == 4) {
+        const uint2 w = *reinterpret_cast<const uint2*>(P.lconn + ge * 4);
+        lc[0] = w.x & 0xffff; lc[1] = w.x >> 16; lc[2] = w.y & 0xffff; lc[3 % n] = w.y >> 16;
+      } else if (n == 8) {
+        const uint4 w = *reinterpret_cast<const uint4*>(P.lconn + ge * 8);
+        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-      for (int a = 0; a < n; ++a) lc[a] = P.lconn[ge * n + a];
+        for (int a = 0; a < n; ++a) lc[a] = (ws[a / 2] >> (16 * (a & 1))) & 0xffff;
+      } else {
+#pragma unroll
+        for (int a = 0; a < n; ++a) lc[a] = P.lconn[ge * n + a];
+      }
       const MatParams& mp = m.mats[P.emat ? P.emat[ge] : 0];
       S dX[3 * 8], du[3 * 8];
 #pragma unroll
@@ -118,10 +132,10 @@ __global__ void __launch_bounds__(kThreads) k_patch_step(DevModel m, DevPatches 
     const int c1 = c0 + kThreads < ne ? c0 + kThreads : ne;
     for (int j = tid; j < L; j += kThreads) {
       int c = cursor[j];
-      const int end = (j + 1 < L) ? P.cbeg[nb + j + 1] : nent;
+      const int end = cbeg[j + 1];
       double f[3] = {fs[j * d], d > 1 ? fs[j * d + 1] : 0.0, d > 2 ? fs[j * d + 2] : 0.0};
       while (c < end) {
-        const int e = ent[c];
+        const int e = ents[c];
         const int le = e >> 3;
         if (le >= c1) break;
         const S* src = contrib + ((le - c0) * n + (e & 7)) * d;
@@ -136,27 +150,24 @@ __global__ void __launch_bounds__(kThreads) k_patch_step(DevModel m, DevPatches 
     __syncthreads();
   }
 
-  // 3. finish the nodes of this patch, hand out the shared ones
-  for (int j = tid; j < L; j += kThreads) {
-    const int64_t g = P.lnodes[nb + j];
+  // 3. finish the nodes of this patch (state re-read, predictor recomputed
+  //    bit for bit), hand out the shared ones
+  for (int k = tid; k < L * d; k += kThreads) {
+    const int j = k / d, i = k - j * d;
     if (j < nint) {
-      const double im = m.inv_mass[g];
-#pragma unroll
-      for (int i = 0; i < d; ++i) {
-        if (flags[j * d + i]) continue;  // blocked DOFs keep u, v, a
-        const int64_t k = g * d + i;
-        double r = fs[j * d + i];
-        if (FEXT) r += m.fext[k];
-        double u = us[j * d + i], v = vs[j * d + i], a = as[j * d + i];
-        fast::correct(dt, r, im, u, v, a);
-        m.u[k] = u;
-        m.v[k] = v;
-        m.a[k] = a;
-      }
+      if (flags[k]) continue;  // blocked DOFs keep u, v, a
+      const int64_t g = P.lnodes[nb + j];
+      const int64_t idx = g * d + i;
+      double u = m.u[idx], v = m.v[idx], a = m.a[idx];
+      fast::predict(dt, u, v, a);
+      double r = fs[k];
+      if (FEXT) r += m.fext[idx];
+      fast::correct(dt, r, m.inv_mass[g], u, v, a);
+      m.u[idx] = u;
+      m.v[idx] = v;
+      m.a[idx] = a;
     } else {
-      const int64_t s = P.slot[nb + j];
-#pragma unroll
-      for (int i = 0; i < d; ++i) P.partial[s * d + i] = fs[j * d + i];
+      P.partial[(int64_t)P.slot[nb + j] * d + i] = fs[k];
     }
   }
 }
@@ -190,7 +201,7 @@ __global__ void k_shared_nodes(DevModel m, DevPatches P, double dt) {
 template <int T, typename S>
 cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool fext,
                          cudaStream_t s) {
-  const SmemLayout lay = layout(p.max_nodes, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
+  const SmemLayout lay = layout(p.max_nodes, p.max_elems, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
   if (fext)
     k_patch_step<T, S, true><<<p.npatch, kThreads, lay.total, s>>>(m, p, dt);
   else
@@ -200,7 +211,7 @@ cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool
 
 template <int T, typename S>
 cudaError_t configure(const DevPatches& p) {
-  const SmemLayout lay = layout(p.max_nodes, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
+  const SmemLayout lay = layout(p.max_nodes, p.max_elems, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
   cudaError_t e = cudaFuncSetAttribute(k_patch_step<T, S, true>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total);
   if (e != cudaSuccess) return e;
@@ -211,7 +222,7 @@ cudaError_t configure(const DevPatches& p) {
 }  // namespace
 
 size_t patch_smem_bytes(const DevPatches& p, int dim, int nnpe, bool fp32, int threads) {
-  return layout(p.max_nodes, dim, nnpe, fp32 ? 4 : 8, threads).total;
+  return layout(p.max_nodes, p.max_elems, dim, nnpe, fp32 ? 4 : 8, threads).total;
 }
 
 cudaError_t patch_configure(const DevModel& m, const DevPatches& p, bool fp32) {

@@ -83,7 +83,8 @@ class SolidMechanicsModel:
     """The explicit lumped-mass SolidMechanicsModel on one GPU."""
 
     def __init__(self, mesh, materials=None, element_material=None,
-                 precision=_abi.MODE_FP64_REFERENCE, device=0, stream=None):
+                 precision=_abi.MODE_FP64_REFERENCE, device=0, stream=None,
+                 patch_elements=0, patch_nodes=0):
         self.mesh = mesh
         self.dim, self.nnpe, self.nqp = element_properties(mesh.element_type)
         self._materials = list(materials) if materials else []
@@ -91,6 +92,7 @@ class SolidMechanicsModel:
         self._precision = precision
         self._device = device
         self._stream = stream
+        self._patch = (int(patch_elements), int(patch_nodes))
         self._h = None
         self._mirrors = {}
         self._checked_out = set()
@@ -119,7 +121,7 @@ class SolidMechanicsModel:
         if self._element_material is not None:
             self._em = np.ascontiguousarray(self._element_material, dtype=np.uint32)
             em = self._em.ctypes.data_as(C.POINTER(C.c_uint32))
-        opt = _abi.ModelOptions(self._precision, self._device, self._stream)
+        opt = _abi.ModelOptions(self._precision, self._device, self._stream, *self._patch)
         h = C.c_void_p()
         check(L.akb_model_create(C.byref(desc), len(self._materials), mats, em,
                                  C.byref(opt), C.byref(h)))

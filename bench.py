@@ -256,7 +256,7 @@ def run_ours(args, dist):
     import torch
     device = dist.local_rank
     torch.cuda.set_device(device)
-    w = configs.cube_tet4()
+    w = configs.cube_tet4(args.cells)
     E = w["mesh"].getNbElement()
     peak, peak_kind = load_peaks()
     m = make_model(w, _abi.MODE_FP64, device)
@@ -299,9 +299,9 @@ def run_ours(args, dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "cube_tet4: 100^3 cells x 6 tetrahedron_4 (6,000,000 "
-                                   "elements, 1,030,301 nodes), linear elastic, FP64, "
-                                   "dt = 0.8 x stable", "elements": E,
+            "config": {"workload": "cube_tet4: %d^3 cells x 6 tetrahedron_4 (%d elements, "
+                                   "%d nodes), linear elastic, FP64, dt = 0.8 x stable"
+                                   % (args.cells, E, w["mesh"].getNbNodes()), "elements": E,
                        "nodes": w["mesh"].getNbNodes(), "time_step": dt,
                        "parallelism": "replicas" if dist.world > 1 else "single GPU",
                        "l2": "no flush: per-step working set %.0f MB > 126 MB L2" % (balg / 1e6)},
@@ -362,6 +362,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cells", type=int, default=100,
+                    help="cells per cube side (100 = the benchmark; smaller for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -382,7 +384,7 @@ def main():
     try:
         res = run_ours(args, dist)
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-            res["cpu_baseline"] = cpu_baseline(configs.cube_tet4())
+            res["cpu_baseline"] = cpu_baseline(configs.cube_tet4(args.cells))
         if dist.rank == 0:
             print(json.dumps(res), flush=True)
     finally:

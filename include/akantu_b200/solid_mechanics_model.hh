@@ -1,0 +1,249 @@
+// solid_mechanics_model.hh -- header-only C++ shim over include/akb.h that
+// keeps the reference's names for the explicit path, so that code written
+// against akantu::SolidMechanicsModel (solid_mechanics_model.hh:58) compiles
+// with `using namespace akantu_b200;` and runs on the GPU:
+//
+//   Mesh mesh(3); ...                               // mesh.hh:100
+//   SolidMechanicsModel model(mesh);                // solid_mechanics_model.hh:85-88
+//   model.addMaterial(MaterialElastic(rho, E, nu)); // material input file section
+//   model.initFull(_analysis_method = _explicit_lumped_mass);  // model.hh:78-99
+//   model.setTimeStep(0.8 * model.getStableTimeStep());
+//   auto & u = model.getDisplacement();  u(n, 0) = ...;   // Array<Real> rows
+//   model.applyBC(BC::Dirichlet::FixedValue(0., _x), nodes);
+//   model.solveStep();
+//   Real ekin = model.getEnergy("kinetic");
+//
+// Nodal arrays returned by reference are host mirrors of the device state:
+// they are refreshed on every get*() call and written back before the next
+// call that uses the state, so in-place edits reach the model as with the
+// reference's model-owned arrays. Errors throw akantu_b200::Exception.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../akb.h"
+
+namespace akantu_b200 {
+
+using Real = double;
+using UInt = unsigned int;
+
+enum AnalysisMethod { _explicit_lumped_mass = 0 };
+enum SpatialDirection { _x = 0, _y = 1, _z = 2 };
+enum ElementType {
+  _segment_2 = AKB_SEGMENT_2,
+  _triangle_3 = AKB_TRIANGLE_3,
+  _tetrahedron_4 = AKB_TETRAHEDRON_4,
+  _hexahedron_8 = AKB_HEXAHEDRON_8
+};
+struct AnalysisMethodArg {
+  AnalysisMethod value;
+};
+struct AnalysisMethodTag {
+  AnalysisMethodArg operator=(AnalysisMethod m) const { return {m}; }
+};
+static constexpr AnalysisMethodTag _analysis_method{};
+
+class Exception : public std::runtime_error {
+ public:
+  Exception(akb_status s, const std::string& what) : std::runtime_error(what), status(s) {}
+  akb_status status;
+};
+
+inline void check(akb_status s) {
+  if (s != AKB_OK) throw Exception(s, akb_last_error());
+}
+
+// Row-major table with the reference Array<T> accessors (aka_array.hh:139-224).
+template <typename T>
+class Array {
+ public:
+  Array() = default;
+  Array(UInt rows, UInt cols, T value = T()) : rows_(rows), cols_(cols), v_(rows * cols, value) {}
+  T& operator()(UInt i, UInt j = 0) { return v_[i * cols_ + j]; }
+  const T& operator()(UInt i, UInt j = 0) const { return v_[i * cols_ + j]; }
+  UInt size() const { return rows_; }
+  UInt getNbComponent() const { return cols_; }
+  T* storage() { return v_.data(); }
+  const T* storage() const { return v_.data(); }
+  void set(T value) { std::fill(v_.begin(), v_.end(), value); }
+  void resize(UInt rows, UInt cols) {
+    rows_ = rows;
+    cols_ = cols;
+    v_.resize(rows * cols);
+  }
+
+ private:
+  UInt rows_ = 0, cols_ = 0;
+  std::vector<T> v_;
+};
+
+class Mesh {
+ public:
+  explicit Mesh(UInt spatial_dimension) : dim_(spatial_dimension), nodes_(0, spatial_dimension) {}
+  Array<Real>& getNodes() { return nodes_; }
+  const Array<Real>& getNodes() const { return nodes_; }
+  Array<uint32_t>& getConnectivity() { return conn_; }
+  const Array<uint32_t>& getConnectivity() const { return conn_; }
+  UInt getSpatialDimension() const { return dim_; }
+  UInt getNbNodes() const { return nodes_.size(); }
+  UInt getNbElement() const { return conn_.size(); }
+  ElementType getElementType() const { return type_; }
+  void setElementType(ElementType t) {
+    type_ = t;
+    conn_.resize(conn_.size(), t == _segment_2 ? 2 : t == _triangle_3 ? 3 : t == _tetrahedron_4 ? 4 : 8);
+  }
+
+ private:
+  UInt dim_;
+  ElementType type_ = _triangle_3;
+  Array<Real> nodes_;
+  Array<uint32_t> conn_;
+};
+
+// material elastic [ rho, E, nu, Plane_Stress, finite_deformation ]
+struct MaterialElastic {
+  MaterialElastic(Real rho, Real E, Real nu, bool plane_stress = false, bool finite = false)
+      : desc{AKB_MATERIAL_ELASTIC, plane_stress, finite, 0, rho, E, nu} {}
+  akb_material_desc desc;
+};
+// material neohookean [ rho, E, nu ]
+struct MaterialNeohookean {
+  MaterialNeohookean(Real rho, Real E, Real nu) : desc{AKB_MATERIAL_NEOHOOKEAN, 0, 1, 0, rho, E, nu} {}
+  akb_material_desc desc;
+};
+
+namespace BC {
+namespace Dirichlet {
+// FixedValue (boundary_condition_functor.hh): blocks one component and sets it.
+struct FixedValue {
+  FixedValue(Real value, SpatialDirection axis) : value(value), axis(axis) {}
+  Real value;
+  SpatialDirection axis;
+};
+}  // namespace Dirichlet
+}  // namespace BC
+
+class SolidMechanicsModel {
+ public:
+  explicit SolidMechanicsModel(Mesh& mesh, int precision = AKB_MODE_FP64, int device = 0)
+      : mesh_(mesh), precision_(precision), device_(device) {}
+  ~SolidMechanicsModel() {
+    if (h_) akb_model_destroy(h_);
+  }
+  SolidMechanicsModel(const SolidMechanicsModel&) = delete;
+  SolidMechanicsModel& operator=(const SolidMechanicsModel&) = delete;
+
+  template <class M>
+  void addMaterial(const M& m) {
+    mats_.push_back(m.desc);
+  }
+  void setMaterialIndex(const std::vector<uint32_t>& per_element) { element_material_ = per_element; }
+
+  void initFull(AnalysisMethodArg arg = {_explicit_lumped_mass}) {
+    if (arg.value != _explicit_lumped_mass) throw Exception(AKB_ERR_UNSUPPORTED, "explicit only");
+    akb_mesh_desc md{(int32_t)mesh_.getSpatialDimension(), (int32_t)mesh_.getElementType(),
+                     (int64_t)mesh_.getNbNodes(), (int64_t)mesh_.getNbElement(),
+                     mesh_.getNodes().storage(), mesh_.getConnectivity().storage()};
+    akb_model_options opt{precision_, device_, nullptr};
+    check(akb_model_create(&md, (int32_t)mats_.size(), mats_.data(),
+                           element_material_.empty() ? nullptr : element_material_.data(), &opt,
+                           &h_));
+    const UInt n = mesh_.getNbNodes(), d = mesh_.getSpatialDimension();
+    for (auto* a : {&u_, &v_, &acc_, &fext_, &fint_, &mass_}) a->resize(n, d);
+    blocked_.resize(n, d);
+  }
+
+  Real getStableTimeStep() {
+    sync_in();
+    Real dt;
+    check(akb_get_stable_time_step(h_, &dt));
+    return dt;
+  }
+  void setTimeStep(Real dt) { check(akb_set_time_step(h_, dt)); }
+  Real getTimeStep() const {
+    Real dt;
+    check(akb_get_time_step(h_, &dt));
+    return dt;
+  }
+  void solveStep() {
+    sync_in();
+    check(akb_solve_step(h_));
+  }
+  void solveSteps(int64_t n) {
+    sync_in();
+    check(akb_solve_steps(h_, n));
+  }
+  void assembleMassLumped() { check(akb_assemble_mass_lumped(h_)); }
+  void assembleInternalForces() {
+    sync_in();
+    check(akb_assemble_internal_forces(h_));
+  }
+
+  Array<Real>& getDisplacement() { return pull(AKB_FIELD_DISPLACEMENT, u_, true); }
+  Array<Real>& getVelocity() { return pull(AKB_FIELD_VELOCITY, v_, true); }
+  Array<Real>& getAcceleration() { return pull(AKB_FIELD_ACCELERATION, acc_, true); }
+  Array<Real>& getExternalForce() { return pull(AKB_FIELD_EXTERNAL_FORCE, fext_, true); }
+  const Array<Real>& getInternalForce() { return pull(AKB_FIELD_INTERNAL_FORCE, fint_, false); }
+  const Array<Real>& getMass() { return pull(AKB_FIELD_MASS, mass_, false); }
+  Array<uint8_t>& getBlockedDOFs() {
+    sync_in();
+    check(akb_get_blocked_dofs(h_, blocked_.storage(), (int64_t)blocked_.size() * blocked_.getNbComponent()));
+    blocked_out_ = true;
+    return blocked_;
+  }
+
+  // applyBC(FixedValue, group): the group is given as its node list
+  void applyBC(const BC::Dirichlet::FixedValue& f, const std::vector<uint32_t>& nodes) {
+    sync_in();
+    std::vector<Real> vals(nodes.size(), f.value);
+    check(akb_apply_dirichlet(h_, nodes.data(), (int64_t)nodes.size(), f.axis, vals.data()));
+  }
+
+  Real getEnergy(const std::string& id) {
+    sync_in();
+    int32_t kind = id == "kinetic" ? AKB_ENERGY_KINETIC
+                 : id == "potential" ? AKB_ENERGY_POTENTIAL
+                 : id == "external work" ? AKB_ENERGY_EXTERNAL_WORK : -1;
+    if (kind < 0) throw Exception(AKB_ERR_INVALID_ARGUMENT, "unknown energy " + id);
+    Real e;
+    check(akb_get_energy(h_, kind, &e));
+    return e;
+  }
+
+  akb_model* handle() { return h_; }
+
+ private:
+  Array<Real>& pull(int32_t field, Array<Real>& a, bool writable) {
+    sync_in();
+    check(akb_get_field(h_, field, a.storage(), (int64_t)a.size() * a.getNbComponent()));
+    if (writable) out_.push_back({field, &a});
+    return a;
+  }
+  void sync_in() {
+    for (auto& o : out_)
+      check(akb_set_field(h_, o.first, o.second->storage(),
+                          (int64_t)o.second->size() * o.second->getNbComponent()));
+    out_.clear();
+    if (blocked_out_) {
+      check(akb_set_blocked_dofs(h_, blocked_.storage(),
+                                 (int64_t)blocked_.size() * blocked_.getNbComponent()));
+      blocked_out_ = false;
+    }
+  }
+
+  Mesh& mesh_;
+  int precision_, device_;
+  akb_model* h_ = nullptr;
+  std::vector<akb_material_desc> mats_;
+  std::vector<uint32_t> element_material_;
+  Array<Real> u_, v_, acc_, fext_, fint_, mass_;
+  Array<uint8_t> blocked_;
+  bool blocked_out_ = false;
+  std::vector<std::pair<int32_t, Array<Real>*>> out_;
+};
+
+}  // namespace akantu_b200

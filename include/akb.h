@@ -113,6 +113,8 @@ typedef struct {
   int32_t precision_mode; /* AKB_MODE_* */
   int32_t device;         /* CUDA device ordinal */
   void* stream;           /* cudaStream_t to run on; NULL = library-owned stream */
+  int32_t patch_elements; /* fast modes: elements per patch (0 = per-type default) */
+  int32_t patch_nodes;    /* fast modes: node cap of a patch (0 = per-type default) */
 } akb_model_options;
 
 typedef struct {
