@@ -22,12 +22,14 @@ namespace {
 constexpr int kThreads = 256;
 
 struct SmemLayout {
-  size_t xs, us, fs, contrib, ents, cbeg, cursor, flags, total;
+  size_t xs, us, fs, contrib, lcs, ents, cbeg, cursor, flags, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-// max_nodes / max_elems: the patch caps; sbytes: element precision
+// Shared-memory layout for patch caps L (nodes) and E (elements). Node
+// arrays are component-major ([i][j]) and the chunk of element vectors is
+// entry-major ([k][thread]), so warps touch consecutive words.
 __host__ __device__ inline SmemLayout layout(int L, int E, int d, int n, int sbytes, int threads) {
   SmemLayout s;
   const size_t nd = (size_t)L * d * sizeof(double);
@@ -35,16 +37,37 @@ __host__ __device__ inline SmemLayout layout(int L, int E, int d, int n, int sby
   s.us = align16(s.xs + nd);
   s.fs = align16(s.us + nd);
   s.contrib = align16(s.fs + nd);
-  s.ents = align16(s.contrib + (size_t)threads * n * d * sbytes);
+  s.lcs = align16(s.contrib + (size_t)threads * n * d * sbytes);
+  s.ents = align16(s.lcs + (size_t)E * n * sizeof(uint16_t));
   s.cbeg = align16(s.ents + (size_t)E * n * sizeof(uint16_t));
   s.cursor = align16(s.cbeg + (size_t)(L + 1) * sizeof(uint16_t));
-  s.flags = align16(s.cursor + (size_t)L * sizeof(uint16_t));
+  s.flags = align16(s.cursor + (size_t)L * d * sizeof(uint16_t));
   s.total = align16(s.flags + (size_t)L * d);
   return s;
 }
 
+// Copies count uint16 from global to shared memory, 4 bytes at a time when
+// both ends allow it.
+__device__ inline void copy_u16(uint16_t* dst, const uint16_t* src, int count, int tid, int nt) {
+  if ((reinterpret_cast<uintptr_t>(src) & 3) == 0) {
+    const int pairs = count >> 1;
+    const uint32_t* s4 = reinterpret_cast<const uint32_t*>(src);
+    uint32_t* d4 = reinterpret_cast<uint32_t*>(dst);
+    for (int k = tid; k < pairs; k += nt) d4[k] = s4[k];
+    if ((count & 1) && tid == 0) dst[count - 1] = src[count - 1];
+  } else {
+    for (int k = tid; k < count; k += nt) dst[k] = src[k];
+  }
+}
+
+// CTAs per SM each instantiation is built for (register budget).
+template <int T, typename S> struct PatchOccupancy { static constexpr int value = 3; };
+template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, float> { static constexpr int value = 2; };
+template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, double> { static constexpr int value = 1; };
+
 template <int T, typename S, bool FEXT>
-__global__ void __launch_bounds__(kThreads) k_patch_step(DevModel m, DevPatches P, double dt) {
+__global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
+    k_patch_step(DevModel m, DevPatches P, double dt) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
   extern __shared__ __align__(16) unsigned char smem[];
   const int p = blockIdx.x;
@@ -54,26 +77,24 @@ __global__ void __launch_bounds__(kThreads) k_patch_step(DevModel m, DevPatches 
   const int ne = P.elem_ptr[p + 1] - eb;
   const int nint = P.ninterior[p];
   const int nent = ne * n;
+  const int LM = P.max_nodes;  // row stride of the component-major arrays
   const SmemLayout lay = layout(P.max_nodes, P.max_elems, d, n, sizeof(S), kThreads);
   double* xs = reinterpret_cast<double*>(smem + lay.xs);
   double* us = reinterpret_cast<double*>(smem + lay.us);
   double* fs = reinterpret_cast<double*>(smem + lay.fs);
   S* contrib = reinterpret_cast<S*>(smem + lay.contrib);
+  uint16_t* lcs = reinterpret_cast<uint16_t*>(smem + lay.lcs);
   uint16_t* ents = reinterpret_cast<uint16_t*>(smem + lay.ents);
   uint16_t* cbeg = reinterpret_cast<uint16_t*>(smem + lay.cbeg);
   uint16_t* cursor = reinterpret_cast<uint16_t*>(smem + lay.cursor);
   uint8_t* flags = smem + lay.flags;
   const int tid = threadIdx.x;
 
-  // 1. stage the patch: CSR of (local element, corner) entries, node offsets,
-  //    and per (node, component) X, predicted u, blocked flag
-  const uint16_t* gent = P.centries + (size_t)eb * n;
-  for (int k = tid; k < nent; k += kThreads) ents[k] = gent[k];
-  for (int j = tid; j < L; j += kThreads) {
-    const uint16_t c = P.cbeg[nb + j];
-    cbeg[j] = c;
-    cursor[j] = c;
-  }
+  // 1. stage the patch: local connectivity, CSR of (local element, corner)
+  //    entries, node offsets; per (node, component) X, predicted u, flag
+  copy_u16(lcs, P.lconn + (size_t)eb * n, nent, tid, kThreads);
+  copy_u16(ents, P.centries + (size_t)eb * n, nent, tid, kThreads);
+  for (int j = tid; j < L; j += kThreads) cbeg[j] = P.cbeg[nb + j];
   if (tid == 0) cbeg[L] = (uint16_t)nent;
   for (int k = tid; k < L * d; k += kThreads) {
     const int j = k / d, i = k - j * d;
@@ -83,69 +104,57 @@ __global__ void __launch_bounds__(kThreads) k_patch_step(DevModel m, DevPatches 
     const double a = m.a[idx];
     const uint8_t b = m.blocked[idx];
     if (!b) fast::predict(dt, u, v, a);
-    xs[k] = x;
-    us[k] = u;
-    fs[k] = 0.0;
+    xs[i * LM + j] = x;
+    us[i * LM + j] = u;
+    fs[i * LM + j] = 0.0;
     flags[k] = b;
   }
   __syncthreads();
+  for (int q = tid; q < L * d; q += kThreads) cursor[q] = cbeg[q % L];
+  // (cursor[q] belongs to item q = i * L + j; visible after the first barrier below)
 
-  // 2. element forces, chunk by chunk; each chunk's vectors added per node in
-  //    ascending local element order
+  // 2. element forces, chunk by chunk; each chunk's vectors added per
+  //    (node, component) in ascending local element order
   for (int c0 = 0; c0 < ne; c0 += kThreads) {
     const int el = c0 + tid;
     if (el < ne) {
-      const size_t ge = (size_t)eb + el;
       int lc[n];
-      if (n == 4) {
-        const uint2 w = *reinterpret_cast<const uint2*>(P.lconn + ge * 4);
-        lc[0] = w.x & 0xffff; lc[1] = w.x >> 16; lc[2] = w.y & 0xffff; lc[3 % n] = w.y >> 16;
-      } else if (n == 8) {
-        const uint4 w = *reinterpret_cast<const uint4*>(P.lconn + ge * 8);
-        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-        for (int a = 0; a < n; ++a) lc[a] = (ws[a / 2] >> (16 * (a & 1))) & 0xffff;
-      } else {
-#pragma unroll
-        for (int a = 0; a < n; ++a) lc[a] = P.lconn[ge * n + a];
-      }
-      const MatParams& mp = m.mats[P.emat ? P.emat[ge] : 0];
+      for (int a = 0; a < n; ++a) lc[a] = lcs[el * n + a];
+      const MatParams& mp = m.mats[P.emat ? P.emat[(size_t)eb + el] : 0];
       S dX[3 * 8], du[3 * 8];
 #pragma unroll
       for (int i = 0; i < d; ++i) {
         dX[i] = 0;
         du[i] = 0;
-      }
+        const double x0 = xs[i * LM + lc[0]], u0 = us[i * LM + lc[0]];
 #pragma unroll
-      for (int a = 1; a < n; ++a)
-#pragma unroll
-        for (int i = 0; i < d; ++i) {
-          dX[a * d + i] = S(xs[lc[a] * d + i] - xs[lc[0] * d + i]);
-          du[a * d + i] = S(us[lc[a] * d + i] - us[lc[0] * d + i]);
+        for (int a = 1; a < n; ++a) {
+          dX[a * d + i] = S(xs[i * LM + lc[a]] - x0);
+          du[a * d + i] = S(us[i * LM + lc[a]] - u0);
         }
+      }
       S fe[3 * 8];
       fast::element_force<T, S>(mp, dX, du, fe);
 #pragma unroll
-      for (int k = 0; k < n * d; ++k) contrib[tid * n * d + k] = fe[k];
+      for (int k = 0; k < n * d; ++k) contrib[k * kThreads + tid] = fe[k];
     }
     __syncthreads();
     const int c1 = c0 + kThreads < ne ? c0 + kThreads : ne;
-    for (int j = tid; j < L; j += kThreads) {
-      int c = cursor[j];
+    for (int q = tid; q < L * d; q += kThreads) {
+      const int i = q / L, j = q - i * L;
+      int c = cursor[q];
       const int end = cbeg[j + 1];
-      double f[3] = {fs[j * d], d > 1 ? fs[j * d + 1] : 0.0, d > 2 ? fs[j * d + 2] : 0.0};
+      double f = fs[i * LM + j];
       while (c < end) {
         const int e = ents[c];
         const int le = e >> 3;
         if (le >= c1) break;
-        const S* src = contrib + ((le - c0) * n + (e & 7)) * d;
-#pragma unroll
-        for (int i = 0; i < d; ++i) f[i] -= double(src[i]);
+        f -= double(contrib[((e & 7) * d + i) * kThreads + (le - c0)]);
         ++c;
       }
-      cursor[j] = (uint16_t)c;
-#pragma unroll
-      for (int i = 0; i < d; ++i) fs[j * d + i] = f[i];
+      cursor[q] = (uint16_t)c;
+      fs[i * LM + j] = f;
     }
     __syncthreads();
   }
@@ -154,20 +163,21 @@ __global__ void __launch_bounds__(kThreads) k_patch_step(DevModel m, DevPatches 
   //    bit for bit), hand out the shared ones
   for (int k = tid; k < L * d; k += kThreads) {
     const int j = k / d, i = k - j * d;
+    const double f = fs[i * LM + j];
     if (j < nint) {
       if (flags[k]) continue;  // blocked DOFs keep u, v, a
       const int64_t g = P.lnodes[nb + j];
       const int64_t idx = g * d + i;
       double u = m.u[idx], v = m.v[idx], a = m.a[idx];
       fast::predict(dt, u, v, a);
-      double r = fs[k];
+      double r = f;
       if (FEXT) r += m.fext[idx];
       fast::correct(dt, r, m.inv_mass[g], u, v, a);
       m.u[idx] = u;
       m.v[idx] = v;
       m.a[idx] = a;
     } else {
-      P.partial[(int64_t)P.slot[nb + j] * d + i] = fs[k];
+      P.partial[(int64_t)P.slot[nb + j] * d + i] = f;
     }
   }
 }
