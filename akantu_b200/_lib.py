@@ -47,6 +47,7 @@ SIGNATURES = {
     "akb_apply_dirichlet": (I32, [P, PU32, I64, I32, PD]),
     "akb_time_kernels": (I32, [P, I64, PD, I32]),
     "akb_kernel_name": (C.c_char_p, [P, I32]),
+    "akb_kinetic_energy_static": (I32, [P, P, I64, I32, P, P]),
     "akb_synchronize": (I32, [P]),
 }
 

@@ -213,6 +213,22 @@ akb_status akb_time_kernels(akb_model* model, int64_t nb_steps,
 /* Name of the step's k-th kernel, or "" past the last one. */
 const char* akb_kernel_name(const akb_model* model, int32_t slot);
 
+/* Kinetic energy 1/2 sum(m v^2) of device arrays, allocating no memory.
+ * No counterpart in the reference: it serves callers that cannot call
+ * cudaMalloc mid-run (inside CUDA stream capture, or under a device-memory
+ * budget owned by another allocator). mass and velocity are device arrays of
+ * nb_nodes x spatial_dimension doubles (e.g. from akb_field_device_pointer),
+ * result a device double the caller provides; work is queued on stream
+ * (cudaStream_t, NULL = default stream) and not waited for. The partial sums
+ * use a fixed 16 KiB array inside the library, held by every GPU that loads
+ * it until exit: nb_nodes above 8 388 608 is rejected
+ * (AKB_ERR_INVALID_ARGUMENT); calls that overlap on the GPU race on that
+ * array; its device address is looked up on the first call per device, which
+ * should therefore come before any stream capture. */
+akb_status akb_kinetic_energy_static(const double* mass, const double* velocity,
+                                     int64_t nb_nodes, int32_t spatial_dimension,
+                                     double* result, void* stream);
+
 /* Waits for all work queued on the model's stream. */
 akb_status akb_synchronize(akb_model* model);
 
