@@ -189,8 +189,12 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
   if ((st = upload(m, P.ninterior, &d.ninterior)) != AKB_OK) return st;
   if ((st = upload(m, P.lnodes, &d.lnodes)) != AKB_OK) return st;
   if ((st = upload(m, P.lconn, &d.lconn)) != AKB_OK) return st;
-  if ((st = upload(m, P.cbeg, &d.cbeg)) != AKB_OK) return st;
-  if ((st = upload(m, P.centries, &d.centries)) != AKB_OK) return st;
+  d.cbeg = nullptr;
+  d.centries = nullptr;
+  if ((st = upload(m, P.cslot, &d.cslot)) != AKB_OK) return st;
+  if ((st = upload(m, P.segs, &d.segs)) != AKB_OK) return st;
+  if ((st = upload(m, P.seg_ptr, &d.seg_ptr)) != AKB_OK) return st;
+  if ((st = upload(m, P.chunk_base, &d.chunk_base)) != AKB_OK) return st;
   if ((st = upload(m, P.slot, &d.slot)) != AKB_OK) return st;
   if ((st = upload(m, P.snodes, &d.snodes)) != AKB_OK) return st;
   if ((st = upload(m, P.sptr, &d.sptr)) != AKB_OK) return st;

@@ -22,14 +22,14 @@ namespace {
 constexpr int kThreads = 256;
 
 struct SmemLayout {
-  size_t xs, us, fs, contrib, lcs, ents, cbeg, cursor, flags, total;
+  size_t xs, us, fs, contrib, lcs, slots, flags, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 // Shared-memory layout for patch caps L (nodes) and E (elements). Node
-// arrays are component-major ([i][j]) and the chunk of element vectors is
-// entry-major ([k][thread]), so warps touch consecutive words.
+// arrays are component-major ([i][j]); the chunk's element vectors are stored
+// at their sorted slots, component-major ([i][slot]).
 __host__ __device__ inline SmemLayout layout(int L, int E, int d, int n, int sbytes, int threads) {
   SmemLayout s;
   const size_t nd = (size_t)L * d * sizeof(double);
@@ -38,16 +38,14 @@ __host__ __device__ inline SmemLayout layout(int L, int E, int d, int n, int sby
   s.fs = align16(s.us + nd);
   s.contrib = align16(s.fs + nd);
   s.lcs = align16(s.contrib + (size_t)threads * n * d * sbytes);
-  s.ents = align16(s.lcs + (size_t)E * n * sizeof(uint16_t));
-  s.cbeg = align16(s.ents + (size_t)E * n * sizeof(uint16_t));
-  s.cursor = align16(s.cbeg + (size_t)(L + 1) * sizeof(uint16_t));
-  s.flags = align16(s.cursor + (size_t)L * d * sizeof(uint16_t));
+  s.slots = align16(s.lcs + (size_t)E * n * sizeof(uint16_t));
+  s.flags = align16(s.slots + (size_t)E * n * sizeof(uint16_t));
   s.total = align16(s.flags + (size_t)L * d);
   return s;
 }
 
 // Copies count uint16 from global to shared memory, 4 bytes at a time when
-// both ends allow it.
+// the source allows it.
 __device__ inline void copy_u16(uint16_t* dst, const uint16_t* src, int count, int tid, int nt) {
   if ((reinterpret_cast<uintptr_t>(src) & 3) == 0) {
     const int pairs = count >> 1;
@@ -69,6 +67,8 @@ template <int T, typename S, bool FEXT>
 __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
     k_patch_step(DevModel m, DevPatches P, double dt) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
+  constexpr int CH = kChunk * n;  // sorted slots of one chunk
+  static_assert(kChunk == kThreads, "one element per thread per chunk");
   extern __shared__ __align__(16) unsigned char smem[];
   const int p = blockIdx.x;
   const int nb = P.node_ptr[p];
@@ -76,7 +76,6 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
   const int eb = P.elem_ptr[p];
   const int ne = P.elem_ptr[p + 1] - eb;
   const int nint = P.ninterior[p];
-  const int nent = ne * n;
   const int LM = P.max_nodes;  // row stride of the component-major arrays
   const SmemLayout lay = layout(P.max_nodes, P.max_elems, d, n, sizeof(S), kThreads);
   double* xs = reinterpret_cast<double*>(smem + lay.xs);
@@ -84,18 +83,14 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
   double* fs = reinterpret_cast<double*>(smem + lay.fs);
   S* contrib = reinterpret_cast<S*>(smem + lay.contrib);
   uint16_t* lcs = reinterpret_cast<uint16_t*>(smem + lay.lcs);
-  uint16_t* ents = reinterpret_cast<uint16_t*>(smem + lay.ents);
-  uint16_t* cbeg = reinterpret_cast<uint16_t*>(smem + lay.cbeg);
-  uint16_t* cursor = reinterpret_cast<uint16_t*>(smem + lay.cursor);
+  uint16_t* slots = reinterpret_cast<uint16_t*>(smem + lay.slots);
   uint8_t* flags = smem + lay.flags;
   const int tid = threadIdx.x;
 
-  // 1. stage the patch: local connectivity, CSR of (local element, corner)
-  //    entries, node offsets; per (node, component) X, predicted u, flag
-  copy_u16(lcs, P.lconn + (size_t)eb * n, nent, tid, kThreads);
-  copy_u16(ents, P.centries + (size_t)eb * n, nent, tid, kThreads);
-  for (int j = tid; j < L; j += kThreads) cbeg[j] = P.cbeg[nb + j];
-  if (tid == 0) cbeg[L] = (uint16_t)nent;
+  // 1. stage the patch: local connectivity, sorted slots; per (node,
+  //    component) X, predicted u, blocked flag
+  copy_u16(lcs, P.lconn + (size_t)eb * n, ne * n, tid, kThreads);
+  copy_u16(slots, P.cslot + (size_t)eb * n, ne * n, tid, kThreads);
   for (int k = tid; k < L * d; k += kThreads) {
     const int j = k / d, i = k - j * d;
     const int64_t idx = (int64_t)P.lnodes[nb + j] * d + i;
@@ -110,12 +105,12 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
     flags[k] = b;
   }
   __syncthreads();
-  for (int q = tid; q < L * d; q += kThreads) cursor[q] = cbeg[q % L];
-  // (cursor[q] belongs to item q = i * L + j; visible after the first barrier below)
 
-  // 2. element forces, chunk by chunk; each chunk's vectors added per
-  //    (node, component) in ascending local element order
-  for (int c0 = 0; c0 < ne; c0 += kThreads) {
+  // 2. element forces chunk by chunk: each element writes its corner vectors
+  //    to the corners' sorted slots, then one thread per run of equal node
+  //    adds the run (ascending element order) to that node
+  const int32_t* seg_ptr = P.seg_ptr + P.chunk_base[p];
+  for (int c0 = 0, chunk = 0; c0 < ne; c0 += kChunk, ++chunk) {
     const int el = c0 + tid;
     if (el < ne) {
       int lc[n];
@@ -137,24 +132,24 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
       S fe[3 * 8];
       fast::element_force<T, S>(mp, dX, du, fe);
 #pragma unroll
-      for (int k = 0; k < n * d; ++k) contrib[k * kThreads + tid] = fe[k];
+      for (int a = 0; a < n; ++a) {
+        const int sl = slots[el * n + a];
+#pragma unroll
+        for (int i = 0; i < d; ++i) contrib[i * CH + sl] = fe[a * d + i];
+      }
     }
     __syncthreads();
-    const int c1 = c0 + kThreads < ne ? c0 + kThreads : ne;
-    for (int q = tid; q < L * d; q += kThreads) {
-      const int i = q / L, j = q - i * L;
-      int c = cursor[q];
-      const int end = cbeg[j + 1];
-      double f = fs[i * LM + j];
-      while (c < end) {
-        const int e = ents[c];
-        const int le = e >> 3;
-        if (le >= c1) break;
-        f -= double(contrib[((e & 7) * d + i) * kThreads + (le - c0)]);
-        ++c;
+    const int sb = seg_ptr[chunk], se = seg_ptr[chunk + 1];
+    for (int s = sb + tid; s < se; s += kThreads) {
+      const uint32_t w = P.segs[s];
+      const int j = (int)(w >> 16), end = (int)(w & 0xffff);
+      const int beg = s == sb ? 0 : (int)(P.segs[s - 1] & 0xffff);
+#pragma unroll
+      for (int i = 0; i < d; ++i) {
+        double f = 0.0;
+        for (int k = beg; k < end; ++k) f += double(contrib[i * CH + k]);
+        fs[i * LM + j] -= f;
       }
-      cursor[q] = (uint16_t)c;
-      fs[i * LM + j] = f;
     }
     __syncthreads();
   }

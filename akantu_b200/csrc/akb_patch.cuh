@@ -31,11 +31,21 @@ struct PatchHost {
   std::vector<uint16_t> lconn;     // per element (patch order) nnpe local indices
   std::vector<uint16_t> cbeg;      // per local node: first CSR entry (relative to the patch)
   std::vector<uint16_t> centries;  // per element corner: (local element << 3) | corner
+  // per chunk of kChunk consecutive elements of a patch: the slot of each
+  // element corner once the chunk's corners are sorted by (local node,
+  // element, corner), and the runs of equal local node in that order
+  std::vector<uint16_t> cslot;     // per element corner (patch order)
+  std::vector<uint32_t> segs;      // per run: (local node << 16) | end slot
+  std::vector<int32_t> seg_ptr;    // nchunks + 1
+  std::vector<int32_t> chunk_base; // npatch: index of the patch's first chunk
   std::vector<uint32_t> slot;      // per local node: partial slot (0xffffffff if interior)
   std::vector<uint32_t> snodes;    // shared nodes, ascending
   std::vector<int32_t> sptr;       // nshared + 1, partial slots of each shared node
   int64_t nslots = 0;
 };
+
+// Elements per chunk: the CTA computes one element per thread per chunk.
+constexpr int kChunk = 256;
 
 // Builds the patches. target_elems: elements per patch; max_nodes: local node
 // cap (<= 65535).
@@ -54,6 +64,10 @@ struct DevPatches {
   const uint16_t* lconn;
   const uint16_t* cbeg;
   const uint16_t* centries;
+  const uint16_t* cslot;
+  const uint32_t* segs;
+  const int32_t* seg_ptr;
+  const int32_t* chunk_base;
   const uint32_t* slot;
   const uint32_t* snodes;
   const int32_t* sptr;

@@ -129,6 +129,8 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
   P.centries.resize((size_t)ne * nnpe);
   std::vector<uint32_t> local;
   std::vector<int32_t> cnt;
+  std::vector<uint64_t> keyed;
+  P.cslot.resize((size_t)ne * nnpe);
   for (int p = 0; p < P.npatch; ++p) {
     const int32_t eb = P.elem_ptr[p], ee = P.elem_ptr[p + 1];
     local.clear();
@@ -176,9 +178,31 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
       const int64_t s = sidx[local[j]];
       P.slot.push_back(s < 0 ? 0xffffffffu : (uint32_t)(P.sptr[s] + sfill[s]++));
     }
+    // chunks: corners sorted by (local node, element, corner); the sort key
+    // orders a node's contributions by ascending element
+    P.chunk_base.push_back((int32_t)P.seg_ptr.size());
+    for (int32_t c0 = eb; c0 < ee; c0 += kChunk) {
+      const int32_t c1 = std::min(ee, c0 + kChunk);
+      keyed.clear();
+      for (int32_t i = c0; i < c1; ++i)
+        for (int a = 0; a < nnpe; ++a) {
+          const uint32_t j = P.lconn[(size_t)i * nnpe + a];
+          keyed.push_back(((uint64_t)j << 32) | ((uint64_t)(i - c0) << 8) | (uint64_t)a);
+        }
+      std::sort(keyed.begin(), keyed.end());
+      P.seg_ptr.push_back((int32_t)P.segs.size());
+      for (size_t k = 0; k < keyed.size(); ++k) {
+        const uint32_t j = (uint32_t)(keyed[k] >> 32);
+        const int32_t le = (int32_t)((keyed[k] >> 8) & 0xffffff), a = (int32_t)(keyed[k] & 0xff);
+        P.cslot[(size_t)(c0 + le) * nnpe + a] = (uint16_t)k;
+        if (k + 1 == keyed.size() || (uint32_t)(keyed[k + 1] >> 32) != j)
+          P.segs.push_back((j << 16) | (uint32_t)(k + 1));
+      }
+    }
     P.lnodes.insert(P.lnodes.end(), local.begin(), local.end());
     P.node_ptr.push_back((int32_t)P.lnodes.size());
   }
+  P.seg_ptr.push_back((int32_t)P.segs.size());
   return P;
 }
 
