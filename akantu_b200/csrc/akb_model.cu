@@ -182,6 +182,7 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
   d.npatch = P.npatch;
   d.max_nodes = P.max_nodes;
   d.max_elems = P.max_elems;
+  d.max_segs = P.max_segs;
   d.nshared = (int64_t)P.snodes.size();
   akb_status st;
   if ((st = upload(m, P.elem_ptr, &d.elem_ptr)) != AKB_OK) return st;

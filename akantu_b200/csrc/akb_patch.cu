@@ -22,15 +22,18 @@ namespace {
 constexpr int kThreads = 256;
 
 struct SmemLayout {
-  size_t xs, us, fs, contrib, lcs, slots, flags, total;
+  size_t xs, us, fs, contrib, lcs, slots, segs, segp, flags, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-// Shared-memory layout for patch caps L (nodes) and E (elements). Node
-// arrays are component-major ([i][j]); the chunk's element vectors are stored
-// at their sorted slots, component-major ([i][slot]).
-__host__ __device__ inline SmemLayout layout(int L, int E, int d, int n, int sbytes, int threads) {
+constexpr int kMaxChunks = 33;  // chunks of a patch (8192 elements) + 1
+
+// Shared-memory layout for patch caps L (nodes), E (elements), R (runs).
+// Node arrays are component-major ([i][j]); the chunk's element vectors are
+// stored at their sorted slots, component-major ([i][slot]).
+__host__ __device__ inline SmemLayout layout(int L, int E, int R, int d, int n, int sbytes,
+                                             int threads) {
   SmemLayout s;
   const size_t nd = (size_t)L * d * sizeof(double);
   s.xs = 0;
@@ -39,7 +42,9 @@ __host__ __device__ inline SmemLayout layout(int L, int E, int d, int n, int sby
   s.contrib = align16(s.fs + nd);
   s.lcs = align16(s.contrib + (size_t)threads * n * d * sbytes);
   s.slots = align16(s.lcs + (size_t)E * n * sizeof(uint16_t));
-  s.flags = align16(s.slots + (size_t)E * n * sizeof(uint16_t));
+  s.segs = align16(s.slots + (size_t)E * n * sizeof(uint16_t));
+  s.segp = align16(s.segs + (size_t)R * sizeof(uint32_t));
+  s.flags = align16(s.segp + (size_t)kMaxChunks * sizeof(int32_t));
   s.total = align16(s.flags + (size_t)L * d);
   return s;
 }
@@ -63,6 +68,10 @@ template <int T, typename S> struct PatchOccupancy { static constexpr int value 
 template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, float> { static constexpr int value = 2; };
 template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, double> { static constexpr int value = 1; };
 
+// (node, component) items handled per thread per round of the staging and
+// finishing loops: their global loads are issued together.
+constexpr int kBatch = 4;
+
 template <int T, typename S, bool FEXT>
 __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
     k_patch_step(DevModel m, DevPatches P, double dt) {
@@ -76,40 +85,69 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
   const int eb = P.elem_ptr[p];
   const int ne = P.elem_ptr[p + 1] - eb;
   const int nint = P.ninterior[p];
+  const int nchunks = (ne + kChunk - 1) / kChunk;
   const int LM = P.max_nodes;  // row stride of the component-major arrays
-  const SmemLayout lay = layout(P.max_nodes, P.max_elems, d, n, sizeof(S), kThreads);
+  const SmemLayout lay = layout(P.max_nodes, P.max_elems, P.max_segs, d, n, sizeof(S), kThreads);
   double* xs = reinterpret_cast<double*>(smem + lay.xs);
   double* us = reinterpret_cast<double*>(smem + lay.us);
   double* fs = reinterpret_cast<double*>(smem + lay.fs);
   S* contrib = reinterpret_cast<S*>(smem + lay.contrib);
   uint16_t* lcs = reinterpret_cast<uint16_t*>(smem + lay.lcs);
   uint16_t* slots = reinterpret_cast<uint16_t*>(smem + lay.slots);
+  uint32_t* segs = reinterpret_cast<uint32_t*>(smem + lay.segs);
+  int32_t* segp = reinterpret_cast<int32_t*>(smem + lay.segp);
   uint8_t* flags = smem + lay.flags;
   const int tid = threadIdx.x;
+  const int items = L * d;
 
-  // 1. stage the patch: local connectivity, sorted slots; per (node,
+  // 1. stage the patch: local connectivity, sorted slots, runs; per (node,
   //    component) X, predicted u, blocked flag
   copy_u16(lcs, P.lconn + (size_t)eb * n, ne * n, tid, kThreads);
   copy_u16(slots, P.cslot + (size_t)eb * n, ne * n, tid, kThreads);
-  for (int k = tid; k < L * d; k += kThreads) {
-    const int j = k / d, i = k - j * d;
-    const int64_t idx = (int64_t)P.lnodes[nb + j] * d + i;
-    const double x = __ldg(&m.X[idx]);
-    double u = m.u[idx], v = m.v[idx];
-    const double a = m.a[idx];
-    const uint8_t b = m.blocked[idx];
-    if (!b) fast::predict(dt, u, v, a);
-    xs[i * LM + j] = x;
-    us[i * LM + j] = u;
-    fs[i * LM + j] = 0.0;
-    flags[k] = b;
+  {
+    const int32_t* gp = P.seg_ptr + P.chunk_base[p];
+    const int s0 = gp[0];
+    if (tid <= nchunks) segp[tid] = gp[tid] - s0;
+    const int nseg = gp[nchunks] - s0;
+    for (int k = tid; k < nseg; k += kThreads) segs[k] = P.segs[s0 + k];
+  }
+  for (int base = 0; base < items; base += kThreads * kBatch) {
+    int64_t idx[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int k = base + b * kThreads + tid;
+      const int j = k / d, i = k - j * d;
+      idx[b] = k < items ? (int64_t)P.lnodes[nb + j] * d + i : -1;
+    }
+    double x[kBatch], u[kBatch], v[kBatch], a[kBatch];
+    uint8_t bl[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (idx[b] >= 0) {
+        x[b] = __ldg(&m.X[idx[b]]);
+        u[b] = m.u[idx[b]];
+        v[b] = m.v[idx[b]];
+        a[b] = m.a[idx[b]];
+        bl[b] = m.blocked[idx[b]];
+      }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int k = base + b * kThreads + tid;
+      if (k >= items) continue;
+      const int j = k / d, i = k - j * d;
+      double uu = u[b], vv = v[b];
+      if (!bl[b]) fast::predict(dt, uu, vv, a[b]);
+      xs[i * LM + j] = x[b];
+      us[i * LM + j] = uu;
+      fs[i * LM + j] = 0.0;
+      flags[k] = bl[b];
+    }
   }
   __syncthreads();
 
   // 2. element forces chunk by chunk: each element writes its corner vectors
-  //    to the corners' sorted slots, then one thread per run of equal node
+  //    to the corners' sorted slots, then one thread per (run, component)
   //    adds the run (ascending element order) to that node
-  const int32_t* seg_ptr = P.seg_ptr + P.chunk_base[p];
   for (int c0 = 0, chunk = 0; c0 < ne; c0 += kChunk, ++chunk) {
     const int el = c0 + tid;
     if (el < ne) {
@@ -139,40 +177,60 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
       }
     }
     __syncthreads();
-    const int sb = seg_ptr[chunk], se = seg_ptr[chunk + 1];
-    for (int s = sb + tid; s < se; s += kThreads) {
-      const uint32_t w = P.segs[s];
+    const int sb = segp[chunk], nrun = segp[chunk + 1] - sb;
+    for (int q = tid; q < nrun * d; q += kThreads) {
+      const int i = q / nrun, r = q - i * nrun;
+      const uint32_t w = segs[sb + r];
       const int j = (int)(w >> 16), end = (int)(w & 0xffff);
-      const int beg = s == sb ? 0 : (int)(P.segs[s - 1] & 0xffff);
-#pragma unroll
-      for (int i = 0; i < d; ++i) {
-        double f = 0.0;
-        for (int k = beg; k < end; ++k) f += double(contrib[i * CH + k]);
-        fs[i * LM + j] -= f;
-      }
+      const int beg = r == 0 ? 0 : (int)(segs[sb + r - 1] & 0xffff);
+      const S* src = contrib + i * CH;
+      double f = 0.0;
+      for (int k = beg; k < end; ++k) f += double(src[k]);
+      fs[i * LM + j] -= f;
     }
     __syncthreads();
   }
 
   // 3. finish the nodes of this patch (state re-read, predictor recomputed
   //    bit for bit), hand out the shared ones
-  for (int k = tid; k < L * d; k += kThreads) {
-    const int j = k / d, i = k - j * d;
-    const double f = fs[i * LM + j];
-    if (j < nint) {
-      if (flags[k]) continue;  // blocked DOFs keep u, v, a
-      const int64_t g = P.lnodes[nb + j];
-      const int64_t idx = g * d + i;
-      double u = m.u[idx], v = m.v[idx], a = m.a[idx];
-      fast::predict(dt, u, v, a);
-      double r = f;
-      if (FEXT) r += m.fext[idx];
-      fast::correct(dt, r, m.inv_mass[g], u, v, a);
-      m.u[idx] = u;
-      m.v[idx] = v;
-      m.a[idx] = a;
-    } else {
-      P.partial[(int64_t)P.slot[nb + j] * d + i] = f;
+  for (int base = 0; base < items; base += kThreads * kBatch) {
+    int64_t idx[kBatch];
+    double u[kBatch], v[kBatch], a[kBatch], im[kBatch], fx[kBatch];
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int k = base + b * kThreads + tid;
+      const int j = k / d, i = k - j * d;
+      idx[b] = -1;
+      if (k < items && j < nint && !flags[k]) {
+        const int64_t g = P.lnodes[nb + j];
+        idx[b] = g * d + i;
+        im[b] = m.inv_mass[g];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b)
+      if (idx[b] >= 0) {
+        u[b] = m.u[idx[b]];
+        v[b] = m.v[idx[b]];
+        a[b] = m.a[idx[b]];
+        fx[b] = FEXT ? m.fext[idx[b]] : 0.0;
+      }
+#pragma unroll
+    for (int b = 0; b < kBatch; ++b) {
+      const int k = base + b * kThreads + tid;
+      if (k >= items) continue;
+      const int j = k / d, i = k - j * d;
+      const double f = fs[i * LM + j];
+      if (j >= nint) {
+        P.partial[(int64_t)P.slot[nb + j] * d + i] = f;
+      } else if (idx[b] >= 0) {  // blocked DOFs keep u, v, a
+        double uu = u[b], vv = v[b], aa = a[b];
+        fast::predict(dt, uu, vv, aa);
+        fast::correct(dt, FEXT ? f + fx[b] : f, im[b], uu, vv, aa);
+        m.u[idx[b]] = uu;
+        m.v[idx[b]] = vv;
+        m.a[idx[b]] = aa;
+      }
     }
   }
 }
@@ -206,7 +264,7 @@ __global__ void k_shared_nodes(DevModel m, DevPatches P, double dt) {
 template <int T, typename S>
 cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool fext,
                          cudaStream_t s) {
-  const SmemLayout lay = layout(p.max_nodes, p.max_elems, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
+  const SmemLayout lay = layout(p.max_nodes, p.max_elems, p.max_segs, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
   if (fext)
     k_patch_step<T, S, true><<<p.npatch, kThreads, lay.total, s>>>(m, p, dt);
   else
@@ -216,7 +274,7 @@ cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool
 
 template <int T, typename S>
 cudaError_t configure(const DevPatches& p) {
-  const SmemLayout lay = layout(p.max_nodes, p.max_elems, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
+  const SmemLayout lay = layout(p.max_nodes, p.max_elems, p.max_segs, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
   cudaError_t e = cudaFuncSetAttribute(k_patch_step<T, S, true>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total);
   if (e != cudaSuccess) return e;
@@ -227,7 +285,7 @@ cudaError_t configure(const DevPatches& p) {
 }  // namespace
 
 size_t patch_smem_bytes(const DevPatches& p, int dim, int nnpe, bool fp32, int threads) {
-  return layout(p.max_nodes, p.max_elems, dim, nnpe, fp32 ? 4 : 8, threads).total;
+  return layout(p.max_nodes, p.max_elems, p.max_segs, dim, nnpe, fp32 ? 4 : 8, threads).total;
 }
 
 cudaError_t patch_configure(const DevModel& m, const DevPatches& p, bool fp32) {

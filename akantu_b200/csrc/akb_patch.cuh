@@ -23,6 +23,7 @@ struct PatchHost {
   int npatch = 0;
   int max_nodes = 0;    // largest local node count of a patch
   int max_elems = 0;    // largest element count of a patch
+  int max_segs = 0;     // largest run count of a patch (all its chunks)
   std::vector<int32_t> elem_ptr;   // npatch + 1, into element order
   std::vector<int32_t> node_ptr;   // npatch + 1, into lnodes
   std::vector<int32_t> ninterior;  // npatch
@@ -55,7 +56,7 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
 // Device copy of a PatchHost.
 struct DevPatches {
   int npatch;
-  int max_nodes, max_elems;
+  int max_nodes, max_elems, max_segs;
   int64_t nshared;
   const int32_t* elem_ptr;
   const int32_t* node_ptr;

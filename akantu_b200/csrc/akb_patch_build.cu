@@ -181,6 +181,7 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
     // chunks: corners sorted by (local node, element, corner); the sort key
     // orders a node's contributions by ascending element
     P.chunk_base.push_back((int32_t)P.seg_ptr.size());
+    const size_t seg_first = P.segs.size();
     for (int32_t c0 = eb; c0 < ee; c0 += kChunk) {
       const int32_t c1 = std::min(ee, c0 + kChunk);
       keyed.clear();
@@ -199,6 +200,7 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
           P.segs.push_back((j << 16) | (uint32_t)(k + 1));
       }
     }
+    P.max_segs = std::max(P.max_segs, (int)(P.segs.size() - seg_first));
     P.lnodes.insert(P.lnodes.end(), local.begin(), local.end());
     P.node_ptr.push_back((int32_t)P.lnodes.size());
   }
