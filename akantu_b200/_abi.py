@@ -83,6 +83,15 @@ class ModelOptions(C.Structure):
         ("stream", C.c_void_p),
         ("patch_elements", C.c_int32),
         ("patch_nodes", C.c_int32),
+        ("patch_grid", C.c_int32),
+    ]
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [
+        ("nb_instances", C.c_int32),
+        ("meshes", C.POINTER(MeshDesc)),
+        ("materials", C.POINTER(MaterialDesc)),
     ]
 
 

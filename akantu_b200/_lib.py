@@ -47,6 +47,12 @@ SIGNATURES = {
     "akb_apply_dirichlet": (I32, [P, PU32, I64, I32, PD]),
     "akb_time_kernels": (I32, [P, I64, PD, I32]),
     "akb_kernel_name": (C.c_char_p, [P, I32]),
+    "akb_batch_create": (I32, [C.POINTER(_abi.BatchDesc), C.POINTER(_abi.ModelOptions),
+                               C.POINTER(P)]),
+    "akb_batch_get_layout": (I32, [P, C.POINTER(I32), C.POINTER(I64), C.POINTER(I64)]),
+    "akb_batch_set_time_steps": (I32, [P, PD]),
+    "akb_batch_get_stable_time_steps": (I32, [P, PD]),
+    "akb_batch_get_energies": (I32, [P, I32, PD]),
     "akb_kinetic_energy_static": (I32, [P, P, I64, I32, P, P]),
     "akb_synchronize": (I32, [P]),
 }

@@ -71,6 +71,52 @@ def block_hex8(n=128, length=1.28, seed=SEED):
                 u0=np.zeros_like(x), v0=v0, dt_factor=0.8, steps=2000)
 
 
+def plates_batch(n_instances=4096, seed=SEED, min_elems=100, max_elems=20000):
+    """Independent triangle_3 plane-strain plates of uneven size: element
+    counts log-uniform in [min_elems, max_elems], aspect a ~ U[1, 8],
+    nx = round(sqrt(n a / 2)), ny = round(sqrt(n / (2 a))) squares of size
+    1/ny m (plate 1 m wide, a m long), two triangles per square; E ~ U[1, 200]
+    GPa, nu ~ U[0.2, 0.4], rho ~ U[1000, 8000]; left edge fixed; initial
+    u_x = 1e-4 L sin(pi x / L); dt = 0.8 x the instance's stable step;
+    500 steps."""
+    rng = np.random.default_rng(seed)
+    n_el = np.exp(rng.uniform(np.log(min_elems), np.log(max_elems), n_instances))
+    aspect = rng.uniform(1.0, 8.0, n_instances)
+    E = rng.uniform(1e9, 200e9, n_instances)
+    nu = rng.uniform(0.2, 0.4, n_instances)
+    rho = rng.uniform(1000.0, 8000.0, n_instances)
+    meshes, mats, blocked, u0 = [], [], [], []
+    for k in range(n_instances):
+        nx = max(1, int(round(math.sqrt(n_el[k] * aspect[k] / 2))))
+        ny = max(1, int(round(math.sqrt(n_el[k] / (2 * aspect[k])))))
+        lx = nx / ny  # square cells of size 1/ny over a 1 m wide plate
+        mesh = plate_triangle3(nx, ny, lx, 1.0)
+        x = mesh.nodes
+        b = np.zeros_like(x, dtype=np.uint8)
+        b[np.isclose(x[:, 0], 0.0)] = 1
+        u = np.zeros_like(x)
+        u[:, 0] = 1e-4 * lx * np.sin(math.pi * x[:, 0] / lx)
+        u[b.astype(bool)] = 0.0
+        meshes.append(mesh)
+        mats.append(dict(kind=_abi.MATERIAL_ELASTIC, rho=float(rho[k]), E=float(E[k]),
+                         nu=float(nu[k])))
+        blocked.append(b)
+        u0.append(u)
+    return dict(name="plates_tri3_batch", meshes=meshes, materials=mats, blocked=blocked,
+                u0=u0, dt_factor=0.8, steps=500)
+
+
+def setup_batch(batch, w):
+    """Boundary and initial conditions of plates_batch on a BatchModel;
+    returns the per-instance time steps."""
+    batch.setBlockedDOFs(np.concatenate(w["blocked"]))
+    batch.setField(_abi.FIELD_DISPLACEMENT, np.concatenate(w["u0"]))
+    batch.setField(_abi.FIELD_VELOCITY, np.zeros((batch.node_offsets[-1], 2)))
+    dts = w["dt_factor"] * batch.getStableTimeSteps()
+    batch.setTimeSteps(dts)
+    return dts
+
+
 def setup_model(model, w):
     """Applies a workload's boundary and initial conditions to a model facade
     (get/set/set_blocked/stable_time_step/set_time_step) and returns dt."""

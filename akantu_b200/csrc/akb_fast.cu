@@ -26,7 +26,7 @@ __global__ void k_element_forces(DevModel m) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= m.ne) return;
-  const MatParams& p = m.mats[m.mat_of ? m.mat_of[e] : 0];
+  const MatParams& p = (m.mat_of ? m.mat_table[m.mat_of[e]] : m.mats[0]);
   uint32_t nodes[8];
 #pragma unroll
   for (int a = 0; a < n; ++a) nodes[a] = __ldg(&m.conn[e * n + a]);

@@ -48,7 +48,8 @@ struct DevModel {
   void* fe;                 // ne x nnpe x dim element forces (double or float)
   const int32_t* node_ptr;  // nn + 1, node -> (element, corner) CSR
   const int32_t* node_ent;  // ne * nnpe entries e * nnpe + a, ascending e
-  MatParams mats[kMaxMaterials];
+  MatParams mats[kMaxMaterials];  // the first materials, by value (kernel parameter space)
+  const MatParams* mat_table;     // all nmat materials (device), indexed by mat_of
 };
 
 // Thread-local last-error helpers.
@@ -87,5 +88,10 @@ cudaError_t stable_dt(const DevModel& m, double* d_scratch, int scratch_len,
 cudaError_t energy(const DevModel& m, int kind, double dt, double* d_scratch,
                    int scratch_len, double* d_out, cudaStream_t s);
 int reduce_blocks(int64_t n);
+// Per-instance reductions of a batch: one block per instance.
+cudaError_t stable_dt_instances(const DevModel& m, const int64_t* elem_off, int ninst,
+                                double* d_out, cudaStream_t s);
+cudaError_t energy_instances(const DevModel& m, int kind, const int64_t* node_off,
+                             const int64_t* elem_off, int ninst, double* d_out, cudaStream_t s);
 
 }  // namespace akb

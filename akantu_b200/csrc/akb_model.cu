@@ -24,6 +24,12 @@ akb_status fail(akb_status s, const std::string& msg) {
 
 using namespace akb;
 
+// Node and element ranges of the instances of a batch, in the union mesh.
+struct BatchLayout {
+  int32_t ninst = 0;
+  std::vector<int64_t> node_off, elem_off;  // ninst + 1 each
+};
+
 struct akb_model {
   DevModel dm{};
   int mode = AKB_MODE_FP64_REFERENCE;
@@ -47,7 +53,13 @@ struct akb_model {
   // fused patch step of the fast modes
   DevPatches patches{};
   bool use_patches = false;
-  int opt_patch_elements = 0, opt_patch_nodes = 0;
+  int opt_patch_elements = 0, opt_patch_nodes = 0, opt_patch_grid = 0;
+  // batch of independent instances (akb_batch_create)
+  int32_t ninst = 0;
+  std::vector<int64_t> node_off, elem_off;
+  double* d_inst_dt = nullptr;
+  const int64_t* d_node_off = nullptr;
+  const int64_t* d_elem_off = nullptr;
   // staging of akb_apply_dirichlet
   uint32_t* d_bc_nodes = nullptr;
   double* d_bc_values = nullptr;
@@ -171,15 +183,64 @@ template <typename T>
 akb_status upload(akb_model* m, const std::vector<T>& v, const T** out);
 
 akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
-                                const uint32_t* element_material) {
+                                const uint32_t* element_material, const BatchLayout* batch) {
   int target, max_nodes;
   patch_params(m->dm.type, &target, &max_nodes);
   if (m->opt_patch_elements > 0) target = std::min(m->opt_patch_elements, 8191);
   if (m->opt_patch_nodes > 0) max_nodes = std::min(m->opt_patch_nodes, 65535);
-  PatchHost P = build_patches(mesh->nodes, mesh->connectivity, mesh->nb_nodes,
-                              mesh->nb_elements, m->dm.dim, m->dm.nnpe, target, max_nodes);
+  PatchHost P;
+  std::vector<uint32_t> patch_inst, snode_inst;
+  if (!batch) {
+    P = build_patches(mesh->nodes, mesh->connectivity, mesh->nb_nodes, mesh->nb_elements,
+                      m->dm.dim, m->dm.nnpe, target, max_nodes);
+  } else {
+    // one instance at a time, so no patch spans two instances; the union is
+    // the concatenation of the instances' patches
+    const int dd = m->dm.dim, nn_ = m->dm.nnpe;
+    P.elem_ptr.push_back(0);
+    P.node_ptr.push_back(0);
+    P.sptr.push_back(0);
+    std::vector<uint32_t> lconn;
+    for (int i = 0; i < batch->ninst; ++i) {
+      const int64_t n0 = batch->node_off[i], e0 = batch->elem_off[i];
+      const int64_t nni = batch->node_off[i + 1] - n0, nei = batch->elem_off[i + 1] - e0;
+      lconn.assign(mesh->connectivity + e0 * nn_, mesh->connectivity + (e0 + nei) * nn_);
+      for (auto& c : lconn) c -= (uint32_t)n0;
+      PatchHost Q = build_patches(mesh->nodes + n0 * dd, lconn.data(), nni, nei, dd, nn_,
+                                  target, max_nodes);
+      const int64_t lbase = (int64_t)P.lnodes.size(), sbase = P.nslots;
+      const int64_t segbase = (int64_t)P.segs.size(), chbase = (int64_t)P.seg_ptr.size();
+      for (int p = 0; p < Q.npatch; ++p) {
+        P.elem_ptr.push_back((int32_t)(e0 + Q.elem_ptr[p + 1]));
+        P.node_ptr.push_back((int32_t)(lbase + Q.node_ptr[p + 1]));
+        P.chunk_base.push_back((int32_t)(chbase + Q.chunk_base[p]));
+        patch_inst.push_back((uint32_t)i);
+      }
+      P.npatch += Q.npatch;
+      P.max_nodes = std::max(P.max_nodes, Q.max_nodes);
+      P.max_elems = std::max(P.max_elems, Q.max_elems);
+      P.max_segs = std::max(P.max_segs, Q.max_segs);
+      P.ninterior.insert(P.ninterior.end(), Q.ninterior.begin(), Q.ninterior.end());
+      for (auto g : Q.lnodes) P.lnodes.push_back((uint32_t)(g + n0));
+      for (auto e : Q.elem_order) P.elem_order.push_back((uint32_t)(e + e0));
+      P.lconn.insert(P.lconn.end(), Q.lconn.begin(), Q.lconn.end());
+      P.cslot.insert(P.cslot.end(), Q.cslot.begin(), Q.cslot.end());
+      for (auto s : Q.slot) P.slot.push_back(s == 0xffffffffu ? s : (uint32_t)(s + sbase));
+      for (auto g : Q.snodes) {
+        P.snodes.push_back((uint32_t)(g + n0));
+        snode_inst.push_back((uint32_t)i);
+      }
+      for (size_t k = 1; k < Q.sptr.size(); ++k) P.sptr.push_back((int32_t)(Q.sptr[k] + sbase));
+      P.nslots += Q.nslots;
+      P.segs.insert(P.segs.end(), Q.segs.begin(), Q.segs.end());
+      for (size_t k = 0; k + 1 < Q.seg_ptr.size(); ++k)
+        P.seg_ptr.push_back((int32_t)(Q.seg_ptr[k] + segbase));
+    }
+    P.seg_ptr.push_back((int32_t)P.segs.size());
+  }
   DevPatches& d = m->patches;
   d.npatch = P.npatch;
+  d.grid = m->opt_patch_grid > 0 ? m->opt_patch_grid : 0;
   d.max_nodes = P.max_nodes;
   d.max_elems = P.max_elems;
   d.max_segs = P.max_segs;
@@ -207,6 +268,13 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
   }
   if ((st = dalloc(m, &d.partial, (size_t)std::max<int64_t>(P.nslots, 1) * m->dm.dim)) != AKB_OK)
     return st;
+  d.inst_dt = nullptr;
+  d.patch_inst = nullptr;
+  d.snode_inst = nullptr;
+  if (batch) {
+    if ((st = upload(m, patch_inst, &d.patch_inst)) != AKB_OK) return st;
+    if ((st = upload(m, snode_inst, &d.snode_inst)) != AKB_OK) return st;
+  }
   AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));  // host vectors go out of scope
   const size_t smem = patch_smem_bytes(d, m->dm.dim, m->dm.nnpe, fp32(m), 256);
   if (smem > 227 * 1024)
@@ -283,6 +351,12 @@ int64_t field_count(const akb_model* m, int32_t field) {
 
 }  // namespace
 
+static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
+                               const akb_material_desc* materials,
+                               const uint32_t* element_material,
+                               const akb_model_options* options, const BatchLayout* batch,
+                               akb_model** out);
+
 extern "C" {
 
 int32_t akb_abi_version(void) { return AKB_ABI_VERSION; }
@@ -295,8 +369,24 @@ akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
                             const akb_model_options* options, akb_model** out) {
   if (!out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output handle");
   *out = nullptr;
-  if (!mesh || !materials || nb_materials < 1 || nb_materials > kMaxMaterials)
-    return fail(AKB_ERR_INVALID_ARGUMENT, "mesh and 1..8 materials are required");
+  return create_model(mesh, nb_materials, materials, element_material, options, nullptr, out);
+}
+
+}  // extern "C"
+
+// Shared by akb_model_create and akb_batch_create. batch (may be null) gives
+// the node and element ranges of independent instances of a union mesh:
+// patches are then built per instance and every instance has its own time
+// step.
+static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
+                               const akb_material_desc* materials,
+                               const uint32_t* element_material,
+                               const akb_model_options* options, const BatchLayout* batch,
+                               akb_model** out) {
+  if (!out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  if (!mesh || !materials || nb_materials < 1 || nb_materials > (1 << 24))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "mesh and 1..2^24 materials are required");
   const int type = mesh->element_type;
   if (type < AKB_SEGMENT_2 || type > AKB_HEXAHEDRON_8)
     return fail(AKB_ERR_UNSUPPORTED, "unsupported element type");
@@ -322,7 +412,7 @@ akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
     if (!(md.rho > 0) || !(md.E > 0))
       return fail(AKB_ERR_INVALID_ARGUMENT, "material needs rho > 0 and E > 0");
   }
-  akb_model_options opt{AKB_MODE_FP64_REFERENCE, 0, nullptr, 0, 0};
+  akb_model_options opt{AKB_MODE_FP64_REFERENCE, 0, nullptr, 0, 0, 0};
   if (options) opt = *options;
   if (opt.precision_mode < AKB_MODE_FP64_REFERENCE || opt.precision_mode > AKB_MODE_FP32_BULK)
     return fail(AKB_ERR_INVALID_ARGUMENT, "unknown precision mode");
@@ -331,6 +421,7 @@ akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
   m->mode = opt.precision_mode;
   m->opt_patch_elements = opt.patch_elements;
   m->opt_patch_nodes = opt.patch_nodes;
+  m->opt_patch_grid = opt.patch_grid;
   m->device = opt.device;
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   if (opt.stream) {
@@ -347,9 +438,15 @@ akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
   dm.nn = nn;
   dm.ne = ne;
   dm.nmat = nb_materials;
-  for (int k = 0; k < nb_materials; ++k) dm.mats[k] = make_params(materials[k], d);
-
   akb_status st;
+  {
+    std::vector<MatParams> table(nb_materials);
+    for (int k = 0; k < nb_materials; ++k) table[k] = make_params(materials[k], d);
+    for (int k = 0; k < nb_materials && k < kMaxMaterials; ++k) dm.mats[k] = table[k];
+    if ((st = upload(m.get(), table, &dm.mat_table)) != AKB_OK) return st;
+    AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  }
+
   const size_t ndof = (size_t)nn * d;
   double* X;
   uint32_t* conn;
@@ -428,7 +525,19 @@ akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
     dm.jac = nullptr;
   }
   if (m->mode != AKB_MODE_FP64_REFERENCE && ne > 0) {
-    if ((st = build_device_patches(m.get(), mesh, element_material)) != AKB_OK) return st;
+    if ((st = build_device_patches(m.get(), mesh, element_material, batch)) != AKB_OK) return st;
+  }
+  if (batch) {
+    m->ninst = batch->ninst;
+    m->node_off = batch->node_off;
+    m->elem_off = batch->elem_off;
+    std::vector<double> dts(batch->ninst, 0.0);
+    if ((st = upload(m.get(), dts, (const double**)&m->d_inst_dt)) != AKB_OK) return st;
+    if ((st = upload(m.get(), batch->elem_off, &m->d_elem_off)) != AKB_OK) return st;
+    if ((st = upload(m.get(), batch->node_off, &m->d_node_off)) != AKB_OK) return st;
+    m->patches.inst_dt = m->d_inst_dt;
+    m->dt = 1.0;  // the step reads the instances' time steps from the device
+    AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
   }
   m->scratch_len = reduce_blocks(ne);
   if ((st = dalloc(m.get(), &m->d_scratch, m->scratch_len)) != AKB_OK) return st;
@@ -437,6 +546,8 @@ akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
   *out = m.release();
   return AKB_OK;
 }
+
+extern "C" {
 
 akb_status akb_model_destroy(akb_model* m) {
   if (!m) return AKB_OK;
@@ -765,6 +876,110 @@ akb_status akb_time_kernels(akb_model* m, int64_t nb_steps, double* ms_per_launc
 const char* akb_kernel_name(const akb_model* m, int32_t slot) {
   if (!m) return "";
   return kernel_name(m, slot);
+}
+
+akb_status akb_batch_create(const akb_batch_desc* batch, const akb_model_options* options,
+                            akb_model** out) {
+  if (!out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  if (!batch || batch->nb_instances < 1 || !batch->meshes || !batch->materials)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "batch needs at least one mesh and its materials");
+  const akb_model_options opt =
+      options ? *options : akb_model_options{AKB_MODE_FP64, 0, nullptr, 0, 0, 0};
+  if (opt.precision_mode == AKB_MODE_FP64_REFERENCE)
+    return fail(AKB_ERR_UNSUPPORTED, "batches run the fast modes (AKB_MODE_FP64 or AKB_MODE_FP32_BULK)");
+  const akb_mesh_desc& m0 = batch->meshes[0];
+  BatchLayout lay;
+  lay.ninst = batch->nb_instances;
+  lay.node_off.push_back(0);
+  lay.elem_off.push_back(0);
+  const int n = nnpe_of(m0.element_type), d = m0.spatial_dimension;
+  for (int i = 0; i < lay.ninst; ++i) {
+    const akb_mesh_desc& mi = batch->meshes[i];
+    if (mi.element_type != m0.element_type || mi.spatial_dimension != d)
+      return fail(AKB_ERR_BAD_MESH, "instances of a batch share one element type");
+    if (mi.nb_nodes <= 0 || mi.nb_elements <= 0 || !mi.nodes || !mi.connectivity)
+      return fail(AKB_ERR_BAD_MESH, "empty instance mesh");
+    for (int64_t k = 0; k < mi.nb_elements * n; ++k)
+      if (mi.connectivity[k] >= (uint64_t)mi.nb_nodes)
+        return fail(AKB_ERR_BAD_MESH, "instance connectivity refers to a node out of range");
+    lay.node_off.push_back(lay.node_off.back() + mi.nb_nodes);
+    lay.elem_off.push_back(lay.elem_off.back() + mi.nb_elements);
+  }
+  if (lay.node_off.back() >= (int64_t)UINT32_MAX)
+    return fail(AKB_ERR_UNSUPPORTED, "more than 2^32 nodes in a batch");
+  std::vector<double> X((size_t)lay.node_off.back() * d);
+  std::vector<uint32_t> conn((size_t)lay.elem_off.back() * n), mat(lay.elem_off.back());
+  for (int i = 0; i < lay.ninst; ++i) {
+    const akb_mesh_desc& mi = batch->meshes[i];
+    std::copy(mi.nodes, mi.nodes + mi.nb_nodes * d, X.begin() + lay.node_off[i] * d);
+    for (int64_t k = 0; k < mi.nb_elements * n; ++k)
+      conn[lay.elem_off[i] * n + k] = (uint32_t)(mi.connectivity[k] + lay.node_off[i]);
+    std::fill(mat.begin() + lay.elem_off[i], mat.begin() + lay.elem_off[i + 1], (uint32_t)i);
+  }
+  akb_mesh_desc um{d, m0.element_type, lay.node_off.back(), lay.elem_off.back(), X.data(),
+                   conn.data()};
+  return create_model(&um, lay.ninst, batch->materials, mat.data(), &opt, &lay, out);
+}
+
+akb_status akb_batch_get_layout(const akb_model* m, int32_t* nb_instances, int64_t* node_offsets,
+                                int64_t* element_offsets) {
+  if (!m) return fail(AKB_ERR_INVALID_ARGUMENT, "null model");
+  if (m->ninst == 0) return fail(AKB_ERR_STATE, "not a batch");
+  if (nb_instances) *nb_instances = m->ninst;
+  if (node_offsets) std::copy(m->node_off.begin(), m->node_off.end(), node_offsets);
+  if (element_offsets) std::copy(m->elem_off.begin(), m->elem_off.end(), element_offsets);
+  return AKB_OK;
+}
+
+akb_status akb_batch_set_time_steps(akb_model* m, const double* dt) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (m->ninst == 0) return fail(AKB_ERR_STATE, "not a batch");
+  if (!dt) return fail(AKB_ERR_INVALID_ARGUMENT, "null time steps");
+  for (int i = 0; i < m->ninst; ++i)
+    if (!(dt[i] > 0) || !std::isfinite(dt[i]))
+      return fail(AKB_ERR_INVALID_ARGUMENT, "time steps must be > 0");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(cudaMemcpyAsync(m->d_inst_dt, dt, m->ninst * sizeof(double), cudaMemcpyHostToDevice,
+                               m->stream));
+  return sync(m);
+}
+
+akb_status akb_batch_get_stable_time_steps(akb_model* m, double* dt) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (m->ninst == 0) return fail(AKB_ERR_STATE, "not a batch");
+  if (!dt) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  double* out;
+  if ((st = dalloc(m, &out, m->ninst)) != AKB_OK) return st;
+  cudaError_t e = stable_dt_instances(m->dm, m->d_elem_off, m->ninst, out, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dt, out, m->ninst * sizeof(double), cudaMemcpyDeviceToHost, m->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+  dfree(m, out);
+  if (e != cudaSuccess) return fail(AKB_ERR_CUDA, cudaGetErrorString(e));
+  return AKB_OK;
+}
+
+akb_status akb_batch_get_energies(akb_model* m, int32_t kind, double* values) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (m->ninst == 0) return fail(AKB_ERR_STATE, "not a batch");
+  if (!values) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  if (kind != AKB_ENERGY_KINETIC && kind != AKB_ENERGY_POTENTIAL)
+    return fail(AKB_ERR_UNSUPPORTED, "per-instance energies: kinetic or potential");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  double* out;
+  if ((st = dalloc(m, &out, m->ninst)) != AKB_OK) return st;
+  cudaError_t e = energy_instances(m->dm, kind, m->d_node_off, m->d_elem_off, m->ninst, out, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(values, out, m->ninst * sizeof(double), cudaMemcpyDeviceToHost, m->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+  dfree(m, out);
+  if (e != cudaSuccess) return fail(AKB_ERR_CUDA, cudaGetErrorString(e));
+  return AKB_OK;
 }
 
 akb_status akb_synchronize(akb_model* m) {

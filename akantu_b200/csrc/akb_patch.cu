@@ -74,12 +74,15 @@ constexpr int kBatch = 4;
 
 template <int T, typename S, bool FEXT>
 __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
-    k_patch_step(DevModel m, DevPatches P, double dt) {
+    k_patch_step(DevModel m, DevPatches P, double dt0) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
   constexpr int CH = kChunk * n;  // sorted slots of one chunk
   static_assert(kChunk == kThreads, "one element per thread per chunk");
   extern __shared__ __align__(16) unsigned char smem[];
-  const int p = blockIdx.x;
+  // one patch per CTA, or several per CTA when the grid is persistent
+  for (int p = blockIdx.x; p < P.npatch; p += gridDim.x) {
+  if (p != (int)blockIdx.x) __syncthreads();  // shared memory of the previous patch is free
+  const double dt = P.inst_dt ? P.inst_dt[P.patch_inst[p]] : dt0;
   const int nb = P.node_ptr[p];
   const int L = P.node_ptr[p + 1] - nb;
   const int eb = P.elem_ptr[p];
@@ -154,7 +157,7 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
       int lc[n];
 #pragma unroll
       for (int a = 0; a < n; ++a) lc[a] = lcs[el * n + a];
-      const MatParams& mp = m.mats[P.emat ? P.emat[(size_t)eb + el] : 0];
+      const MatParams& mp = (P.emat ? m.mat_table[P.emat[(size_t)eb + el]] : m.mats[0]);
       S dX[3 * 8], du[3 * 8];
 #pragma unroll
       for (int i = 0; i < d; ++i) {
@@ -233,13 +236,15 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
       }
     }
   }
+  }  // patches of this CTA
 }
 
 template <int D, bool FEXT>
-__global__ void k_shared_nodes(DevModel m, DevPatches P, double dt) {
+__global__ void k_shared_nodes(DevModel m, DevPatches P, double dt0) {
   const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= P.nshared) return;
   const int64_t g = P.snodes[s];
+  const double dt = P.inst_dt ? P.inst_dt[P.snode_inst[s]] : dt0;
   const int k0 = P.sptr[s], k1 = P.sptr[s + 1];
   double f[3] = {0, 0, 0};
   for (int k = k0; k < k1; ++k)
@@ -261,14 +266,20 @@ __global__ void k_shared_nodes(DevModel m, DevPatches P, double dt) {
   }
 }
 
+// grid of the patch kernel: one CTA per patch, or a persistent grid of
+// P.grid CTAs that stride over the patches
+inline int grid_of(const DevPatches& p) {
+  return (p.grid > 0 && p.grid < p.npatch) ? p.grid : p.npatch;
+}
+
 template <int T, typename S>
 cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool fext,
                          cudaStream_t s) {
   const SmemLayout lay = layout(p.max_nodes, p.max_elems, p.max_segs, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
   if (fext)
-    k_patch_step<T, S, true><<<p.npatch, kThreads, lay.total, s>>>(m, p, dt);
+    k_patch_step<T, S, true><<<grid_of(p), kThreads, lay.total, s>>>(m, p, dt);
   else
-    k_patch_step<T, S, false><<<p.npatch, kThreads, lay.total, s>>>(m, p, dt);
+    k_patch_step<T, S, false><<<grid_of(p), kThreads, lay.total, s>>>(m, p, dt);
   return cudaGetLastError();
 }
 

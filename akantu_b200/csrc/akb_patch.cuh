@@ -56,6 +56,7 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
 // Device copy of a PatchHost.
 struct DevPatches {
   int npatch;
+  int grid;  // 0: one CTA per patch; > 0: persistent grid of that many CTAs
   int max_nodes, max_elems, max_segs;
   int64_t nshared;
   const int32_t* elem_ptr;
@@ -74,6 +75,10 @@ struct DevPatches {
   const int32_t* sptr;
   const uint32_t* emat;  // material of each patch-ordered element, or null
   double* partial;       // nslots x dim
+  // batches: per-instance time step, instance of each patch and shared node
+  const double* inst_dt;       // null for a single model (scalar dt)
+  const uint32_t* patch_inst;
+  const uint32_t* snode_inst;
 };
 
 size_t patch_smem_bytes(const DevPatches& p, int dim, int nnpe, bool fp32, int threads);

@@ -109,7 +109,7 @@ __global__ void k_stable_dt(DevModel m, double* partial) {
       }
     }
     const double h = inradius<T>(Xel);
-    const double c = m.mats[m.mat_of ? m.mat_of[e] : 0].celerity;
+    const double c = (m.mat_of ? m.mat_table[m.mat_of[e]] : m.mats[0]).celerity;
     acc = fmin(acc, h / c);
   }
   acc = block_reduce<kMin>(acc);
@@ -155,7 +155,7 @@ __global__ void k_potential(DevModel m, double* partial) {
   double acc = 0.;
   for (int64_t e = blockIdx.x * (int64_t)kThreads + threadIdx.x; e < m.ne;
        e += (int64_t)gridDim.x * kThreads) {
-    const MatParams& p = m.mats[m.mat_of ? m.mat_of[e] : 0];
+    const MatParams& p = (m.mat_of ? m.mat_table[m.mat_of[e]] : m.mats[0]);
     double Xel[3 * 8], uel[3 * 8];
     for (int a = 0; a < n; ++a) {
       const uint32_t node = m.conn[e * n + a];
@@ -176,6 +176,72 @@ __global__ void k_potential(DevModel m, double* partial) {
   }
   acc = block_reduce<kSum>(acc);
   if (threadIdx.x == 0) partial[blockIdx.x] = acc;
+}
+
+// Batches: block b reduces instance b's elements (or nodes).
+template <int T>
+__global__ void k_stable_dt_inst(DevModel m, const int64_t* elem_off, double* out) {
+  constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
+  double acc = DBL_MAX;
+  for (int64_t e = elem_off[blockIdx.x] + threadIdx.x; e < elem_off[blockIdx.x + 1]; e += kThreads) {
+    double Xel[3 * 8];
+    for (int a = 0; a < n; ++a) {
+      const uint32_t node = m.conn[e * n + a];
+      for (int i = 0; i < d; ++i) {
+        double x = m.X[(int64_t)node * d + i];
+        x += m.u[(int64_t)node * d + i];
+        Xel[a * d + i] = x;
+      }
+    }
+    const double c = (m.mat_of ? m.mat_table[m.mat_of[e]] : m.mats[0]).celerity;
+    acc = fmin(acc, inradius<T>(Xel) / c);
+  }
+  acc = block_reduce<kMin>(acc);
+  if (threadIdx.x == 0) out[blockIdx.x] = acc;
+}
+
+__global__ void k_kinetic_inst(DevModel m, const int64_t* node_off, double* out) {
+  const int d = m.dim;
+  double acc = 0.;
+  for (int64_t node = node_off[blockIdx.x] + threadIdx.x; node < node_off[blockIdx.x + 1];
+       node += kThreads) {
+    double mv2 = 0.;
+    for (int i = 0; i < d; ++i) {
+      const double mm = m.mass[node * d + i], vv = m.v[node * d + i];
+      if (mm > DBL_EPSILON) mv2 += vv * vv * mm;
+    }
+    acc += mv2;
+  }
+  acc = block_reduce<kSum>(acc);
+  if (threadIdx.x == 0) out[blockIdx.x] = acc * 0.5;
+}
+
+template <int T>
+__global__ void k_potential_inst(DevModel m, const int64_t* elem_off, double* out) {
+  constexpr int d = ET<T>::dim, n = ET<T>::nnpe, q = ET<T>::nqp;
+  double acc = 0.;
+  for (int64_t e = elem_off[blockIdx.x] + threadIdx.x; e < elem_off[blockIdx.x + 1]; e += kThreads) {
+    const MatParams& p = (m.mat_of ? m.mat_table[m.mat_of[e]] : m.mats[0]);
+    double Xel[3 * 8], uel[3 * 8];
+    for (int a = 0; a < n; ++a) {
+      const uint32_t node = m.conn[e * n + a];
+      for (int i = 0; i < d; ++i) {
+        Xel[i + a * d] = m.X[(int64_t)node * d + i];
+        uel[i + a * d] = m.u[(int64_t)node * d + i];
+      }
+    }
+    double inte = 0.;
+    for (int pq = 0; pq < q; ++pq) {
+      double B[3 * 8], jac, g[9], s[9];
+      ref::geometry<T>(Xel, pq, B, &jac);
+      ref::mmt<d, d, n>(uel, B, g);
+      ref::stress<d>(p, g, s);
+      inte += ref::energy_density<d>(p, g, s) * jac;
+    }
+    acc += inte;
+  }
+  acc = block_reduce<kSum>(acc);
+  if (threadIdx.x == 0) out[blockIdx.x] = acc;
 }
 
 int grid_for(int64_t n) {
@@ -227,6 +293,38 @@ cudaError_t energy(const DevModel& m, int kind, double dt, double* scratch, int 
     }
   }
   k_finish<kSum><<<1, kThreads, 0, s>>>(scratch, g, scale, out);
+  return cudaGetLastError();
+}
+
+}  // namespace akb
+
+namespace akb {
+
+cudaError_t stable_dt_instances(const DevModel& m, const int64_t* elem_off, int ninst,
+                                double* out, cudaStream_t s) {
+  if (ninst <= 0) return cudaSuccess;
+  switch (m.type) {
+  case AKB_SEGMENT_2: k_stable_dt_inst<AKB_SEGMENT_2><<<ninst, kThreads, 0, s>>>(m, elem_off, out); break;
+  case AKB_TRIANGLE_3: k_stable_dt_inst<AKB_TRIANGLE_3><<<ninst, kThreads, 0, s>>>(m, elem_off, out); break;
+  case AKB_TETRAHEDRON_4: k_stable_dt_inst<AKB_TETRAHEDRON_4><<<ninst, kThreads, 0, s>>>(m, elem_off, out); break;
+  default: k_stable_dt_inst<AKB_HEXAHEDRON_8><<<ninst, kThreads, 0, s>>>(m, elem_off, out); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t energy_instances(const DevModel& m, int kind, const int64_t* node_off,
+                             const int64_t* elem_off, int ninst, double* out, cudaStream_t s) {
+  if (ninst <= 0) return cudaSuccess;
+  if (kind == AKB_ENERGY_KINETIC) {
+    k_kinetic_inst<<<ninst, kThreads, 0, s>>>(m, node_off, out);
+  } else {
+    switch (m.type) {
+    case AKB_SEGMENT_2: k_potential_inst<AKB_SEGMENT_2><<<ninst, kThreads, 0, s>>>(m, elem_off, out); break;
+    case AKB_TRIANGLE_3: k_potential_inst<AKB_TRIANGLE_3><<<ninst, kThreads, 0, s>>>(m, elem_off, out); break;
+    case AKB_TETRAHEDRON_4: k_potential_inst<AKB_TETRAHEDRON_4><<<ninst, kThreads, 0, s>>>(m, elem_off, out); break;
+    default: k_potential_inst<AKB_HEXAHEDRON_8><<<ninst, kThreads, 0, s>>>(m, elem_off, out); break;
+    }
+  }
   return cudaGetLastError();
 }
 

@@ -68,7 +68,7 @@ __global__ void k_element_forces(DevModel m) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe, q = ET<T>::nqp;
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= m.ne) return;
-  const MatParams& p = m.mats[m.mat_of ? m.mat_of[e] : 0];
+  const MatParams& p = (m.mat_of ? m.mat_table[m.mat_of[e]] : m.mats[0]);
   double uel[3 * 8], inte[3 * 8], r[3 * 8];
   gather_el<T>(m, e, m.u, uel);
 #pragma unroll
@@ -138,7 +138,7 @@ __global__ void k_mass_element(DevModel m) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe, q = ET<T>::nqp;
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= m.ne) return;
-  const MatParams& p = m.mats[m.mat_of ? m.mat_of[e] : 0];
+  const MatParams& p = (m.mat_of ? m.mat_table[m.mat_of[e]] : m.mats[0]);
   double inte[3 * 8];
 #pragma unroll
   for (int k = 0; k < d * n; ++k) inte[k] = 0.;
@@ -181,7 +181,7 @@ __global__ void k_compute_stresses(DevModel m, bool recompute_geometry) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe, q = ET<T>::nqp;
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= m.ne) return;
-  const MatParams& p = m.mats[m.mat_of ? m.mat_of[e] : 0];
+  const MatParams& p = (m.mat_of ? m.mat_table[m.mat_of[e]] : m.mats[0]);
   double uel[3 * 8], Xel[3 * 8];
   gather_el<T>(m, e, m.u, uel);
   if (recompute_geometry) gather_el<T>(m, e, m.X, Xel);

@@ -321,6 +321,118 @@ def run_ours(args, dist):
     return result
 
 
+def run_hex8(args, device, peak):
+    """3D finite-strain neo-Hookean block, 128^3 hexahedron_8 (2 097 152
+    elements), FP32 element arithmetic with FP64 nodal state, against the
+    FP64 GPU run of the same steps (the FP64 CPU oracle at this size would
+    take hours; the small-size parity tests compare both to the oracle)."""
+    w = configs.block_hex8(args.hex_cells, 0.01 * args.hex_cells)
+    E = w["mesh"].getNbElement()
+    steps = w["steps"] if args.hex_steps <= 0 else args.hex_steps
+    out = {"workload": "block_hex8: %d^3 hexahedron_8, 2x2x2 Gauss, neo-Hookean lambda = 1 MPa, "
+                       "mu = 0.4 MPa, rho = 1100, face x = 0 fixed, v ~ N(0, 0.05)" % args.hex_cells,
+           "elements": E, "steps": steps}
+    states = {}
+    for name, mode in (("fp32_bulk", _abi.MODE_FP32_BULK), ("fp64", _abi.MODE_FP64)):
+        m = make_model(w, mode, device)
+        dt = configs.setup_model(Facade(m), w)
+        m.solveSteps(3)
+        reset_state(m, w)
+        ms = m.timeSolveSteps(steps)
+        fb = b_alg_bytes(w, mode == _abi.MODE_FP32_BULK)
+        states[name] = (m.getDisplacement().copy(), m.getInternalForce().copy())
+        out[name] = {"value": E * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+                     "hbm_roofline_frac": fb / (ms / steps / 1e3) / 1e9 / peak,
+                     "kernels_ms": dict(kernel_times(m, 10))}
+        m.close()
+    (u32, f32), (u64, f64) = states["fp32_bulk"], states["fp64"]
+    out["fp32_vs_fp64"] = {"rel_err_displacement": float(np.abs(u32 - u64).max() / np.abs(u64).max()),
+                           "rel_err_internal_force": float(np.abs(f32 - f64).max() / np.abs(f64).max())}
+    out["time_step"] = dt
+    return out
+
+
+def run_batch(args, device, log=None):
+    """4096 triangle_3 plates of uneven size in one batch (one fused launch
+    per step, CUDA-graph replay, autotuned patch shape and schedule), and the
+    same plates as separate models on a sample of instances."""
+    from akantu_b200 import autotune
+    from akantu_b200.batch import BatchModel
+    w = configs.plates_batch(args.batch_instances)
+    E = sum(m.getNbElement() for m in w["meshes"])
+    steps = w["steps"] if args.batch_steps <= 0 else args.batch_steps
+    # tune on a sample of the instances, then build the whole batch
+    rng = np.random.default_rng(1)
+    sample = sorted(rng.choice(len(w["meshes"]), size=min(256, len(w["meshes"])), replace=False))
+    ws = {k: ([w[k][i] for i in sample] if isinstance(w[k], list) else w[k]) for k in w}
+
+    def build(pe, pn, grid, ww=ws):
+        b = BatchModel(ww["meshes"], ww["materials"], precision=_abi.MODE_FP64, device=device,
+                       patch_elements=pe, patch_nodes=pn, patch_grid=grid)
+        b.initFull()
+        configs.setup_batch(b, ww)
+        return b
+    best, trials = autotune.tune(build, _abi.TRIANGLE_3, _abi.MODE_FP64,
+                                 sum(m.getNbElement() for m in ws["meshes"]) * len(w["meshes"]) // len(sample),
+                                 log=log)
+    b = build(best["patch_elements"], best["patch_nodes"], best["patch_grid"], w)
+    b.solveSteps(3)
+    configs.setup_batch(b, w)
+    ms = b.timeSolveSteps(steps)
+    out = {"workload": "%d triangle_3 plates, %d elements, %d nodes, per-plate E, nu, rho, dt"
+                       % (len(w["meshes"]), E, int(b.node_offsets[-1])),
+           "elements": E, "steps": steps,
+           "batched": {"value": E * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+                       "launches_per_step": len(kernel_times(b, 5)), "tuned": best,
+                       "trials_ms_per_step": [[t[0], t[1]] for t in trials]}}
+    b.close()
+    # the same sample as separate models (one model per plate, graph replays)
+    sub_steps = 20
+    models = []
+    for i in sample:
+        m = SolidMechanicsModel_for(w, i, device, best)
+        models.append(m)
+    import torch
+    for m in models:  # instantiates each model's graph outside the timed loop
+        m.solveSteps(sub_steps)
+    for m in models:
+        m.synchronize()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for m in models:
+        m.solveSteps(sub_steps)
+    for m in models:
+        m.synchronize()
+    t1 = time.perf_counter()
+    Es = sum(w["meshes"][i].getNbElement() for i in sample)
+    bs = build(best["patch_elements"], best["patch_nodes"], best["patch_grid"], ws)
+    bs.solveSteps(2 * sub_steps)
+    ub = bs.getField(_abi.FIELD_DISPLACEMENT)
+    same = all(np.array_equal(ub[bs.instance_rows(j)], m.getDisplacement())
+               for j, m in enumerate(models))
+    msb = bs.timeSolveSteps(sub_steps)
+    out["per_mesh_sample"] = {"instances": len(sample), "elements": Es, "steps": sub_steps,
+                              "per_mesh_value": Es * sub_steps / (t1 - t0),
+                              "batched_value": Es * sub_steps / (msb / 1e3),
+                              "bitwise_equal_to_batched": bool(same), "unit": UNIT}
+    for m in models:
+        m.close()
+    bs.close()
+    return out
+
+
+def SolidMechanicsModel_for(w, i, device, opts):
+    from akantu_b200.model import SolidMechanicsModel, material_from_dict
+    m = SolidMechanicsModel(w["meshes"][i], [material_from_dict(w["materials"][i])],
+                            precision=_abi.MODE_FP64, device=device,
+                            patch_elements=opts["patch_elements"], patch_nodes=opts["patch_nodes"])
+    m.initFull()
+    m.setBlockedDOFs(w["blocked"][i])
+    m.setField(_abi.FIELD_DISPLACEMENT, w["u0"][i])
+    m.setTimeStep(w["dt_factor"] * m.getStableTimeStep())
+    return m
+
+
 def run_reference(args, dist):
     if dist.rank != 0:
         return None
@@ -364,6 +476,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cells", type=int, default=100,
                     help="cells per cube side (100 = the benchmark; smaller for profiling)")
+    ap.add_argument("--only-headline", action="store_true",
+                    help="skip the hexahedron and batch workloads")
+    ap.add_argument("--hex-cells", type=int, default=128)
+    ap.add_argument("--hex-steps", type=int, default=0, help="0 = the workload's 2000 steps")
+    ap.add_argument("--batch-instances", type=int, default=4096)
+    ap.add_argument("--batch-steps", type=int, default=0, help="0 = the workload's 500 steps")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -385,6 +503,13 @@ def main():
         res = run_ours(args, dist)
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(configs.cube_tet4(args.cells))
+        if dist.rank == 0 and not args.only_headline:
+            peak, _ = load_peaks()
+            res["workloads"] = {
+                "block_hex8": run_hex8(args, dist.local_rank, peak),
+                "plates_batch": run_batch(args, dist.local_rank,
+                                          log=lambda s: print(s, file=sys.stderr, flush=True)),
+            }
         if dist.rank == 0:
             print(json.dumps(res), flush=True)
     finally:

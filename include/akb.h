@@ -115,6 +115,8 @@ typedef struct {
   void* stream;           /* cudaStream_t to run on; NULL = library-owned stream */
   int32_t patch_elements; /* fast modes: elements per patch (0 = per-type default) */
   int32_t patch_nodes;    /* fast modes: node cap of a patch (0 = per-type default) */
+  int32_t patch_grid;     /* fast modes: 0 = one CTA per patch; > 0 = persistent grid
+                             of that many CTAs striding over the patches */
 } akb_model_options;
 
 typedef struct {
@@ -212,6 +214,33 @@ akb_status akb_time_kernels(akb_model* model, int64_t nb_steps,
                             double* ms_per_launch, int32_t nb_slots);
 /* Name of the step's k-th kernel, or "" past the last one. */
 const char* akb_kernel_name(const akb_model* model, int32_t slot);
+
+/* ------------------------------------------------------------------------
+ * Batches: many independent meshes of one element type stepped together.
+ * No counterpart in the reference (it runs one SolidMechanicsModel per
+ * process); each instance follows the single-model path exactly: its own
+ * material (one per instance), its own time step, the same per-instance
+ * patches, so its state is bitwise the one a model of that mesh alone gives.
+ * The batch is an akb_model over the union mesh (instances concatenated in
+ * order; fields, blocked DOFs, Dirichlet values and akb_solve_steps work on
+ * the union arrays). Fast modes only (AKB_MODE_FP64, AKB_MODE_FP32_BULK). */
+typedef struct {
+  int32_t nb_instances;
+  const akb_mesh_desc* meshes;        /* nb_instances meshes, same element type */
+  const akb_material_desc* materials; /* one material per instance */
+} akb_batch_desc;
+
+akb_status akb_batch_create(const akb_batch_desc* batch, const akb_model_options* options,
+                            akb_model** model);
+/* node_offsets / element_offsets: nb_instances + 1 entries each, or NULL. */
+akb_status akb_batch_get_layout(const akb_model* model, int32_t* nb_instances,
+                                int64_t* node_offsets, int64_t* element_offsets);
+/* Per-instance time steps (nb_instances values). */
+akb_status akb_batch_set_time_steps(akb_model* model, const double* time_steps);
+/* getStableTimeStep of every instance (solid_mechanics_model.cc:482-533). */
+akb_status akb_batch_get_stable_time_steps(akb_model* model, double* time_steps);
+/* getEnergy of every instance, AKB_ENERGY_KINETIC or AKB_ENERGY_POTENTIAL. */
+akb_status akb_batch_get_energies(akb_model* model, int32_t kind, double* values);
 
 /* Kinetic energy 1/2 sum(m v^2) of device arrays, allocating no memory.
  * No counterpart in the reference: it serves callers that cannot call
