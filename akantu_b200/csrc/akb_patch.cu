@@ -13,6 +13,8 @@
 //      back; nodes shared with other patches: FP64 partial force to its slot.
 // k_shared_nodes: one thread per shared node adds its partials in patch order
 // and applies the same predictor/corrector arithmetic.
+#include <mutex>
+
 #include "akb_fastmath.cuh"
 #include "akb_patch.cuh"
 
@@ -72,16 +74,13 @@ template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, double> { static constexpr i
 // finishing loops: their global loads are issued together.
 constexpr int kBatch = 4;
 
+// One patch p, by the whole CTA.
 template <int T, typename S, bool FEXT>
-__global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
-    k_patch_step(DevModel m, DevPatches P, double dt0) {
+__device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& P, double dt0,
+                                           int p, unsigned char* smem) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
   constexpr int CH = kChunk * n;  // sorted slots of one chunk
   static_assert(kChunk == kThreads, "one element per thread per chunk");
-  extern __shared__ __align__(16) unsigned char smem[];
-  // one patch per CTA, or several per CTA when the grid is persistent
-  for (int p = blockIdx.x; p < P.npatch; p += gridDim.x) {
-  if (p != (int)blockIdx.x) __syncthreads();  // shared memory of the previous patch is free
   const double dt = P.inst_dt ? P.inst_dt[P.patch_inst[p]] : dt0;
   const int nb = P.node_ptr[p];
   const int L = P.node_ptr[p + 1] - nb;
@@ -236,7 +235,23 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
       }
     }
   }
-  }  // patches of this CTA
+}
+
+// One CTA per patch, or (PERSIST) a grid smaller than the patch count whose
+// CTAs stride over the patches. The loop is a separate instantiation: kept
+// out of the one-patch kernel it would raise that kernel's register pressure.
+template <int T, typename S, bool FEXT, bool PERSIST>
+__global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
+    k_patch_step(DevModel m, DevPatches P, double dt0) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if constexpr (PERSIST) {
+    for (int p = blockIdx.x; p < P.npatch; p += gridDim.x) {
+      if (p != (int)blockIdx.x) __syncthreads();  // shared memory of the previous patch is free
+      patch_body<T, S, FEXT>(m, P, dt0, p, smem);
+    }
+  } else {
+    patch_body<T, S, FEXT>(m, P, dt0, blockIdx.x, smem);
+  }
 }
 
 template <int D, bool FEXT>
@@ -276,21 +291,45 @@ template <int T, typename S>
 cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool fext,
                          cudaStream_t s) {
   const SmemLayout lay = layout(p.max_nodes, p.max_elems, p.max_segs, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
-  if (fext)
-    k_patch_step<T, S, true><<<grid_of(p), kThreads, lay.total, s>>>(m, p, dt);
-  else
-    k_patch_step<T, S, false><<<grid_of(p), kThreads, lay.total, s>>>(m, p, dt);
+  const int grid = grid_of(p);
+  if (grid < p.npatch) {
+    if (fext)
+      k_patch_step<T, S, true, true><<<grid, kThreads, lay.total, s>>>(m, p, dt);
+    else
+      k_patch_step<T, S, false, true><<<grid, kThreads, lay.total, s>>>(m, p, dt);
+  } else {
+    if (fext)
+      k_patch_step<T, S, true, false><<<grid, kThreads, lay.total, s>>>(m, p, dt);
+    else
+      k_patch_step<T, S, false, false><<<grid, kThreads, lay.total, s>>>(m, p, dt);
+  }
   return cudaGetLastError();
+}
+
+// The dynamic shared memory limit is an attribute of the kernel function in
+// the device's context, shared by every model of the process: it is only ever
+// raised, so that a model built later with smaller patches cannot lower it
+// below what an earlier model launches with.
+std::mutex g_attr_mutex;
+
+template <typename K>
+cudaError_t raise_smem_limit(K kernel, size_t bytes) {
+  cudaFuncAttributes attr;
+  cudaError_t e = cudaFuncGetAttributes(&attr, kernel);
+  if (e != cudaSuccess) return e;
+  if ((size_t)attr.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 template <int T, typename S>
 cudaError_t configure(const DevPatches& p) {
   const SmemLayout lay = layout(p.max_nodes, p.max_elems, p.max_segs, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
-  cudaError_t e = cudaFuncSetAttribute(k_patch_step<T, S, true>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_patch_step<T, S, false>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay.total);
+  std::lock_guard<std::mutex> lock(g_attr_mutex);
+  cudaError_t e;
+  if ((e = raise_smem_limit(k_patch_step<T, S, true, false>, lay.total)) != cudaSuccess) return e;
+  if ((e = raise_smem_limit(k_patch_step<T, S, false, false>, lay.total)) != cudaSuccess) return e;
+  if ((e = raise_smem_limit(k_patch_step<T, S, true, true>, lay.total)) != cudaSuccess) return e;
+  return raise_smem_limit(k_patch_step<T, S, false, true>, lay.total);
 }
 
 }  // namespace

@@ -71,6 +71,27 @@ def test_batch_matches_oracle_and_energies():
         assert ep[k] == pytest.approx(cpu.energy(_abi.ENERGY_POTENTIAL), rel=1e-10)
 
 
+def test_models_with_different_patch_sizes_coexist():
+    """The kernel's shared-memory limit is process-wide: a model built after
+    another with smaller patches must not break the first one's launches."""
+    w = small_batch(8)
+    sizes = [m.getNbElement() for m in w["meshes"]]
+    big, small = int(np.argmax(sizes)), int(np.argmin(sizes))
+    opts = dict(patch_elements=2048, patch_nodes=1100)
+    a = single_model(w, big, _abi.MODE_FP64, opts)
+    a.setTimeStep(w["dt_factor"] * a.getStableTimeStep())
+    b = single_model(w, small, _abi.MODE_FP64, dict(patch_elements=128, patch_nodes=100))
+    b.setTimeStep(w["dt_factor"] * b.getStableTimeStep())
+    a.solveSteps(40)
+    b.solveSteps(40)
+    ref = single_model(w, big, _abi.MODE_FP64, opts)
+    ref.setTimeStep(w["dt_factor"] * ref.getStableTimeStep())
+    ref.solveSteps(40)
+    assert np.array_equal(a.getDisplacement(), ref.getDisplacement())
+    for m in (a, b, ref):
+        m.close()
+
+
 def test_batch_rejects_reference_mode_and_mixed_types():
     from akantu_b200._lib import AkbError
     w = small_batch(2)
