@@ -9,7 +9,7 @@ from . import _abi
 from ._abi import (MODE_FP32_BULK, MODE_FP64, MODE_FP64_REFERENCE, HEXAHEDRON_8,
                    SEGMENT_2, TETRAHEDRON_4, TRIANGLE_3)
 from .mesh import Mesh
-from .model import (MaterialElastic, MaterialNeohookean, SolidMechanicsModel,
+from .model import (MaterialElastic, MaterialNeohookean, MaterialUser, SolidMechanicsModel,
                     _explicit_lumped_mass)
 
 _segment_2 = SEGMENT_2
@@ -17,5 +17,5 @@ _triangle_3 = TRIANGLE_3
 _tetrahedron_4 = TETRAHEDRON_4
 _hexahedron_8 = HEXAHEDRON_8
 
-__all__ = ["Mesh", "SolidMechanicsModel", "MaterialElastic", "MaterialNeohookean",
+__all__ = ["Mesh", "SolidMechanicsModel", "MaterialElastic", "MaterialNeohookean", "MaterialUser",
            "_explicit_lumped_mass", "MODE_FP64_REFERENCE", "MODE_FP64", "MODE_FP32_BULK"]

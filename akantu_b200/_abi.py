@@ -30,6 +30,7 @@ HEXAHEDRON_8 = 4
 # materials
 MATERIAL_ELASTIC = 0
 MATERIAL_NEOHOOKEAN = 1
+MATERIAL_USER = 2
 
 # precision modes
 MODE_FP64_REFERENCE = 0
@@ -107,3 +108,22 @@ class ModelInfo(C.Structure):
         ("nb_materials", C.c_int32),
         ("device_bytes", C.c_int64),
     ]
+
+
+# ---- include/akb_fe2.h
+class RveDesc(C.Structure):
+    _fields_ = [("cells", C.c_int32), ("nb_materials", C.c_int32), ("length", C.c_double),
+                ("voxel_material", C.POINTER(C.c_uint8)),
+                ("materials", C.POINTER(MaterialDesc))]
+
+
+class RveOptions(C.Structure):
+    _fields_ = [("precision_mode", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p),
+                ("max_iterations", C.c_int32), ("check_interval", C.c_int32),
+                ("tolerance", C.c_double), ("time_step_factor", C.c_double),
+                ("damping_factor", C.c_double)]
+
+
+class RveInfo(C.Structure):
+    _fields_ = [("cells", C.c_int32), ("precision_mode", C.c_int32), ("nb_nodes", C.c_int64),
+                ("volume_fraction", C.c_double * 8), ("shared_bytes", C.c_int64)]

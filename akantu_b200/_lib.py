@@ -55,6 +55,15 @@ SIGNATURES = {
     "akb_batch_get_energies": (I32, [P, I32, PD]),
     "akb_kinetic_energy_static": (I32, [P, P, I64, I32, P, P]),
     "akb_synchronize": (I32, [P]),
+    # include/akb_fe2.h
+    "akb_step_begin": (I32, [P]),
+    "akb_step_end": (I32, [P]),
+    "akb_model_get_stream": (I32, [P, C.POINTER(P)]),
+    "akb_rve_create": (I32, [C.POINTER(_abi.RveDesc), C.POINTER(_abi.RveOptions), C.POINTER(P)]),
+    "akb_rve_destroy": (I32, [P]),
+    "akb_rve_get_info": (I32, [P, C.POINTER(_abi.RveInfo)]),
+    "akb_rve_solve": (I32, [P, I64, P, P, P, P, P, P]),
+    "akb_rve_stress": (I32, [P, I64, P, P, P, P, P]),
 }
 
 

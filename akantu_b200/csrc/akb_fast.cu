@@ -98,6 +98,79 @@ cudaError_t launch_elements(const DevModel& m, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// User materials: displacement gradient at every quadrature point (FP64,
+// column-major per point, like Material::gradu) ...
+template <int T>
+__global__ void k_qp_gradu(DevModel m) {
+  constexpr int d = ET<T>::dim, n = ET<T>::nnpe, nq = ET<T>::nqp;
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= m.ne) return;
+  double dX[3 * 8], du[3 * 8];
+  uint32_t nodes[8];
+#pragma unroll
+  for (int a = 0; a < n; ++a) nodes[a] = m.conn[e * n + a];
+#pragma unroll
+  for (int a = 0; a < n; ++a)
+#pragma unroll
+    for (int i = 0; i < d; ++i) {
+      dX[a * d + i] = m.X[(int64_t)nodes[a] * d + i] - m.X[(int64_t)nodes[0] * d + i];
+      du[a * d + i] = m.u[(int64_t)nodes[a] * d + i] - m.u[(int64_t)nodes[0] * d + i];
+    }
+#pragma unroll 1
+  for (int q = 0; q < nq; ++q) {
+    double B[3 * 8];
+    fast::shape_gradients<T, double>(dX, q, B);
+    double* g = m.gradu + (e * nq + q) * d * d;
+#pragma unroll
+    for (int i = 0; i < d; ++i)
+#pragma unroll
+      for (int j = 0; j < d; ++j) {
+        double c = 0;
+#pragma unroll
+        for (int a = 1; a < n; ++a) c += du[a * d + i] * B[a * d + j];
+        g[i + j * d] = c;
+      }
+  }
+}
+
+// ... and the element force vectors sum_q w_q det J_q stress_q grad N_a from
+// the stresses the caller wrote.
+template <int T>
+__global__ void k_qp_forces(DevModel m) {
+  constexpr int d = ET<T>::dim, n = ET<T>::nnpe, nq = ET<T>::nqp;
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= m.ne) return;
+  double dX[3 * 8], fe[3 * 8];
+  uint32_t nodes[8];
+#pragma unroll
+  for (int a = 0; a < n; ++a) nodes[a] = m.conn[e * n + a];
+#pragma unroll
+  for (int a = 0; a < n; ++a)
+#pragma unroll
+    for (int i = 0; i < d; ++i) {
+      dX[a * d + i] = m.X[(int64_t)nodes[a] * d + i] - m.X[(int64_t)nodes[0] * d + i];
+      fe[a * d + i] = 0.0;
+    }
+#pragma unroll 1
+  for (int q = 0; q < nq; ++q) {
+    double B[3 * 8];
+    const double wq = fast::weight<T>() * fast::shape_gradients<T, double>(dX, q, B);
+    const double* P = m.stress + (e * nq + q) * d * d;
+#pragma unroll
+    for (int a = 0; a < n; ++a)
+#pragma unroll
+      for (int i = 0; i < d; ++i) {
+        double c = 0;
+#pragma unroll
+        for (int j = 0; j < d; ++j) c += P[i + j * d] * B[a * d + j];
+        fe[a * d + i] += wq * c;
+      }
+  }
+  double* out = static_cast<double*>(m.fe) + e * d * n;
+#pragma unroll
+  for (int k = 0; k < d * n; ++k) out[k] = fe[k];
+}
+
 __global__ void k_apply_dirichlet(DevModel m, const uint32_t* nodes, int64_t n, int comp,
                                   const double* values) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -114,6 +187,28 @@ __global__ void k_apply_dirichlet(DevModel m, const uint32_t* nodes, int64_t n, 
 cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n, int comp,
                             const double* values, cudaStream_t s) {
   k_apply_dirichlet<<<blocks_for(n), kThreads, 0, s>>>(m, nodes, n, comp, values);
+  return cudaGetLastError();
+}
+
+cudaError_t user_qp_gradients(const DevModel& m, cudaStream_t s) {
+  if (m.ne == 0) return cudaSuccess;
+  switch (m.type) {
+  case AKB_SEGMENT_2: k_qp_gradu<AKB_SEGMENT_2><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  case AKB_TRIANGLE_3: k_qp_gradu<AKB_TRIANGLE_3><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  case AKB_TETRAHEDRON_4: k_qp_gradu<AKB_TETRAHEDRON_4><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  default: k_qp_gradu<AKB_HEXAHEDRON_8><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t user_element_forces(const DevModel& m, cudaStream_t s) {
+  if (m.ne == 0) return cudaSuccess;
+  switch (m.type) {
+  case AKB_SEGMENT_2: k_qp_forces<AKB_SEGMENT_2><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  case AKB_TRIANGLE_3: k_qp_forces<AKB_TRIANGLE_3><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  case AKB_TETRAHEDRON_4: k_qp_forces<AKB_TETRAHEDRON_4><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  default: k_qp_forces<AKB_HEXAHEDRON_8><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  }
   return cudaGetLastError();
 }
 

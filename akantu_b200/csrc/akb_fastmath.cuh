@@ -232,6 +232,36 @@ __device__ inline void simplex_force(const MatParams& p, const S* dX, const S* d
     }
 }
 
+// Physical shape gradients at quadrature point q: B[a*d + j] = dN_a/dX_j,
+// returns det J (dX[a*d+i] = X_a - X_0).
+template <int T, typename S>
+__device__ inline S shape_gradients(const S* dX, int q, S* B) {
+  constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
+  S J[9];
+#pragma unroll
+  for (int k = 0; k < d; ++k)
+#pragma unroll
+    for (int j = 0; j < d; ++j) {
+      S c = 0;
+#pragma unroll
+      for (int a = 1; a < n; ++a) c += dN<T, S>(k, a, q) * dX[a * d + j];
+      J[k * d + j] = c;
+    }
+  S A[9];
+  const S detJ = adjugate<d, S>(J, A);
+  const S idet = S(1) / detJ;
+#pragma unroll
+  for (int a = 0; a < n; ++a)
+#pragma unroll
+    for (int j = 0; j < d; ++j) {
+      S c = 0;
+#pragma unroll
+      for (int k = 0; k < d; ++k) c += A[j * d + k] * dN<T, S>(k, a, q);
+      B[a * d + j] = c * idet;
+    }
+  return detJ;
+}
+
 // Element internal force (without the -1 of the assembly):
 // fe[a*d + i] = sum_q w_q det J_q sum_j P_ij dN_a/dx_j.
 // dX[a*d+i] = X_a - X_0, du[a*d+i] = u_a - u_0 (entry a = 0 is zero).

@@ -78,6 +78,11 @@ cudaError_t fast_element_forces(const DevModel& m, bool fp32, cudaStream_t s);
 cudaError_t fast_gather_correct(const DevModel& m, double dt, bool fp32, bool correct,
                                 bool has_fext, cudaStream_t s);
 
+// User materials (akb_fast.cu): grad u at the quadrature points into gradu;
+// element force vectors (FP64, into fe) from the caller's stress.
+cudaError_t user_qp_gradients(const DevModel& m, cudaStream_t s);
+cudaError_t user_element_forces(const DevModel& m, cudaStream_t s);
+
 // Dirichlet values (akb_fast.cu): blocked[node][comp] = 1, u[node][comp] = value.
 cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n, int comp,
                             const double* values, cudaStream_t s);

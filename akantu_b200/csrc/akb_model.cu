@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/akb_fe2.h"
 #include "akb_internal.cuh"
 #include "akb_patch.cuh"
 
@@ -42,6 +43,9 @@ struct akb_model {
   bool has_fext = false;
   bool fint_valid = false;
   bool stresses_valid = false;
+  // user materials: stresses come from the caller between step_begin/end
+  bool user = false;
+  bool in_step = false;
   double* d_scratch = nullptr;  // reduction partials
   int scratch_len = 0;
   double* d_result = nullptr;
@@ -97,6 +101,7 @@ MatParams make_params(const akb_material_desc& d, int dim) {
   MatParams p{};
   p.kind = d.kind;
   p.finite = (d.kind == AKB_MATERIAL_NEOHOOKEAN) || d.finite_deformation != 0;
+  // a user material's E and nu only give the wave speed of the stable step
   p.rho = d.rho;
   p.E = d.E;
   p.nu = dim == 1 ? 0. : d.nu;
@@ -304,6 +309,10 @@ cudaError_t enqueue_internal_forces(akb_model* m) {
     if ((e = ref_element_forces(d, m->stream)) != cudaSuccess) return e;
     return ref_gather_correct(d, m->dt, false, m->stream);
   }
+  if (m->user) {  // from the stresses the caller wrote last
+    if ((e = user_element_forces(d, m->stream)) != cudaSuccess) return e;
+    return fast_gather_correct(d, m->dt, false, false, m->has_fext, m->stream);
+  }
   if ((e = fast_element_forces(d, fp32(m), m->stream)) != cudaSuccess) return e;
   return fast_gather_correct(d, m->dt, fp32(m), false, m->has_fext, m->stream);
 }
@@ -405,10 +414,13 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
     for (int64_t e = 0; e < ne; ++e)
       if (element_material[e] >= (uint32_t)nb_materials)
         return fail(AKB_ERR_INVALID_ARGUMENT, "material index out of range");
+  int nb_user = 0;
   for (int k = 0; k < nb_materials; ++k) {
     const auto& md = materials[k];
-    if (md.kind != AKB_MATERIAL_ELASTIC && md.kind != AKB_MATERIAL_NEOHOOKEAN)
+    if (md.kind != AKB_MATERIAL_ELASTIC && md.kind != AKB_MATERIAL_NEOHOOKEAN &&
+        md.kind != AKB_MATERIAL_USER)
       return fail(AKB_ERR_UNSUPPORTED, "unsupported material kind");
+    nb_user += md.kind == AKB_MATERIAL_USER;
     if (!(md.rho > 0) || !(md.E > 0))
       return fail(AKB_ERR_INVALID_ARGUMENT, "material needs rho > 0 and E > 0");
   }
@@ -416,9 +428,13 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
   if (options) opt = *options;
   if (opt.precision_mode < AKB_MODE_FP64_REFERENCE || opt.precision_mode > AKB_MODE_FP32_BULK)
     return fail(AKB_ERR_INVALID_ARGUMENT, "unknown precision mode");
+  if (nb_user && (nb_user != nb_materials || opt.precision_mode != AKB_MODE_FP64 || batch))
+    return fail(AKB_ERR_UNSUPPORTED,
+                "user materials: every material of the model, AKB_MODE_FP64, no batch");
 
   auto m = std::make_unique<akb_model>();
   m->mode = opt.precision_mode;
+  m->user = nb_user > 0;
   m->opt_patch_elements = opt.patch_elements;
   m->opt_patch_nodes = opt.patch_nodes;
   m->opt_patch_grid = opt.patch_grid;
@@ -524,7 +540,10 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
     dm.B = nullptr;
     dm.jac = nullptr;
   }
-  if (m->mode != AKB_MODE_FP64_REFERENCE && ne > 0) {
+  if (m->user) {
+    if ((st = ensure_stress_arrays(m.get())) != AKB_OK) return st;
+    AKB_CUDA_TRY(cudaMemsetAsync(dm.stress, 0, (size_t)ne * q * d * d * sizeof(double), m->stream));
+  } else if (m->mode != AKB_MODE_FP64_REFERENCE && ne > 0) {
     if ((st = build_device_patches(m.get(), mesh, element_material, batch)) != AKB_OK) return st;
   }
   if (batch) {
@@ -610,7 +629,7 @@ akb_status akb_get_field(akb_model* m, int32_t field, double* values, int64_t co
     AKB_CUDA_TRY(enqueue_internal_forces(m));
     m->fint_valid = true;
   }
-  if ((field == AKB_FIELD_GRAD_U || field == AKB_FIELD_STRESS) && !m->stresses_valid) {
+  if ((field == AKB_FIELD_GRAD_U || field == AKB_FIELD_STRESS) && !m->stresses_valid && !m->user) {
     if ((st = akb_compute_stresses(m)) != AKB_OK) return st;
   }
   AKB_CUDA_TRY(cudaMemcpyAsync(values, field_ptr(m, field), count * sizeof(double),
@@ -727,6 +746,8 @@ static akb_status prepare_graphs(akb_model* m, int64_t nb_steps, cudaGraphExec_t
 akb_status akb_solve_steps(akb_model* m, int64_t nb_steps) {
   akb_status st;
   if ((st = check_model(m)) != AKB_OK) return st;
+  if (m->user)
+    return fail(AKB_ERR_STATE, "user material: step with akb_step_begin / akb_step_end");
   if (nb_steps < 0) return fail(AKB_ERR_INVALID_ARGUMENT, "negative step count");
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   if (nb_steps == 0) return AKB_OK;
@@ -751,6 +772,8 @@ akb_status akb_solve_steps(akb_model* m, int64_t nb_steps) {
 akb_status akb_time_solve_steps(akb_model* m, int64_t nb_steps, double* elapsed_ms) {
   akb_status st;
   if ((st = check_model(m)) != AKB_OK) return st;
+  if (m->user)
+    return fail(AKB_ERR_STATE, "user material: step with akb_step_begin / akb_step_end");
   if (!elapsed_ms) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
@@ -785,6 +808,7 @@ akb_status akb_assemble_internal_forces(akb_model* m) {
 akb_status akb_compute_stresses(akb_model* m) {
   akb_status st;
   if ((st = check_model(m)) != AKB_OK) return st;
+  if (m->user) return fail(AKB_ERR_UNSUPPORTED, "user material: the caller computes the stresses");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   if ((st = ensure_stress_arrays(m)) != AKB_OK) return st;
   AKB_CUDA_TRY(ref_compute_stresses(m->dm, m->dm.B == nullptr, m->stream));
@@ -798,6 +822,8 @@ akb_status akb_get_energy(akb_model* m, int32_t kind, double* value) {
   if (!value) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
   if (kind < AKB_ENERGY_KINETIC || kind > AKB_ENERGY_EXTERNAL_WORK)
     return fail(AKB_ERR_INVALID_ARGUMENT, "unknown energy");
+  if (m->user && kind == AKB_ENERGY_POTENTIAL)
+    return fail(AKB_ERR_UNSUPPORTED, "user material: no potential energy");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   if (kind == AKB_ENERGY_EXTERNAL_WORK && !m->fint_valid) {
     AKB_CUDA_TRY(enqueue_internal_forces(m));
@@ -849,6 +875,8 @@ akb_status akb_time_kernels(akb_model* m, int64_t nb_steps, double* ms_per_launc
   if ((st = check_model(m)) != AKB_OK) return st;
   if (!ms_per_launch || nb_slots < 0 || nb_steps < 1)
     return fail(AKB_ERR_INVALID_ARGUMENT, "bad timing arguments");
+  if (m->user)
+    return fail(AKB_ERR_STATE, "user material: step with akb_step_begin / akb_step_end");
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   StepTimer t;
@@ -987,6 +1015,44 @@ akb_status akb_synchronize(akb_model* m) {
   if ((st = check_model(m)) != AKB_OK) return st;
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   return sync(m);
+}
+
+akb_status akb_model_get_stream(akb_model* m, void** stream) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!stream) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  *stream = (void*)m->stream;
+  return AKB_OK;
+}
+
+// The explicit step split around Material::computeStress: predictor and
+// grad u (begin), then the caller's stresses, then internal forces, lumped
+// solve and corrector (end) -- the order of NonLinearSolverLumped::solve
+// (non_linear_solver_lumped.cc:58-82) with computeAllStresses between.
+akb_status akb_step_begin(akb_model* m) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!m->user) return fail(AKB_ERR_STATE, "akb_step_begin needs AKB_MATERIAL_USER materials");
+  if (m->in_step) return fail(AKB_ERR_STATE, "akb_step_begin called twice");
+  if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(fast_predictor(m->dm, m->dt, m->stream));
+  AKB_CUDA_TRY(user_qp_gradients(m->dm, m->stream));
+  m->in_step = true;
+  m->fint_valid = false;
+  return AKB_OK;
+}
+
+akb_status akb_step_end(akb_model* m) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!m->in_step) return fail(AKB_ERR_STATE, "akb_step_end without akb_step_begin");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(user_element_forces(m->dm, m->stream));
+  AKB_CUDA_TRY(fast_gather_correct(m->dm, m->dt, false, true, m->has_fext, m->stream));
+  m->in_step = false;
+  m->fint_valid = true;
+  return AKB_OK;
 }
 
 }  // extern "C"

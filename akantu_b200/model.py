@@ -70,6 +70,34 @@ class MaterialNeohookean(Material):
         super().__init__(rho, E, nu, finite_deformation=True, **kw)
 
 
+class MaterialUser(Material):
+    """A material written outside the library: the Material::computeStress
+    plugin (material.hh:110; registered through MaterialFactory,
+    material.hh:59, 670-691, in the reference). Subclass it and override
+    computeStress(grad_u, stress): both are (E*q, d, d) torch CUDA tensors
+    viewing the model's device arrays ([k, i, j] = du_i/dX_j at quadrature
+    point k); write into stress in place the Cauchy stress (small strain) or
+    the first Piola-Kirchhoff stress (finite_deformation=True). rho, E and nu
+    give the density and the wave speed of getStableTimeStep."""
+    kind = _abi.MATERIAL_USER
+
+    def __init__(self, rho, E, nu=0.0, finite_deformation=True, **kw):
+        super().__init__(rho=rho, E=E, nu=nu, finite_deformation=finite_deformation, **kw)
+
+    def computeStress(self, grad_u, stress):
+        raise NotImplementedError
+
+
+def _device_tensor(ptr, shape, device):
+    """Zero-copy torch view of FP64 device memory owned by the library."""
+    import torch
+
+    class _Cai:
+        __cuda_array_interface__ = dict(shape=tuple(shape), typestr="<f8", data=(int(ptr), False),
+                                        version=3, strides=None, stream=None)
+    return torch.as_tensor(_Cai(), device="cuda:%d" % device)
+
+
 def material_from_dict(d):
     kind = d.get("kind", _abi.MATERIAL_ELASTIC)
     cls = MaterialNeohookean if kind == _abi.MATERIAL_NEOHOOKEAN else MaterialElastic
@@ -121,6 +149,11 @@ class SolidMechanicsModel:
         if self._element_material is not None:
             self._em = np.ascontiguousarray(self._element_material, dtype=np.uint32)
             em = self._em.ctypes.data_as(C.POINTER(C.c_uint32))
+        self._user = [m for m in self._materials if isinstance(m, MaterialUser)]
+        if self._user and self._stream is None:
+            # user stresses are computed with torch: share its stream
+            import torch
+            self._stream = torch.cuda.current_stream(self._device).cuda_stream
         opt = _abi.ModelOptions(self._precision, self._device, self._stream, *self._patch)
         h = C.c_void_p()
         check(L.akb_model_create(C.byref(desc), len(self._materials), mats, em,
@@ -243,12 +276,46 @@ class SolidMechanicsModel:
 
     def solveStep(self, solver_id=""):
         self._sync_in()
+        if self._user:
+            self.stepBegin()
+            self._user[0].computeStress(self.deviceTensor(_abi.FIELD_GRAD_U),
+                                        self.deviceTensor(_abi.FIELD_STRESS))
+            self.stepEnd()
+            return
         check(lib().akb_solve_step(self.handle))
 
     def solveSteps(self, nb_steps):
         """nb_steps solveStep() calls replayed from a CUDA graph."""
         self._sync_in()
+        if self._user:
+            for _ in range(int(nb_steps)):
+                self.solveStep()
+            return
         check(lib().akb_solve_steps(self.handle, int(nb_steps)))
+
+    def stepBegin(self):
+        """Predictor and grad u at the quadrature points (user materials)."""
+        self._sync_in()
+        check(lib().akb_step_begin(self.handle))
+
+    def stepEnd(self):
+        """Internal forces from the stress field, lumped solve, corrector."""
+        check(lib().akb_step_end(self.handle))
+
+    def stream(self):
+        p = C.c_void_p()
+        check(lib().akb_model_get_stream(self.handle, C.byref(p)))
+        return p.value
+
+    def deviceTensor(self, field):
+        """Zero-copy torch view of a device field: (N, d) nodal fields, or
+        (E*q, d, d) [k, i, j] quadrature fields (column-major storage)."""
+        ptr = self.devicePointer(field)
+        if field in (_abi.FIELD_GRAD_U, _abi.FIELD_STRESS):
+            n = self.mesh.getNbElement() * self.nqp
+            t = _device_tensor(ptr, (n, self.dim, self.dim), self._device)
+            return t.transpose(1, 2)
+        return _device_tensor(ptr, (self.mesh.getNbNodes(), self.dim), self._device)
 
     def timeSolveSteps(self, nb_steps):
         """Device time (ms) of nb_steps steps, CUDA events on the model's stream."""

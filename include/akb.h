@@ -52,7 +52,10 @@ enum {
 /* Constitutive laws on the path. */
 enum {
   AKB_MATERIAL_ELASTIC = 0,    /* materials/material_elastic.cc */
-  AKB_MATERIAL_NEOHOOKEAN = 1  /* material_finite_deformation/material_neohookean.cc */
+  AKB_MATERIAL_NEOHOOKEAN = 1, /* material_finite_deformation/material_neohookean.cc */
+  AKB_MATERIAL_USER = 2        /* stresses written by the caller between
+                                  akb_step_begin and akb_step_end (akb_fe2.h):
+                                  the Material::computeStress plugin, material.hh:110 */
 };
 
 /* Arithmetic modes.

@@ -392,7 +392,7 @@ void svk_stress(const Material& mat, int d, const double* g, double* s) {
 // MaterialNeohookean::computeStressOnQuad (material_neohookean_inline_impl.hh:46-65):
 // F = I + grad_u, C = F^T F, J = det F, S = mu I + (lambda ln J - mu) C^-1.
 void neohookean_stress(const Material& mat, int d, const double* g, double* S) {
-  double F[9], C[9], Ci[9];
+  double F[9] = {0}, C[9], Ci[9];
   for (int i = 0; i < d; ++i)
     for (int j = 0; j < d; ++j) F[i + j * d] = double(i == j);
   for (int i = 0; i < d; ++i)

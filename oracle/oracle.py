@@ -163,3 +163,79 @@ class OracleModel:
 
     def time_steps(self, n):
         return self.lib.oracle_time_steps(self.h, n)
+
+
+# ---------------------------------------------------------------- FE^2 (RVE)
+def _fe2_lib():
+    lib = _lib()
+    if getattr(lib, "_fe2_ready", False):
+        return lib
+    D, I32 = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    U8 = C.POINTER(C.c_uint8)
+    lib.oracle_rve_solve.restype = C.c_int32
+    lib.oracle_rve_solve.argtypes = [C.c_int32, C.c_double, U8, C.c_int32, D, D, I32, D, D,
+                                     C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                     D, D]
+    lib.oracle_rve_parameters.argtypes = [C.c_int32, C.c_double, C.c_int32, D, D, I32, D,
+                                          C.c_double, C.c_double, D, D]
+    lib.oracle_rve_stress.argtypes = [C.c_int32, C.c_double, U8, D, D, I32, D, D, D, D]
+    lib._fe2_ready = True
+    return lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class OracleRVE:
+    """FP64 periodic voxel RVE (oracle/akb_fe2_oracle.cc)."""
+
+    def __init__(self, cells, length, voxel_material, lambdas, mus, kinds):
+        self.n = int(cells)
+        self.L = float(length)
+        self.vm = np.ascontiguousarray(voxel_material, dtype=np.uint8).ravel()
+        assert self.vm.size == self.n ** 3
+        self.lam = np.ascontiguousarray(lambdas, dtype=np.float64)
+        self.mu = np.ascontiguousarray(mus, dtype=np.float64)
+        self.kind = np.ascontiguousarray(kinds, dtype=np.int32)
+        self.lib = _fe2_lib()
+
+    def _H(self, grad_u):
+        return np.ascontiguousarray(np.asarray(grad_u, dtype=np.float64).reshape(3, 3).T.ravel())
+
+    def parameters(self, grad_u, time_step_factor=0.5, damping_factor=1.0):
+        dt, cd = C.c_double(), C.c_double()
+        H = self._H(grad_u)
+        self.lib.oracle_rve_parameters(self.n, self.L, len(self.lam), _p(self.lam, C.c_double),
+                                       _p(self.mu, C.c_double), _p(self.kind, C.c_int32),
+                                       _p(H, C.c_double), time_step_factor, damping_factor,
+                                       C.byref(dt), C.byref(cd))
+        return dt.value, cd.value
+
+    def solve(self, grad_u, fluct=None, max_iterations=2000, check_interval=10, tolerance=1e-4,
+              time_step_factor=0.5, damping_factor=1.0):
+        """grad_u: 3x3 (row i, column j = du_i/dX_j). Returns (P 3x3, fluct,
+        iterations, residual)."""
+        H = self._H(grad_u)
+        w = np.zeros((self.n ** 3, 3)) if fluct is None else np.array(fluct, dtype=np.float64)
+        w = np.ascontiguousarray(w)
+        P = np.zeros(9)
+        r = C.c_double()
+        it = self.lib.oracle_rve_solve(self.n, self.L, _p(self.vm, C.c_uint8), len(self.lam),
+                                       _p(self.lam, C.c_double), _p(self.mu, C.c_double),
+                                       _p(self.kind, C.c_int32), _p(H, C.c_double),
+                                       _p(w, C.c_double), max_iterations, check_interval,
+                                       tolerance, time_step_factor, damping_factor,
+                                       _p(P, C.c_double), C.byref(r))
+        return P.reshape(3, 3).T.copy(), w, it, r.value
+
+    def stress(self, grad_u, fluct):
+        H = self._H(grad_u)
+        w = np.ascontiguousarray(fluct, dtype=np.float64)
+        P = np.zeros(9)
+        f = np.zeros((self.n ** 3, 3))
+        self.lib.oracle_rve_stress(self.n, self.L, _p(self.vm, C.c_uint8), _p(self.lam, C.c_double),
+                                   _p(self.mu, C.c_double), _p(self.kind, C.c_int32),
+                                   _p(H, C.c_double), _p(w, C.c_double), _p(P, C.c_double),
+                                   _p(f, C.c_double))
+        return P.reshape(3, 3).T.copy(), f

@@ -10,7 +10,8 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "akb.h")).read()
+    import glob
+    text = "".join(open(f).read() for f in sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))))
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(akb_[a-z0-9_]+)\s*\(", text)))
 
