@@ -1,0 +1,821 @@
+// akb_mlp.cu -- the learned RVE surrogate: a multilayer perceptron
+// (inputs <= 16, L hidden layers of width <= 256 with SiLU, outputs <= 16)
+// trained and evaluated with 5th-generation tensor cores.
+//
+// Every GEMM is a tcgen05.mma (kind::f16, BF16 operands, FP32 accumulators
+// in tensor memory), issued by one thread of the CTA, with operands in shared
+// memory in the canonical no-swizzle layout: 8 x 8 BF16 core matrices of 128
+// contiguous bytes. A row-major (rows, cols) tile is stored core matrix by
+// core matrix, row group major:
+//   offset(r, c) = ((r / 8) (cols / 8) + c / 8) 128 + (r % 8) 16 + (c % 8) 2,
+// which is a K-major operand (rows = M or N, cols = K; leading byte offset
+// 128, stride byte offset 16 cols) and, read the other way, an MN-major one
+// (MN = cols, K = rows; stride byte offset 128, leading byte offset 16 cols).
+// Activations, their gradients and the weights are kept in this layout in
+// global memory too, so staging a tile is a flat copy.
+//
+//   forward  (one CTA per 128 samples): H_l = SiLU(H_{l-1} W_l^T + b_l),
+//            A = H_{l-1} (K-major), B = W_l (N x K, K-major);
+//   backward (one CTA per 128 samples): dH_{l-1} = dZ_l W_l,
+//            A = dZ_l (K-major), B = W_l^T (K-major);
+//   weight gradients (a CTA per range of tiles): dW_l = dZ_l^T H_{l-1},
+//            A = dZ_l and B = H_{l-1} both MN-major (samples are K);
+//   Adam on FP32 master weights, then the BF16 copies are repacked.
+// Each wait on an MMA completion is bounded: past the limit the kernel
+// raises the error flag, frees its tensor memory and returns.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "../../include/akb_fe2.h"
+#include "akb_internal.cuh"
+
+namespace akb {
+namespace mlp {
+
+constexpr int kTile = 128;      // samples per CTA (UMMA M)
+constexpr int kMaxWidth = 256;  // one TMEM accumulator of 256 FP32 columns
+constexpr int kIO = 16;         // padded input / output width
+constexpr int kMaxLayers = 6;   // linear layers
+constexpr int kThreads = 128;   // one thread per TMEM lane / sample row
+constexpr uint32_t kWaitLimit = 1u << 20;
+
+struct Net {
+  int nl;                       // linear layers
+  int nin, nout;                // real input / output counts
+  int K[kMaxLayers], N[kMaxLayers];    // padded shapes (K[0] = N[nl-1] = 16)
+  int Kr[kMaxLayers], Nr[kMaxLayers];  // real shapes
+  const __nv_bfloat16* W[kMaxLayers];  // packed N x K
+  const __nv_bfloat16* Wt[kMaxLayers]; // packed K x N
+  const float* b[kMaxLayers];          // N (zero past the real outputs)
+  float in_shift[kIO], in_scale[kIO], out_shift[kIO], out_scale[kIO];
+  int* error;
+};
+
+// Training workspace: packed BF16 layer inputs act[l] (act[0] = the
+// normalised input, 16 columns), FP32 pre-activations z[l] of the hidden
+// layers ([rows][N]), packed BF16 gradients dz[l] of the layers'
+// pre-activations (dz[nl-1] = dY), normalised outputs, per-tile losses.
+struct Bufs {
+  unsigned char* act[kMaxLayers];
+  float* z[kMaxLayers];
+  unsigned char* dz[kMaxLayers];
+  float* ynorm;
+  float* loss_tiles;
+};
+
+__host__ __device__ inline size_t pk_off(int r, int c, int cols) {
+  return ((size_t)(r >> 3) * (cols >> 3) + (c >> 3)) * 128 + (r & 7) * 16 + (c & 7) * 2;
+}
+
+// ------------------------------------------------------------ PTX wrappers
+__device__ inline uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (no swizzle): start address, leading and
+// stride byte offsets, descriptor version 1.
+__device__ inline uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: BF16 x BF16 -> FP32, M x N.
+__host__ __device__ constexpr uint32_t idesc(int M, int N, bool a_mn, bool b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) |
+         ((b_mn ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ inline void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(id), "r"(acc)
+      : "memory");
+}
+__device__ inline void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+__device__ inline void mbar_init(uint32_t a) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ inline bool mbar_wait(uint32_t a, uint32_t parity) {
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ inline void tmem_alloc(uint32_t holder, uint32_t cols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(holder), "r"(cols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ inline void tmem_free(uint32_t taddr, uint32_t cols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
+}
+__device__ inline void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ inline void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ inline void fence_smem_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 (or 16) FP32 columns of this warp's 32 TMEM lanes; the wait is in the
+// same statement so no use of the registers can be scheduled before it.
+__device__ inline void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+      "%30, %31}, [%32];\n\ttcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+__device__ inline void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];\n\ttcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ inline float silu(float z) { return z / (1.0f + __expf(-z)); }
+__device__ inline float dsilu(float z) {
+  const float s = 1.0f / (1.0f + __expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+__device__ inline uint32_t pack2(float a, float b) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// 8 consecutive values (columns c..c+7, c % 8 == 0) of row r as one 16-byte
+// store into a packed tile with `cols` columns.
+__device__ inline void store8(unsigned char* tile, int r, int c, int cols, const float* v) {
+  uint4 q;
+  q.x = pack2(v[0], v[1]);
+  q.y = pack2(v[2], v[3]);
+  q.z = pack2(v[4], v[5]);
+  q.w = pack2(v[6], v[7]);
+  *reinterpret_cast<uint4*>(tile + pk_off(r, c, cols)) = q;
+}
+
+__device__ inline void copy16(void* dst, const void* src, size_t bytes, int tid, int nt) {
+  const uint4* s = static_cast<const uint4*>(src);
+  uint4* d = static_cast<uint4*>(dst);
+  for (size_t k = tid; k < bytes / 16; k += nt) d[k] = s[k];
+}
+
+// Issues A (M x K) times B^T (N x K) into tmem_d, K in steps of 16, both
+// K-major packed tiles (A with K columns, B with K columns), then commits.
+__device__ inline void gemm_kmajor(uint32_t tmem_d, uint32_t a, uint32_t b, int K, int N) {
+  const uint32_t id = idesc(kTile, N, false, false);
+  for (int s = 0; s < K / 16; ++s)
+    mma(tmem_d, sdesc(a + s * 256, 128, 16 * K), sdesc(b + s * 256, 128, 16 * K), id, s > 0);
+}
+
+struct Shared {
+  unsigned char* act;  // 128 x 256 packed BF16 (64 KB)
+  unsigned char* wgt;  // 256 x 256 packed BF16 (128 KB)
+  float* bias;         // 256
+  uint64_t* mbar;
+  uint32_t* tmem_holder;
+};
+
+constexpr size_t kActBytes = (size_t)kTile * kMaxWidth * 2;
+constexpr size_t kWgtBytes = (size_t)kMaxWidth * kMaxWidth * 2;
+constexpr size_t kFwdSmem = kActBytes + kWgtBytes + kMaxWidth * 4 + 64;
+
+__device__ inline Shared carve(unsigned char* smem) {
+  Shared s;
+  s.act = smem;
+  s.wgt = smem + kActBytes;
+  s.bias = reinterpret_cast<float*>(smem + kActBytes + kWgtBytes);
+  s.mbar = reinterpret_cast<uint64_t*>(smem + kActBytes + kWgtBytes + kMaxWidth * 4);
+  s.tmem_holder = reinterpret_cast<uint32_t*>(s.mbar + 1);
+  return s;
+}
+
+// Forward pass of one tile of 128 samples. x: [nb][nin] FP64 raw inputs.
+// TRAIN stores the packed BF16 input and hidden activations (act[l], tile
+// major), the pre-activations Z (z[l], [nb_pad][N] FP32) and the normalised
+// outputs (ynorm, [nb_pad][16] FP32); otherwise y: [nb][nout] FP64 outputs.
+template <bool TRAIN>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_forward(Net net, int64_t nb, const double* __restrict__ x, double* __restrict__ y,
+              Bufs bufs) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  Shared s = carve(smem);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int64_t tile = blockIdx.x;
+  const int64_t row = tile * kTile + tid;
+  if (warp == 0) tmem_alloc(saddr(s.tmem_holder), 256);
+  if (tid == 0) mbar_init(saddr(s.mbar));
+  // inputs, normalised, padded to 16 columns
+  {
+    float v[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      float t = 0.0f;
+      if (j < net.nin && row < nb) t = (float)((x[row * net.nin + j] - net.in_shift[j]) * net.in_scale[j]);
+      v[j] = t;
+    }
+    store8(s.act, tid, 0, 16, v);
+    store8(s.act, tid, 8, 16, v + 8);
+    if (TRAIN) {
+      unsigned char* g = bufs.act[0] + tile * (size_t)kTile * 16 * 2;
+      store8(g, tid, 0, 16, v);
+      store8(g, tid, 8, 16, v + 8);
+    }
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *s.tmem_holder;
+  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int l = 0; l < net.nl && ok; ++l) {
+    const int K = net.K[l], N = net.N[l];
+    copy16(s.wgt, net.W[l], (size_t)N * K * 2, tid, kThreads);
+    for (int c = tid; c < N; c += kThreads) s.bias[c] = net.b[l][c];
+    fence_smem_async();
+    __syncthreads();
+    if (tid == 0) {
+      fence_after();
+      gemm_kmajor(tmem, saddr(s.act), saddr(s.wgt), K, N);
+      mma_commit(saddr(s.mbar));
+    }
+    ok = mbar_wait(saddr(s.mbar), phase);
+    phase ^= 1;
+    fence_after();
+    if (!ok) break;
+    const bool last = l == net.nl - 1;
+    if (!last) {
+      for (int c0 = 0; c0 < N; c0 += 32) {
+        float v[32];
+        tmem_ld32(tmem + lane_base + c0, v);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const float zz = v[j] + s.bias[c0 + j];
+          if (TRAIN && row < nb) bufs.z[l][row * N + c0 + j] = zz;
+          v[j] = silu(zz);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) store8(s.act, tid, c0 + 8 * q, N, v + 8 * q);
+        if (TRAIN) {
+          unsigned char* g = bufs.act[l + 1] + tile * (size_t)kTile * N * 2;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) store8(g, tid, c0 + 8 * q, N, v + 8 * q);
+        }
+      }
+    } else {
+      float v[16];
+      tmem_ld16(tmem + lane_base, v);
+      if (row < nb) {
+        for (int j = 0; j < 16; ++j) {
+          const float yy = v[j] + s.bias[j];
+          if (TRAIN) bufs.ynorm[row * 16 + j] = yy;
+          if (!TRAIN && j < net.nout)
+            y[row * net.nout + j] = (double)yy * net.out_scale[j] + net.out_shift[j];
+        }
+      }
+    }
+    fence_before();
+    __syncthreads();  // TMEM read and activations written before the next MMA
+  }
+  if (!ok) {  // drain the MMA that did not complete in time before freeing TMEM
+    mbar_wait(saddr(s.mbar), phase ^ 1);
+    if (tid == 0) atomicExch(net.error, 1);
+  }
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, 256);
+}
+
+// Backward pass of one tile: dY from the normalised outputs and targets
+// (loss = mean over samples and outputs of (y - t)^2), then
+// dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1}) down to the first hidden layer.
+// Stores packed BF16 dY (dz[nl-1]) and dZ (dz[l]) tiles and the tile's loss.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_backward(Net net, int64_t nb, const double* __restrict__ target, Bufs bufs) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  Shared s = carve(smem);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int64_t tile = blockIdx.x;
+  const int64_t row = tile * kTile + tid;
+  if (warp == 0) tmem_alloc(saddr(s.tmem_holder), 256);
+  if (tid == 0) mbar_init(saddr(s.mbar));
+  const int L = net.nl;
+  {
+    float d[16];
+    float sq = 0.0f;
+    const float scale = 2.0f / (float)((double)nb * net.nout);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      float e = 0.0f;
+      if (row < nb && j < net.nout) {
+        const float t = (float)((target[row * net.nout + j] - net.out_shift[j]) / net.out_scale[j]);
+        e = bufs.ynorm[row * 16 + j] - t;
+        sq += e * e;
+      }
+      d[j] = scale * e;
+    }
+    store8(s.act, tid, 0, 16, d);
+    store8(s.act, tid, 8, 16, d + 8);
+    unsigned char* g = bufs.dz[L - 1] + tile * (size_t)kTile * 16 * 2;
+    store8(g, tid, 0, 16, d);
+    store8(g, tid, 8, 16, d + 8);
+    // tile loss: warp sums then warp 0
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    float* red = s.bias;
+    if ((tid & 31) == 0) red[warp] = sq;
+    __syncthreads();
+    if (tid == 0) bufs.loss_tiles[tile] = red[0] + red[1] + red[2] + red[3];
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *s.tmem_holder;
+  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int l = L - 1; l >= 1 && ok; --l) {
+    const int K = net.N[l], N = net.K[l];  // reduce over the layer's outputs
+    copy16(s.wgt, net.Wt[l], (size_t)N * K * 2, tid, kThreads);
+    fence_smem_async();
+    __syncthreads();
+    if (tid == 0) {
+      fence_after();
+      gemm_kmajor(tmem, saddr(s.act), saddr(s.wgt), K, N);
+      mma_commit(saddr(s.mbar));
+    }
+    ok = mbar_wait(saddr(s.mbar), phase);
+    phase ^= 1;
+    fence_after();
+    if (!ok) break;
+    unsigned char* g = bufs.dz[l - 1] + tile * (size_t)kTile * N * 2;
+    for (int c0 = 0; c0 < N; c0 += 32) {
+      float v[32];
+      tmem_ld32(tmem + lane_base + c0, v);
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        v[j] = row < nb ? v[j] * dsilu(bufs.z[l - 1][row * N + c0 + j]) : 0.0f;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        store8(s.act, tid, c0 + 8 * q, N, v + 8 * q);
+        store8(g, tid, c0 + 8 * q, N, v + 8 * q);
+      }
+    }
+    fence_before();
+    __syncthreads();
+  }
+  if (!ok) {  // drain the MMA that did not complete in time before freeing TMEM
+    mbar_wait(saddr(s.mbar), phase ^ 1);
+    if (tid == 0) atomicExch(net.error, 1);
+  }
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, 256);
+}
+
+// Partial weight gradients G[m][n] = sum_s A[s][m] B[s][n] over the tiles
+// [tile0, tile1) of this CTA: A tiles with ca columns (128 or 256), B tiles
+// with cb columns (16..256); written to part[blockIdx.x][ca][cb].
+__global__ void __launch_bounds__(kThreads, 1)
+    k_wgrad(const unsigned char* __restrict__ A, int ca, const unsigned char* __restrict__ B,
+            int cb, int64_t ntiles, int tiles_per_cta, float* part, int* error) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* sa = smem;
+  unsigned char* sb = smem + (size_t)kTile * kMaxWidth * 2;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sb + (size_t)kTile * kMaxWidth * 2);
+  uint32_t* holder = reinterpret_cast<uint32_t*>(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) tmem_alloc(saddr(holder), 512);
+  if (tid == 0) mbar_init(saddr(mbar));
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *holder;
+  const int64_t t0 = (int64_t)blockIdx.x * tiles_per_cta;
+  const int64_t t1 = t0 + tiles_per_cta < ntiles ? t0 + tiles_per_cta : ntiles;
+  const int halves = ca / kTile;
+  const uint32_t id = idesc(kTile, cb, true, true);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int64_t t = t0; t < t1 && ok; ++t) {
+    copy16(sa, A + t * (size_t)kTile * ca * 2, (size_t)kTile * ca * 2, tid, kThreads);
+    copy16(sb, B + t * (size_t)kTile * cb * 2, (size_t)kTile * cb * 2, tid, kThreads);
+    fence_smem_async();
+    __syncthreads();
+    if (tid == 0) {
+      fence_after();
+      for (int h = 0; h < halves; ++h)
+        for (int s = 0; s < kTile / 16; ++s)
+          mma(tmem + h * cb,
+              sdesc(saddr(sa) + h * (kTile / 8) * 128 + s * 2 * 16 * ca, 16 * ca, 128),
+              sdesc(saddr(sb) + s * 2 * 16 * cb, 16 * cb, 128), id, (t > t0 || s > 0) ? 1u : 0u);
+      mma_commit(saddr(mbar));
+    }
+    ok = mbar_wait(saddr(mbar), phase);
+    phase ^= 1;
+    fence_after();
+    __syncthreads();  // shared tiles free for the next copy
+  }
+  if (ok && t1 > t0) {
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    float* out = part + (size_t)blockIdx.x * ca * cb;
+    for (int h = 0; h < halves; ++h)
+      for (int c0 = 0; c0 < cb; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + lane_base + h * cb + c0, v);
+        const int m = h * kTile + tid;
+        for (int j = 0; j < 16; ++j) out[(size_t)m * cb + c0 + j] = v[j];
+      }
+  } else if (t1 <= t0) {
+    float* out = part + (size_t)blockIdx.x * ca * cb;
+    for (int k = tid; k < ca * cb; k += kThreads) out[k] = 0.0f;
+  }
+  if (!ok) {
+    mbar_wait(saddr(mbar), phase ^ 1);
+    if (tid == 0) atomicExch(error, 1);
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, 512);
+}
+
+// grad[m][n] (real rows/cols, row stride ncols) = sum over CTAs of the
+// partials, in CTA order; TRANSPOSE reads part[.][n][m].
+__global__ void k_sum_partials(const float* part, int nparts, int ca, int cb, int rows, int cols,
+                               bool transpose, float* grad) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= rows * cols) return;
+  const int m = k / cols, n = k % cols;
+  const size_t idx = transpose ? (size_t)n * cb + m : (size_t)m * cb + n;
+  float acc = 0.0f;
+  for (int p = 0; p < nparts; ++p) acc += part[(size_t)p * ca * cb + idx];
+  grad[k] = acc;
+}
+
+// Bias gradient of a layer: sum over samples of the packed BF16 dZ tiles.
+__global__ void k_bias_grad(const unsigned char* dz, int cols, int real, int64_t ntiles,
+                            float* grad) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= real) return;
+  float acc = 0.0f;
+  for (int64_t t = 0; t < ntiles; ++t) {
+    const unsigned char* tile = dz + t * (size_t)kTile * cols * 2;
+    for (int r = 0; r < kTile; ++r)
+      acc += __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(tile + pk_off(r, n, cols)));
+  }
+  grad[n] = acc;
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master parameters.
+__global__ void k_adam(float* p, const float* g, float* m1, float* m2, int64_t n, float lr,
+                       float b1, float b2, float eps, float c1, float c2) {
+  const int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float gk = g[k];
+  const float a = b1 * m1[k] + (1.0f - b1) * gk;
+  const float b = b2 * m2[k] + (1.0f - b2) * gk * gk;
+  m1[k] = a;
+  m2[k] = b;
+  p[k] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
+}
+
+// Packed BF16 W (N x K) and W^T (K x N) of one layer from the real FP32
+// row-major weights (nr x kr) and bias, zero padded.
+__global__ void k_pack(const float* w, const float* bias, int nr, int kr, int N, int K,
+                       __nv_bfloat16* W, __nv_bfloat16* Wt, float* b) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < N) b[k] = k < nr ? bias[k] : 0.0f;
+  if (k >= N * K) return;
+  const int r = k / K, c = k % K;
+  const float v = (r < nr && c < kr) ? w[(size_t)r * kr + c] : 0.0f;
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<unsigned char*>(W) + pk_off(r, c, K)) = h;
+  *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<unsigned char*>(Wt) + pk_off(c, r, N)) = h;
+}
+
+}  // namespace mlp
+}  // namespace akb
+
+using namespace akb;
+using namespace akb::mlp;
+
+struct akb_mlp {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool owns_stream = false;
+  Net net{};
+  int64_t nparams = 0;
+  std::vector<int64_t> w_off, b_off;
+  float *d_params = nullptr, *d_grad = nullptr, *d_m1 = nullptr, *d_m2 = nullptr;
+  int* d_error = nullptr;
+  std::vector<void*> allocs;  // device memory owned
+  int64_t adam_step = 0;
+  // training workspace
+  int64_t cap_tiles = 0;
+  std::vector<void*> work;
+  Bufs bufs{};
+  float* d_part = nullptr;
+  size_t part_cap = 0;
+  float* h_loss = nullptr;  // pinned, one float per tile
+};
+
+namespace {
+
+template <typename T>
+cudaError_t dmalloc(std::vector<void*>& owner, T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+  if (e == cudaSuccess) owner.push_back(*p);
+  return e;
+}
+
+cudaError_t set_smem(const void* fn, size_t bytes) {
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+constexpr size_t kWgradSmem = 2 * (size_t)kTile * kMaxWidth * 2 + 64;
+
+akb_status repack(akb_mlp* m) {
+  for (int l = 0; l < m->net.nl; ++l) {
+    const Net& n = m->net;
+    const int total = n.N[l] * n.K[l];
+    k_pack<<<(total + 255) / 256, 256, 0, m->stream>>>(
+        m->d_params + m->w_off[l], m->d_params + m->b_off[l], n.Nr[l], n.Kr[l], n.N[l], n.K[l],
+        const_cast<__nv_bfloat16*>(n.W[l]), const_cast<__nv_bfloat16*>(n.Wt[l]),
+        const_cast<float*>(n.b[l]));
+    AKB_CUDA_TRY(cudaGetLastError());
+  }
+  return AKB_OK;
+}
+
+akb_status ensure_workspace(akb_mlp* m, int64_t ntiles) {
+  if (ntiles <= m->cap_tiles) return AKB_OK;
+  for (void* p : m->work) cudaFree(p);
+  m->work.clear();
+  const Net& n = m->net;
+  const size_t rows = (size_t)ntiles * kTile;
+  Bufs b{};
+  for (int l = 0; l < n.nl; ++l) {
+    AKB_CUDA_TRY(dmalloc(m->work, &b.act[l], rows * n.K[l] * 2));
+    AKB_CUDA_TRY(dmalloc(m->work, &b.dz[l], rows * n.N[l] * 2));
+    if (l < n.nl - 1) AKB_CUDA_TRY(dmalloc(m->work, &b.z[l], rows * n.N[l]));
+  }
+  AKB_CUDA_TRY(dmalloc(m->work, &b.ynorm, rows * 16));
+  AKB_CUDA_TRY(dmalloc(m->work, &b.loss_tiles, (size_t)ntiles));
+  m->bufs = b;
+  if (m->h_loss) cudaFreeHost(m->h_loss);
+  AKB_CUDA_TRY(cudaMallocHost((void**)&m->h_loss, ntiles * sizeof(float)));
+  m->cap_tiles = ntiles;
+  return AKB_OK;
+}
+
+// Forward, backward and gradient assembly of one batch; *loss = mean
+// squared error of the normalised outputs.
+akb_status gradients(akb_mlp* m, int64_t nb, const double* x, const double* target, float* loss) {
+  const int64_t ntiles = (nb + kTile - 1) / kTile;
+  akb_status st;
+  if ((st = ensure_workspace(m, ntiles)) != AKB_OK) return st;
+  const Net& n = m->net;
+  AKB_CUDA_TRY(cudaMemsetAsync(m->d_error, 0, sizeof(int), m->stream));
+  k_forward<true><<<(unsigned)ntiles, kThreads, kFwdSmem, m->stream>>>(n, nb, x, nullptr, m->bufs);
+  AKB_CUDA_TRY(cudaGetLastError());
+  k_backward<<<(unsigned)ntiles, kThreads, kFwdSmem, m->stream>>>(n, nb, target, m->bufs);
+  AKB_CUDA_TRY(cudaGetLastError());
+  const int tpc = (int)std::max<int64_t>(1, (ntiles + 147) / 148);
+  const int nparts = (int)((ntiles + tpc - 1) / tpc);
+  for (int l = 0; l < n.nl; ++l) {
+    const bool last = l == n.nl - 1;
+    // dW_l = dZ_l^T H_l (the output layer as its transpose: M must be 128 or 256)
+    const unsigned char* A = last ? m->bufs.act[l] : m->bufs.dz[l];
+    const unsigned char* B = last ? m->bufs.dz[l] : m->bufs.act[l];
+    const int ca = last ? n.K[l] : n.N[l], cb = last ? n.N[l] : n.K[l];
+    const size_t need = (size_t)nparts * ca * cb;
+    if (need > m->part_cap) {
+      if (m->d_part) cudaFree(m->d_part);
+      m->d_part = nullptr;
+      AKB_CUDA_TRY(cudaMalloc((void**)&m->d_part, need * sizeof(float)));
+      m->part_cap = need;
+    }
+    k_wgrad<<<nparts, kThreads, kWgradSmem, m->stream>>>(A, ca, B, cb, ntiles, tpc, m->d_part,
+                                                         m->d_error);
+    AKB_CUDA_TRY(cudaGetLastError());
+    const int cnt = n.Nr[l] * n.Kr[l];
+    k_sum_partials<<<(cnt + 255) / 256, 256, 0, m->stream>>>(m->d_part, nparts, ca, cb, n.Nr[l],
+                                                             n.Kr[l], last, m->d_grad + m->w_off[l]);
+    AKB_CUDA_TRY(cudaGetLastError());
+    k_bias_grad<<<(n.Nr[l] + 127) / 128, 128, 0, m->stream>>>(m->bufs.dz[l], n.N[l], n.Nr[l],
+                                                               ntiles, m->d_grad + m->b_off[l]);
+    AKB_CUDA_TRY(cudaGetLastError());
+  }
+  AKB_CUDA_TRY(cudaMemcpyAsync(m->h_loss, m->bufs.loss_tiles, ntiles * sizeof(float),
+                               cudaMemcpyDeviceToHost, m->stream));
+  int err = 0;
+  AKB_CUDA_TRY(cudaMemcpyAsync(&err, m->d_error, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  if (err) return fail(AKB_ERR_TIMEOUT, "tensor-core MMA completion wait timed out");
+  double acc = 0.0;
+  for (int64_t t = 0; t < ntiles; ++t) acc += m->h_loss[t];
+  if (loss) *loss = (float)(acc / ((double)nb * n.nout));
+  return AKB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+akb_status akb_mlp_create(int32_t nb_inputs, int32_t nb_outputs, int32_t width,
+                          int32_t nb_hidden, int32_t device, void* stream, akb_mlp** out) {
+  if (!out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  if (nb_inputs < 1 || nb_inputs > kIO || nb_outputs < 1 || nb_outputs > kIO)
+    return fail(AKB_ERR_UNSUPPORTED, "1..16 inputs and outputs");
+  if (width != 128 && width != 256) return fail(AKB_ERR_UNSUPPORTED, "hidden width 128 or 256");
+  if (nb_hidden < 1 || nb_hidden > kMaxLayers - 1)
+    return fail(AKB_ERR_UNSUPPORTED, "1..5 hidden layers");
+  auto m = std::make_unique<akb_mlp>();
+  Net& n = m->net;
+  n.nl = nb_hidden + 1;
+  n.nin = nb_inputs;
+  n.nout = nb_outputs;
+  for (int l = 0; l < n.nl; ++l) {
+    n.K[l] = l == 0 ? kIO : width;
+    n.N[l] = l == n.nl - 1 ? kIO : width;
+    n.Kr[l] = l == 0 ? nb_inputs : width;
+    n.Nr[l] = l == n.nl - 1 ? nb_outputs : width;
+    m->w_off.push_back(m->nparams);
+    m->nparams += (int64_t)n.Nr[l] * n.Kr[l];
+    m->b_off.push_back(m->nparams);
+    m->nparams += n.Nr[l];
+  }
+  for (int j = 0; j < kIO; ++j) {
+    n.in_shift[j] = n.out_shift[j] = 0.0f;
+    n.in_scale[j] = n.out_scale[j] = 1.0f;
+  }
+  m->device = device;
+  AKB_CUDA_TRY(cudaSetDevice(device));
+  if (stream) {
+    m->stream = (cudaStream_t)stream;
+  } else {
+    AKB_CUDA_TRY(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+    m->owns_stream = true;
+  }
+  AKB_CUDA_TRY(dmalloc(m->allocs, &m->d_params, m->nparams));
+  AKB_CUDA_TRY(dmalloc(m->allocs, &m->d_grad, m->nparams));
+  AKB_CUDA_TRY(dmalloc(m->allocs, &m->d_m1, m->nparams));
+  AKB_CUDA_TRY(dmalloc(m->allocs, &m->d_m2, m->nparams));
+  AKB_CUDA_TRY(dmalloc(m->allocs, &m->d_error, 1));
+  for (int l = 0; l < n.nl; ++l) {
+    __nv_bfloat16 *W, *Wt;
+    float* b;
+    AKB_CUDA_TRY(dmalloc(m->allocs, &W, (size_t)n.N[l] * n.K[l]));
+    AKB_CUDA_TRY(dmalloc(m->allocs, &Wt, (size_t)n.N[l] * n.K[l]));
+    AKB_CUDA_TRY(dmalloc(m->allocs, &b, (size_t)n.N[l]));
+    n.W[l] = W;
+    n.Wt[l] = Wt;
+    n.b[l] = b;
+  }
+  n.error = m->d_error;
+  AKB_CUDA_TRY(cudaMemsetAsync(m->d_params, 0, m->nparams * sizeof(float), m->stream));
+  AKB_CUDA_TRY(cudaMemsetAsync(m->d_m1, 0, m->nparams * sizeof(float), m->stream));
+  AKB_CUDA_TRY(cudaMemsetAsync(m->d_m2, 0, m->nparams * sizeof(float), m->stream));
+  akb_status st;
+  if ((st = repack(m.get())) != AKB_OK) return st;
+  AKB_CUDA_TRY(set_smem((const void*)k_forward<true>, kFwdSmem));
+  AKB_CUDA_TRY(set_smem((const void*)k_forward<false>, kFwdSmem));
+  AKB_CUDA_TRY(set_smem((const void*)k_backward, kFwdSmem));
+  AKB_CUDA_TRY(set_smem((const void*)k_wgrad, kWgradSmem));
+  AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  *out = m.release();
+  return AKB_OK;
+}
+
+akb_status akb_mlp_destroy(akb_mlp* m) {
+  if (!m) return AKB_OK;
+  cudaSetDevice(m->device);
+  cudaStreamSynchronize(m->stream);
+  for (void* p : m->allocs) cudaFree(p);
+  for (void* p : m->work) cudaFree(p);
+  if (m->d_part) cudaFree(m->d_part);
+  if (m->h_loss) cudaFreeHost(m->h_loss);
+  if (m->owns_stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return AKB_OK;
+}
+
+akb_status akb_mlp_get_parameter_count(const akb_mlp* m, int64_t* count) {
+  if (!m || !count) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  *count = m->nparams;
+  return AKB_OK;
+}
+
+akb_status akb_mlp_set_parameters(akb_mlp* m, const float* values, int64_t count) {
+  if (!m || !values) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (count != m->nparams) return fail(AKB_ERR_INVALID_ARGUMENT, "wrong parameter count");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(cudaMemcpyAsync(m->d_params, values, count * sizeof(float), cudaMemcpyHostToDevice,
+                               m->stream));
+  AKB_CUDA_TRY(cudaMemsetAsync(m->d_m1, 0, count * sizeof(float), m->stream));
+  AKB_CUDA_TRY(cudaMemsetAsync(m->d_m2, 0, count * sizeof(float), m->stream));
+  m->adam_step = 0;
+  akb_status st;
+  if ((st = repack(m)) != AKB_OK) return st;
+  AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return AKB_OK;
+}
+
+akb_status akb_mlp_get_parameters(akb_mlp* m, float* values, int64_t count) {
+  if (!m || !values) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (count != m->nparams) return fail(AKB_ERR_INVALID_ARGUMENT, "wrong parameter count");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(cudaMemcpyAsync(values, m->d_params, count * sizeof(float), cudaMemcpyDeviceToHost,
+                               m->stream));
+  AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return AKB_OK;
+}
+
+akb_status akb_mlp_set_scaling(akb_mlp* m, const float* in_shift, const float* in_scale,
+                               const float* out_shift, const float* out_scale) {
+  if (!m || !in_shift || !in_scale || !out_shift || !out_scale)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  for (int j = 0; j < m->net.nin; ++j) {
+    m->net.in_shift[j] = in_shift[j];
+    m->net.in_scale[j] = in_scale[j];
+  }
+  for (int j = 0; j < m->net.nout; ++j) {
+    if (!(out_scale[j] != 0.0f)) return fail(AKB_ERR_INVALID_ARGUMENT, "zero output scale");
+    m->net.out_shift[j] = out_shift[j];
+    m->net.out_scale[j] = out_scale[j];
+  }
+  return AKB_OK;
+}
+
+akb_status akb_mlp_forward(akb_mlp* m, int64_t nb, const double* x, double* y, void* stream) {
+  if (!m) return fail(AKB_ERR_INVALID_ARGUMENT, "null network");
+  if (nb < 0 || (nb > 0 && (!x || !y))) return fail(AKB_ERR_INVALID_ARGUMENT, "x and y are required");
+  if (nb == 0) return AKB_OK;
+  const int64_t ntiles = (nb + kTile - 1) / kTile;
+  if (ntiles > INT32_MAX) return fail(AKB_ERR_UNSUPPORTED, "too many samples");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : m->stream;
+  k_forward<false><<<(unsigned)ntiles, kThreads, kFwdSmem, s>>>(m->net, nb, x, y, Bufs{});
+  AKB_CUDA_TRY(cudaGetLastError());
+  return AKB_OK;
+}
+
+akb_status akb_mlp_gradients(akb_mlp* m, int64_t nb, const double* x, const double* target,
+                             float* grad, float* loss) {
+  if (!m) return fail(AKB_ERR_INVALID_ARGUMENT, "null network");
+  if (nb < 1 || !x || !target) return fail(AKB_ERR_INVALID_ARGUMENT, "x and target are required");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  akb_status st;
+  if ((st = gradients(m, nb, x, target, loss)) != AKB_OK) return st;
+  if (grad) {
+    AKB_CUDA_TRY(cudaMemcpyAsync(grad, m->d_grad, m->nparams * sizeof(float),
+                                 cudaMemcpyDeviceToHost, m->stream));
+    AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
+  }
+  return AKB_OK;
+}
+
+akb_status akb_mlp_train_step(akb_mlp* m, int64_t nb, const double* x, const double* target,
+                              float learning_rate, float* loss) {
+  if (!m) return fail(AKB_ERR_INVALID_ARGUMENT, "null network");
+  if (nb < 1 || !x || !target) return fail(AKB_ERR_INVALID_ARGUMENT, "x and target are required");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  akb_status st;
+  if ((st = gradients(m, nb, x, target, loss)) != AKB_OK) return st;
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  m->adam_step += 1;
+  const float c1 = 1.0f - std::pow(b1, (float)m->adam_step);
+  const float c2 = 1.0f - std::pow(b2, (float)m->adam_step);
+  k_adam<<<(unsigned)((m->nparams + 255) / 256), 256, 0, m->stream>>>(
+      m->d_params, m->d_grad, m->d_m1, m->d_m2, m->nparams, learning_rate, b1, b2, eps, c1, c2);
+  AKB_CUDA_TRY(cudaGetLastError());
+  return repack(m);
+}
+
+}  // extern "C"

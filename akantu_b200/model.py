@@ -88,6 +88,14 @@ class MaterialUser(Material):
         raise NotImplementedError
 
 
+def torch_stream(device):
+    """cudaStream_t of torch's current stream on a device. torch's default
+    stream is the legacy NULL stream, for which the library (where NULL means
+    "a stream of its own") is given cudaStreamLegacy."""
+    import torch
+    return torch.cuda.current_stream(device).cuda_stream or 1
+
+
 def _device_tensor(ptr, shape, device):
     """Zero-copy torch view of FP64 device memory owned by the library."""
     import torch
@@ -122,6 +130,7 @@ class SolidMechanicsModel:
         self._stream = stream
         self._patch = (int(patch_elements), int(patch_nodes))
         self._h = None
+        self._user = []
         self._mirrors = {}
         self._checked_out = set()
         self._blocked = None
@@ -152,8 +161,7 @@ class SolidMechanicsModel:
         self._user = [m for m in self._materials if isinstance(m, MaterialUser)]
         if self._user and self._stream is None:
             # user stresses are computed with torch: share its stream
-            import torch
-            self._stream = torch.cuda.current_stream(self._device).cuda_stream
+            self._stream = torch_stream(self._device)
         opt = _abi.ModelOptions(self._precision, self._device, self._stream, *self._patch)
         h = C.c_void_p()
         check(L.akb_model_create(C.byref(desc), len(self._materials), mats, em,

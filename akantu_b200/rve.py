@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _abi
 from ._lib import check, lib
-from .model import material_from_dict
+from .model import material_from_dict, torch_stream
 
 
 def _torch():
@@ -96,7 +96,7 @@ class SolidMechanicsModelRVE:
         P = torch.empty((nb, 3, 3), dtype=torch.float64, device=dev)
         it = torch.empty(nb, dtype=torch.int32, device=dev)
         res = torch.empty(nb, dtype=torch.float64, device=dev)
-        stream = torch.cuda.current_stream(dev).cuda_stream
+        stream = torch_stream(dev)
         check(lib().akb_rve_solve(self._h, nb, H.data_ptr(),
                                   fluctuation.data_ptr() if fluctuation is not None else None,
                                   P.data_ptr(), it.data_ptr(), res.data_ptr(), stream))
@@ -111,7 +111,7 @@ class SolidMechanicsModelRVE:
         P = torch.empty((nb, 3, 3), dtype=torch.float64, device=H.device)
         f = torch.empty((nb, self.nb_nodes, 3), dtype=torch.float64, device=H.device)
         w = fluctuation.to(self.fluctuation_dtype).contiguous()
-        stream = torch.cuda.current_stream(H.device).cuda_stream
+        stream = torch_stream(H.device)
         check(lib().akb_rve_stress(self._h, nb, H.data_ptr(), w.data_ptr(), P.data_ptr(),
                                    f.data_ptr(), stream))
         return P.transpose(1, 2), f

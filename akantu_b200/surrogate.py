@@ -1,0 +1,169 @@
+"""The learned RVE surrogate (include/akb_fe2.h: akb_mlp_*).
+
+MLPSurrogate maps a macroscopic displacement gradient H (9 values) to the
+homogenised first Piola-Kirchhoff stress (9 values) with a 9-256-256-256-9
+SiLU perceptron whose GEMMs run on the tensor cores (tcgen05, BF16 operands,
+FP32 accumulation). Training, gradients and inference all run in libakb.so;
+torch only holds the device arrays. Tensors are (nb, 3, 3) with
+[b, i, j] = du_i/dX_j (inputs) or P_ij (outputs); the network's features are
+their column-major flattening, the library's layout of grad_u and stress.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import check, lib
+from .model import torch_stream
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _flat(t, torch):
+    """(nb, 3, 3) -> (nb, 9) column-major features, FP64, contiguous."""
+    return t.reshape(-1, 3, 3).transpose(1, 2).reshape(-1, 9).to(torch.float64).contiguous()
+
+
+class MLPSurrogate:
+    def __init__(self, nb_inputs=9, nb_outputs=9, width=256, nb_hidden=3, device=0, seed=0):
+        self.shape = (nb_inputs, nb_outputs, width, nb_hidden)
+        self.device = device
+        h = C.c_void_p()
+        # on torch's stream, so the device arrays torch fills are ordered with it
+        check(lib().akb_mlp_create(nb_inputs, nb_outputs, width, nb_hidden, device,
+                                   torch_stream(device), C.byref(h)))
+        self._h = h
+        n = C.c_int64()
+        check(lib().akb_mlp_get_parameter_count(h, C.byref(n)))
+        self.nb_parameters = n.value
+        self.scaling = dict(in_shift=np.zeros(nb_inputs, np.float32),
+                            in_scale=np.ones(nb_inputs, np.float32),
+                            out_shift=np.zeros(nb_outputs, np.float32),
+                            out_scale=np.ones(nb_outputs, np.float32))
+        self.set_parameters(self.initial_parameters(seed))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().akb_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def layer_shapes(self):
+        nin, nout, w, nh = self.shape
+        return [(w if l else nin, nout if l == nh else w) for l in range(nh + 1)]
+
+    def initial_parameters(self, seed):
+        """Uniform +-sqrt(6 / (fan_in + fan_out)) weights (Glorot & Bengio
+        2010), zero biases."""
+        rng = np.random.default_rng(seed)
+        out = []
+        for k, n in self.layer_shapes():
+            a = np.sqrt(6.0 / (k + n))
+            out += [rng.uniform(-a, a, n * k), np.zeros(n)]
+        return np.concatenate(out).astype(np.float32)
+
+    def set_parameters(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib().akb_mlp_set_parameters(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+
+    def get_parameters(self):
+        p = np.zeros(self.nb_parameters, np.float32)
+        check(lib().akb_mlp_get_parameters(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+        return p
+
+    def set_scaling(self, in_shift, in_scale, out_shift, out_scale):
+        s = {k: np.ascontiguousarray(v, dtype=np.float32) for k, v in
+             dict(in_shift=in_shift, in_scale=in_scale, out_shift=out_shift,
+                  out_scale=out_scale).items()}
+        F = C.POINTER(C.c_float)
+        check(lib().akb_mlp_set_scaling(self._h, *[s[k].ctypes.data_as(F) for k in
+                                                   ("in_shift", "in_scale", "out_shift",
+                                                    "out_scale")]))
+        self.scaling = s
+
+    def fit_scaling(self, x, y):
+        """Per-feature shift/scale from training data ((nb, d) FP64 features)."""
+        x = np.asarray(x)
+        y = np.asarray(y)
+        xs = x.std(0)
+        ys = y.std(0)
+        self.set_scaling(x.mean(0), 1.0 / np.where(xs > 0, xs, 1.0), y.mean(0),
+                         np.where(ys > 0, ys, 1.0))
+
+    # -- device features (nb, d) FP64 --------------------------------------
+    def forward_features(self, x, stream=None):
+        torch = _torch()
+        x = x.to(torch.float64).contiguous()
+        y = torch.empty((x.shape[0], self.shape[1]), dtype=torch.float64, device=x.device)
+        s = stream if stream is not None else torch_stream(x.device)
+        check(lib().akb_mlp_forward(self._h, x.shape[0], x.data_ptr(), y.data_ptr(), s))
+        return y
+
+    def gradients_features(self, x, t):
+        torch = _torch()
+        torch.cuda.synchronize()
+        g = np.zeros(self.nb_parameters, np.float32)
+        loss = C.c_float()
+        check(lib().akb_mlp_gradients(self._h, x.shape[0], x.data_ptr(), t.data_ptr(),
+                                      g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
+        return loss.value, g
+
+    def train_step_features(self, x, t, lr):
+        loss = C.c_float()
+        check(lib().akb_mlp_train_step(self._h, x.shape[0], x.data_ptr(), t.data_ptr(),
+                                       float(lr), C.byref(loss)))
+        return loss.value
+
+    def train(self, x, t, epochs=20, batch=4096, lr=1e-3, lr_final=1e-5, seed=0, log=None):
+        """Adam over shuffled minibatches with a cosine-decayed learning
+        rate; x, t device (nb, d) FP64 features. Returns the epoch losses."""
+        torch = _torch()
+        torch.cuda.synchronize()
+        n = x.shape[0]
+        g = torch.Generator(device=x.device)
+        g.manual_seed(seed)
+        steps = epochs * max(1, n // batch)
+        k = 0
+        losses = []
+        for ep in range(epochs):
+            perm = torch.randperm(n, device=x.device, generator=g)
+            tot = 0.0
+            nbat = max(1, n // batch)
+            for b in range(nbat):
+                idx = perm[b * batch:(b + 1) * batch]
+                xb = x[idx].contiguous()
+                tb = t[idx].contiguous()
+                lr_k = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / steps))
+                tot += self.train_step_features(xb, tb, lr_k)
+                k += 1
+            losses.append(tot / nbat)
+            if log:
+                log("epoch %d loss %.3e" % (ep, losses[-1]))
+        return losses
+
+    # -- tensors (nb, 3, 3) -------------------------------------------------
+    def __call__(self, grad_u, stream=None):
+        torch = _torch()
+        y = self.forward_features(_flat(torch.as_tensor(grad_u), torch), stream)
+        return y.reshape(-1, 3, 3).transpose(1, 2)
+
+    def save(self, path):
+        np.savez(path, params=self.get_parameters(), shape=np.array(self.shape), **self.scaling)
+
+    @classmethod
+    def load(cls, path, device=0):
+        d = np.load(path)
+        s = tuple(int(v) for v in d["shape"])
+        m = cls(*s, device=device)
+        m.set_parameters(d["params"])
+        m.set_scaling(d["in_shift"], d["in_scale"], d["out_shift"], d["out_scale"])
+        return m

@@ -102,6 +102,38 @@ akb_status akb_rve_stress(akb_rve* rve, int64_t nb, const double* grad_u,
                           const void* fluctuation, double* stress, double* internal_force,
                           void* stream);
 
+/* ---------------------------------------------------------- surrogate */
+
+/* A multilayer perceptron nb_inputs -> width (SiLU) x nb_hidden -> nb_outputs
+ * run on the tensor cores (BF16 operands, FP32 accumulation, FP32 master
+ * weights): the learned map grad_u -> homogenised stress that replaces RVE
+ * solves inside its training envelope. Inputs and outputs are normalised
+ * inside (x' = (x - in_shift) in_scale, y = y' out_scale + out_shift).
+ * Parameters are FP32, layer by layer: W_l (rows = outputs, row-major), then
+ * b_l. Supported: 1..16 inputs and outputs, width 128 or 256, 1..5 hidden
+ * layers. */
+typedef struct akb_mlp akb_mlp;
+
+akb_status akb_mlp_create(int32_t nb_inputs, int32_t nb_outputs, int32_t width,
+                          int32_t nb_hidden, int32_t device, void* stream, akb_mlp** out);
+akb_status akb_mlp_destroy(akb_mlp* mlp);
+akb_status akb_mlp_get_parameter_count(const akb_mlp* mlp, int64_t* count);
+/* Host arrays; setting the parameters resets the optimiser state. */
+akb_status akb_mlp_set_parameters(akb_mlp* mlp, const float* values, int64_t count);
+akb_status akb_mlp_get_parameters(akb_mlp* mlp, float* values, int64_t count);
+akb_status akb_mlp_set_scaling(akb_mlp* mlp, const float* in_shift, const float* in_scale,
+                               const float* out_shift, const float* out_scale);
+/* y[nb][nb_outputs] = network(x[nb][nb_inputs]), device FP64 arrays, queued
+ * on stream (NULL = the network's stream). */
+akb_status akb_mlp_forward(akb_mlp* mlp, int64_t nb, const double* x, double* y, void* stream);
+/* Mean squared error of the normalised outputs against target (device FP64
+ * [nb][nb_outputs]) and its gradient (host, parameter layout; may be NULL). */
+akb_status akb_mlp_gradients(akb_mlp* mlp, int64_t nb, const double* x, const double* target,
+                             float* grad, float* loss);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on that loss. */
+akb_status akb_mlp_train_step(akb_mlp* mlp, int64_t nb, const double* x, const double* target,
+                              float learning_rate, float* loss);
+
 #ifdef __cplusplus
 }
 #endif

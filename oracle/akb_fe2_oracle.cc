@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 namespace {
@@ -272,6 +273,134 @@ int32_t oracle_rve_solve(int32_t n, double L, const uint8_t* voxel_material,
   oracle_rve_stress(n, L, voxel_material, lambda, mu, kind, grad_u, fluct, stress, nullptr);
   *residual = r;
   return k;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------- MLP
+namespace {
+
+float bf16_round(float f) {  // round to nearest even, BF16 kept in a float
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  u &= 0xFFFF0000u;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+
+struct MlpShape {
+  int nl, nin, nout, width;
+  std::vector<int> K, N;
+  std::vector<int64_t> woff, boff;
+};
+
+MlpShape mlp_shape(int nin, int nout, int width, int nhidden) {
+  MlpShape s;
+  s.nl = nhidden + 1;
+  s.nin = nin;
+  s.nout = nout;
+  s.width = width;
+  int64_t off = 0;
+  for (int l = 0; l < s.nl; ++l) {
+    s.K.push_back(l == 0 ? nin : width);
+    s.N.push_back(l == s.nl - 1 ? nout : width);
+    s.woff.push_back(off);
+    off += (int64_t)s.K[l] * s.N[l];
+    s.boff.push_back(off);
+    off += s.N[l];
+  }
+  return s;
+}
+
+// Forward of one sample; keeps per-layer inputs (as consumed) and
+// pre-activations for the backward pass.
+void mlp_sample(const MlpShape& S, const float* P, const float* sc, const double* x, bool bf,
+                std::vector<std::vector<double>>& in, std::vector<std::vector<double>>& z,
+                std::vector<double>& out) {
+  auto R = [&](double v) { return bf ? (double)bf16_round((float)v) : v; };
+  auto F = [&](double v) { return bf ? (double)(float)v : v; };
+  in.assign(S.nl, {});
+  z.assign(S.nl, {});
+  in[0].resize(S.nin);
+  for (int j = 0; j < S.nin; ++j) in[0][j] = R((double)(float)((x[j] - sc[j]) * sc[S.nin + j]));
+  for (int l = 0; l < S.nl; ++l) {
+    z[l].resize(S.N[l]);
+    for (int o = 0; o < S.N[l]; ++o) {
+      double acc = 0;
+      for (int k = 0; k < S.K[l]; ++k) acc += R(P[S.woff[l] + (int64_t)o * S.K[l] + k]) * in[l][k];
+      z[l][o] = F(F(acc) + P[S.boff[l] + o]);
+    }
+    if (l < S.nl - 1) {
+      in[l + 1].resize(S.N[l]);
+      for (int o = 0; o < S.N[l]; ++o) in[l + 1][o] = R(z[l][o] / (1.0 + std::exp(-z[l][o])));
+    }
+  }
+  out = z[S.nl - 1];
+}
+
+}  // namespace
+
+extern "C" {
+
+void oracle_mlp_forward(int32_t nin, int32_t nout, int32_t width, int32_t nhidden,
+                        const float* params, const float* scaling, int64_t nb, const double* x,
+                        double* y, int32_t emulate_bf16) {
+  const MlpShape S = mlp_shape(nin, nout, width, nhidden);
+  const float* osh = scaling + 2 * nin;
+  const float* osc = scaling + 2 * nin + nout;
+  std::vector<std::vector<double>> in, z;
+  std::vector<double> out;
+  for (int64_t r = 0; r < nb; ++r) {
+    mlp_sample(S, params, scaling, x + r * nin, emulate_bf16 != 0, in, z, out);
+    for (int j = 0; j < nout; ++j) y[r * nout + j] = out[j] * osc[j] + osh[j];
+  }
+}
+
+double oracle_mlp_gradients(int32_t nin, int32_t nout, int32_t width, int32_t nhidden,
+                            const float* params, const float* scaling, int64_t nb,
+                            const double* x, const double* target, double* grad,
+                            int32_t emulate_bf16) {
+  const MlpShape S = mlp_shape(nin, nout, width, nhidden);
+  const bool bf = emulate_bf16 != 0;
+  auto R = [&](double v) { return bf ? (double)bf16_round((float)v) : v; };
+  const float* osh = scaling + 2 * nin;
+  const float* osc = scaling + 2 * nin + nout;
+  const int64_t np = S.boff[S.nl - 1] + S.N[S.nl - 1];
+  std::fill(grad, grad + np, 0.0);
+  double loss = 0;
+  const double scale = 2.0 / ((double)nb * nout);
+  std::vector<std::vector<double>> in, z;
+  std::vector<double> out;
+  for (int64_t r = 0; r < nb; ++r) {
+    mlp_sample(S, params, scaling, x + r * nin, bf, in, z, out);
+    std::vector<double> d(nout);
+    for (int j = 0; j < nout; ++j) {
+      const double t = bf ? (double)(float)((target[r * nout + j] - osh[j]) / osc[j])
+                          : (target[r * nout + j] - osh[j]) / osc[j];
+      const double e = out[j] - t;
+      loss += e * e;
+      d[j] = R(bf ? (double)((float)scale * (float)e) : scale * e);
+    }
+    for (int l = S.nl - 1; l >= 0; --l) {
+      for (int o = 0; o < S.N[l]; ++o) {
+        grad[S.boff[l] + o] += d[o];
+        for (int k = 0; k < S.K[l]; ++k) grad[S.woff[l] + (int64_t)o * S.K[l] + k] += d[o] * in[l][k];
+      }
+      if (l == 0) break;
+      std::vector<double> dp(S.K[l]);
+      for (int k = 0; k < S.K[l]; ++k) {
+        double acc = 0;
+        for (int o = 0; o < S.N[l]; ++o) acc += d[o] * R(params[S.woff[l] + (int64_t)o * S.K[l] + k]);
+        const double zz = z[l - 1][k];
+        const double sg = 1.0 / (1.0 + std::exp(-zz));
+        dp[k] = R(acc * sg * (1.0 + zz * (1.0 - sg)));
+      }
+      d.swap(dp);
+    }
+  }
+  return loss / ((double)nb * nout);
 }
 
 }  // extern "C"

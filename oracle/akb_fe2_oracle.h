@@ -48,6 +48,22 @@ void oracle_rve_stress(int32_t n, double L, const uint8_t* voxel_material,
                        const double* grad_u, const double* fluct, double* stress,
                        double* internal_force /* n^3 x 3 or null */);
 
+/* The surrogate MLP (akantu_b200/csrc/akb_mlp.cu) in FP64: nin -> width
+ * (SiLU) x nhidden -> nout, parameters in the library's layout (per layer
+ * W row-major [out][in], then b). With emulate_bf16 the values the tensor
+ * cores consume are rounded to BF16 where the CUDA kernels round them (the
+ * normalised input, weights, hidden activations, dY and dZ) and the output
+ * and pre-activations to FP32; sums stay FP64. scaling: in_shift, in_scale
+ * [nin], out_shift, out_scale [nout]. y: [nb][nout]. */
+void oracle_mlp_forward(int32_t nin, int32_t nout, int32_t width, int32_t nhidden,
+                        const float* params, const float* scaling, int64_t nb, const double* x,
+                        double* y, int32_t emulate_bf16);
+/* Loss (mean squared error of the normalised outputs) and its gradient. */
+double oracle_mlp_gradients(int32_t nin, int32_t nout, int32_t width, int32_t nhidden,
+                            const float* params, const float* scaling, int64_t nb,
+                            const double* x, const double* target, double* grad,
+                            int32_t emulate_bf16);
+
 #ifdef __cplusplus
 }
 #endif

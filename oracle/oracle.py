@@ -239,3 +239,50 @@ class OracleRVE:
                                    _p(H, C.c_double), _p(w, C.c_double), _p(P, C.c_double),
                                    _p(f, C.c_double))
         return P.reshape(3, 3).T.copy(), f
+
+
+# ----------------------------------------------------------------- FE^2 (MLP)
+def _mlp_lib():
+    lib = _fe2_lib()
+    if getattr(lib, "_mlp_ready", False):
+        return lib
+    D, F = C.POINTER(C.c_double), C.POINTER(C.c_float)
+    lib.oracle_mlp_forward.argtypes = [C.c_int32] * 4 + [F, F, C.c_int64, D, D, C.c_int32]
+    lib.oracle_mlp_gradients.restype = C.c_double
+    lib.oracle_mlp_gradients.argtypes = [C.c_int32] * 4 + [F, F, C.c_int64, D, D, D, C.c_int32]
+    lib._mlp_ready = True
+    return lib
+
+
+class OracleMLP:
+    """FP64 twin of the tensor-core MLP (oracle/akb_fe2_oracle.cc)."""
+
+    def __init__(self, nin, nout, width, nhidden, params, in_shift=None, in_scale=None,
+                 out_shift=None, out_scale=None):
+        self.shape = (nin, nout, width, nhidden)
+        self.params = np.ascontiguousarray(params, dtype=np.float32)
+        z = lambda n, v: np.full(n, v, np.float32)
+        self.scaling = np.ascontiguousarray(np.concatenate([
+            z(nin, 0) if in_shift is None else np.asarray(in_shift, np.float32),
+            z(nin, 1) if in_scale is None else np.asarray(in_scale, np.float32),
+            z(nout, 0) if out_shift is None else np.asarray(out_shift, np.float32),
+            z(nout, 1) if out_scale is None else np.asarray(out_scale, np.float32)]))
+        self.lib = _mlp_lib()
+
+    def forward(self, x, emulate_bf16=True):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros((x.shape[0], self.shape[1]))
+        self.lib.oracle_mlp_forward(*self.shape, _p(self.params, C.c_float),
+                                    _p(self.scaling, C.c_float), x.shape[0], _p(x, C.c_double),
+                                    _p(y, C.c_double), int(emulate_bf16))
+        return y
+
+    def gradients(self, x, target, emulate_bf16=True):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        g = np.zeros(self.params.size)
+        loss = self.lib.oracle_mlp_gradients(*self.shape, _p(self.params, C.c_float),
+                                             _p(self.scaling, C.c_float), x.shape[0],
+                                             _p(x, C.c_double), _p(t, C.c_double),
+                                             _p(g, C.c_double), int(emulate_bf16))
+        return loss, g

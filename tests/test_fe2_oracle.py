@@ -81,3 +81,42 @@ def test_relaxation_reaches_equilibrium(solved):
     P3, _, it3, r3 = R.solve(H, tolerance=1e-4)
     assert r3 <= 1e-4 and it3 > 0
     assert np.abs(P3 - P).max() <= 1e-3 * np.abs(P).max()
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    from oracle.oracle import OracleMLP
+    rng = np.random.default_rng(0)
+    nin, nout, width, nh = 9, 9, 8, 2
+    sizes = [(nin, width), (width, width), (width, nout)]
+    n = sum(k * m + m for k, m in sizes)
+    p = rng.normal(0, 0.5, n).astype(np.float32)
+    x = rng.normal(size=(5, nin))
+    t = rng.normal(size=(5, nout))
+    O = OracleMLP(nin, nout, width, nh, p)
+    loss, g = O.gradients(x, t, emulate_bf16=False)
+    for k in rng.choice(n, 25, replace=False):
+        h = 1e-3
+        # central difference through the float32 parameter vector, with the
+        # step float32 actually represents
+        up, dn = p.copy(), p.copy()
+        up[k] += np.float32(h)
+        dn[k] -= np.float32(h)
+        step = float(up[k]) - float(dn[k])
+        lu, _ = OracleMLP(nin, nout, width, nh, up).gradients(x, t, emulate_bf16=False)
+        ld, _ = OracleMLP(nin, nout, width, nh, dn).gradients(x, t, emulate_bf16=False)
+        fd = (lu - ld) / step
+        assert abs(fd - g[k]) <= 1e-5 * max(1.0, abs(g[k])), (k, fd, g[k])
+
+
+def test_mlp_oracle_bf16_emulation_is_close():
+    from oracle.oracle import OracleMLP
+    rng = np.random.default_rng(1)
+    nin, nout, width, nh = 9, 9, 64, 3
+    sizes = [(nin, width)] + [(width, width)] * (nh - 1) + [(width, nout)]
+    p = np.concatenate([np.concatenate([rng.uniform(-1, 1, k * m) * np.sqrt(6 / (k + m)),
+                                        np.zeros(m)]) for k, m in sizes]).astype(np.float32)
+    O = OracleMLP(nin, nout, width, nh, p)
+    x = rng.normal(size=(64, nin))
+    y64 = O.forward(x, emulate_bf16=False)
+    y16 = O.forward(x, emulate_bf16=True)
+    assert np.abs(y16 - y64).max() <= 3e-2 * np.abs(y64).max()
