@@ -17,7 +17,10 @@
 // voxel), dt = factor h s_min(F) / c_J (s_min the smallest singular value of
 // F, c_J the P-wave speed raised by compression, ln J < 0) and
 // c = factor 2 (2 pi / L) min sqrt(mu / (lambda + 2 mu)) (critical damping of
-// the lowest shear mode). The homogenised stress is sum w_q P / L^3.
+// the lowest shear mode). Strain concentrates in the soft phase beyond what
+// F shows, so an attempt whose residual turns non-finite or explodes is
+// restarted from its initial state with a 0.6x time step (at most 3 times).
+// The homogenised stress is sum w_q P / L^3.
 #include <cmath>
 #include <memory>
 #include <mutex>
@@ -46,7 +49,10 @@ struct akb_rve {
 namespace akb {
 namespace {
 
-constexpr int kRveThreads = 512;
+constexpr int kRveThreads = 256;  // 2 voxels per thread and colour at n = 16; no register spills
+constexpr double kDivergence = 1e4;     // relative residual taken as divergence
+constexpr double kRestartFactor = 0.6;  // time-step factor of each restart
+constexpr int kMaxRestarts = 3;
 
 struct RveArgs {
   int n, nn, nmat, max_it, check;
@@ -115,10 +121,53 @@ __device__ inline RveSmem<S> carve(unsigned char* smem, int nn) {
   return s;
 }
 
+// First Piola-Kirchhoff stress of a voxel point (row-major, g = grad u):
+// neo-Hookean P = mu F + (lambda ln J - mu) F^-T with F^-T = cof(F) / J (the
+// reference's F S, S = mu (I - C^-1) + lambda ln J C^-1, since F C^-1 =
+// F^-T), or small-strain elastic sigma.
+template <typename S>
+__device__ inline void voxel_stress(const MatParams& mp, const S* g, S* P) {
+  const S lam = S(mp.lambda), mu = S(mp.mu);
+  if (mp.kind != AKB_MATERIAL_NEOHOOKEAN) {
+    const S tr = g[0] + g[4] + g[8];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) P[i * 3 + j] = mu * (g[i * 3 + j] + g[j * 3 + i]) + (i == j ? lam * tr : S(0));
+    return;
+  }
+  S F[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) F[k] = g[k] + (k % 4 == 0 ? S(1) : S(0));
+  S c[9];  // cofactors: c[i*3+j] = dJ/dF_ij
+  c[0] = F[4] * F[8] - F[5] * F[7];
+  c[1] = F[5] * F[6] - F[3] * F[8];
+  c[2] = F[3] * F[7] - F[4] * F[6];
+  c[3] = F[2] * F[7] - F[1] * F[8];
+  c[4] = F[0] * F[8] - F[2] * F[6];
+  c[5] = F[1] * F[6] - F[0] * F[7];
+  c[6] = F[1] * F[5] - F[2] * F[4];
+  c[7] = F[2] * F[3] - F[0] * F[5];
+  c[8] = F[0] * F[4] - F[1] * F[3];
+  const S J = F[0] * c[0] + F[1] * c[1] + F[2] * c[2];
+  const S k = (lam * log(J) - mu) / J;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) P[q] = mu * F[q] + k * c[q];
+}
+
 // f -= element forces of every voxel (8 colours); PSUM also adds
 // sum_q w_q P (row-major) of this thread's voxels to psum.
+//
+// The voxel is a cube, so its shape gradients factor along its 12 edges:
+// with corners o = ox + 2 oy + 4 oz and s(b) = 2 b - 1,
+//   dN_o/dx at Gauss point q = s(ox) (1 + s(oy) c_y)(1 + s(oz) c_z) / (4 h),
+// so du/dx at q is sum over the 4 x-edges e = oy + 2 oz of
+// W[q][x][e] (u(1, oy, oz) - u(0, oy, oz)) (and likewise along y, z), and the
+// corner force sum_q w_q P grad N_o is s(ox) T_x[e_x(o)] + s(oy) T_y[e_y(o)]
+// + s(oz) T_z[e_z(o)] with the edge sums T_j[e] = sum_q W[q][j][e] w_q P[:, j].
+// Same arithmetic content as the shape-gradient form, half the operations.
 template <typename S, bool PSUM>
-__device__ void voxel_forces(const RveArgs& R, const RveSmem<S>& s, const S* H,
+__device__ void voxel_forces(const RveArgs& R, const RveSmem<S>& s, const S* hH,
                              const MatParams* mats, double* psum) {
   const int n = R.n, nn = R.nn, hn = n >> 1, nc = hn * hn * hn;
   const S wq = S(R.h * R.h * R.h / 8.0);
@@ -131,54 +180,69 @@ __device__ void voxel_forces(const RveArgs& R, const RveSmem<S>& s, const S* H,
                 z1 = ez + 1 == n ? 0 : ez + 1;
       int nd[8];
 #pragma unroll
-      for (int a = 0; a < 8; ++a)
-        nd[a] = (corner_x(a) ? x1 : ex) + n * ((corner_y(a) ? y1 : ey) + n * (corner_z(a) ? z1 : ez));
-      S du[24];
+      for (int o = 0; o < 8; ++o)
+        nd[o] = ((o & 1) ? x1 : ex) + n * (((o & 2) ? y1 : ey) + n * ((o & 4) ? z1 : ez));
+      S D[3][4][3];  // edge differences [direction][edge][component]
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        const S w0 = s.u[i * nn + nd[0]];
-        du[i] = 0;
+        S uc[8];
 #pragma unroll
-        for (int a = 1; a < 8; ++a) du[a * 3 + i] = s.u[i * nn + nd[a]] - w0;
+        for (int o = 0; o < 8; ++o) uc[o] = s.u[i * nn + nd[o]];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          // total displacement along the edge: fluctuation + h H e_j (the
+          // weights of a direction sum to 1/h, so sum_e W D = H + grad w)
+          const int b0 = e & 1, b1 = e >> 1;
+          D[0][e][i] = (uc[1 + 2 * b0 + 4 * b1] - uc[2 * b0 + 4 * b1]) + hH[i * 3 + 0];
+          D[1][e][i] = (uc[b0 + 2 + 4 * b1] - uc[b0 + 4 * b1]) + hH[i * 3 + 1];
+          D[2][e][i] = (uc[b0 + 2 * b1 + 4] - uc[b0 + 2 * b1]) + hH[i * 3 + 2];
+        }
       }
       const MatParams& mp = mats[s.mat[ex + n * (ey + n * ez)]];
-      S fe[24];
+      S T[3][4][3];
 #pragma unroll
-      for (int k = 0; k < 24; ++k) fe[k] = 0;
+      for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+#pragma unroll
+          for (int i = 0; i < 3; ++i) T[j][e][i] = 0;
 #pragma unroll 1
       for (int q = 0; q < 8; ++q) {
-        const S* Bq = s.B + q * 24;
+        const S* Wq = s.B + q * 12;  // [direction][edge]
         S g[9];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
           for (int j = 0; j < 3; ++j) {
-            S c = H[i * 3 + j];
+            S c = Wq[j * 4] * D[j][0][i];
 #pragma unroll
-            for (int a = 1; a < 8; ++a) c += du[a * 3 + i] * Bq[a * 3 + j];
+            for (int e = 1; e < 4; ++e) c += Wq[j * 4 + e] * D[j][e][i];
             g[i * 3 + j] = c;
           }
         S P[9];
-        fast::stress_P<3, S>(mp, g, P);
+        voxel_stress<S>(mp, g, P);
 #pragma unroll
         for (int k = 0; k < 9; ++k) P[k] *= wq;
 #pragma unroll
-        for (int a = 0; a < 8; ++a)
+        for (int j = 0; j < 3; ++j)
 #pragma unroll
-          for (int i = 0; i < 3; ++i) {
-            S c = fe[a * 3 + i];
+          for (int e = 0; e < 4; ++e)
 #pragma unroll
-            for (int j = 0; j < 3; ++j) c += P[i * 3 + j] * Bq[a * 3 + j];
-            fe[a * 3 + i] = c;
-          }
+            for (int i = 0; i < 3; ++i) T[j][e][i] += Wq[j * 4 + e] * P[i * 3 + j];
         if (PSUM)
 #pragma unroll
           for (int k = 0; k < 9; ++k) psum[k] += double(P[k]);
       }
 #pragma unroll
-      for (int a = 0; a < 8; ++a)
+      for (int o = 0; o < 8; ++o) {
+        const int ox = o & 1, oy = (o >> 1) & 1, oz = o >> 2;
 #pragma unroll
-        for (int i = 0; i < 3; ++i) s.f[i * nn + nd[a]] -= fe[a * 3 + i];
+        for (int i = 0; i < 3; ++i) {
+          const S tx = T[0][oy + 2 * oz][i], ty = T[1][ox + 2 * oz][i], tz = T[2][ox + 2 * oy][i];
+          const S fo = (ox ? tx : -tx) + (oy ? ty : -ty) + (oz ? tz : -tz);
+          s.f[i * nn + nd[o]] -= fo;
+        }
+      }
     }
     __syncthreads();
   }
@@ -208,26 +272,19 @@ __global__ void __launch_bounds__(kRveThreads, 1)
   RveSmem<S> s = carve<S>(smem, nn);
   __shared__ MatParams mats[8];
 
-  // stage the state and the constant tables
+  // the constant tables
   const S* im_g = static_cast<const S*>(R.inv_mass);
-  for (int k = tid; k < 3 * nn; k += bs) {
-    const int node = k / 3, i = k - 3 * node;
-    s.u[i * nn + node] = fluct ? fluct[inst * 3 * nn + k] : S(0);
-    s.v[k] = 0;
-  }
   for (int k = tid; k < nn; k += bs) {
     s.im[k] = im_g[k];
     s.mat[k] = R.vmat[k];
   }
-  if (tid < 192) {
-    const int q = tid / 24, a = (tid / 3) % 8, j = tid % 3;
+  if (tid < 96) {  // edge weights W[q][direction][edge] (see voxel_forces)
+    const int q = tid / 12, j = (tid / 4) % 3, e = tid % 4;
     const double gp = 1.0 / sqrt(3.0);
     const double c[3] = {(q & 1) ? gp : -gp, (q & 2) ? gp : -gp, (q & 4) ? gp : -gp};
-    const double sg[3] = {2.0 * corner_x(a) - 1, 2.0 * corner_y(a) - 1, 2.0 * corner_z(a) - 1};
-    double val = 0.125 * sg[j];
-    for (int k = 0; k < 3; ++k)
-      if (k != j) val *= 1.0 + sg[k] * c[k];
-    s.B[tid] = S(val * (2.0 / R.h));
+    const int d1 = j == 0 ? 1 : 0, d2 = j == 2 ? 1 : 2;  // the two other directions
+    const double s1 = 2.0 * (e & 1) - 1.0, s2 = 2.0 * (e >> 1) - 1.0;
+    s.B[tid] = S((1.0 + s1 * c[d1]) * (1.0 + s2 * c[d2]) / (4.0 * R.h));
   }
   if (tid < R.nmat) {
     MatParams mp{};
@@ -238,17 +295,15 @@ __global__ void __launch_bounds__(kRveThreads, 1)
     mp.E = 1.0;
     mats[tid] = mp;
   }
-  S H[9];
+  __shared__ S hH[9];  // h H, row-major
   double Hd[9];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      Hd[i * 3 + j] = grad_u[inst * 9 + i + 3 * j];
-      H[i * 3 + j] = S(Hd[i * 3 + j]);
-    }
+    for (int j = 0; j < 3; ++j) Hd[i * 3 + j] = grad_u[inst * 9 + i + 3 * j];
+  if (tid < 9) hH[tid] = S(R.h * Hd[tid]);
   if (tid == 0) {
-    // time step, damping and residual scale of this instance
+    // time-step scale, damping and residual scale of this instance
     double F[9], C[9];
     for (int k = 0; k < 9; ++k) F[k] = Hd[k] + (k % 4 == 0 ? 1.0 : 0.0);
     for (int i = 0; i < 3; ++i)
@@ -269,43 +324,59 @@ __global__ void __launch_bounds__(kRveThreads, 1)
       mumax = fmax(mumax, R.mu[m]);
     }
     for (int k = 0; k < 9; ++k) hmax = fmax(hmax, fabs(Hd[k]));
-    s.par[0] = R.tsf * R.h * smin / sqrt(c2);
+    s.par[0] = R.h * smin / sqrt(c2);
     s.par[1] = R.dampf * 2.0 * (2.0 * M_PI / R.L) * cs;
     s.par[2] = R.h * R.h * mumax * fmax(hmax, 1e-6);
   }
   __syncthreads();
-  const S dt = S(s.par[0]);
-  const S a1 = S(1.0 - 0.5 * s.par[1] * s.par[0]), a2 = S(1.0 + 0.5 * s.par[1] * s.par[0]);
   const double fscale = s.par[2];
 
-  int k = 0;
-  double r = 0.0;
-  for (;; ++k) {
-    for (int idx = tid; idx < 3 * nn; idx += bs) s.f[idx] = 0;
-    __syncthreads();
-    voxel_forces<S, false>(R, s, H, mats, nullptr);
-    const bool last = k >= R.max_it;
-    if (last || (R.check > 0 && k % R.check == 0)) {
-      double lm = 0.0;
-      for (int idx = tid; idx < 3 * nn; idx += bs) {
-        const double x = double(s.f[idx]);
-        lm = isfinite(x) ? fmax(lm, fabs(x)) : INFINITY;
-      }
-      lm = warp_max(lm);
-      if (lane == 0) s.red[warp] = lm;
-      __syncthreads();
-      double m = 0.0;
-      for (int w = 0; w < nwarps; ++w) m = fmax(m, s.red[w]);
-      r = isfinite(m) ? m / fscale : INFINITY;
-      __syncthreads();  // s.red is reused
-      if (last || !isfinite(r) || (R.tol >= 0 && r <= R.tol)) break;
-    }
+  // Relaxation; an attempt whose residual turns non-finite or exceeds
+  // kDivergence restarts from the initial state with a 0.6x time step.
+  int total = 0, k = 0;
+  double r = 0.0, tsf = R.tsf;
+  for (int attempt = 0;; ++attempt, tsf *= kRestartFactor) {
     for (int idx = tid; idx < 3 * nn; idx += bs) {
-      const int node = idx % nn;
-      const S vv = (a1 * s.v[idx] + dt * s.f[idx] * s.im[node]) / a2;
-      s.v[idx] = vv;
-      s.u[idx] += dt * vv;
+      const int node = idx / 3, i = idx - 3 * node;
+      s.u[i * nn + node] = fluct ? fluct[inst * 3 * nn + idx] : S(0);
+      s.v[idx] = 0;
     }
+    const double dtd = tsf * s.par[0];
+    const S dt = S(dtd);
+    const S a1 = S(1.0 - 0.5 * s.par[1] * dtd), a2 = S(1.0 + 0.5 * s.par[1] * dtd);
+    __syncthreads();
+    bool diverged = false;
+    for (k = 0;; ++k) {
+      for (int idx = tid; idx < 3 * nn; idx += bs) s.f[idx] = 0;
+      __syncthreads();
+      voxel_forces<S, false>(R, s, hH, mats, nullptr);
+      const bool last = k >= R.max_it;
+      if (last || (R.check > 0 && k % R.check == 0)) {
+        double lm = 0.0;
+        for (int idx = tid; idx < 3 * nn; idx += bs) {
+          const double x = double(s.f[idx]);
+          lm = isfinite(x) ? fmax(lm, fabs(x)) : INFINITY;
+        }
+        lm = warp_max(lm);
+        if (lane == 0) s.red[warp] = lm;
+        __syncthreads();
+        double m = 0.0;
+        for (int w = 0; w < nwarps; ++w) m = fmax(m, s.red[w]);
+        r = isfinite(m) ? m / fscale : INFINITY;
+        __syncthreads();  // s.red is reused
+        diverged = !(r <= kDivergence);
+        if (last || diverged || (R.tol >= 0 && r <= R.tol)) break;
+      }
+      for (int idx = tid; idx < 3 * nn; idx += bs) {
+        const int node = idx % nn;
+        const S vv = (a1 * s.v[idx] + dt * s.f[idx] * s.im[node]) / a2;
+        s.v[idx] = vv;
+        s.u[idx] += dt * vv;
+      }
+      __syncthreads();
+    }
+    total += k;
+    if (!diverged || attempt >= kMaxRestarts) break;
     __syncthreads();
   }
 
@@ -315,7 +386,7 @@ __global__ void __launch_bounds__(kRveThreads, 1)
   double ps[9];
 #pragma unroll
   for (int q = 0; q < 9; ++q) ps[q] = 0.0;
-  voxel_forces<S, true>(R, s, H, mats, ps);
+  voxel_forces<S, true>(R, s, hH, mats, ps);
 #pragma unroll
   for (int q = 0; q < 9; ++q) {
     const double x = warp_sum(ps[q]);
@@ -329,7 +400,7 @@ __global__ void __launch_bounds__(kRveThreads, 1)
     stress[inst * 9 + i + 3 * j] = t / (R.L * R.L * R.L);
   }
   if (tid == 0) {
-    if (iterations) iterations[inst] = k;
+    if (iterations) iterations[inst] = total;
     if (residual) residual[inst] = r;
   }
   for (int idx = tid; idx < 3 * nn; idx += bs) {

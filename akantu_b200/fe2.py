@@ -58,3 +58,149 @@ def in_envelope(H, amplitude=0.3, min_det=0.5):
     H = np.asarray(H).reshape(-1, 3, 3)
     return (np.abs(H).max(axis=(1, 2)) <= amplitude) & \
            (np.linalg.det(np.eye(3) + H) >= min_det)
+
+
+# --------------------------------------------------------------- the macro side
+def voigt_material(mats, fractions, rho=1100.0):
+    """Material descriptor with the Voigt (upper-bound) Lame moduli of the
+    mixture: its wave speed bounds the macroscopic one, so the stable time
+    step computed from it is safe for the homogenised material."""
+    lam = sum(f * m["lam"] for f, m in zip(fractions, mats))
+    mu = sum(f * m["mu"] for f, m in zip(fractions, mats))
+    return dict(rho=rho, E=mu * (3 * lam + 2 * mu) / (lam + mu), nu=lam / (2 * (lam + mu)))
+
+
+def spec_rve(cells=16, precision=None, **options):
+    """The periodic RVE of the FE^2 workload: 16^3 voxels, centred sphere of
+    voxel fraction ~0.2, neo-Hookean matrix lambda = 1 MPa, mu = 0.4 MPa and
+    an inclusion 10 times stiffer."""
+    from .rve import SolidMechanicsModelRVE
+    vm, vf = sphere_inclusion_rve(cells)
+    mats = matrix_inclusion_materials()
+    kw = dict(options)
+    if precision is not None:
+        kw["precision"] = precision
+    return SolidMechanicsModelRVE(cells, vm, mats, **kw), mats, vf
+
+
+def generate_dataset(rve, count, seed=SEED, chunk=32768, amplitude=0.3, min_det=0.5):
+    """count samples (H, P) with H drawn in the envelope and P the relaxed
+    RVE's homogenised stress. Returns device FP64 features X, Y (count, 9)
+    (column-major flattening) and the iteration counts."""
+    import torch
+    H = sample_gradients(count, seed=seed, amplitude=amplitude, min_det=min_det)
+    X, Y, its = [], [], []
+    for k in range(0, count, chunk):
+        Hc = torch.as_tensor(H[k:k + chunk], device="cuda:%d" % rve.device)
+        out = rve.solve(Hc)
+        X.append(Hc.transpose(1, 2).reshape(-1, 9))
+        Y.append(out["stress"].transpose(1, 2).reshape(-1, 9))
+        its.append(out["iterations"])
+    return torch.cat(X).contiguous(), torch.cat(Y).contiguous(), torch.cat(its)
+
+
+def surrogate_error(net, X, Y):
+    """Relative stress errors of the surrogate on (X, Y) features: the global
+    relative L2 error, the median and the 99th percentile of the per-sample
+    relative error ||P_net - P|| / ||P||."""
+    import torch
+    P = net.forward_features(X)
+    d = torch.linalg.norm(P - Y, dim=1)
+    r = torch.linalg.norm(Y, dim=1)
+    per = (d / r.clamp_min(1e-30)).cpu().numpy()
+    return dict(relative_l2=float(torch.linalg.norm(P - Y) / torch.linalg.norm(Y)),
+                median=float(np.median(per)), p99=float(np.percentile(per, 99)))
+
+
+class MaterialFE2:
+    """Stress provider of the FE^2 macro material: the homogenised stress of a
+    periodic RVE per quadrature point (warm-started from that point's previous
+    fluctuation), or the learned surrogate inside its training envelope with
+    RVE solves for the points outside it. Plugged into a SolidMechanicsModel
+    through MaterialUser (the reference's MaterialFE2::computeStress,
+    extra_packages/extra-materials/src/material_FE2/material_FE2.cc:116-157)."""
+
+    def __init__(self, rve, surrogate=None, amplitude=0.3, min_det=0.5, chunk=32768,
+                 warm_start=True):
+        self.rve = rve
+        self.surrogate = surrogate
+        self.amplitude = amplitude
+        self.min_det = min_det
+        self.chunk = chunk
+        self.warm_start = warm_start
+        self.fluct = None
+        self.stats = dict(rve_solves=0, fallback=0, iterations=0)
+
+    def material(self, mats, fractions, rho=1100.0):
+        from .model import MaterialUser
+        outer = self
+
+        class _M(MaterialUser):
+            def computeStress(self, grad_u, stress):
+                outer.compute(grad_u, stress)
+        d = voigt_material(mats, fractions, rho)
+        return _M(rho=d["rho"], E=d["E"], nu=d["nu"], finite_deformation=True)
+
+    def _rve(self, H, idx=None):
+        import torch
+        n = H.shape[0]
+        if self.warm_start and (self.fluct is None or self.fluct.shape[0] != self.nq):
+            self.fluct = self.rve.zero_fluctuation(self.nq)
+        P = torch.empty((n, 3, 3), dtype=torch.float64, device=H.device)
+        for k in range(0, n, self.chunk):
+            sl = slice(k, min(n, k + self.chunk))
+            w = None
+            if self.warm_start:
+                rows = torch.arange(sl.start, sl.stop, device=H.device) if idx is None else idx[sl]
+                w = self.fluct[rows].contiguous()
+            out = self.rve.solve(H[sl], w)
+            if self.warm_start:
+                self.fluct[rows] = w
+            P[sl] = out["stress"]
+            self.stats["iterations"] += int(out["iterations"].sum())
+        self.stats["rve_solves"] += n
+        return P
+
+    def compute(self, grad_u, stress):
+        import torch
+        self.nq = grad_u.shape[0]
+        if self.surrogate is None:
+            stress.copy_(self._rve(grad_u))
+            return
+        P = self.surrogate(grad_u)
+        hmax = grad_u.abs().flatten(1).max(dim=1).values
+        det = torch.linalg.det(torch.eye(3, dtype=grad_u.dtype, device=grad_u.device) + grad_u)
+        out = (hmax > self.amplitude) | (det < self.min_det)
+        idx = torch.nonzero(out).flatten()
+        if idx.numel():
+            P[idx] = self._rve(grad_u[idx].contiguous(), idx)
+            self.stats["fallback"] += int(idx.numel())
+        stress.copy_(P)
+
+
+def macro_block(material, cells=32, length=1.0, precision=None):
+    """The FE^2 macro problem: a cube of cells^3 hexahedron_8, face x = 0
+    fixed, face x = L pulled along x (its x displacement prescribed)."""
+    from . import _abi
+    from .mesh import block_hexahedron8
+    from .model import SolidMechanicsModel
+    mesh = block_hexahedron8(cells, length)
+    m = SolidMechanicsModel(mesh, [material], precision=_abi.MODE_FP64)
+    m.initFull()
+    x = mesh.nodes
+    left = np.nonzero(np.isclose(x[:, 0], 0.0))[0]
+    right = np.nonzero(np.isclose(x[:, 0], length))[0]
+    blocked = np.zeros_like(x, dtype=np.uint8)
+    blocked[left] = 1
+    blocked[right, 0] = 1
+    m.setBlockedDOFs(blocked)
+    m.fe2_right = right
+    m.fe2_length = length
+    return m
+
+
+def macro_step(model, step, ramp_steps=200, stretch=0.05):
+    """One macro step with the pulled face at stretch * L * min(step / ramp, 1)."""
+    ux = stretch * model.fe2_length * min(step / ramp_steps, 1.0)
+    model.applyDirichlet(model.fe2_right, 0, ux)
+    model.solveStep()

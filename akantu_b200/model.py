@@ -258,6 +258,17 @@ class SolidMechanicsModel:
         check(lib().akb_set_blocked_dofs(self.handle, b.ctypes.data_as(C.POINTER(C.c_uint8)),
                                          b.size))
 
+    def applyDirichlet(self, nodes, component, values):
+        """applyBC(FixedValue(value, axis), group) for a node group
+        (boundary_condition_tmpl.hh:63-200): blocks the DOFs and sets their
+        displacement on the device."""
+        self._sync_in()
+        n = np.ascontiguousarray(nodes, dtype=np.uint32)
+        v = np.ascontiguousarray(np.broadcast_to(values, n.shape), dtype=np.float64)
+        check(lib().akb_apply_dirichlet(self.handle, n.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                        n.size, int(component),
+                                        v.ctypes.data_as(C.POINTER(C.c_double))))
+
     def getGradU(self):
         return self.getField(_abi.FIELD_GRAD_U)
 

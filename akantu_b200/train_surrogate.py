@@ -1,0 +1,63 @@
+"""Trains the learned RVE surrogate of the FE^2 workload and writes its
+weights (python -m akantu_b200.train_surrogate --samples N --out PATH).
+
+1. Macroscopic gradients H with H_ij ~ U[-0.3, 0.3], det(I + H) >= 0.5,
+   each relaxed on the 16^3 periodic sphere-inclusion RVE (batched RVE
+   kernel, FP32, residual 1e-4) for its homogenised stress P.
+2. A held-out set from another seed.
+3. The 9-256-256-256-9 SiLU MLP trained with Adam on the tensor cores
+   (normalised inputs and outputs, cosine learning-rate decay).
+Prints one JSON line: sizes, RVE solve rate, training time, held-out errors.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_OUT = os.path.join(HERE, "data", "rve_surrogate.npz")
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--samples", type=int, default=2_000_000)
+    ap.add_argument("--heldout", type=int, default=16384)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--out", default=DEFAULT_OUT)
+    ap.add_argument("--seed", type=int, default=20261203)
+    a = ap.parse_args(argv)
+    import torch
+    from . import fe2
+    from .surrogate import MLPSurrogate
+    rve, mats, vf = fe2.spec_rve(16)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    X, Y, it = fe2.generate_dataset(rve, a.samples, seed=a.seed)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    Xh, Yh, _ = fe2.generate_dataset(rve, a.heldout, seed=a.seed + 1)
+    net = MLPSurrogate(seed=a.seed)
+    net.fit_scaling(X.cpu().numpy(), Y.cpu().numpy())
+    t1 = time.perf_counter()
+    losses = net.train(X, Y, epochs=a.epochs, batch=a.batch, lr=a.lr, lr_final=a.lr * 1e-3,
+                       seed=a.seed)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t1
+    err = fe2.surrogate_error(net, Xh, Yh)
+    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+    net.save(a.out)
+    print(json.dumps(dict(samples=a.samples, heldout=a.heldout, voxel_fraction=vf,
+                          rve_solves_per_s=a.samples / t_data,
+                          mean_iterations=float(it.float().mean()), data_s=t_data,
+                          train_s=t_train, epochs=a.epochs, final_loss=losses[-1],
+                          heldout_error=err, out=a.out)))
+
+
+if __name__ == "__main__":
+    main()

@@ -250,29 +250,41 @@ int32_t oracle_rve_solve(int32_t n, double L, const uint8_t* voxel_material,
   for (int k = 0; k < 9; ++k) hmax = std::max(hmax, std::fabs(grad_u[k]));
   for (int m = 0; m < nb_materials; ++m) mumax = std::max(mumax, mu[m]);
   const double fscale = h * h * mumax * std::max(hmax, 1e-6);
-  const double a1 = 1.0 - 0.5 * cd * dt, a2 = 1.0 + 0.5 * cd * dt;
-  std::vector<double> f(3 * nn), v(3 * nn, 0.0);
-  int k = 0;
-  double r = 0;
-  for (;; ++k) {
-    forces(R, fluct, f.data(), nullptr);
-    const bool last = k >= max_iterations;
-    if (last || (check_interval > 0 && k % check_interval == 0)) {
-      double fm = 0;
-      for (double x : f) fm = std::isfinite(x) ? std::max(fm, std::fabs(x)) : INFINITY;
-      r = fm / fscale;
-      if (last || (tolerance >= 0 && r <= tolerance)) break;
-    }
-    for (int a = 0; a < nn; ++a)
-      for (int i = 0; i < 3; ++i) {
-        const int idx = a * 3 + i;
-        v[idx] = (a1 * v[idx] + dt * f[idx] / mass[a]) / a2;
-        fluct[idx] += dt * v[idx];
+  // an attempt whose residual turns non-finite or exceeds 1e4 restarts from
+  // the initial state with a 0.6x time step, at most 3 times
+  const std::vector<double> start(fluct, fluct + 3 * nn);
+  std::vector<double> f(3 * nn), v(3 * nn);
+  int total = 0, k = 0;
+  double r = 0, tsf = 1.0;
+  for (int attempt = 0;; ++attempt, tsf *= 0.6) {
+    std::copy(start.begin(), start.end(), fluct);
+    std::fill(v.begin(), v.end(), 0.0);
+    const double dta = tsf * dt;
+    const double a1 = 1.0 - 0.5 * cd * dta, a2 = 1.0 + 0.5 * cd * dta;
+    bool diverged = false;
+    for (k = 0;; ++k) {
+      forces(R, fluct, f.data(), nullptr);
+      const bool last = k >= max_iterations;
+      if (last || (check_interval > 0 && k % check_interval == 0)) {
+        double fm = 0;
+        for (double x : f) fm = std::isfinite(x) ? std::max(fm, std::fabs(x)) : INFINITY;
+        r = fm / fscale;
+        diverged = !(r <= 1e4);
+        if (last || diverged || (tolerance >= 0 && r <= tolerance)) break;
       }
+      for (int a = 0; a < nn; ++a)
+        for (int i = 0; i < 3; ++i) {
+          const int idx = a * 3 + i;
+          v[idx] = (a1 * v[idx] + dta * f[idx] / mass[a]) / a2;
+          fluct[idx] += dta * v[idx];
+        }
+    }
+    total += k;
+    if (!diverged || attempt >= 3) break;
   }
   oracle_rve_stress(n, L, voxel_material, lambda, mu, kind, grad_u, fluct, stress, nullptr);
   *residual = r;
-  return k;
+  return total;
 }
 
 }  // extern "C"

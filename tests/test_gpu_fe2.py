@@ -1,0 +1,66 @@
+"""FE^2 on the GPU: macro model with the RVE-backed material, the surrogate
+path with its envelope fallback, and dataset generation."""
+import numpy as np
+import pytest
+
+from akantu_b200 import _abi, fe2
+
+pytestmark = pytest.mark.gpu
+
+
+def small_rve():
+    vm, vf = fe2.sphere_inclusion_rve(8)
+    mats = fe2.matrix_inclusion_materials()
+    from akantu_b200.rve import SolidMechanicsModelRVE
+    return SolidMechanicsModelRVE(8, vm, mats, tolerance=1e-5), mats, vf
+
+
+def run_macro(provider, mats, vf, steps=12, cells=2):
+    m = fe2.macro_block(provider.material(mats, [1 - vf, vf]), cells=cells)
+    m.setTimeStep(0.8 * m.getStableTimeStep())
+    for s in range(1, steps + 1):
+        fe2.macro_step(m, s, ramp_steps=steps, stretch=0.05)
+    u = m.getDisplacement().copy()
+    m.close()
+    return u
+
+
+def test_fallback_everywhere_equals_plain_fe2():
+    """A surrogate whose envelope excludes every point hands all of them to
+    the RVEs: the result is the plain FE^2 result bit for bit."""
+    from akantu_b200.surrogate import MLPSurrogate
+    rve, mats, vf = small_rve()
+    u_plain = run_macro(fe2.MaterialFE2(rve), mats, vf)
+    net = MLPSurrogate()
+    prov = fe2.MaterialFE2(rve, surrogate=net, amplitude=-1.0)
+    u_fb = run_macro(prov, mats, vf)
+    assert prov.stats["fallback"] == prov.stats["rve_solves"] > 0
+    assert np.array_equal(u_plain, u_fb)
+    assert np.abs(u_plain[:, 0]).max() == pytest.approx(0.05 * 1.0, rel=1e-12)
+
+
+def test_plain_fe2_pulls_the_block():
+    rve, mats, vf = small_rve()
+    prov = fe2.MaterialFE2(rve)
+    u = run_macro(prov, mats, vf, steps=12, cells=2)
+    assert prov.stats["rve_solves"] == 12 * 8 * 8
+    # the free faces contract laterally under the stretch
+    assert np.isfinite(u).all() and np.abs(u[:, 1:]).max() > 0
+
+
+def test_dataset_and_surrogate_error_metrics():
+    import torch
+    from akantu_b200.surrogate import MLPSurrogate
+    rve, mats, vf = small_rve()
+    X, Y, it = fe2.generate_dataset(rve, 600, seed=5, chunk=256)
+    assert X.shape == (600, 9) and Y.shape == (600, 9)
+    H = fe2.sample_gradients(600, seed=5)
+    assert np.allclose(X[:, [0, 4, 8]].cpu().numpy(), H[:, [0, 1, 2], [0, 1, 2]])
+    assert np.allclose(X[:, 1].cpu().numpy(), H[:, 1, 0])  # column-major features
+    net = MLPSurrogate()
+    net.fit_scaling(X.cpu().numpy(), Y.cpu().numpy())
+    e = fe2.surrogate_error(net, X, Y)
+    assert e["relative_l2"] > 0 and e["p99"] >= e["median"]
+    net.train(X, Y, epochs=30, batch=128, lr=2e-3)
+    e2 = fe2.surrogate_error(net, X, Y)
+    assert e2["relative_l2"] < e["relative_l2"]
