@@ -86,17 +86,20 @@ def spec_rve(cells=16, precision=None, **options):
 def generate_dataset(rve, count, seed=SEED, chunk=32768, amplitude=0.3, min_det=0.5):
     """count samples (H, P) with H drawn in the envelope and P the relaxed
     RVE's homogenised stress. Returns device FP64 features X, Y (count, 9)
-    (column-major flattening) and the iteration counts."""
+    (column-major flattening), the iteration counts and the final relative
+    residuals."""
     import torch
     H = sample_gradients(count, seed=seed, amplitude=amplitude, min_det=min_det)
-    X, Y, its = [], [], []
+    X, Y, its, res = [], [], [], []
     for k in range(0, count, chunk):
         Hc = torch.as_tensor(H[k:k + chunk], device="cuda:%d" % rve.device)
         out = rve.solve(Hc)
         X.append(Hc.transpose(1, 2).reshape(-1, 9))
         Y.append(out["stress"].transpose(1, 2).reshape(-1, 9))
         its.append(out["iterations"])
-    return torch.cat(X).contiguous(), torch.cat(Y).contiguous(), torch.cat(its)
+        res.append(out["residual"])
+    return (torch.cat(X).contiguous(), torch.cat(Y).contiguous(), torch.cat(its),
+            torch.cat(res))
 
 
 def surrogate_error(net, X, Y):

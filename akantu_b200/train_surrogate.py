@@ -14,6 +14,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import sys
 import time
 
 import numpy as np
@@ -26,7 +27,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--samples", type=int, default=2_000_000)
     ap.add_argument("--heldout", type=int, default=16384)
-    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=DEFAULT_OUT)
@@ -38,21 +39,27 @@ def main(argv=None):
     rve, mats, vf = fe2.spec_rve(16)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    X, Y, it = fe2.generate_dataset(rve, a.samples, seed=a.seed)
+    X, Y, it, res = fe2.generate_dataset(rve, a.samples, seed=a.seed)
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
-    Xh, Yh, _ = fe2.generate_dataset(rve, a.heldout, seed=a.seed + 1)
+    # labels of relaxations that did not reach the tolerance are left out
+    keep = torch.isfinite(res) & (res <= 10 * 1e-4)
+    X, Y = X[keep].contiguous(), Y[keep].contiguous()
+    Xh, Yh, _, rh = fe2.generate_dataset(rve, a.heldout, seed=a.seed + 1)
+    kh = torch.isfinite(rh) & (rh <= 10 * 1e-4)
+    Xh, Yh = Xh[kh].contiguous(), Yh[kh].contiguous()
     net = MLPSurrogate(seed=a.seed)
     net.fit_scaling(X.cpu().numpy(), Y.cpu().numpy())
     t1 = time.perf_counter()
     losses = net.train(X, Y, epochs=a.epochs, batch=a.batch, lr=a.lr, lr_final=a.lr * 1e-3,
-                       seed=a.seed)
+                       seed=a.seed, log=lambda s: print(s, file=sys.stderr, flush=True))
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t1
     err = fe2.surrogate_error(net, Xh, Yh)
     os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
     net.save(a.out)
-    print(json.dumps(dict(samples=a.samples, heldout=a.heldout, voxel_fraction=vf,
+    print(json.dumps(dict(samples=a.samples, kept=int(keep.sum()), heldout=int(kh.sum()),
+                          voxel_fraction=vf,
                           rve_solves_per_s=a.samples / t_data,
                           mean_iterations=float(it.float().mean()), data_s=t_data,
                           train_s=t_train, epochs=a.epochs, final_loss=losses[-1],

@@ -421,6 +421,102 @@ def run_batch(args, device, log=None):
     return out
 
 
+def run_fe2(args, device, log=None):
+    """FE^2 of a 32^3 hexahedron_8 block with a 16^3 periodic RVE at each of its
+    262 144 Gauss points: the learned surrogate against held-out RVE solves,
+    the learned and the plain (RVE) macro step times, and the macro
+    displacement of a learned run against a plain run on a coarser block."""
+    import torch
+    from akantu_b200 import fe2
+    from akantu_b200.surrogate import MLPSurrogate
+    rve, mats, vf = fe2.spec_rve(16)
+    frac = [1 - vf, vf]
+    out = {"workload": "macro %d^3 hexahedron_8 (%d Gauss points), RVE 16^3 voxels, sphere "
+                       "voxel fraction %.4f, neo-Hookean matrix lambda 1 MPa mu 0.4 MPa, "
+                       "inclusion x10; stretch 5%% over %d steps"
+                       % (args.fe2_cells, 8 * args.fe2_cells ** 3, vf, args.fe2_ramp)}
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        a, b = ev(), ev()
+        torch.cuda.synchronize()
+        a.record()
+        r = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b), r
+
+    # RVE solves: held-out samples (another seed than the training set's)
+    ms, (Xh, Yh, it, _) = timed(lambda: fe2.generate_dataset(rve, args.fe2_heldout, seed=7))
+    out["rve"] = {"solves": args.fe2_heldout, "ms": ms,
+                  "solves_per_s": args.fe2_heldout / ms * 1e3,
+                  "mean_iterations": float(it.float().mean()),
+                  "shared_bytes_per_solve": rve.shared_bytes}
+    path = os.path.join(ROOT, "akantu_b200", "data", "rve_surrogate.npz")
+    if not os.path.exists(path):
+        out["surrogate"] = "no trained weights (run python -m akantu_b200.train_surrogate)"
+        return out
+    net = MLPSurrogate.load(path, device=device)
+    out["surrogate"] = {"heldout_error": fe2.surrogate_error(net, Xh, Yh)}
+    # inference throughput over one macro step's Gauss points
+    nq = 8 * args.fe2_cells ** 3
+    Hq = torch.as_tensor(fe2.sample_gradients(nq, seed=9), device="cuda")
+    Xq = Hq.transpose(1, 2).reshape(-1, 9).contiguous()
+    net.forward_features(Xq)
+    reps = 10
+    ms, _ = timed(lambda: [net.forward_features(Xq) for _ in range(reps)])
+    flop = 2 * sum(max(k, 16) * max(n, 16) for k, n in net.layer_shapes())
+    out["surrogate"]["inference"] = {"samples": nq, "ms": ms / reps,
+                                     "tflops": flop * nq / (ms / reps * 1e-3) / 1e12,
+                                     "flop_per_sample": flop}
+
+    # learned FE^2: the whole ramp on the full block
+    learned = fe2.MaterialFE2(rve, surrogate=net)
+    m = fe2.macro_block(learned.material(mats, frac), cells=args.fe2_cells)
+    dt = 0.8 * m.getStableTimeStep()
+    m.setTimeStep(dt)
+    step_ms = []
+    for s in range(1, args.fe2_ramp + 1):
+        ms, _ = timed(lambda: fe2.macro_step(m, s, ramp_steps=args.fe2_ramp))
+        step_ms.append(ms)
+    learned_ms = float(np.median(step_ms[5:]))
+    u_learned = m.getDisplacement().copy()
+    out["learned_step"] = {"ms_median": learned_ms, "steps": args.fe2_ramp,
+                           "fallback_points": learned.stats["fallback"], "time_step": dt}
+    # plain FE^2 step at the end state: every Gauss point relaxes its RVE,
+    # first from zero fluctuations, then warm-started from the previous step
+    learned.surrogate = None
+    ms_cold, _ = timed(lambda: fe2.macro_step(m, args.fe2_ramp + 1, ramp_steps=args.fe2_ramp))
+    it_cold = learned.stats["iterations"]
+    ms_warm, _ = timed(lambda: fe2.macro_step(m, args.fe2_ramp + 2, ramp_steps=args.fe2_ramp))
+    out["plain_step"] = {"ms_cold_start": ms_cold, "ms_warm_start": ms_warm,
+                         "rve_solves_per_step": nq,
+                         "mean_iterations_cold": it_cold / nq,
+                         "mean_iterations_warm": (learned.stats["iterations"] - it_cold) / nq}
+    out["speedup_learned_vs_plain"] = {"cold": ms_cold / learned_ms, "warm": ms_warm / learned_ms}
+    m.close()
+    if log:
+        log("fe2: learned %.3f ms/step, plain %.1f / %.1f ms" % (learned_ms, ms_cold, ms_warm))
+    # macro displacement error: learned vs plain FE^2 over the whole ramp on a
+    # coarser block (a plain run of the full block is 200 x the plain step)
+    us = {}
+    for name, sur in (("plain", None), ("learned", net)):
+        prov = fe2.MaterialFE2(rve, surrogate=sur)
+        mm = fe2.macro_block(prov.material(mats, frac), cells=args.fe2_check_cells)
+        mm.setTimeStep(0.8 * mm.getStableTimeStep())
+        ms, _ = timed(lambda: [fe2.macro_step(mm, s, ramp_steps=args.fe2_ramp)
+                               for s in range(1, args.fe2_ramp + 1)])
+        us[name] = (mm.getDisplacement().copy(), ms)
+        mm.close()
+    (up, msp), (ul, msl) = us["plain"], us["learned"]
+    out["displacement_check"] = {
+        "cells": args.fe2_check_cells, "steps": args.fe2_ramp,
+        "rel_err_displacement": float(np.abs(ul - up).max() / np.abs(up).max()),
+        "plain_run_s": msp / 1e3, "learned_run_s": msl / 1e3}
+    out["learned_full_run_max_ux"] = float(np.abs(u_learned[:, 0]).max())
+    return out
+
+
 def SolidMechanicsModel_for(w, i, device, opts):
     from akantu_b200.model import SolidMechanicsModel, material_from_dict
     m = SolidMechanicsModel(w["meshes"][i], [material_from_dict(w["materials"][i])],
@@ -482,6 +578,11 @@ def main():
     ap.add_argument("--hex-steps", type=int, default=0, help="0 = the workload's 2000 steps")
     ap.add_argument("--batch-instances", type=int, default=4096)
     ap.add_argument("--batch-steps", type=int, default=0, help="0 = the workload's 500 steps")
+    ap.add_argument("--fe2-cells", type=int, default=32)
+    ap.add_argument("--fe2-ramp", type=int, default=200)
+    ap.add_argument("--fe2-heldout", type=int, default=4096)
+    ap.add_argument("--fe2-check-cells", type=int, default=8)
+    ap.add_argument("--no-fe2", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -510,6 +611,9 @@ def main():
                 "plates_batch": run_batch(args, dist.local_rank,
                                           log=lambda s: print(s, file=sys.stderr, flush=True)),
             }
+            if not args.no_fe2:
+                res["workloads"]["fe2"] = run_fe2(
+                    args, dist.local_rank, log=lambda s: print(s, file=sys.stderr, flush=True))
         if dist.rank == 0:
             print(json.dumps(res), flush=True)
     finally:

@@ -52,7 +52,7 @@ def test_dataset_and_surrogate_error_metrics():
     import torch
     from akantu_b200.surrogate import MLPSurrogate
     rve, mats, vf = small_rve()
-    X, Y, it = fe2.generate_dataset(rve, 600, seed=5, chunk=256)
+    X, Y, it, res = fe2.generate_dataset(rve, 600, seed=5, chunk=256)
     assert X.shape == (600, 9) and Y.shape == (600, 9)
     H = fe2.sample_gradients(600, seed=5)
     assert np.allclose(X[:, [0, 4, 8]].cpu().numpy(), H[:, [0, 1, 2], [0, 1, 2]])
