@@ -122,9 +122,13 @@ __device__ inline RveSmem<S> carve(unsigned char* smem, int nn) {
 }
 
 // First Piola-Kirchhoff stress of a voxel point (row-major, g = grad u):
-// neo-Hookean P = mu F + (lambda ln J - mu) F^-T with F^-T = cof(F) / J (the
-// reference's F S, S = mu (I - C^-1) + lambda ln J C^-1, since F C^-1 =
-// F^-T), or small-strain elastic sigma.
+// neo-Hookean P = mu (F - F^-T) + lambda ln J F^-T (the reference's F S with
+// S = mu (I - C^-1) + lambda ln J C^-1, since F C^-1 = F^-T), written without
+// O(1) terms that cancel at small strain: with t = tr g, I2 = (t^2 - tr g^2)/2,
+//   J - 1 = t + I2 + det g,  adj(F) = (1 + t + I2) I - (1 + t) g + g^2,
+//   F - F^-T = g + (det(g) I + (1 + t) g^T - (g^T)^2) / J,  F^-T = adj(F)^T / J,
+//   ln J = log1p(J - 1);
+// or small-strain elastic sigma.
 template <typename S>
 __device__ inline void voxel_stress(const MatParams& mp, const S* g, S* P) {
   const S lam = S(mp.lambda), mu = S(mp.mu);
@@ -136,23 +140,28 @@ __device__ inline void voxel_stress(const MatParams& mp, const S* g, S* P) {
       for (int j = 0; j < 3; ++j) P[i * 3 + j] = mu * (g[i * 3 + j] + g[j * 3 + i]) + (i == j ? lam * tr : S(0));
     return;
   }
-  S F[9];
+  S gg[9];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) F[k] = g[k] + (k % 4 == 0 ? S(1) : S(0));
-  S c[9];  // cofactors: c[i*3+j] = dJ/dF_ij
-  c[0] = F[4] * F[8] - F[5] * F[7];
-  c[1] = F[5] * F[6] - F[3] * F[8];
-  c[2] = F[3] * F[7] - F[4] * F[6];
-  c[3] = F[2] * F[7] - F[1] * F[8];
-  c[4] = F[0] * F[8] - F[2] * F[6];
-  c[5] = F[1] * F[6] - F[0] * F[7];
-  c[6] = F[1] * F[5] - F[2] * F[4];
-  c[7] = F[2] * F[3] - F[0] * F[5];
-  c[8] = F[0] * F[4] - F[1] * F[3];
-  const S J = F[0] * c[0] + F[1] * c[1] + F[2] * c[2];
-  const S k = (lam * log(J) - mu) / J;
+  for (int i = 0; i < 3; ++i)
 #pragma unroll
-  for (int q = 0; q < 9; ++q) P[q] = mu * F[q] + k * c[q];
+    for (int j = 0; j < 3; ++j)
+      gg[i * 3 + j] = g[i * 3] * g[j] + g[i * 3 + 1] * g[3 + j] + g[i * 3 + 2] * g[6 + j];
+  const S t = g[0] + g[4] + g[8];
+  const S I2 = S(0.5) * (t * t - (gg[0] + gg[4] + gg[8]));
+  const S dg = g[0] * (g[4] * g[8] - g[5] * g[7]) - g[1] * (g[3] * g[8] - g[5] * g[6]) +
+               g[2] * (g[3] * g[7] - g[4] * g[6]);
+  const S jm1 = t + I2 + dg;
+  const S iJ = S(1) / (S(1) + jm1);
+  const S a = mu * iJ, b = lam * log1p(jm1) * iJ, c = S(1) + t;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const S gt = g[j * 3 + i], ggt = gg[j * 3 + i];
+      const S adjT = (i == j ? c + I2 : S(0)) - c * gt + ggt;
+      const S dev = (i == j ? dg : S(0)) + c * gt - ggt;
+      P[i * 3 + j] = mu * g[i * 3 + j] + a * dev + b * adjT;
+    }
 }
 
 // f -= element forces of every voxel (8 colours); PSUM also adds

@@ -53,6 +53,17 @@ def sample_gradients(count, seed=SEED, amplitude=0.3, min_det=0.5):
     return out[:count].copy()
 
 
+def sample_small_gradients(count, seed=SEED, r_min=1e-4, r_max=0.3):
+    """Gradients of log-uniform magnitude |H| in [r_min, r_max] (Frobenius)
+    and uniformly distributed direction: the small strains a macro model
+    passes through, which the uniform envelope sampling almost never draws."""
+    rng = np.random.default_rng(seed)
+    D = rng.normal(size=(count, 3, 3))
+    D /= np.linalg.norm(D.reshape(count, 9), axis=1)[:, None, None]
+    r = np.exp(rng.uniform(np.log(r_min), np.log(r_max), count))
+    return D * r[:, None, None]
+
+
 def in_envelope(H, amplitude=0.3, min_det=0.5):
     """The training envelope of the surrogate: |H_ij| <= a and det F >= d."""
     H = np.asarray(H).reshape(-1, 3, 3)
@@ -83,13 +94,15 @@ def spec_rve(cells=16, precision=None, **options):
     return SolidMechanicsModelRVE(cells, vm, mats, **kw), mats, vf
 
 
-def generate_dataset(rve, count, seed=SEED, chunk=32768, amplitude=0.3, min_det=0.5):
-    """count samples (H, P) with H drawn in the envelope and P the relaxed
-    RVE's homogenised stress. Returns device FP64 features X, Y (count, 9)
-    (column-major flattening), the iteration counts and the final relative
-    residuals."""
+def generate_dataset(rve, count, seed=SEED, chunk=32768, amplitude=0.3, min_det=0.5,
+                     small=False):
+    """count samples (H, P) with H drawn in the envelope (or, small=True,
+    with log-uniform magnitude) and P the relaxed RVE's homogenised stress.
+    Returns device FP64 X, Y (count, 9) (column-major flattening), the
+    iteration counts and the final relative residuals."""
     import torch
-    H = sample_gradients(count, seed=seed, amplitude=amplitude, min_det=min_det)
+    H = (sample_small_gradients(count, seed=seed) if small else
+         sample_gradients(count, seed=seed, amplitude=amplitude, min_det=min_det))
     X, Y, its, res = [], [], [], []
     for k in range(0, count, chunk):
         Hc = torch.as_tensor(H[k:k + chunk], device="cuda:%d" % rve.device)
@@ -103,11 +116,11 @@ def generate_dataset(rve, count, seed=SEED, chunk=32768, amplitude=0.3, min_det=
 
 
 def surrogate_error(net, X, Y):
-    """Relative stress errors of the surrogate on (X, Y) features: the global
-    relative L2 error, the median and the 99th percentile of the per-sample
-    relative error ||P_net - P|| / ||P||."""
+    """Relative stress errors of the surrogate on (H, P) column-major
+    samples: the global relative L2 error, the median and the 99th
+    percentile of the per-sample relative error ||P_net - P|| / ||P||."""
     import torch
-    P = net.forward_features(X)
+    P = net.predict_flat(X)
     d = torch.linalg.norm(P - Y, dim=1)
     r = torch.linalg.norm(Y, dim=1)
     per = (d / r.clamp_min(1e-30)).cpu().numpy()

@@ -1,12 +1,18 @@
 """The learned RVE surrogate (include/akb_fe2.h: akb_mlp_*).
 
-MLPSurrogate maps a macroscopic displacement gradient H (9 values) to the
-homogenised first Piola-Kirchhoff stress (9 values) with a 9-256-256-256-9
-SiLU perceptron whose GEMMs run on the tensor cores (tcgen05, BF16 operands,
-FP32 accumulation). Training, gradients and inference all run in libakb.so;
-torch only holds the device arrays. Tensors are (nb, 3, 3) with
-[b, i, j] = du_i/dX_j (inputs) or P_ij (outputs); the network's features are
-their column-major flattening, the library's layout of grad_u and stress.
+MLPSurrogate maps a macroscopic displacement gradient H to the homogenised
+first Piola-Kirchhoff stress P with a SiLU perceptron (3 hidden layers of
+256) whose GEMMs run on the tensor cores (tcgen05, BF16 operands, FP32
+accumulation). Training, gradients and inference all run in libakb.so; torch
+only holds the device arrays. Tensors are (nb, 3, 3) with [b, i, j] =
+du_i/dX_j (inputs) or P_ij (outputs); features are their column-major
+flattening, the library's layout of grad_u and stress.
+
+Features: with r = |H| (Frobenius), the network reads (H / r, log r) (10
+inputs) and predicts P / r (9 outputs), so P = r net(H / r, log r). P is
+homogeneous of degree 1 in H at small strain, so this keeps the relative
+error uniform from r = 1e-4 to the envelope's edge (a network on raw H has
+an absolute error floor that dominates small-strain stresses).
 """
 from __future__ import annotations
 
@@ -23,13 +29,25 @@ def _torch():
     return torch
 
 
+R_MIN = 1e-8
+
+
 def _flat(t, torch):
     """(nb, 3, 3) -> (nb, 9) column-major features, FP64, contiguous."""
     return t.reshape(-1, 3, 3).transpose(1, 2).reshape(-1, 9).to(torch.float64).contiguous()
 
 
+def scaled_features(h, p=None):
+    """(nb, 9) column-major H (and P) -> network inputs (nb, 10) = (H / r,
+    log r) and targets P / r, r = |H| clamped to R_MIN."""
+    import torch
+    r = torch.linalg.norm(h, dim=1, keepdim=True).clamp_min(R_MIN)
+    x = torch.cat([h / r, torch.log(r)], dim=1).contiguous()
+    return (x, None) if p is None else (x, (p / r).contiguous())
+
+
 class MLPSurrogate:
-    def __init__(self, nb_inputs=9, nb_outputs=9, width=256, nb_hidden=3, device=0, seed=0):
+    def __init__(self, nb_inputs=10, nb_outputs=9, width=256, nb_hidden=3, device=0, seed=0):
         self.shape = (nb_inputs, nb_outputs, width, nb_hidden)
         self.device = device
         h = C.c_void_p()
@@ -84,6 +102,10 @@ class MLPSurrogate:
         s = {k: np.ascontiguousarray(v, dtype=np.float32) for k, v in
              dict(in_shift=in_shift, in_scale=in_scale, out_shift=out_shift,
                   out_scale=out_scale).items()}
+        nin, nout = self.shape[0], self.shape[1]
+        if any(s[k].shape != (nin,) for k in ("in_shift", "in_scale")) or \
+                any(s[k].shape != (nout,) for k in ("out_shift", "out_scale")):
+            raise ValueError("scaling needs %d input and %d output entries" % (nin, nout))
         F = C.POINTER(C.c_float)
         check(lib().akb_mlp_set_scaling(self._h, *[s[k].ctypes.data_as(F) for k in
                                                    ("in_shift", "in_scale", "out_shift",
@@ -150,10 +172,19 @@ class MLPSurrogate:
                 log("epoch %d loss %.3e" % (ep, losses[-1]))
         return losses
 
-    # -- tensors (nb, 3, 3) -------------------------------------------------
+    # -- stresses ------------------------------------------------------------
+    def predict_flat(self, h, stream=None):
+        """(nb, 9) column-major H -> (nb, 9) column-major P."""
+        torch = _torch()
+        if self.shape[0] == 9:  # raw features
+            return self.forward_features(h, stream)
+        x, _ = scaled_features(h)
+        r = torch.linalg.norm(h, dim=1, keepdim=True)
+        return r * self.forward_features(x, stream)
+
     def __call__(self, grad_u, stream=None):
         torch = _torch()
-        y = self.forward_features(_flat(torch.as_tensor(grad_u), torch), stream)
+        y = self.predict_flat(_flat(torch.as_tensor(grad_u), torch), stream)
         return y.reshape(-1, 3, 3).transpose(1, 2)
 
     def save(self, path):

@@ -57,10 +57,19 @@ def test_dataset_and_surrogate_error_metrics():
     H = fe2.sample_gradients(600, seed=5)
     assert np.allclose(X[:, [0, 4, 8]].cpu().numpy(), H[:, [0, 1, 2], [0, 1, 2]])
     assert np.allclose(X[:, 1].cpu().numpy(), H[:, 1, 0])  # column-major features
+    from akantu_b200.surrogate import scaled_features
     net = MLPSurrogate()
-    net.fit_scaling(X.cpu().numpy(), Y.cpu().numpy())
+    x, y = scaled_features(X, Y)
+    assert x.shape == (600, 10) and y.shape == (600, 9)
+    r = torch.linalg.norm(X, dim=1)
+    assert torch.allclose(torch.exp(x[:, 9]), r) and torch.allclose(y * r[:, None], Y)
+    net.fit_scaling(x.cpu().numpy(), y.cpu().numpy())
     e = fe2.surrogate_error(net, X, Y)
     assert e["relative_l2"] > 0 and e["p99"] >= e["median"]
-    net.train(X, Y, epochs=30, batch=128, lr=2e-3)
+    net.train(x, y, epochs=30, batch=128, lr=2e-3)
     e2 = fe2.surrogate_error(net, X, Y)
     assert e2["relative_l2"] < e["relative_l2"]
+    # small-strain samples: log-uniform magnitudes
+    Hs = fe2.sample_small_gradients(1000, seed=2)
+    rs = np.linalg.norm(Hs.reshape(-1, 9), axis=1)
+    assert rs.min() >= 1e-4 * (1 - 1e-12) and rs.max() <= 0.3 * (1 + 1e-12)
