@@ -68,6 +68,17 @@ __host__ __device__ inline int corner_x(int a) { return ((a & 3) == 1 || (a & 3)
 __host__ __device__ inline int corner_y(int a) { return (a >> 1) & 1; }
 __host__ __device__ inline int corner_z(int a) { return a >> 2; }
 
+// Shared-memory position of node (or voxel) (x, y, z): grouped by parity
+// class (x, y, z mod 2), then (x/2, y/2, z/2) lexicographic. A voxel colour
+// reaches each of its corners in one parity class, and its threads' voxels
+// are consecutive in that class, so the gathers and scatters of a warp hit
+// consecutive words (no bank conflicts).
+__device__ inline int pidx(int x, int y, int z, int n) {
+  const int hn = n >> 1;
+  return ((x & 1) | ((y & 1) << 1) | ((z & 1) << 2)) * (hn * hn * hn) + (x >> 1) +
+         hn * ((y >> 1) + hn * (z >> 1));
+}
+
 __device__ inline double det3d(const double* m) {
   return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
          m[2] * (m[3] * m[7] - m[4] * m[6]);
@@ -189,8 +200,7 @@ __device__ void voxel_forces(const RveArgs& R, const RveSmem<S>& s, const S* hH,
                 z1 = ez + 1 == n ? 0 : ez + 1;
       int nd[8];
 #pragma unroll
-      for (int o = 0; o < 8; ++o)
-        nd[o] = ((o & 1) ? x1 : ex) + n * (((o & 2) ? y1 : ey) + n * ((o & 4) ? z1 : ez));
+      for (int o = 0; o < 8; ++o) nd[o] = pidx((o & 1) ? x1 : ex, (o & 2) ? y1 : ey, (o & 4) ? z1 : ez, n);
       S D[3][4][3];  // edge differences [direction][edge][component]
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
@@ -207,7 +217,7 @@ __device__ void voxel_forces(const RveArgs& R, const RveSmem<S>& s, const S* hH,
           D[2][e][i] = (uc[b0 + 2 * b1 + 4] - uc[b0 + 2 * b1]) + hH[i * 3 + 2];
         }
       }
-      const MatParams& mp = mats[s.mat[ex + n * (ey + n * ez)]];
+      const MatParams& mp = mats[s.mat[pidx(ex, ey, ez, n)]];
       S T[3][4][3];
 #pragma unroll
       for (int j = 0; j < 3; ++j)
@@ -284,8 +294,9 @@ __global__ void __launch_bounds__(kRveThreads, 1)
   // the constant tables
   const S* im_g = static_cast<const S*>(R.inv_mass);
   for (int k = tid; k < nn; k += bs) {
-    s.im[k] = im_g[k];
-    s.mat[k] = R.vmat[k];
+    const int q = pidx(k % R.n, (k / R.n) % R.n, k / (R.n * R.n), R.n);
+    s.im[q] = im_g[k];
+    s.mat[q] = R.vmat[k];
   }
   if (tid < 96) {  // edge weights W[q][direction][edge] (see voxel_forces)
     const int q = tid / 12, j = (tid / 4) % 3, e = tid % 4;
@@ -347,7 +358,8 @@ __global__ void __launch_bounds__(kRveThreads, 1)
   for (int attempt = 0;; ++attempt, tsf *= kRestartFactor) {
     for (int idx = tid; idx < 3 * nn; idx += bs) {
       const int node = idx / 3, i = idx - 3 * node;
-      s.u[i * nn + node] = fluct ? fluct[inst * 3 * nn + idx] : S(0);
+      const int q = pidx(node % R.n, (node / R.n) % R.n, node / (R.n * R.n), R.n);
+      s.u[i * nn + q] = fluct ? fluct[inst * 3 * nn + idx] : S(0);
       s.v[idx] = 0;
     }
     const double dtd = tsf * s.par[0];
@@ -414,8 +426,9 @@ __global__ void __launch_bounds__(kRveThreads, 1)
   }
   for (int idx = tid; idx < 3 * nn; idx += bs) {
     const int node = idx / 3, i = idx - 3 * node;
-    if (fluct && R.write_fluct) fluct[inst * 3 * nn + idx] = s.u[i * nn + node];
-    if (internal_force) internal_force[inst * 3 * nn + idx] = double(s.f[i * nn + node]);
+    const int q = pidx(node % R.n, (node / R.n) % R.n, node / (R.n * R.n), R.n);
+    if (fluct && R.write_fluct) fluct[inst * 3 * nn + idx] = s.u[i * nn + q];
+    if (internal_force) internal_force[inst * 3 * nn + idx] = double(s.f[i * nn + q]);
   }
 }
 
