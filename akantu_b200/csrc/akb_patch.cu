@@ -5,9 +5,10 @@
 //      u+ = u + dt v + dt^2/2 a, v* = v + dt a on free DOFs
 //      (NewmarkBeta::predictor, newmark-beta.cc:60-89);
 //   2. element forces in chunks of blockDim elements from shared memory
-//      (akb_fastmath.cuh), each chunk's vectors added to the node
-//      accumulators in ascending local element order through the patch CSR
-//      (the -1 scatter of dof_manager.cc:83-137, without atomics);
+//      (akb_fastmath.cuh), written to the chunk's corners sorted by node;
+//      one thread per node run adds the run (ascending local element order)
+//      to the node accumulators (the -1 scatter of dof_manager.cc:83-137,
+//      without atomics);
 //   3. nodes of this patch only: residual, lumped solve and corrector
 //      (non_linear_solver_lumped.cc:85-98, newmark-beta.cc:176-210), written
 //      back; nodes shared with other patches: FP64 partial force to its slot.
@@ -180,15 +181,16 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
     }
     __syncthreads();
     const int sb = segp[chunk], nrun = segp[chunk + 1] - sb;
-    for (int q = tid; q < nrun * d; q += kThreads) {
-      const int i = q / nrun, r = q - i * nrun;
+    for (int r = tid; r < nrun; r += kThreads) {  // one thread per run, all components
       const uint32_t w = segs[sb + r];
       const int j = (int)(w >> 16), end = (int)(w & 0xffff);
       const int beg = r == 0 ? 0 : (int)(segs[sb + r - 1] & 0xffff);
-      const S* src = contrib + i * CH;
-      double f = 0.0;
-      for (int k = beg; k < end; ++k) f += double(src[k]);
-      fs[i * LM + j] -= f;
+      double f[3] = {0.0, 0.0, 0.0};
+      for (int k = beg; k < end; ++k)
+#pragma unroll
+        for (int i = 0; i < d; ++i) f[i] += double(contrib[i * CH + k]);
+#pragma unroll
+      for (int i = 0; i < d; ++i) fs[i * LM + j] -= f[i];
     }
     __syncthreads();
   }

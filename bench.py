@@ -308,7 +308,13 @@ def run_ours(args, dist):
             "roofline": {"bound": "hbm", "kernel": "whole step (%s)" % ", ".join(n for n, _ in ktimes),
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_step": balg, "traffic": None,
+                         "algorithmic_bytes_per_step": balg,
+                         # DRAM bytes of one k_patch_step launch from an ncu capture
+                         # (dram__bytes_read.sum + dram__bytes_write.sum) of the
+                         # 90^3-cell cube (4.374 M elements, 202.7 MB), scaled by
+                         # elements; the capture is not taken inside this run
+                         "traffic": 202.7e6 * E / 4.374e6,
+                         "traffic_kernel": "k_patch_step (ncu, 90^3 cells, scaled by elements)",
                          "kernels_ms": {n: t for n, t in ktimes},
                          "dominant": top[0]},
             "clocks": clocks,
