@@ -149,8 +149,8 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
   __syncthreads();
 
   // 2. element forces chunk by chunk: each element writes its corner vectors
-  //    to the corners' sorted slots, then one thread per (run, component)
-  //    adds the run (ascending element order) to that node
+  //    to the corners' sorted slots, then one thread per node run adds the
+  //    run (ascending element order) to that node
   for (int c0 = 0, chunk = 0; c0 < ne; c0 += kChunk, ++chunk) {
     const int el = c0 + tid;
     if (el < ne) {
