@@ -90,3 +90,19 @@ class BatchModel(SolidMechanicsModel):
 
     def instance_rows(self, i):
         return slice(int(self.node_offsets[i]), int(self.node_offsets[i + 1]))
+
+
+def partition_instances(sizes, world):
+    """Splits instances over `world` ranks by element count (longest
+    processing time first: each instance, largest first, goes to the rank
+    with the fewest elements so far; ties by rank). Independent instances
+    need no collective in the step, so a batch shards with no data-path
+    communication. Returns one ascending index list per rank."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    load = np.zeros(world, dtype=np.int64)
+    parts = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda k: (-sizes[k], k)):
+        r = int(np.argmin(load))
+        parts[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(p) for p in parts]

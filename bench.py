@@ -119,9 +119,12 @@ class Dist:
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local_rank))
+            if os.environ.get("AKB_DIST_BACKEND", "nccl") == "gloo":  # CPU tests of the plumbing
+                dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+            else:
+                torch.cuda.set_device(self.local_rank)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                        device_id=torch.device("cuda", self.local_rank))
             self.pg = dist
 
     def barrier(self):
@@ -132,8 +135,18 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dev = "cpu" if self.pg.get_backend() == "gloo" else "cuda"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        if not self.pg:
+            return x
+        import torch
+        dev = "cpu" if self.pg.get_backend() == "gloo" else "cuda"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
         return float(t.item())
 
     def close(self):
@@ -530,6 +543,35 @@ def run_fe2(args, device, log=None):
     return out
 
 
+def run_batch_sharded(args, dist):
+    """The 4096-plate batch split over the ranks by element count (no
+    collective in the step; device time max over ranks). Every rank calls
+    this; rank 0 returns the result."""
+    from akantu_b200.batch import BatchModel, partition_instances
+    w = configs.plates_batch(args.batch_instances)
+    sizes = [m.getNbElement() for m in w["meshes"]]
+    mine = partition_instances(sizes, dist.world)[dist.rank]
+    ws = {k: ([w[k][i] for i in mine] if isinstance(w[k], list) else w[k]) for k in w}
+    steps = w["steps"] if args.batch_steps <= 0 else args.batch_steps
+    b = BatchModel(ws["meshes"], ws["materials"], precision=_abi.MODE_FP64,
+                   device=dist.local_rank, patch_elements=768, patch_nodes=480)
+    b.initFull()
+    configs.setup_batch(b, ws)
+    b.solveSteps(3)
+    configs.setup_batch(b, ws)
+    b.synchronize()
+    dist.barrier()
+    ms = dist.max(b.timeSolveSteps(steps))
+    dist.barrier()
+    b.close()
+    E = float(sum(sizes))
+    return {"workload": "%d triangle_3 plates over %d ranks (elements per rank balanced)"
+                        % (len(sizes), dist.world),
+            "elements": E, "steps": steps, "value": E * steps / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / steps, "scaling": "strong",
+            "elements_rank0": float(sum(sizes[i] for i in mine))}
+
+
 def SolidMechanicsModel_for(w, i, device, opts):
     from akantu_b200.model import SolidMechanicsModel, material_from_dict
     m = SolidMechanicsModel(w["meshes"][i], [material_from_dict(w["materials"][i])],
@@ -617,7 +659,11 @@ def main():
         res = run_ours(args, dist)
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
             res["cpu_baseline"] = cpu_baseline(configs.cube_tet4(args.cells))
-        if dist.rank == 0 and not args.only_headline:
+        if dist.world > 1 and not args.only_headline:
+            sharded = run_batch_sharded(args, dist)  # every rank takes part
+            if dist.rank == 0:
+                res["workloads"] = {"plates_batch_sharded": sharded}
+        elif dist.rank == 0 and not args.only_headline:
             peak, _ = load_peaks()
             res["workloads"] = {
                 "block_hex8": run_hex8(args, dist.local_rank, peak),
