@@ -20,11 +20,14 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../akb.h"
+#include "../akb_fe2.h"
 
 namespace akantu_b200 {
 
@@ -116,6 +119,23 @@ struct MaterialNeohookean {
   akb_material_desc desc;
 };
 
+// A material written outside the library: the Material::computeStress plugin
+// (material.hh:110). computeStress(grad_u, stress, nb_points, stream) gets
+// the model's device arrays of Gauss-point displacement gradients and
+// stresses (3 x 3 column-major per point, like the reference's Matrix) and
+// the CUDA stream the model runs on; it writes the Cauchy stress (small
+// strain) or the first Piola-Kirchhoff stress (finite). rho, E, nu give the
+// density and the wave speed of getStableTimeStep. All materials of a model
+// using it must be user materials.
+struct MaterialUser {
+  using Compute = std::function<void(const double* grad_u, double* stress, int64_t nb_points,
+                                     void* stream)>;
+  MaterialUser(Real rho, Real E, Real nu, Compute compute, bool finite = true)
+      : desc{AKB_MATERIAL_USER, 0, finite, 0, rho, E, nu}, computeStress(std::move(compute)) {}
+  akb_material_desc desc;
+  Compute computeStress;
+};
+
 namespace BC {
 namespace Dirichlet {
 // FixedValue (boundary_condition_functor.hh): blocks one component and sets it.
@@ -140,6 +160,10 @@ class SolidMechanicsModel {
   template <class M>
   void addMaterial(const M& m) {
     mats_.push_back(m.desc);
+  }
+  void addMaterial(const MaterialUser& m) {
+    mats_.push_back(m.desc);
+    user_ = m.computeStress;
   }
   void setMaterialIndex(const std::vector<uint32_t>& per_element) { element_material_ = per_element; }
 
@@ -171,10 +195,15 @@ class SolidMechanicsModel {
   }
   void solveStep() {
     sync_in();
+    if (user_) return userStep();
     check(akb_solve_step(h_));
   }
   void solveSteps(int64_t n) {
     sync_in();
+    if (user_) {
+      for (int64_t s = 0; s < n; ++s) userStep();
+      return;
+    }
     check(akb_solve_steps(h_, n));
   }
   void assembleMassLumped() { check(akb_assemble_mass_lumped(h_)); }
@@ -217,6 +246,20 @@ class SolidMechanicsModel {
   akb_model* handle() { return h_; }
 
  private:
+  // predictor + grad u, the user's computeStress, then forces and corrector
+  void userStep() {
+    check(akb_step_begin(h_));
+    void *gradu, *stress, *stream;
+    check(akb_field_device_pointer(h_, AKB_FIELD_GRAD_U, &gradu));
+    check(akb_field_device_pointer(h_, AKB_FIELD_STRESS, &stress));
+    check(akb_model_get_stream(h_, &stream));
+    akb_model_info info;
+    check(akb_model_get_info(h_, &info));
+    user_(static_cast<const double*>(gradu), static_cast<double*>(stress),
+          info.nb_elements * info.quadrature_points_per_element, stream);
+    check(akb_step_end(h_));
+  }
+
   Array<Real>& pull(int32_t field, Array<Real>& a, bool writable) {
     sync_in();
     check(akb_get_field(h_, field, a.storage(), (int64_t)a.size() * a.getNbComponent()));
@@ -244,6 +287,7 @@ class SolidMechanicsModel {
   Array<uint8_t> blocked_;
   bool blocked_out_ = false;
   std::vector<std::pair<int32_t, Array<Real>*>> out_;
+  MaterialUser::Compute user_;
 };
 
 }  // namespace akantu_b200

@@ -12,11 +12,11 @@ from tests.golden_cases import OracleAdapter
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 
 
-def build_program(tmp_path):
-    exe = str(tmp_path / "shim_plate")
+def build_program(tmp_path, name="shim_plate"):
+    exe = str(tmp_path / name)
     lib = os.path.join(ROOT, "akantu_b200")
     subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
-                    os.path.join(ROOT, "tests", "cpp", "shim_plate.cc"), "-o", exe,
+                    os.path.join(ROOT, "tests", "cpp", name + ".cc"), "-o", exe,
                     "-L", lib, "-lakb", "-Wl,-rpath," + lib], check=True)
     return exe
 
@@ -24,6 +24,19 @@ def build_program(tmp_path):
 def test_shim_compiles(tmp_path):
     """The shim header compiles and links against libakb.so (no GPU needed)."""
     build_program(tmp_path)
+    build_program(tmp_path, "shim_fe2")
+
+
+@pytest.mark.gpu
+def test_shim_fe2_user_material_with_rves(tmp_path):
+    """A user material backed by homogeneous RVE solves equals the built-in
+    neo-Hookean material, through the C++ shim."""
+    exe = build_program(tmp_path, "shim_fe2")
+    out = subprocess.run([exe, "40"], check=True, capture_output=True, text=True).stdout
+    v = np.array([[float(x) for x in ln.split()] for ln in out.strip().splitlines()])
+    a, b = v[:, 0], v[:, 1]
+    assert np.abs(a).max() > 0
+    assert np.abs(a - b).max() <= 1e-10 * np.abs(a).max()
 
 
 @pytest.mark.gpu
