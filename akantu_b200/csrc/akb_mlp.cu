@@ -21,8 +21,12 @@
 //   weight gradients (a CTA per range of tiles): dW_l = dZ_l^T H_{l-1},
 //            A = dZ_l and B = H_{l-1} both MN-major (samples are K);
 //   Adam on FP32 master weights, then the BF16 copies are repacked.
-// Each wait on an MMA completion is bounded: past the limit the kernel
-// raises the error flag, frees its tensor memory and returns.
+// Weights and activation tiles are staged by TMA bulk copies completing on an
+// mbarrier (no multicast); in the forward and backward passes the next
+// layer's weights are copied while the current layer's epilogue runs. Each
+// wait (copy or MMA completion) is bounded: past the limit the kernel raises
+// the error flag, waits (bounded) for what is still in flight, frees its
+// tensor memory and returns.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -114,6 +118,31 @@ __device__ inline bool mbar_wait(uint32_t a, uint32_t parity) {
   }
   return false;
 }
+// One-dimensional bulk copy global -> this CTA's shared memory (TMA engine,
+// no multicast), completing `bytes` of transaction on mbarrier `mbar`; the
+// issuing thread first arms the barrier with the expected byte count.
+__device__ inline void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(mbar),
+               "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+// Two bulk copies on one barrier (both byte counts armed at once).
+__device__ inline void bulk_load2(uint32_t d0, const void* s0, uint32_t b0, uint32_t d1,
+                                  const void* s1, uint32_t b1, uint32_t mbar) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(mbar),
+               "r"(b0 + b1)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d0),
+               "l"(s0), "r"(b0), "r"(mbar)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d1),
+               "l"(s1), "r"(b1), "r"(mbar)
+               : "memory");
+}
+
 __device__ inline void tmem_alloc(uint32_t holder, uint32_t cols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(holder), "r"(cols)
                : "memory");
@@ -180,11 +209,6 @@ __device__ inline void store8(unsigned char* tile, int r, int c, int cols, const
   *reinterpret_cast<uint4*>(tile + pk_off(r, c, cols)) = q;
 }
 
-__device__ inline void copy16(void* dst, const void* src, size_t bytes, int tid, int nt) {
-  const uint4* s = static_cast<const uint4*>(src);
-  uint4* d = static_cast<uint4*>(dst);
-  for (size_t k = tid; k < bytes / 16; k += nt) d[k] = s[k];
-}
 
 // Issues A (M x K) times B^T (N x K) into tmem_d, K in steps of 16, both
 // K-major packed tiles (A with K columns, B with K columns), then commits.
@@ -198,7 +222,7 @@ struct Shared {
   unsigned char* act;  // 128 x 256 packed BF16 (64 KB)
   unsigned char* wgt;  // 256 x 256 packed BF16 (128 KB)
   float* bias;         // 256
-  uint64_t* mbar;
+  uint64_t* mbar;      // [0] MMA completion, [1] weights landed
   uint32_t* tmem_holder;
 };
 
@@ -212,7 +236,7 @@ __device__ inline Shared carve(unsigned char* smem) {
   s.wgt = smem + kActBytes;
   s.bias = reinterpret_cast<float*>(smem + kActBytes + kWgtBytes);
   s.mbar = reinterpret_cast<uint64_t*>(smem + kActBytes + kWgtBytes + kMaxWidth * 4);
-  s.tmem_holder = reinterpret_cast<uint32_t*>(s.mbar + 1);
+  s.tmem_holder = reinterpret_cast<uint32_t*>(s.mbar + 2);
   return s;
 }
 
@@ -229,8 +253,13 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int tid = threadIdx.x, warp = tid >> 5;
   const int64_t tile = blockIdx.x;
   const int64_t row = tile * kTile + tid;
+  const uint32_t mb_mma = saddr(s.mbar), mb_w = saddr(s.mbar + 1);
   if (warp == 0) tmem_alloc(saddr(s.tmem_holder), 256);
-  if (tid == 0) mbar_init(saddr(s.mbar));
+  if (tid == 0) {
+    mbar_init(mb_mma);
+    mbar_init(mb_w);
+    bulk_load(saddr(s.wgt), net.W[0], (uint32_t)(net.N[0] * net.K[0] * 2), mb_w);
+  }
   // inputs, normalised, padded to 16 columns
   {
     float v[16];
@@ -253,23 +282,35 @@ __global__ void __launch_bounds__(kThreads, 1)
   fence_after();
   const uint32_t tmem = *s.tmem_holder;
   const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-  uint32_t phase = 0;
-  bool ok = true;
+  // the weights of layer l + 1 are copied (TMA bulk) while layer l's
+  // epilogue runs: the copy starts as soon as layer l's MMAs completed
+  uint32_t pm = 0, pw = 0;
+  bool ok = true, w_pending = true, m_pending = false;
   for (int l = 0; l < net.nl && ok; ++l) {
     const int K = net.K[l], N = net.N[l];
-    copy16(s.wgt, net.W[l], (size_t)N * K * 2, tid, kThreads);
     for (int c = tid; c < N; c += kThreads) s.bias[c] = net.b[l][c];
     fence_smem_async();
     __syncthreads();
+    ok = mbar_wait(mb_w, pw);
+    if (!ok) break;
+    pw ^= 1;
+    w_pending = false;
     if (tid == 0) {
       fence_after();
       gemm_kmajor(tmem, saddr(s.act), saddr(s.wgt), K, N);
-      mma_commit(saddr(s.mbar));
+      mma_commit(mb_mma);
     }
-    ok = mbar_wait(saddr(s.mbar), phase);
-    phase ^= 1;
-    fence_after();
+    m_pending = true;
+    ok = mbar_wait(mb_mma, pm);
     if (!ok) break;
+    pm ^= 1;
+    m_pending = false;
+    fence_after();
+    if (l + 1 < net.nl) {
+      if (tid == 0)
+        bulk_load(saddr(s.wgt), net.W[l + 1], (uint32_t)(net.N[l + 1] * net.K[l + 1] * 2), mb_w);
+      w_pending = true;
+    }
     const bool last = l == net.nl - 1;
     if (!last) {
       for (int c0 = 0; c0 < N; c0 += 32) {
@@ -304,8 +345,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     fence_before();
     __syncthreads();  // TMEM read and activations written before the next MMA
   }
-  if (!ok) {  // drain the MMA that did not complete in time before freeing TMEM
-    mbar_wait(saddr(s.mbar), phase ^ 1);
+  if (!ok) {  // drain the copy / MMA still in flight before leaving (bounded)
+    if (w_pending) mbar_wait(mb_w, pw);
+    if (m_pending) mbar_wait(mb_mma, pm);
     if (tid == 0) atomicExch(net.error, 1);
   }
   __syncthreads();
@@ -323,9 +365,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int tid = threadIdx.x, warp = tid >> 5;
   const int64_t tile = blockIdx.x;
   const int64_t row = tile * kTile + tid;
-  if (warp == 0) tmem_alloc(saddr(s.tmem_holder), 256);
-  if (tid == 0) mbar_init(saddr(s.mbar));
+  const uint32_t mb_mma = saddr(s.mbar), mb_w = saddr(s.mbar + 1);
   const int L = net.nl;
+  if (warp == 0) tmem_alloc(saddr(s.tmem_holder), 256);
+  if (tid == 0) {
+    mbar_init(mb_mma);
+    mbar_init(mb_w);
+    bulk_load(saddr(s.wgt), net.Wt[L - 1], (uint32_t)(net.N[L - 1] * net.K[L - 1] * 2), mb_w);
+  }
   {
     float d[16];
     float sq = 0.0f;
@@ -358,22 +405,32 @@ __global__ void __launch_bounds__(kThreads, 1)
   fence_after();
   const uint32_t tmem = *s.tmem_holder;
   const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-  uint32_t phase = 0;
-  bool ok = true;
+  uint32_t pm = 0, pw = 0;
+  bool ok = true, w_pending = true, m_pending = false;
   for (int l = L - 1; l >= 1 && ok; --l) {
     const int K = net.N[l], N = net.K[l];  // reduce over the layer's outputs
-    copy16(s.wgt, net.Wt[l], (size_t)N * K * 2, tid, kThreads);
     fence_smem_async();
     __syncthreads();
+    ok = mbar_wait(mb_w, pw);
+    if (!ok) break;
+    pw ^= 1;
+    w_pending = false;
     if (tid == 0) {
       fence_after();
       gemm_kmajor(tmem, saddr(s.act), saddr(s.wgt), K, N);
-      mma_commit(saddr(s.mbar));
+      mma_commit(mb_mma);
     }
-    ok = mbar_wait(saddr(s.mbar), phase);
-    phase ^= 1;
-    fence_after();
+    m_pending = true;
+    ok = mbar_wait(mb_mma, pm);
     if (!ok) break;
+    pm ^= 1;
+    m_pending = false;
+    fence_after();
+    if (l - 1 >= 1) {  // next layer's W^T, copied while this epilogue runs
+      if (tid == 0)
+        bulk_load(saddr(s.wgt), net.Wt[l - 1], (uint32_t)(net.N[l - 1] * net.K[l - 1] * 2), mb_w);
+      w_pending = true;
+    }
     unsigned char* g = bufs.dz[l - 1] + tile * (size_t)kTile * N * 2;
     for (int c0 = 0; c0 < N; c0 += 32) {
       float v[32];
@@ -390,9 +447,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     fence_before();
     __syncthreads();
   }
-  if (!ok) {  // drain the MMA that did not complete in time before freeing TMEM
-    mbar_wait(saddr(s.mbar), phase ^ 1);
-    if (tid == 0) atomicExch(net.error, 1);
+  if (!ok || w_pending) {  // drain what is still in flight before leaving (bounded)
+    if (w_pending) mbar_wait(mb_w, pw);
+    if (m_pending) mbar_wait(mb_mma, pm);
+    if (!ok && tid == 0) atomicExch(net.error, 1);
   }
   __syncthreads();
   if (warp == 0) tmem_free(tmem, 256);
@@ -408,10 +466,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   unsigned char* sa = smem;
   unsigned char* sb = smem + (size_t)kTile * kMaxWidth * 2;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sb + (size_t)kTile * kMaxWidth * 2);
-  uint32_t* holder = reinterpret_cast<uint32_t*>(mbar + 1);
+  uint32_t* holder = reinterpret_cast<uint32_t*>(mbar + 2);
+  const uint32_t mb_mma = saddr(mbar), mb_t = saddr(mbar + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
   if (warp == 0) tmem_alloc(saddr(holder), 512);
-  if (tid == 0) mbar_init(saddr(mbar));
+  if (tid == 0) {
+    mbar_init(mb_mma);
+    mbar_init(mb_t);
+  }
   fence_before();
   __syncthreads();
   fence_after();
@@ -420,13 +482,18 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int64_t t1 = t0 + tiles_per_cta < ntiles ? t0 + tiles_per_cta : ntiles;
   const int halves = ca / kTile;
   const uint32_t id = idesc(kTile, cb, true, true);
-  uint32_t phase = 0;
-  bool ok = true;
+  uint32_t pm = 0, pt = 0;
+  bool ok = true, t_pending = false, m_pending = false;
   for (int64_t t = t0; t < t1 && ok; ++t) {
-    copy16(sa, A + t * (size_t)kTile * ca * 2, (size_t)kTile * ca * 2, tid, kThreads);
-    copy16(sb, B + t * (size_t)kTile * cb * 2, (size_t)kTile * cb * 2, tid, kThreads);
-    fence_smem_async();
-    __syncthreads();
+    // both tiles by TMA bulk copies (the previous tile's MMAs have completed)
+    if (tid == 0)
+      bulk_load2(saddr(sa), A + t * (size_t)kTile * ca * 2, (uint32_t)(kTile * ca * 2), saddr(sb),
+                 B + t * (size_t)kTile * cb * 2, (uint32_t)(kTile * cb * 2), mb_t);
+    t_pending = true;
+    ok = mbar_wait(mb_t, pt);
+    if (!ok) break;
+    pt ^= 1;
+    t_pending = false;
     if (tid == 0) {
       fence_after();
       for (int h = 0; h < halves; ++h)
@@ -434,10 +501,13 @@ __global__ void __launch_bounds__(kThreads, 1)
           mma(tmem + h * cb,
               sdesc(saddr(sa) + h * (kTile / 8) * 128 + s * 2 * 16 * ca, 16 * ca, 128),
               sdesc(saddr(sb) + s * 2 * 16 * cb, 16 * cb, 128), id, (t > t0 || s > 0) ? 1u : 0u);
-      mma_commit(saddr(mbar));
+      mma_commit(mb_mma);
     }
-    ok = mbar_wait(saddr(mbar), phase);
-    phase ^= 1;
+    m_pending = true;
+    ok = mbar_wait(mb_mma, pm);
+    if (!ok) break;
+    pm ^= 1;
+    m_pending = false;
     fence_after();
     __syncthreads();  // shared tiles free for the next copy
   }
@@ -455,8 +525,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     float* out = part + (size_t)blockIdx.x * ca * cb;
     for (int k = tid; k < ca * cb; k += kThreads) out[k] = 0.0f;
   }
-  if (!ok) {
-    mbar_wait(saddr(mbar), phase ^ 1);
+  if (!ok) {  // drain what is still in flight before leaving (bounded)
+    if (t_pending) mbar_wait(mb_t, pt);
+    if (m_pending) mbar_wait(mb_mma, pm);
     if (tid == 0) atomicExch(error, 1);
   }
   fence_before();
@@ -557,7 +628,7 @@ cudaError_t set_smem(const void* fn, size_t bytes) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-constexpr size_t kWgradSmem = 2 * (size_t)kTile * kMaxWidth * 2 + 64;
+constexpr size_t kWgradSmem = 2 * (size_t)kTile * kMaxWidth * 2 + 64;  // tiles, 2 barriers, TMEM address
 
 akb_status repack(akb_mlp* m) {
   for (int l = 0; l < m->net.nl; ++l) {
