@@ -111,6 +111,35 @@ __device__ inline void stress_P(const MatParams& p, const S* g, S* P) {
       for (int j = 0; j < d; ++j) P[i * d + j] = mu * (g[i * d + j] + g[j * d + i]) + (i == j ? lam * tr : S(0));
     return;
   }
+  if (d == 3 && p.kind == AKB_MATERIAL_NEOHOOKEAN) {
+    // P = F S = mu (F - F^-T) + lambda ln J F^-T (F C^-1 = F^-T), written
+    // without O(1) terms that cancel near F = I: with t = tr g,
+    // I2 = (t^2 - tr g^2)/2, J - 1 = t + I2 + det g,
+    // adj(F) = (1 + t + I2) I - (1 + t) g + g^2, F^-T = adj(F)^T / J and
+    // F - F^-T = g + (det(g) I + (1 + t) g^T - (g^T)^2) / J.
+    S gg[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        gg[i * 3 + j] = g[i * 3] * g[j] + g[i * 3 + 1] * g[3 + j] + g[i * 3 + 2] * g[6 + j];
+    const S t = g[0] + g[4] + g[8];
+    const S I2 = S(0.5) * (t * t - (gg[0] + gg[4] + gg[8]));
+    const S dg = det<3, S>(g);
+    const S jm1 = t + I2 + dg;
+    const S iJ = S(1) / (S(1) + jm1);
+    const S a = mu * iJ, b = lam * log1p(jm1) * iJ, c = S(1) + t;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const S gt = g[j * 3 + i], ggt = gg[j * 3 + i];
+        const S adjT = (i == j ? c + I2 : S(0)) - c * gt + ggt;
+        const S dev = (i == j ? dg : S(0)) + c * gt - ggt;
+        P[i * 3 + j] = mu * g[i * 3 + j] + a * dev + b * adjT;
+      }
+    return;
+  }
   // Written in terms of grad u so that no O(1) quantity cancels near F = I
   // (in FP32, C - I computed as C minus the identity loses eps/strain):
   //   E2 = C - I = g + g^T + g^T g

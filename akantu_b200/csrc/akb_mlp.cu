@@ -43,7 +43,9 @@ constexpr int kTile = 128;      // samples per CTA (UMMA M)
 constexpr int kMaxWidth = 256;  // one TMEM accumulator of 256 FP32 columns
 constexpr int kIO = 16;         // padded input / output width
 constexpr int kMaxLayers = 6;   // linear layers
-constexpr int kThreads = 128;   // one thread per TMEM lane / sample row
+constexpr int kThreads = 128;   // weight-gradient kernel: one thread per TMEM lane
+constexpr int kFwdThreads = 256;  // forward / backward: two threads per sample row, each
+                                  // reading half of the accumulator columns
 constexpr uint32_t kWaitLimit = 1u << 20;
 
 struct Net {
@@ -187,9 +189,11 @@ __device__ inline void tmem_ld16(uint32_t taddr, float* v) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ inline float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU and its derivative (the result is rounded to BF16 anyway: fast
+// division; exp(-z) overflowing gives the limits 0 and 0)
+__device__ inline float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ inline float dsilu(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -245,14 +249,15 @@ __device__ inline Shared carve(unsigned char* smem) {
 // major), the pre-activations Z (z[l], [nb_pad][N] FP32) and the normalised
 // outputs (ynorm, [nb_pad][16] FP32); otherwise y: [nb][nout] FP64 outputs.
 template <bool TRAIN>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kFwdThreads, 1)
     k_forward(Net net, int64_t nb, const double* __restrict__ x, double* __restrict__ y,
               Bufs bufs) {
   extern __shared__ __align__(1024) unsigned char smem[];
   Shared s = carve(smem);
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int r = tid & (kTile - 1), half = tid >> 7;  // row in the tile, column half
   const int64_t tile = blockIdx.x;
-  const int64_t row = tile * kTile + tid;
+  const int64_t row = tile * kTile + r;
   const uint32_t mb_mma = saddr(s.mbar), mb_w = saddr(s.mbar + 1);
   if (warp == 0) tmem_alloc(saddr(s.tmem_holder), 256);
   if (tid == 0) {
@@ -260,35 +265,31 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(mb_w);
     bulk_load(saddr(s.wgt), net.W[0], (uint32_t)(net.N[0] * net.K[0] * 2), mb_w);
   }
-  // inputs, normalised, padded to 16 columns
+  // inputs, normalised, padded to 16 columns (8 per thread)
   {
-    float v[16];
+    float v[8];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
+    for (int q = 0; q < 8; ++q) {
+      const int j = 8 * half + q;
       float t = 0.0f;
       if (j < net.nin && row < nb) t = (float)((x[row * net.nin + j] - net.in_shift[j]) * net.in_scale[j]);
-      v[j] = t;
+      v[q] = t;
     }
-    store8(s.act, tid, 0, 16, v);
-    store8(s.act, tid, 8, 16, v + 8);
-    if (TRAIN) {
-      unsigned char* g = bufs.act[0] + tile * (size_t)kTile * 16 * 2;
-      store8(g, tid, 0, 16, v);
-      store8(g, tid, 8, 16, v + 8);
-    }
+    store8(s.act, r, 8 * half, 16, v);
+    if (TRAIN) store8(bufs.act[0] + tile * (size_t)kTile * 16 * 2, r, 8 * half, 16, v);
   }
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = *s.tmem_holder;
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
   // the weights of layer l + 1 are copied (TMA bulk) while layer l's
   // epilogue runs: the copy starts as soon as layer l's MMAs completed
   uint32_t pm = 0, pw = 0;
   bool ok = true, w_pending = true, m_pending = false;
   for (int l = 0; l < net.nl && ok; ++l) {
     const int K = net.K[l], N = net.N[l];
-    for (int c = tid; c < N; c += kThreads) s.bias[c] = net.b[l][c];
+    for (int c = tid; c < N; c += kFwdThreads) s.bias[c] = net.b[l][c];
     fence_smem_async();
     __syncthreads();
     ok = mbar_wait(mb_w, pw);
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     const bool last = l == net.nl - 1;
     if (!last) {
-      for (int c0 = 0; c0 < N; c0 += 32) {
+      for (int c0 = half * (N >> 1); c0 < (half + 1) * (N >> 1); c0 += 32) {
         float v[32];
         tmem_ld32(tmem + lane_base + c0, v);
 #pragma unroll
@@ -323,14 +324,14 @@ __global__ void __launch_bounds__(kThreads, 1)
           v[j] = silu(zz);
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) store8(s.act, tid, c0 + 8 * q, N, v + 8 * q);
+        for (int q = 0; q < 4; ++q) store8(s.act, r, c0 + 8 * q, N, v + 8 * q);
         if (TRAIN) {
           unsigned char* g = bufs.act[l + 1] + tile * (size_t)kTile * N * 2;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) store8(g, tid, c0 + 8 * q, N, v + 8 * q);
+          for (int q = 0; q < 4; ++q) store8(g, r, c0 + 8 * q, N, v + 8 * q);
         }
       }
-    } else {
+    } else if (half == 0) {  // warp-uniform: warps 0-3 read the 16 output columns
       float v[16];
       tmem_ld16(tmem + lane_base, v);
       if (row < nb) {
@@ -358,13 +359,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 // (loss = mean over samples and outputs of (y - t)^2), then
 // dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1}) down to the first hidden layer.
 // Stores packed BF16 dY (dz[nl-1]) and dZ (dz[l]) tiles and the tile's loss.
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kFwdThreads, 1)
     k_backward(Net net, int64_t nb, const double* __restrict__ target, Bufs bufs) {
   extern __shared__ __align__(1024) unsigned char smem[];
   Shared s = carve(smem);
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int r = tid & (kTile - 1), half = tid >> 7;  // row in the tile, column half
   const int64_t tile = blockIdx.x;
-  const int64_t row = tile * kTile + tid;
+  const int64_t row = tile * kTile + r;
   const uint32_t mb_mma = saddr(s.mbar), mb_w = saddr(s.mbar + 1);
   const int L = net.nl;
   if (warp == 0) tmem_alloc(saddr(s.tmem_holder), 256);
@@ -374,37 +376,39 @@ __global__ void __launch_bounds__(kThreads, 1)
     bulk_load(saddr(s.wgt), net.Wt[L - 1], (uint32_t)(net.N[L - 1] * net.K[L - 1] * 2), mb_w);
   }
   {
-    float d[16];
+    float d[8];  // 8 of the 16 (padded) outputs per thread
     float sq = 0.0f;
     const float scale = 2.0f / (float)((double)nb * net.nout);
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
+    for (int q = 0; q < 8; ++q) {
+      const int j = 8 * half + q;
       float e = 0.0f;
       if (row < nb && j < net.nout) {
         const float t = (float)((target[row * net.nout + j] - net.out_shift[j]) / net.out_scale[j]);
         e = bufs.ynorm[row * 16 + j] - t;
         sq += e * e;
       }
-      d[j] = scale * e;
+      d[q] = scale * e;
     }
-    store8(s.act, tid, 0, 16, d);
-    store8(s.act, tid, 8, 16, d + 8);
-    unsigned char* g = bufs.dz[L - 1] + tile * (size_t)kTile * 16 * 2;
-    store8(g, tid, 0, 16, d);
-    store8(g, tid, 8, 16, d + 8);
-    // tile loss: warp sums then warp 0
+    store8(s.act, r, 8 * half, 16, d);
+    store8(bufs.dz[L - 1] + tile * (size_t)kTile * 16 * 2, r, 8 * half, 16, d);
+    // tile loss: warp sums, then the 8 warps in order
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
     float* red = s.bias;
     if ((tid & 31) == 0) red[warp] = sq;
     __syncthreads();
-    if (tid == 0) bufs.loss_tiles[tile] = red[0] + red[1] + red[2] + red[3];
+    if (tid == 0) {
+      float t = 0.0f;
+      for (int w = 0; w < kFwdThreads / 32; ++w) t += red[w];
+      bufs.loss_tiles[tile] = t;
+    }
   }
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = *s.tmem_holder;
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
   uint32_t pm = 0, pw = 0;
   bool ok = true, w_pending = true, m_pending = false;
   for (int l = L - 1; l >= 1 && ok; --l) {
@@ -432,7 +436,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       w_pending = true;
     }
     unsigned char* g = bufs.dz[l - 1] + tile * (size_t)kTile * N * 2;
-    for (int c0 = 0; c0 < N; c0 += 32) {
+    for (int c0 = half * (N >> 1); c0 < (half + 1) * (N >> 1); c0 += 32) {
       float v[32];
       tmem_ld32(tmem + lane_base + c0, v);
 #pragma unroll
@@ -440,8 +444,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         v[j] = row < nb ? v[j] * dsilu(bufs.z[l - 1][row * N + c0 + j]) : 0.0f;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        store8(s.act, tid, c0 + 8 * q, N, v + 8 * q);
-        store8(g, tid, c0 + 8 * q, N, v + 8 * q);
+        store8(s.act, r, c0 + 8 * q, N, v + 8 * q);
+        store8(g, r, c0 + 8 * q, N, v + 8 * q);
       }
     }
     fence_before();
@@ -672,9 +676,9 @@ akb_status gradients(akb_mlp* m, int64_t nb, const double* x, const double* targ
   if ((st = ensure_workspace(m, ntiles)) != AKB_OK) return st;
   const Net& n = m->net;
   AKB_CUDA_TRY(cudaMemsetAsync(m->d_error, 0, sizeof(int), m->stream));
-  k_forward<true><<<(unsigned)ntiles, kThreads, kFwdSmem, m->stream>>>(n, nb, x, nullptr, m->bufs);
+  k_forward<true><<<(unsigned)ntiles, kFwdThreads, kFwdSmem, m->stream>>>(n, nb, x, nullptr, m->bufs);
   AKB_CUDA_TRY(cudaGetLastError());
-  k_backward<<<(unsigned)ntiles, kThreads, kFwdSmem, m->stream>>>(n, nb, target, m->bufs);
+  k_backward<<<(unsigned)ntiles, kFwdThreads, kFwdSmem, m->stream>>>(n, nb, target, m->bufs);
   AKB_CUDA_TRY(cudaGetLastError());
   const int tpc = (int)std::max<int64_t>(1, (ntiles + 147) / 148);
   const int nparts = (int)((ntiles + tpc - 1) / tpc);
@@ -852,7 +856,7 @@ akb_status akb_mlp_forward(akb_mlp* m, int64_t nb, const double* x, double* y, v
   if (ntiles > INT32_MAX) return fail(AKB_ERR_UNSUPPORTED, "too many samples");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   cudaStream_t s = stream ? (cudaStream_t)stream : m->stream;
-  k_forward<false><<<(unsigned)ntiles, kThreads, kFwdSmem, s>>>(m->net, nb, x, y, Bufs{});
+  k_forward<false><<<(unsigned)ntiles, kFwdThreads, kFwdSmem, s>>>(m->net, nb, x, y, Bufs{});
   AKB_CUDA_TRY(cudaGetLastError());
   return AKB_OK;
 }

@@ -109,11 +109,13 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
           ++count[c[a]];
         }
     }
-  // shared nodes and their node-major partial slots
+  // shared nodes and their node-major partial slots; nodes of no element
+  // join them with no slot, so they get the reference's lumped solve with
+  // M = 0 (r / M not finite, solid_mechanics_model_mass.cc:79-95)
   std::vector<int64_t> sidx(nn, -1);
   P.sptr.push_back(0);
   for (int64_t i = 0; i < nn; ++i)
-    if (count[i] >= 2) {
+    if (count[i] >= 2 || count[i] == 0) {
       sidx[i] = (int64_t)P.snodes.size();
       P.snodes.push_back((uint32_t)i);
       P.sptr.push_back(P.sptr.back() + count[i]);

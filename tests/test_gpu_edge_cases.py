@@ -1,0 +1,67 @@
+"""Edge cases of the explicit path against the oracle: a node that belongs
+to no element (lumped mass 0: the reference's r / M is not finite,
+solid_mechanics_model_mass.cc:79-95), a mesh without elements, and a blocked
+node with zero mass (untouched, like every blocked DOF)."""
+import numpy as np
+import pytest
+
+from akantu_b200 import _abi, configs
+from akantu_b200.mesh import Mesh
+from tests.golden_cases import GpuAdapter, OracleAdapter
+
+pytestmark = pytest.mark.gpu
+
+
+def plate_with_orphan():
+    w = configs.plate_tri3(nx=10, ny=3, lx=1.0, ly=0.3)
+    m = w["mesh"]
+    nodes = np.vstack([m.nodes, [[2.0, 2.0]]])
+    mesh = Mesh(2, m.element_type, nodes, m.connectivity)
+    w["mesh"] = mesh
+    for k in ("blocked", "u0", "v0"):
+        w[k] = np.vstack([w[k], np.zeros((1, 2), dtype=w[k].dtype)])
+    w["v0"][-1] = [0.1, -0.2]
+    return w
+
+
+@pytest.mark.parametrize("mode", [_abi.MODE_FP64_REFERENCE, _abi.MODE_FP64, _abi.MODE_FP32_BULK])
+def test_orphan_node_follows_the_reference(mode):
+    w = plate_with_orphan()
+    cpu = OracleAdapter(w["mesh"], w["materials"])
+    dt = configs.setup_model(cpu, w)
+    cpu.solve_steps(20)
+    dev = GpuAdapter(w["mesh"], w["materials"], precision=mode)
+    configs.setup_model(dev, w)
+    dev.set_time_step(dt)
+    dev.solve_steps(20)
+    for f in (_abi.FIELD_DISPLACEMENT, _abi.FIELD_VELOCITY, _abi.FIELD_ACCELERATION):
+        a, b = dev.get(f), cpu.get(f)
+        # the orphan node: not finite in both
+        assert not np.isfinite(b[-1]).all()
+        assert np.array_equal(np.isfinite(a), np.isfinite(b))
+        tol = {0: 0.0, 1: 1e-10, 2: 2e-4}[mode]
+        ok = np.isfinite(b)
+        assert np.abs(a[ok] - b[ok]).max() <= tol * np.abs(b[ok]).max() + 1e-300
+
+
+def test_blocked_orphan_node_is_untouched():
+    w = plate_with_orphan()
+    w["blocked"][-1] = 1
+    dev = GpuAdapter(w["mesh"], w["materials"], precision=_abi.MODE_FP64)
+    configs.setup_model(dev, w)
+    dev.solve_steps(10)
+    assert np.array_equal(dev.get(_abi.FIELD_VELOCITY)[-1], w["v0"][-1])
+    assert np.isfinite(dev.get(_abi.FIELD_DISPLACEMENT)).all()
+
+
+def test_mesh_without_elements():
+    from akantu_b200.model import MaterialElastic, SolidMechanicsModel
+    mesh = Mesh(3, _abi.TETRAHEDRON_4, np.zeros((4, 3)), np.zeros((0, 4), np.uint32))
+    m = SolidMechanicsModel(mesh, [MaterialElastic(rho=1.0, E=1.0, nu=0.2)],
+                            precision=_abi.MODE_FP64)
+    m.initFull()
+    assert m.getInfo().nb_elements == 0
+    assert np.abs(m.getMass()).max() == 0.0
+    m.setTimeStep(1e-3)
+    m.solveSteps(3)
+    m.close()
