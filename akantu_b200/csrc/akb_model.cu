@@ -255,16 +255,40 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
   if ((st = upload(m, P.node_ptr, &d.node_ptr)) != AKB_OK) return st;
   if ((st = upload(m, P.ninterior, &d.ninterior)) != AKB_OK) return st;
   if ((st = upload(m, P.lnodes, &d.lnodes)) != AKB_OK) return st;
-  if ((st = upload(m, P.lconn, &d.lconn)) != AKB_OK) return st;
-  d.cbeg = nullptr;
-  d.centries = nullptr;
-  if ((st = upload(m, P.cslot, &d.cslot)) != AKB_OK) return st;
-  if ((st = upload(m, P.segs, &d.segs)) != AKB_OK) return st;
   if ((st = upload(m, P.seg_ptr, &d.seg_ptr)) != AKB_OK) return st;
   if ((st = upload(m, P.chunk_base, &d.chunk_base)) != AKB_OK) return st;
   if ((st = upload(m, P.slot, &d.slot)) != AKB_OK) return st;
   if ((st = upload(m, P.snodes, &d.snodes)) != AKB_OK) return st;
   if ((st = upload(m, P.sptr, &d.sptr)) != AKB_OK) return st;
+  {  // per-patch copies padded to 16 bytes: sources of the TMA bulk staging
+    std::vector<uint16_t> lcp, csp;
+    std::vector<uint32_t> sgp, lco(P.npatch), sgo(P.npatch);
+    const int n_ = m->dm.nnpe;
+    for (int p = 0; p < P.npatch; ++p) {
+      const int64_t eb = P.elem_ptr[p], ne = P.elem_ptr[p + 1] - eb;
+      lco[p] = (uint32_t)lcp.size();
+      lcp.insert(lcp.end(), P.lconn.begin() + eb * n_, P.lconn.begin() + (eb + ne) * n_);
+      csp.insert(csp.end(), P.cslot.begin() + eb * n_, P.cslot.begin() + (eb + ne) * n_);
+      while (lcp.size() % 8) {
+        lcp.push_back(0);
+        csp.push_back(0);
+      }
+      const int64_t nch = (ne + 255) / 256, c0 = P.chunk_base[p];
+      const int64_t s0 = P.seg_ptr[c0], s1 = P.seg_ptr[c0 + nch];
+      sgo[p] = (uint32_t)sgp.size();
+      sgp.insert(sgp.end(), P.segs.begin() + s0, P.segs.begin() + s1);
+      while (sgp.size() % 4) sgp.push_back(0);
+    }
+    if ((st = upload(m, lcp, &d.lconn_pad)) != AKB_OK) return st;
+    if ((st = upload(m, csp, &d.cslot_pad)) != AKB_OK) return st;
+    if ((st = upload(m, sgp, &d.segs_pad)) != AKB_OK) return st;
+    if ((st = upload(m, lco, &d.lc_off)) != AKB_OK) return st;
+    if ((st = upload(m, sgo, &d.sg_off)) != AKB_OK) return st;
+    int* e;
+    if ((st = dalloc(m, &e, 1)) != AKB_OK) return st;
+    AKB_CUDA_TRY(cudaMemsetAsync(e, 0, sizeof(int), m->stream));
+    d.err = e;
+  }
   d.emat = nullptr;
   if (element_material) {
     std::vector<uint32_t> em(P.elem_order.size());
@@ -325,6 +349,15 @@ akb_status check_model(const akb_model* m) {
 akb_status sync(akb_model* m) {
   cudaError_t e = cudaStreamSynchronize(m->stream);
   if (e != cudaSuccess) return fail(AKB_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+  if (m->use_patches && m->patches.err) {  // a bounded wait of the fused step gave up
+    int flag = 0;
+    e = cudaMemcpy(&flag, m->patches.err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(AKB_ERR_CUDA, std::string("flag: ") + cudaGetErrorString(e));
+    if (flag) {
+      cudaMemset(m->patches.err, 0, sizeof(int));
+      return fail(AKB_ERR_TIMEOUT, "fused step: staging copy did not complete in time");
+    }
+  }
   return AKB_OK;
 }
 

@@ -1,7 +1,9 @@
 // akb_patch.cu -- the fused explicit step (AKB_MODE_FP64, AKB_MODE_FP32_BULK).
 //
 // k_patch_step: one CTA per patch.
-//   1. stage the patch's nodes: X, u, v, a, blocked flags; predictor
+//   1. stage the patch: its local connectivity, sorted slots and runs by TMA
+//      bulk copies completing on an mbarrier, while the threads gather the
+//      nodes' X, u, v, a and blocked flags and apply the predictor
 //      u+ = u + dt v + dt^2/2 a, v* = v + dt a on free DOFs
 //      (NewmarkBeta::predictor, newmark-beta.cc:60-89);
 //   2. element forces in chunks of blockDim elements from shared memory
@@ -10,8 +12,12 @@
 //      to the node accumulators (the -1 scatter of dof_manager.cc:83-137,
 //      without atomics);
 //   3. nodes of this patch only: residual, lumped solve and corrector
-//      (non_linear_solver_lumped.cc:85-98, newmark-beta.cc:176-210), written
-//      back; nodes shared with other patches: FP64 partial force to its slot.
+//      (non_linear_solver_lumped.cc:85-98, newmark-beta.cc:176-210) on u+
+//      kept in shared memory and v, a re-read, written back; nodes shared
+//      with other patches: FP64 partial force to its slot.
+// The wait on the staging copies is bounded: past it the CTA flags the
+// error (P.err, read by the host on its next synchronisation), waits again
+// (bounded) for its copies and skips the patch.
 // k_shared_nodes: one thread per shared node adds its partials in patch order
 // and applies the same predictor/corrector arithmetic.
 #include <mutex>
@@ -25,7 +31,7 @@ namespace {
 constexpr int kThreads = 256;
 
 struct SmemLayout {
-  size_t xs, us, fs, contrib, lcs, slots, segs, segp, flags, total;
+  size_t xs, us, fs, contrib, lcs, slots, segs, segp, flags, mbar, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -48,22 +54,9 @@ __host__ __device__ inline SmemLayout layout(int L, int E, int R, int d, int n, 
   s.segs = align16(s.slots + (size_t)E * n * sizeof(uint16_t));
   s.segp = align16(s.segs + (size_t)R * sizeof(uint32_t));
   s.flags = align16(s.segp + (size_t)kMaxChunks * sizeof(int32_t));
-  s.total = align16(s.flags + (size_t)L * d);
+  s.mbar = align16(s.flags + (size_t)L * d);
+  s.total = s.mbar + 16;
   return s;
-}
-
-// Copies count uint16 from global to shared memory, 4 bytes at a time when
-// the source allows it.
-__device__ inline void copy_u16(uint16_t* dst, const uint16_t* src, int count, int tid, int nt) {
-  if ((reinterpret_cast<uintptr_t>(src) & 3) == 0) {
-    const int pairs = count >> 1;
-    const uint32_t* s4 = reinterpret_cast<const uint32_t*>(src);
-    uint32_t* d4 = reinterpret_cast<uint32_t*>(dst);
-    for (int k = tid; k < pairs; k += nt) d4[k] = s4[k];
-    if ((count & 1) && tid == 0) dst[count - 1] = src[count - 1];
-  } else {
-    for (int k = tid; k < count; k += nt) dst[k] = src[k];
-  }
 }
 
 // CTAs per SM each instantiation is built for (register budget).
@@ -74,11 +67,32 @@ template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, double> { static constexpr i
 // (node, component) items handled per thread per round of the staging and
 // finishing loops: their global loads are issued together.
 constexpr int kBatch = 4;
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+__device__ inline uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ inline void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+__device__ inline bool mbar_wait(uint32_t a, uint32_t parity) {
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
 
 // One patch p, by the whole CTA.
 template <int T, typename S, bool FEXT>
 __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& P, double dt0,
-                                           int p, unsigned char* smem) {
+                                           int p, unsigned char* smem, uint32_t parity) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
   constexpr int CH = kChunk * n;  // sorted slots of one chunk
   static_assert(kChunk == kThreads, "one element per thread per chunk");
@@ -103,16 +117,24 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
   const int tid = threadIdx.x;
   const int items = L * d;
 
-  // 1. stage the patch: local connectivity, sorted slots, runs; per (node,
-  //    component) X, predicted u, blocked flag
-  copy_u16(lcs, P.lconn + (size_t)eb * n, ne * n, tid, kThreads);
-  copy_u16(slots, P.cslot + (size_t)eb * n, ne * n, tid, kThreads);
+  // 1. stage the patch: local connectivity, sorted slots and runs by TMA
+  //    bulk copies (one thread, completing on an mbarrier) while the CTA
+  //    gathers per (node, component) X, predicted u, blocked flag
+  const uint32_t mb = saddr(smem + lay.mbar);
   {
     const int32_t* gp = P.seg_ptr + P.chunk_base[p];
     const int s0 = gp[0];
     if (tid <= nchunks) segp[tid] = gp[tid] - s0;
-    const int nseg = gp[nchunks] - s0;
-    for (int k = tid; k < nseg; k += kThreads) segs[k] = P.segs[s0 + k];
+    if (tid == 0) {
+      const uint32_t blc = ((uint32_t)(ne * n * 2) + 15u) & ~15u;
+      const uint32_t bsg = ((uint32_t)((gp[nchunks] - s0) * 4) + 15u) & ~15u;
+      asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
+                   "r"(2 * blc + bsg)
+                   : "memory");
+      bulk_copy(saddr(lcs), P.lconn_pad + P.lc_off[p], blc, mb);
+      bulk_copy(saddr(slots), P.cslot_pad + P.lc_off[p], blc, mb);
+      if (bsg) bulk_copy(saddr(segs), P.segs_pad + P.sg_off[p], bsg, mb);
+    }
   }
   for (int base = 0; base < items; base += kThreads * kBatch) {
     int64_t idx[kBatch];
@@ -147,6 +169,11 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
     }
   }
   __syncthreads();
+  if (!mbar_wait(mb, parity)) {  // bounded: flag, drain, skip the patch
+    if (tid == 0) atomicExch(P.err, 1);
+    mbar_wait(mb, parity);
+    return;
+  }
 
   // 2. element forces chunk by chunk: each element writes its corner vectors
   //    to the corners' sorted slots, then one thread per node run adds the
@@ -199,7 +226,7 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
   //    bit for bit), hand out the shared ones
   for (int base = 0; base < items; base += kThreads * kBatch) {
     int64_t idx[kBatch];
-    double u[kBatch], v[kBatch], a[kBatch], im[kBatch], fx[kBatch];
+    double v[kBatch], a[kBatch], im[kBatch], fx[kBatch];
 #pragma unroll
     for (int b = 0; b < kBatch; ++b) {
       const int k = base + b * kThreads + tid;
@@ -214,7 +241,6 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
 #pragma unroll
     for (int b = 0; b < kBatch; ++b)
       if (idx[b] >= 0) {
-        u[b] = m.u[idx[b]];
         v[b] = m.v[idx[b]];
         a[b] = m.a[idx[b]];
         fx[b] = FEXT ? m.fext[idx[b]] : 0.0;
@@ -228,8 +254,8 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
       if (j >= nint) {
         P.partial[(int64_t)P.slot[nb + j] * d + i] = f;
       } else if (idx[b] >= 0) {  // blocked DOFs keep u, v, a
-        double uu = u[b], vv = v[b], aa = a[b];
-        fast::predict(dt, uu, vv, aa);
+        // u+ from the staging, v* recomputed bit for bit
+        double uu = us[i * LM + j], vv = __dadd_rn(v[b], __dmul_rn(dt, a[b])), aa = a[b];
         fast::correct(dt, FEXT ? f + fx[b] : f, im[b], uu, vv, aa);
         m.u[idx[b]] = uu;
         m.v[idx[b]] = vv;
@@ -246,13 +272,23 @@ template <int T, typename S, bool FEXT, bool PERSIST>
 __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
     k_patch_step(DevModel m, DevPatches P, double dt0) {
   extern __shared__ __align__(16) unsigned char smem[];
+  {
+    const SmemLayout lay = layout(P.max_nodes, P.max_elems, P.max_segs, ET<T>::dim, ET<T>::nnpe,
+                                  sizeof(S), kThreads);
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(smem + lay.mbar)) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+  }
   if constexpr (PERSIST) {
-    for (int p = blockIdx.x; p < P.npatch; p += gridDim.x) {
+    uint32_t parity = 0;
+    for (int p = blockIdx.x; p < P.npatch; p += gridDim.x, parity ^= 1) {
       if (p != (int)blockIdx.x) __syncthreads();  // shared memory of the previous patch is free
-      patch_body<T, S, FEXT>(m, P, dt0, p, smem);
+      patch_body<T, S, FEXT>(m, P, dt0, p, smem, parity);
     }
   } else {
-    patch_body<T, S, FEXT>(m, P, dt0, blockIdx.x, smem);
+    patch_body<T, S, FEXT>(m, P, dt0, blockIdx.x, smem, 0);
   }
 }
 

@@ -63,17 +63,20 @@ struct DevPatches {
   const int32_t* node_ptr;
   const int32_t* ninterior;
   const uint32_t* lnodes;
-  const uint16_t* lconn;
-  const uint16_t* cbeg;
-  const uint16_t* centries;
-  const uint16_t* cslot;
-  const uint32_t* segs;
   const int32_t* seg_ptr;
   const int32_t* chunk_base;
   const uint32_t* slot;
   const uint32_t* snodes;
   const int32_t* sptr;
   const uint32_t* emat;  // material of each patch-ordered element, or null
+  // per-patch local connectivity, sorted corner slots and runs, each patch's
+  // slice padded to 16 bytes: the sources of the TMA bulk staging
+  const uint16_t* lconn_pad;
+  const uint16_t* cslot_pad;
+  const uint32_t* segs_pad;
+  const uint32_t* lc_off;  // per patch, in uint16 (multiple of 8)
+  const uint32_t* sg_off;  // per patch, in uint32 (multiple of 4)
+  int* err;                // set when a bounded wait gave up
   double* partial;       // nslots x dim
   // batches: per-instance time step, instance of each patch and shared node
   const double* inst_dt;       // null for a single model (scalar dt)
