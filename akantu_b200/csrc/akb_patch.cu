@@ -59,6 +59,33 @@ __host__ __device__ inline SmemLayout layout(int L, int E, int R, int d, int n, 
   return s;
 }
 
+// The n local indices of element el (uint16, n per element): one vector load
+// when n * 2 bytes is a power of two (2, 4 and 8 corners), else n loads.
+template <int n>
+__device__ inline void load_corners(const uint16_t* base, int el, int* out) {
+  if (n == 2 || n == 4 || n == 8) {
+    uint32_t w[4];
+    if (n == 2) {
+      w[0] = reinterpret_cast<const uint32_t*>(base)[el];
+    } else if (n == 4) {
+      const uint2 q = reinterpret_cast<const uint2*>(base)[el];
+      w[0] = q.x;
+      w[1] = q.y;
+    } else {
+      const uint4 q = reinterpret_cast<const uint4*>(base)[el];
+      w[0] = q.x;
+      w[1] = q.y;
+      w[2] = q.z;
+      w[3] = q.w;
+    }
+#pragma unroll
+    for (int a = 0; a < n; ++a) out[a] = (int)((w[a >> 1] >> (16 * (a & 1))) & 0xffffu);
+  } else {
+#pragma unroll
+    for (int a = 0; a < n; ++a) out[a] = base[el * n + a];
+  }
+}
+
 // CTAs per SM each instantiation is built for (register budget).
 template <int T, typename S> struct PatchOccupancy { static constexpr int value = 3; };
 template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, float> { static constexpr int value = 2; };
@@ -181,9 +208,9 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
   for (int c0 = 0, chunk = 0; c0 < ne; c0 += kChunk, ++chunk) {
     const int el = c0 + tid;
     if (el < ne) {
-      int lc[n];
-#pragma unroll
-      for (int a = 0; a < n; ++a) lc[a] = lcs[el * n + a];
+      int lc[n], sl[n];
+      load_corners<n>(lcs, el, lc);
+      load_corners<n>(slots, el, sl);
       const MatParams& mp = (P.emat ? m.mat_table[P.emat[(size_t)eb + el]] : m.mats[0]);
       S dX[3 * 8], du[3 * 8];
 #pragma unroll
@@ -200,11 +227,9 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
       S fe[3 * 8];
       fast::element_force<T, S>(mp, dX, du, fe);
 #pragma unroll
-      for (int a = 0; a < n; ++a) {
-        const int sl = slots[el * n + a];
+      for (int a = 0; a < n; ++a)
 #pragma unroll
-        for (int i = 0; i < d; ++i) contrib[i * CH + sl] = fe[a * d + i];
-      }
+        for (int i = 0; i < d; ++i) contrib[i * CH + sl[a]] = fe[a * d + i];
     }
     __syncthreads();
     const int sb = segp[chunk], nrun = segp[chunk + 1] - sb;
