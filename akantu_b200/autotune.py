@@ -20,7 +20,7 @@ DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "akantu_b200", "
 CANDIDATES = {
     _abi.TRIANGLE_3: [(1024, 640, 0), (512, 320, 0), (2048, 1100, 0), (1024, 640, 3), (768, 480, 0)],
     _abi.TETRAHEDRON_4: [(1024, 400, 0), (512, 220, 0), (1536, 500, 0), (1024, 400, 3)],
-    _abi.HEXAHEDRON_8: [(256, 448, 0), (128, 256, 0), (512, 800, 0), (256, 448, 2)],
+    _abi.HEXAHEDRON_8: [(512, 800, 0), (256, 448, 0), (384, 640, 0), (512, 800, 2)],
     _abi.SEGMENT_2: [(1024, 1100, 0), (512, 600, 0)],
 }
 
