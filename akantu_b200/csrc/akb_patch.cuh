@@ -30,8 +30,6 @@ struct PatchHost {
   std::vector<uint32_t> lnodes;    // global node ids: interior first, then shared
   std::vector<uint32_t> elem_order;  // patch-ordered position -> original element
   std::vector<uint16_t> lconn;     // per element (patch order) nnpe local indices
-  std::vector<uint16_t> cbeg;      // per local node: first CSR entry (relative to the patch)
-  std::vector<uint16_t> centries;  // per element corner: (local element << 3) | corner
   // per chunk of kChunk consecutive elements of a patch: the slot of each
   // element corner once the chunk's corners are sorted by (local node,
   // element, corner), and the runs of equal local node in that order

@@ -128,9 +128,7 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
   std::vector<int32_t> lidx(nn, -1);
   P.node_ptr.push_back(0);
   P.lconn.resize((size_t)ne * nnpe);
-  P.centries.resize((size_t)ne * nnpe);
   std::vector<uint32_t> local;
-  std::vector<int32_t> cnt;
   std::vector<uint64_t> keyed;
   P.cslot.resize((size_t)ne * nnpe);
   for (int p = 0; p < P.npatch; ++p) {
@@ -156,25 +154,9 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
     P.ninterior.push_back(nint);
     P.max_nodes = std::max(P.max_nodes, (int)local.size());
     P.max_elems = std::max(P.max_elems, (int)(ee - eb));
-    cnt.assign(local.size() + 1, 0);
     for (int32_t i = eb; i < ee; ++i) {
       const uint32_t* c = conn + (int64_t)P.elem_order[i] * nnpe;
-      for (int a = 0; a < nnpe; ++a) {
-        P.lconn[(size_t)i * nnpe + a] = (uint16_t)lidx[c[a]];
-        cnt[lidx[c[a]] + 1]++;
-      }
-    }
-    for (size_t j = 0; j < local.size(); ++j) cnt[j + 1] += cnt[j];
-    for (size_t j = 0; j < local.size(); ++j) P.cbeg.push_back((uint16_t)cnt[j]);
-    // entries in ascending local element order (corner order within an element)
-    std::vector<int32_t> fill(cnt.begin(), cnt.end() - 1);
-    uint16_t* ent = &P.centries[(size_t)eb * nnpe];
-    for (int32_t i = eb; i < ee; ++i) {
-      const uint32_t* c = conn + (int64_t)P.elem_order[i] * nnpe;
-      for (int a = 0; a < nnpe; ++a) {
-        const int j = lidx[c[a]];
-        ent[fill[j]++] = (uint16_t)(((i - eb) << 3) | a);
-      }
+      for (int a = 0; a < nnpe; ++a) P.lconn[(size_t)i * nnpe + a] = (uint16_t)lidx[c[a]];
     }
     for (size_t j = 0; j < local.size(); ++j) {
       const int64_t s = sidx[local[j]];
