@@ -2,6 +2,7 @@
 // explicit step driver and its CUDA-graph replay.
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <memory>
 #include <string>
@@ -176,12 +177,14 @@ const char* kernel_name(const akb_model* m, int slot) {
 // Patch sizes per element type: elements per patch and the local node cap,
 // chosen so three 256-thread CTAs (two for hexahedra) fit an SM (measured
 // sweeps on the tet4 cube and the hex8 block).
-void patch_params(int type, int* target, int* max_nodes) {
+// Patch size (elements, local node cap) and piece length (contributions one
+// thread adds per node) of the fused step, per element type.
+void patch_params(int type, int* target, int* max_nodes, int* piece) {
   switch (type) {
-  case AKB_SEGMENT_2: *target = 1024; *max_nodes = 1100; break;
-  case AKB_TRIANGLE_3: *target = 1024; *max_nodes = 640; break;
-  case AKB_TETRAHEDRON_4: *target = 1024; *max_nodes = 400; break;
-  default: *target = 512; *max_nodes = 800; break;
+  case AKB_SEGMENT_2: *target = 1024; *max_nodes = 1100; *piece = 2; break;
+  case AKB_TRIANGLE_3: *target = 1024; *max_nodes = 640; *piece = 6; break;
+  case AKB_TETRAHEDRON_4: *target = 1024; *max_nodes = 400; *piece = 6; break;
+  default: *target = 512; *max_nodes = 800; *piece = 8; break;
   }
 }
 
@@ -190,101 +193,96 @@ akb_status upload(akb_model* m, const std::vector<T>& v, const T** out);
 
 akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
                                 const uint32_t* element_material, const BatchLayout* batch) {
-  int target, max_nodes;
-  patch_params(m->dm.type, &target, &max_nodes);
+  int target, max_nodes, piece;
+  patch_params(m->dm.type, &target, &max_nodes, &piece);
   if (m->opt_patch_elements > 0) target = std::min(m->opt_patch_elements, 8191);
-  if (m->opt_patch_nodes > 0) max_nodes = std::min(m->opt_patch_nodes, 65535);
+  if (m->opt_patch_nodes > 0) max_nodes = std::min(m->opt_patch_nodes, 60000);
+  const int cbytes = fp32(m) ? 4 : 8;  // element vector precision
   PatchHost P;
   std::vector<uint32_t> patch_inst, snode_inst;
-  if (!batch) {
-    P = build_patches(mesh->nodes, mesh->connectivity, mesh->nb_nodes, mesh->nb_elements,
-                      m->dm.dim, m->dm.nnpe, target, max_nodes);
-  } else {
-    // one instance at a time, so no patch spans two instances; the union is
-    // the concatenation of the instances' patches
-    const int dd = m->dm.dim, nn_ = m->dm.nnpe;
-    P.elem_ptr.push_back(0);
-    P.node_ptr.push_back(0);
-    P.sptr.push_back(0);
-    std::vector<uint32_t> lconn;
-    for (int i = 0; i < batch->ninst; ++i) {
-      const int64_t n0 = batch->node_off[i], e0 = batch->elem_off[i];
-      const int64_t nni = batch->node_off[i + 1] - n0, nei = batch->elem_off[i + 1] - e0;
-      lconn.assign(mesh->connectivity + e0 * nn_, mesh->connectivity + (e0 + nei) * nn_);
-      for (auto& c : lconn) c -= (uint32_t)n0;
-      PatchHost Q = build_patches(mesh->nodes + n0 * dd, lconn.data(), nni, nei, dd, nn_,
-                                  target, max_nodes);
-      const int64_t lbase = (int64_t)P.lnodes.size(), sbase = P.nslots;
-      const int64_t segbase = (int64_t)P.segs.size(), chbase = (int64_t)P.seg_ptr.size();
-      for (int p = 0; p < Q.npatch; ++p) {
-        P.elem_ptr.push_back((int32_t)(e0 + Q.elem_ptr[p + 1]));
-        P.node_ptr.push_back((int32_t)(lbase + Q.node_ptr[p + 1]));
-        P.chunk_base.push_back((int32_t)(chbase + Q.chunk_base[p]));
-        patch_inst.push_back((uint32_t)i);
+  try {
+    if (!batch) {
+      P = build_patches(mesh->nodes, mesh->connectivity, mesh->nb_nodes, mesh->nb_elements,
+                        m->dm.dim, m->dm.nnpe, target, max_nodes, cbytes, piece);
+    } else {
+      // one instance at a time, so no patch spans two instances; the union is
+      // the concatenation of the instances' patches
+      const int dd = m->dm.dim, nn_ = m->dm.nnpe;
+      P.elem_ptr.push_back(0);
+      P.node_ptr.push_back(0);
+      P.sptr.push_back(0);
+      std::vector<uint32_t> lconn;
+      for (int i = 0; i < batch->ninst; ++i) {
+        const int64_t n0 = batch->node_off[i], e0 = batch->elem_off[i];
+        const int64_t nni = batch->node_off[i + 1] - n0, nei = batch->elem_off[i + 1] - e0;
+        lconn.assign(mesh->connectivity + e0 * nn_, mesh->connectivity + (e0 + nei) * nn_);
+        for (auto& c : lconn) c -= (uint32_t)n0;
+        PatchHost Q = build_patches(mesh->nodes + n0 * dd, lconn.data(), nni, nei, dd, nn_,
+                                    target, max_nodes, cbytes, piece);
+        const int64_t lbase = (int64_t)P.lnodes.size(), sbase = P.nslots;
+        const int64_t chbase = (int64_t)P.chunks.size();
+        const uint32_t dbase16 = (uint32_t)(P.cdata.size() / 8);
+        for (int p = 0; p < Q.npatch; ++p) {
+          P.elem_ptr.push_back((int32_t)(e0 + Q.elem_ptr[p + 1]));
+          P.node_ptr.push_back((int32_t)(lbase + Q.node_ptr[p + 1]));
+          P.chunk_base.push_back((int32_t)(chbase + Q.chunk_base[p]));
+          patch_inst.push_back((uint32_t)i);
+        }
+        P.npatch += Q.npatch;
+        P.max_nodes = std::max(P.max_nodes, Q.max_nodes);
+        P.node_stride = std::max(P.node_stride, Q.node_stride);
+        P.contrib_slots = std::max(P.contrib_slots, Q.contrib_slots);
+        P.max_pieces = std::max(P.max_pieces, Q.max_pieces);
+        P.chunk_bytes = std::max(P.chunk_bytes, Q.chunk_bytes);
+        P.ninterior.insert(P.ninterior.end(), Q.ninterior.begin(), Q.ninterior.end());
+        for (auto g : Q.lnodes) P.lnodes.push_back((uint32_t)(g + n0));
+        P.lpos.insert(P.lpos.end(), Q.lpos.begin(), Q.lpos.end());
+        for (auto e : Q.elem_order) P.elem_order.push_back((uint32_t)(e + e0));
+        for (auto c : Q.chunks) {
+          c.off16 += dbase16;
+          P.chunks.push_back(c);
+        }
+        P.cdata.insert(P.cdata.end(), Q.cdata.begin(), Q.cdata.end());
+        for (auto s : Q.slot) P.slot.push_back(s == 0xffffffffu ? s : (uint32_t)(s + sbase));
+        for (auto g : Q.snodes) {
+          P.snodes.push_back((uint32_t)(g + n0));
+          snode_inst.push_back((uint32_t)i);
+        }
+        for (size_t k = 1; k < Q.sptr.size(); ++k) P.sptr.push_back((int32_t)(Q.sptr[k] + sbase));
+        P.nslots += Q.nslots;
       }
-      P.npatch += Q.npatch;
-      P.max_nodes = std::max(P.max_nodes, Q.max_nodes);
-      P.max_elems = std::max(P.max_elems, Q.max_elems);
-      P.max_segs = std::max(P.max_segs, Q.max_segs);
-      P.ninterior.insert(P.ninterior.end(), Q.ninterior.begin(), Q.ninterior.end());
-      for (auto g : Q.lnodes) P.lnodes.push_back((uint32_t)(g + n0));
-      for (auto e : Q.elem_order) P.elem_order.push_back((uint32_t)(e + e0));
-      P.lconn.insert(P.lconn.end(), Q.lconn.begin(), Q.lconn.end());
-      P.cslot.insert(P.cslot.end(), Q.cslot.begin(), Q.cslot.end());
-      for (auto s : Q.slot) P.slot.push_back(s == 0xffffffffu ? s : (uint32_t)(s + sbase));
-      for (auto g : Q.snodes) {
-        P.snodes.push_back((uint32_t)(g + n0));
-        snode_inst.push_back((uint32_t)i);
-      }
-      for (size_t k = 1; k < Q.sptr.size(); ++k) P.sptr.push_back((int32_t)(Q.sptr[k] + sbase));
-      P.nslots += Q.nslots;
-      P.segs.insert(P.segs.end(), Q.segs.begin(), Q.segs.end());
-      for (size_t k = 0; k + 1 < Q.seg_ptr.size(); ++k)
-        P.seg_ptr.push_back((int32_t)(Q.seg_ptr[k] + segbase));
+      P.chunk_base.push_back((int32_t)P.chunks.size());
     }
-    P.seg_ptr.push_back((int32_t)P.segs.size());
+  } catch (const std::exception& ex) {
+    return fail(AKB_ERR_UNSUPPORTED, std::string("patch construction: ") + ex.what());
   }
   DevPatches& d = m->patches;
   d.npatch = P.npatch;
   d.grid = m->opt_patch_grid > 0 ? m->opt_patch_grid : 0;
   d.max_nodes = P.max_nodes;
-  d.max_elems = P.max_elems;
-  d.max_segs = P.max_segs;
+  d.node_stride = P.node_stride;
+  d.contrib_slots = P.contrib_slots;
+  d.max_pieces = P.max_pieces;
+  d.chunk_bytes = P.chunk_bytes;
   d.nshared = (int64_t)P.snodes.size();
   akb_status st;
   if ((st = upload(m, P.elem_ptr, &d.elem_ptr)) != AKB_OK) return st;
   if ((st = upload(m, P.node_ptr, &d.node_ptr)) != AKB_OK) return st;
   if ((st = upload(m, P.ninterior, &d.ninterior)) != AKB_OK) return st;
   if ((st = upload(m, P.lnodes, &d.lnodes)) != AKB_OK) return st;
-  if ((st = upload(m, P.seg_ptr, &d.seg_ptr)) != AKB_OK) return st;
+  if ((st = upload(m, P.lpos, &d.lpos)) != AKB_OK) return st;
   if ((st = upload(m, P.chunk_base, &d.chunk_base)) != AKB_OK) return st;
+  if ((st = upload(m, P.cdata, &d.cdata)) != AKB_OK) return st;
+  {
+    static_assert(sizeof(ChunkDesc) == sizeof(uint2), "chunk descriptor is one 8-byte load");
+    std::vector<uint2> cd(P.chunks.size());
+    std::memcpy(cd.data(), P.chunks.data(), cd.size() * sizeof(uint2));
+    if ((st = upload(m, cd, &d.chunks)) != AKB_OK) return st;
+  }
   if ((st = upload(m, P.slot, &d.slot)) != AKB_OK) return st;
   if ((st = upload(m, P.snodes, &d.snodes)) != AKB_OK) return st;
   if ((st = upload(m, P.sptr, &d.sptr)) != AKB_OK) return st;
-  {  // per-patch copies padded to 16 bytes: sources of the TMA bulk staging
-    std::vector<uint16_t> lcp, csp;
-    std::vector<uint32_t> sgp, lco(P.npatch), sgo(P.npatch);
-    const int n_ = m->dm.nnpe;
-    for (int p = 0; p < P.npatch; ++p) {
-      const int64_t eb = P.elem_ptr[p], ne = P.elem_ptr[p + 1] - eb;
-      lco[p] = (uint32_t)lcp.size();
-      lcp.insert(lcp.end(), P.lconn.begin() + eb * n_, P.lconn.begin() + (eb + ne) * n_);
-      csp.insert(csp.end(), P.cslot.begin() + eb * n_, P.cslot.begin() + (eb + ne) * n_);
-      while (lcp.size() % 8) {
-        lcp.push_back(0);
-        csp.push_back(0);
-      }
-      const int64_t nch = (ne + 255) / 256, c0 = P.chunk_base[p];
-      const int64_t s0 = P.seg_ptr[c0], s1 = P.seg_ptr[c0 + nch];
-      sgo[p] = (uint32_t)sgp.size();
-      sgp.insert(sgp.end(), P.segs.begin() + s0, P.segs.begin() + s1);
-      while (sgp.size() % 4) sgp.push_back(0);
-    }
-    if ((st = upload(m, lcp, &d.lconn_pad)) != AKB_OK) return st;
-    if ((st = upload(m, csp, &d.cslot_pad)) != AKB_OK) return st;
-    if ((st = upload(m, sgp, &d.segs_pad)) != AKB_OK) return st;
-    if ((st = upload(m, lco, &d.lc_off)) != AKB_OK) return st;
-    if ((st = upload(m, sgo, &d.sg_off)) != AKB_OK) return st;
+  {
     int* e;
     if ((st = dalloc(m, &e, 1)) != AKB_OK) return st;
     AKB_CUDA_TRY(cudaMemsetAsync(e, 0, sizeof(int), m->stream));
@@ -306,7 +304,8 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
     if ((st = upload(m, snode_inst, &d.snode_inst)) != AKB_OK) return st;
   }
   AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));  // host vectors go out of scope
-  const size_t smem = patch_smem_bytes(d, m->dm.dim, m->dm.nnpe, fp32(m), 256);
+  d.nbuf = patch_buffers(d, m->dm.type, fp32(m));
+  const size_t smem = patch_smem_bytes(d, m->dm.dim, m->dm.nnpe, fp32(m), d.nbuf);
   if (smem > 227 * 1024)
     return fail(AKB_ERR_UNSUPPORTED, "patch does not fit in shared memory");
   AKB_CUDA_TRY(patch_configure(m->dm, d, fp32(m)));

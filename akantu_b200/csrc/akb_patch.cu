@@ -1,23 +1,25 @@
 // akb_patch.cu -- the fused explicit step (AKB_MODE_FP64, AKB_MODE_FP32_BULK).
 //
 // k_patch_step: one CTA per patch.
-//   1. stage the patch: its local connectivity, sorted slots and runs by TMA
-//      bulk copies completing on an mbarrier, while the threads gather the
-//      nodes' X, u, v, a and blocked flags and apply the predictor
-//      u+ = u + dt v + dt^2/2 a, v* = v + dt a on free DOFs
-//      (NewmarkBeta::predictor, newmark-beta.cc:60-89);
+//   1. stage the patch's nodes: the threads gather X, u, v, a and blocked
+//      flags to the nodes' planned shared-memory positions and apply the
+//      predictor u+ = u + dt v + dt^2/2 a, v* = v + dt a on free DOFs
+//      (NewmarkBeta::predictor, newmark-beta.cc:60-89), while a TMA bulk copy
+//      brings the first chunk record (corner positions, contribution slots,
+//      runs, index blocks: akb_patch.cuh);
 //   2. element forces in chunks of blockDim elements from shared memory
-//      (akb_fastmath.cuh), written to the chunk's corners sorted by node;
-//      one thread per node run adds the run (ascending local element order)
-//      to the node accumulators (the -1 scatter of dof_manager.cc:83-137,
-//      without atomics);
+//      (akb_fastmath.cuh), each corner vector written to its contribution
+//      slot; one thread per node run adds the run (ascending local element
+//      order) to the node accumulators (the -1 scatter of
+//      dof_manager.cc:83-137, without atomics). The record of the next chunk
+//      is copied while this one is used (two buffers, when they fit);
 //   3. nodes of this patch only: residual, lumped solve and corrector
 //      (non_linear_solver_lumped.cc:85-98, newmark-beta.cc:176-210) on u+
 //      kept in shared memory and v, a re-read, written back; nodes shared
 //      with other patches: FP64 partial force to its slot.
-// The wait on the staging copies is bounded: past it the CTA flags the
-// error (P.err, read by the host on its next synchronisation), waits again
-// (bounded) for its copies and skips the patch.
+// Every wait on a chunk copy is bounded: past it the CTA flags the error
+// (P.err, read by the host on its next synchronisation), waits again (bounded)
+// for the copies it issued and stops.
 // k_shared_nodes: one thread per shared node adds its partials in patch order
 // and applies the same predictor/corrector arithmetic.
 #include <mutex>
@@ -31,32 +33,36 @@ namespace {
 constexpr int kThreads = 256;
 
 struct SmemLayout {
-  size_t xs, us, fs, contrib, lcs, slots, segs, segp, flags, mbar, total;
+  size_t xs, us, fs, contrib, scratch, buf, buf_stride, flags, mbar, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+__host__ __device__ inline size_t align128(size_t x) { return (x + 127) & ~size_t(127); }
 
-constexpr int kMaxChunks = 33;  // chunks of a patch (8192 elements) + 1
-
-// Shared-memory layout for patch caps L (nodes), E (elements), R (runs).
-// Node arrays are component-major ([i][j]); the chunk's element vectors are
-// stored at their sorted slots, component-major ([i][slot]).
-__host__ __device__ inline SmemLayout layout(int L, int E, int R, int d, int n, int sbytes,
-                                             int threads) {
+// Shared-memory layout: node arrays component-major ([i][position], row
+// stride LM), the chunk's element vectors component-major ([i][slot], CH
+// slots), FP32 only: FP64 piece sums ([i][piece], PM pieces), nbuf chunk
+// record buffers of CB bytes, per-(node, component) blocked flags for up to
+// Lmax nodes, one mbarrier per buffer.
+__host__ __device__ inline SmemLayout layout(int LM, int CH, int PM, int CB, int Lmax, int d,
+                                             int sbytes, int nbuf) {
   SmemLayout s;
-  const size_t nd = (size_t)L * d * sizeof(double);
+  const size_t nd = align16((size_t)LM * d * sizeof(double));
   s.xs = 0;
-  s.us = align16(s.xs + nd);
-  s.fs = align16(s.us + nd);
-  s.contrib = align16(s.fs + nd);
-  s.lcs = align16(s.contrib + (size_t)threads * n * d * sbytes);
-  s.slots = align16(s.lcs + (size_t)E * n * sizeof(uint16_t));
-  s.segs = align16(s.slots + (size_t)E * n * sizeof(uint16_t));
-  s.segp = align16(s.segs + (size_t)R * sizeof(uint32_t));
-  s.flags = align16(s.segp + (size_t)kMaxChunks * sizeof(int32_t));
-  s.mbar = align16(s.flags + (size_t)L * d);
+  s.us = s.xs + nd;
+  s.fs = s.us + nd;
+  s.contrib = s.fs + nd;
+  s.scratch = align16(s.contrib + (size_t)CH * d * sbytes);
+  s.buf = align128(s.scratch + (sbytes == 8 ? 0 : (size_t)PM * d * sizeof(double)));
+  s.buf_stride = align128((size_t)CB);
+  s.flags = s.buf + nbuf * s.buf_stride;
+  s.mbar = align16(s.flags + (size_t)Lmax * d);
   s.total = s.mbar + 16;
   return s;
+}
+__host__ __device__ inline SmemLayout layout(const DevPatches& p, int d, int sbytes, int nbuf) {
+  return layout(p.node_stride, p.contrib_slots, p.max_pieces, p.chunk_bytes, p.max_nodes, d, sbytes,
+                nbuf);
 }
 
 // The n local indices of element el (uint16, n per element): one vector load
@@ -93,7 +99,7 @@ template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, double> { static constexpr i
 
 // (node, component) items handled per thread per round of the staging and
 // finishing loops: their global loads are issued together.
-constexpr int kBatch = 4;
+constexpr int kBatch = 5;
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 __device__ inline uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -116,12 +122,19 @@ __device__ inline bool mbar_wait(uint32_t a, uint32_t parity) {
   return false;
 }
 
-// One patch p, by the whole CTA.
+__device__ inline void expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(mbar),
+               "r"(bytes)
+               : "memory");
+}
+
+// One patch p, by the whole CTA. uses: chunk records this CTA has consumed
+// before (it picks the buffer and the mbarrier phase). Returns false when a
+// bounded wait gave up.
 template <int T, typename S, bool FEXT>
-__device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& P, double dt0,
-                                           int p, unsigned char* smem, uint32_t parity) {
+__device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& P, double dt0,
+                                           int p, unsigned char* smem, uint32_t& uses) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
-  constexpr int CH = kChunk * n;  // sorted slots of one chunk
   static_assert(kChunk == kThreads, "one element per thread per chunk");
   const double dt = P.inst_dt ? P.inst_dt[P.patch_inst[p]] : dt0;
   const int nb = P.node_ptr[p];
@@ -130,39 +143,37 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
   const int ne = P.elem_ptr[p + 1] - eb;
   const int nint = P.ninterior[p];
   const int nchunks = (ne + kChunk - 1) / kChunk;
-  const int LM = P.max_nodes;  // row stride of the component-major arrays
-  const SmemLayout lay = layout(P.max_nodes, P.max_elems, P.max_segs, d, n, sizeof(S), kThreads);
+  const int ch0 = P.chunk_base[p];
+  const int LM = P.node_stride, CH = P.contrib_slots;
+  const bool two = P.nbuf == 2;  // buffers: 1 or 2
+  const SmemLayout lay = layout(P, d, sizeof(S), two ? 2 : 1);
   double* xs = reinterpret_cast<double*>(smem + lay.xs);
   double* us = reinterpret_cast<double*>(smem + lay.us);
   double* fs = reinterpret_cast<double*>(smem + lay.fs);
   S* contrib = reinterpret_cast<S*>(smem + lay.contrib);
-  uint16_t* lcs = reinterpret_cast<uint16_t*>(smem + lay.lcs);
-  uint16_t* slots = reinterpret_cast<uint16_t*>(smem + lay.slots);
-  uint32_t* segs = reinterpret_cast<uint32_t*>(smem + lay.segs);
-  int32_t* segp = reinterpret_cast<int32_t*>(smem + lay.segp);
+  double* scratch = reinterpret_cast<double*>(smem + lay.scratch);  // FP32: piece sums
+  const int PM = P.max_pieces;
   uint8_t* flags = smem + lay.flags;
   const int tid = threadIdx.x;
   const int items = L * d;
+  const uint32_t mb0 = saddr(smem + lay.mbar);
 
-  // 1. stage the patch: local connectivity, sorted slots and runs by TMA
-  //    bulk copies (one thread, completing on an mbarrier) while the CTA
-  //    gathers per (node, component) X, predicted u, blocked flag
-  const uint32_t mb = saddr(smem + lay.mbar);
-  {
-    const int32_t* gp = P.seg_ptr + P.chunk_base[p];
-    const int s0 = gp[0];
-    if (tid <= nchunks) segp[tid] = gp[tid] - s0;
-    if (tid == 0) {
-      const uint32_t blc = ((uint32_t)(ne * n * 2) + 15u) & ~15u;
-      const uint32_t bsg = ((uint32_t)((gp[nchunks] - s0) * 4) + 15u) & ~15u;
-      asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
-                   "r"(2 * blc + bsg)
-                   : "memory");
-      bulk_copy(saddr(lcs), P.lconn_pad + P.lc_off[p], blc, mb);
-      bulk_copy(saddr(slots), P.cslot_pad + P.lc_off[p], blc, mb);
-      if (bsg) bulk_copy(saddr(segs), P.segs_pad + P.sg_off[p], bsg, mb);
-    }
+  // record k (counted over the CTA's chunks) uses buffer k % nbuf, and the
+  // (k / nbuf)-th phase of that buffer's mbarrier
+  auto buffer = [&](uint32_t k) { return two ? (k & 1u) : 0u; };
+  auto phase = [&](uint32_t k) { return (two ? (k >> 1) : k) & 1u; };
+  auto issue = [&](int c) {  // chunk c's record, by thread 0
+    const uint2 cd = __ldg(reinterpret_cast<const uint2*>(&P.chunks[ch0 + c]));  // off16, bytes
+    const uint32_t b = buffer(uses + c), bar = mb0 + 8 * b;
+    expect_tx(bar, cd.y);
+    bulk_copy(saddr(smem + lay.buf + b * lay.buf_stride), P.cdata + (size_t)cd.x * 8, cd.y, bar);
+  };
+  if (tid == 0) {
+    issue(0);
+    if (two && nchunks > 1) issue(1);
   }
+
+  // 1. stage the nodes at their positions
   for (int base = 0; base < items; base += kThreads * kBatch) {
     int64_t idx[kBatch];
 #pragma unroll
@@ -187,31 +198,40 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
       const int k = base + b * kThreads + tid;
       if (k >= items) continue;
       const int j = k / d, i = k - j * d;
+      const int pj = P.lpos[nb + j];
       double uu = u[b], vv = v[b];
       if (!bl[b]) fast::predict(dt, uu, vv, a[b]);
-      xs[i * LM + j] = x[b];
-      us[i * LM + j] = uu;
-      fs[i * LM + j] = 0.0;
+      xs[i * LM + pj] = x[b];
+      us[i * LM + pj] = uu;
+      fs[i * LM + pj] = 0.0;
       flags[k] = bl[b];
     }
   }
-  __syncthreads();
-  if (!mbar_wait(mb, parity)) {  // bounded: flag, drain, skip the patch
-    if (tid == 0) atomicExch(P.err, 1);
-    mbar_wait(mb, parity);
-    return;
-  }
 
   // 2. element forces chunk by chunk: each element writes its corner vectors
-  //    to the corners' sorted slots, then one thread per node run adds the
+  //    to their contribution slots, then one thread per node run adds the
   //    run (ascending element order) to that node
-  for (int c0 = 0, chunk = 0; c0 < ne; c0 += kChunk, ++chunk) {
-    const int el = c0 + tid;
-    if (el < ne) {
+  for (int c = 0; c < nchunks; ++c) {
+    const int ahead = two ? 1 : 0;  // chunks in flight beyond this one
+    if (tid == 0 && c > 0 && c + ahead < nchunks) issue(c + ahead);  // into chunk c-1's buffer
+    const uint32_t b = buffer(uses + c);
+    const bool ok = mbar_wait(mb0 + 8 * b, phase(uses + c));
+    if (__syncthreads_or(!ok)) {  // bounded: flag, drain what was issued, stop
+      if (tid == 0) {
+        atomicExch(P.err, 1);
+        for (int k = c; k <= c + ahead && k < nchunks; ++k)
+          mbar_wait(mb0 + 8 * buffer(uses + k), phase(uses + k));
+      }
+      return false;
+    }
+    const int c0 = c * kChunk, nec = min(kChunk, ne - c0);
+    const uint32_t A = (uint32_t)align16((size_t)nec * n * 2);
+    if (tid < nec) {
+      const uint16_t* lcs = reinterpret_cast<const uint16_t*>(smem + lay.buf + b * lay.buf_stride + 16);
       int lc[n], sl[n];
-      load_corners<n>(lcs, el, lc);
-      load_corners<n>(slots, el, sl);
-      const MatParams& mp = (P.emat ? m.mat_table[P.emat[(size_t)eb + el]] : m.mats[0]);
+      load_corners<n>(lcs, tid, lc);
+      load_corners<n>(lcs + A / 2, tid, sl);
+      const MatParams& mp = (P.emat ? m.mat_table[P.emat[(size_t)eb + c0 + tid]] : m.mats[0]);
       S dX[3 * 8], du[3 * 8];
 #pragma unroll
       for (int i = 0; i < d; ++i) {
@@ -232,20 +252,77 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
         for (int i = 0; i < d; ++i) contrib[i * CH + sl[a]] = fe[a * d + i];
     }
     __syncthreads();
-    const int sb = segp[chunk], nrun = segp[chunk + 1] - sb;
-    for (int r = tid; r < nrun; r += kThreads) {  // one thread per run, all components
-      const uint32_t w = segs[sb + r];
-      const int j = (int)(w >> 16), end = (int)(w & 0xffff);
-      const int beg = r == 0 ? 0 : (int)(segs[sb + r - 1] & 0xffff);
-      double f[3] = {0.0, 0.0, 0.0};
-      for (int k = beg; k < end; ++k)
+    // first level: one thread per piece (up to kMaxPiece contributions of
+    // one node, ascending element order); a node in one piece is done, the
+    // sum of a piece of a node in several is left for the second level. The
+    // index loads depend on the header only, so they issue together.
+    const unsigned char* buf = smem + lay.buf + b * lay.buf_stride;
+    const uint4 hd = *reinterpret_cast<const uint4*>(buf);  // header: 8 x uint16
+    {
+      const int R1 = (int)(hd.x & 0xffff), rows = (int)(hd.x >> 16);
+      const uint32_t* sums = reinterpret_cast<const uint32_t*>(buf + 16 + 2 * A);
+      const uint16_t* ixs = reinterpret_cast<const uint16_t*>(buf + (hd.y & 0xffff));
+      for (int q = tid; q < R1; q += kThreads) {
+        const uint32_t w = sums[q];
+        int k[kMaxPiece];
 #pragma unroll
-        for (int i = 0; i < d; ++i) f[i] += double(contrib[i * CH + k]);
+        for (int t = 0; t < kMaxPiece; ++t) k[t] = t < rows ? ixs[t * R1 + q] : 0;
+        const int len = (int)((w >> 16) & 0xff), jp = (int)(w & 0xffff);
+        double f[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-      for (int i = 0; i < d; ++i) fs[i * LM + j] -= f[i];
+        for (int t = 0; t < kMaxPiece; ++t)
+          if (t < len)
+#pragma unroll
+            for (int i = 0; i < d; ++i) f[i] += double(contrib[i * CH + k[t]]);
+        if (len == 0) continue;
+        if (w >> 24) {  // FP64: over the piece's first slot; FP32: by piece
+#pragma unroll
+          for (int i = 0; i < d; ++i) {
+            if constexpr (sizeof(S) == 8)
+              contrib[i * CH + k[0]] = f[i];
+            else
+              scratch[i * PM + q] = f[i];
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < d; ++i) fs[i * LM + jp] -= f[i];
+        }
+      }
+    }
+    if ((hd.y >> 16) != 0) {  // second level: nodes cut in several pieces
+      __syncthreads();
+      const int R2 = (int)(hd.y >> 16), rows = (int)(hd.z & 0xffff);
+      const uint32_t* sums = reinterpret_cast<const uint32_t*>(buf + (hd.z >> 16));
+      const uint16_t* ixs = reinterpret_cast<const uint16_t*>(buf + (hd.w & 0xffff));
+      for (int q = tid; q < R2; q += kThreads) {
+        const uint32_t w = sums[q];
+        constexpr int kUnroll = 4;  // pieces per node read together
+        int k[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) k[j] = j < rows ? ixs[j * R2 + q] : 0;
+        const int np = (int)(w >> 16), jp = (int)(w & 0xffff);
+        double f[3] = {0.0, 0.0, 0.0};
+        auto add = [&](int kk) {
+#pragma unroll
+          for (int i = 0; i < d; ++i) {
+            if constexpr (sizeof(S) == 8)
+              f[i] += double(contrib[i * CH + kk]);
+            else
+              f[i] += scratch[i * PM + kk];
+          }
+        };
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j)
+          if (j < np) add(k[j]);
+        for (int j = kUnroll; j < np; ++j) add(ixs[j * R2 + q]);
+        if (np == 0) continue;
+#pragma unroll
+        for (int i = 0; i < d; ++i) fs[i * LM + jp] -= f[i];
+      }
     }
     __syncthreads();
   }
+  uses += nchunks;
 
   // 3. finish the nodes of this patch (state re-read, predictor recomputed
   //    bit for bit), hand out the shared ones
@@ -275,12 +352,13 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
       const int k = base + b * kThreads + tid;
       if (k >= items) continue;
       const int j = k / d, i = k - j * d;
-      const double f = fs[i * LM + j];
+      const int pj = P.lpos[nb + j];
+      const double f = fs[i * LM + pj];
       if (j >= nint) {
         P.partial[(int64_t)P.slot[nb + j] * d + i] = f;
       } else if (idx[b] >= 0) {  // blocked DOFs keep u, v, a
         // u+ from the staging, v* recomputed bit for bit
-        double uu = us[i * LM + j], vv = __dadd_rn(v[b], __dmul_rn(dt, a[b])), aa = a[b];
+        double uu = us[i * LM + pj], vv = __dadd_rn(v[b], __dmul_rn(dt, a[b])), aa = a[b];
         fast::correct(dt, FEXT ? f + fx[b] : f, im[b], uu, vv, aa);
         m.u[idx[b]] = uu;
         m.v[idx[b]] = vv;
@@ -288,6 +366,7 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
       }
     }
   }
+  return true;
 }
 
 // One CTA per patch, or (PERSIST) a grid smaller than the patch count whose
@@ -296,24 +375,25 @@ __device__ __forceinline__ void patch_body(const DevModel& m, const DevPatches& 
 template <int T, typename S, bool FEXT, bool PERSIST>
 __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
     k_patch_step(DevModel m, DevPatches P, double dt0) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(128) unsigned char smem[];
   {
-    const SmemLayout lay = layout(P.max_nodes, P.max_elems, P.max_segs, ET<T>::dim, ET<T>::nnpe,
-                                  sizeof(S), kThreads);
+    const SmemLayout lay = layout(P, ET<T>::dim, sizeof(S), P.nbuf);
     if (threadIdx.x == 0) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(smem + lay.mbar)) : "memory");
+      for (int b = 0; b < P.nbuf; ++b)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(smem + lay.mbar + 8 * b))
+                     : "memory");
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
   }
+  uint32_t uses = 0;
   if constexpr (PERSIST) {
-    uint32_t parity = 0;
-    for (int p = blockIdx.x; p < P.npatch; p += gridDim.x, parity ^= 1) {
+    for (int p = blockIdx.x; p < P.npatch; p += gridDim.x) {
       if (p != (int)blockIdx.x) __syncthreads();  // shared memory of the previous patch is free
-      patch_body<T, S, FEXT>(m, P, dt0, p, smem, parity);
+      if (!patch_body<T, S, FEXT>(m, P, dt0, p, smem, uses)) return;
     }
   } else {
-    patch_body<T, S, FEXT>(m, P, dt0, blockIdx.x, smem, 0);
+    patch_body<T, S, FEXT>(m, P, dt0, blockIdx.x, smem, uses);
   }
 }
 
@@ -353,7 +433,7 @@ inline int grid_of(const DevPatches& p) {
 template <int T, typename S>
 cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool fext,
                          cudaStream_t s) {
-  const SmemLayout lay = layout(p.max_nodes, p.max_elems, p.max_segs, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
+  const SmemLayout lay = layout(p, ET<T>::dim, sizeof(S), p.nbuf);
   const int grid = grid_of(p);
   if (grid < p.npatch) {
     if (fext)
@@ -386,7 +466,7 @@ cudaError_t raise_smem_limit(K kernel, size_t bytes) {
 
 template <int T, typename S>
 cudaError_t configure(const DevPatches& p) {
-  const SmemLayout lay = layout(p.max_nodes, p.max_elems, p.max_segs, ET<T>::dim, ET<T>::nnpe, sizeof(S), kThreads);
+  const SmemLayout lay = layout(p, ET<T>::dim, sizeof(S), p.nbuf);
   std::lock_guard<std::mutex> lock(g_attr_mutex);
   cudaError_t e;
   if ((e = raise_smem_limit(k_patch_step<T, S, true, false>, lay.total)) != cudaSuccess) return e;
@@ -397,8 +477,26 @@ cudaError_t configure(const DevPatches& p) {
 
 }  // namespace
 
-size_t patch_smem_bytes(const DevPatches& p, int dim, int nnpe, bool fp32, int threads) {
-  return layout(p.max_nodes, p.max_elems, p.max_segs, dim, nnpe, fp32 ? 4 : 8, threads).total;
+size_t patch_smem_bytes(const DevPatches& p, int dim, int nnpe, bool fp32, int nbuf) {
+  (void)nnpe;
+  return layout(p, dim, fp32 ? 4 : 8, nbuf).total;
+}
+
+int patch_buffers(const DevPatches& p, int type, bool fp32) {
+  // CTAs per SM: 228 KB of shared memory, 1 KB reserved per CTA, and the
+  // register budget the instantiation is built for
+  int regs;
+  switch (type) {
+  case AKB_HEXAHEDRON_8: regs = fp32 ? PatchOccupancy<AKB_HEXAHEDRON_8, float>::value
+                                     : PatchOccupancy<AKB_HEXAHEDRON_8, double>::value; break;
+  default: regs = PatchOccupancy<AKB_TETRAHEDRON_4, double>::value; break;
+  }
+  const int dim = type == AKB_SEGMENT_2 ? 1 : type == AKB_TRIANGLE_3 ? 2 : 3;
+  auto ctas = [&](int nbuf) {
+    const size_t s = layout(p, dim, fp32 ? 4 : 8, nbuf).total + 1024;
+    return std::min<int>(regs, (int)((228 * 1024) / s));
+  };
+  return ctas(2) >= ctas(1) ? 2 : 1;
 }
 
 cudaError_t patch_configure(const DevModel& m, const DevPatches& p, bool fp32) {

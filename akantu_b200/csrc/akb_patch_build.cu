@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cstring>
 #include <numeric>
+#include <stdexcept>
 
 #include "akb_patch.cuh"
 
@@ -27,10 +28,124 @@ inline uint64_t spread2(uint64_t x) {  // 31 bits -> every second bit
   return x;
 }
 
+// Positions of a patch's L local nodes in the shared-memory node arrays. The
+// CTA reads corner a of 16 consecutive elements (a half-warp) as 8-byte words
+// in one instruction; each distinct node of such a group should sit at its own
+// word index mod 16 (bank pair). Greedy in first-touch order: a node takes the
+// residue least used by the groups it belongs to, then the least filled one;
+// each residue holds at most ceil(L / 16) nodes, so positions stay below
+// 16 * ceil(L / 16).
+void place_nodes(const std::vector<uint16_t>& lc, int ne, int nnpe, int L, uint16_t* pos) {
+  const int G = kBankPairs;
+  const int nhalf = (ne + G - 1) / G;
+  std::vector<std::pair<int32_t, int32_t>> mem;  // (node, group), each pair once
+  mem.reserve((size_t)ne * nnpe);
+  for (int h = 0; h < nhalf; ++h)
+    for (int a = 0; a < nnpe; ++a) {
+      const int e0 = h * G, e1 = std::min(ne, e0 + G);
+      for (int e = e0; e < e1; ++e) {
+        const int v = lc[(size_t)e * nnpe + a];
+        bool dup = false;
+        for (int f = e0; f < e && !dup; ++f) dup = lc[(size_t)f * nnpe + a] == v;
+        if (!dup) mem.push_back({v, h * nnpe + a});
+      }
+    }
+  std::sort(mem.begin(), mem.end());
+  std::vector<int32_t> gptr(L + 1, 0);
+  for (auto& m : mem) ++gptr[m.first + 1];
+  for (int v = 0; v < L; ++v) gptr[v + 1] += gptr[v];
+  std::vector<int32_t> used((size_t)nhalf * nnpe * G, 0);
+  std::vector<int32_t> order;
+  order.reserve(L);
+  std::vector<char> seen(L, 0);
+  for (int e = 0; e < ne; ++e)
+    for (int a = 0; a < nnpe; ++a) {
+      const int v = lc[(size_t)e * nnpe + a];
+      if (!seen[v]) {
+        seen[v] = 1;
+        order.push_back(v);
+      }
+    }
+  for (int v = 0; v < L; ++v)
+    if (!seen[v]) order.push_back(v);
+  const int cap = (L + G - 1) / G;
+  int fill[kBankPairs] = {0};
+  for (int v : order) {
+    int64_t cost[kBankPairs] = {0};
+    for (int k = gptr[v]; k < gptr[v + 1]; ++k) {
+      const int32_t* u = &used[(size_t)mem[k].second * G];
+      for (int r = 0; r < G; ++r) cost[r] += u[r];
+    }
+    int best = -1;
+    for (int r = 0; r < G; ++r) {
+      if (fill[r] >= cap) continue;
+      if (best < 0 || cost[r] < cost[best] || (cost[r] == cost[best] && fill[r] < fill[best])) best = r;
+    }
+    pos[v] = (uint16_t)(best + G * fill[best]++);
+    for (int k = gptr[v]; k < gptr[v + 1]; ++k) ++used[(size_t)mem[k].second * G + best];
+  }
+}
+
+// Proper edge colouring of a bipartite multigraph with C colours, C at least
+// its largest degree (Koenig's edge-colouring theorem). Edges are added one at
+// a time: with a the first colour free at the left end u and b the first free
+// at the right end v, an edge takes a if a is free at v, else b if b is free
+// at u, else the path from v alternating colours a, b is recoloured (a <-> b),
+// which frees a at v; in a bipartite graph that path cannot reach u.
+class BipartiteColouring {
+ public:
+  BipartiteColouring(int nl, int nr, int C)
+      : C_(C), at_l_((size_t)nl * C, -1), at_r_((size_t)nr * C, -1) {}
+  void add(int u, int v) {
+    const int e = (int)eu_.size();
+    eu_.push_back(u);
+    ev_.push_back(v);
+    col_.push_back(-1);
+    int a = 0, b = 0;
+    while (at_l_[(size_t)u * C_ + a] >= 0) ++a;
+    while (at_r_[(size_t)v * C_ + b] >= 0) ++b;
+    if (at_r_[(size_t)v * C_ + a] >= 0) {
+      if (at_l_[(size_t)u * C_ + b] < 0) {
+        a = b;
+      } else {
+        path_.clear();
+        int x = v, c = a;
+        bool right = true;
+        for (;;) {
+          const int f = right ? at_r_[(size_t)x * C_ + c] : at_l_[(size_t)x * C_ + c];
+          if (f < 0) break;
+          path_.push_back(f);
+          x = right ? eu_[f] : ev_[f];
+          right = !right;
+          c = c == a ? b : a;
+        }
+        for (int f : path_) {
+          at_l_[(size_t)eu_[f] * C_ + col_[f]] = -1;
+          at_r_[(size_t)ev_[f] * C_ + col_[f]] = -1;
+        }
+        for (int f : path_) {
+          col_[f] = col_[f] == a ? b : a;
+          at_l_[(size_t)eu_[f] * C_ + col_[f]] = f;
+          at_r_[(size_t)ev_[f] * C_ + col_[f]] = f;
+        }
+      }
+    }
+    col_[e] = a;
+    at_l_[(size_t)u * C_ + a] = e;
+    at_r_[(size_t)v * C_ + a] = e;
+  }
+  int colour(int e) const { return col_[e]; }
+
+ private:
+  int C_;
+  std::vector<int32_t> at_l_, at_r_, eu_, ev_, col_, path_;
+};
+
 }  // namespace
 
 PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64_t ne, int dim,
-                        int nnpe, int target_elems, int max_nodes) {
+                        int nnpe, int target_elems, int max_nodes, int contrib_bytes,
+                        int piece) {
   PatchHost P;
   // 1. Morton order of element centroids
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -123,16 +238,30 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
   P.nslots = P.sptr.back();
   std::vector<int32_t> sfill(P.snodes.size(), 0);
 
-  // 4. per-patch local nodes, local connectivity, CSR, slots
+  // 4. per patch: local nodes, their shared-memory positions, chunk records
   std::fill(stamp.begin(), stamp.end(), -1);
   std::vector<int32_t> lidx(nn, -1);
   P.node_ptr.push_back(0);
-  P.lconn.resize((size_t)ne * nnpe);
   std::vector<uint32_t> local;
+  std::vector<uint16_t> lcl, pos;
   std::vector<uint64_t> keyed;
-  P.cslot.resize((size_t)ne * nnpe);
+  struct Run { int32_t node, first, len; };
+  struct Piece { int32_t run, first, len, j; };
+  std::vector<Run> runs;
+  std::vector<Piece> pieces;
+  std::vector<int> multi;
+  std::vector<int32_t> hlen, rgbase, eslot, cls;
+  std::vector<uint16_t> rec;
+  // contribution bank groups: 16 bank pairs for 8-byte contributions, 32
+  // banks for 4-byte ones; the FP32 kernel keeps piece sums in a separate
+  // FP64 array indexed by piece, the FP64 one over the piece's first slot
+  if (piece < 1 || piece > kMaxPiece) throw std::invalid_argument("piece length out of range");
+  const int G = contrib_bytes == 8 ? kBankPairs : 32;
+  const bool by_piece = contrib_bytes != 8;
+  std::vector<int32_t> run_piece0, qof;
   for (int p = 0; p < P.npatch; ++p) {
     const int32_t eb = P.elem_ptr[p], ee = P.elem_ptr[p + 1];
+    const int ne_p = ee - eb;
     local.clear();
     for (int32_t i = eb; i < ee; ++i) {
       const uint32_t* c = conn + (int64_t)P.elem_order[i] * nnpe;
@@ -146,49 +275,152 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
       const bool sx = count[x] >= 2, sy = count[y] >= 2;
       return sx != sy ? !sx : x < y;
     });
+    const int L = (int)local.size();
     int nint = 0;
-    for (size_t j = 0; j < local.size(); ++j) {
-      lidx[local[j]] = (int32_t)j;
+    for (int j = 0; j < L; ++j) {
+      lidx[local[j]] = j;
       nint += count[local[j]] < 2;
     }
     P.ninterior.push_back(nint);
-    P.max_nodes = std::max(P.max_nodes, (int)local.size());
-    P.max_elems = std::max(P.max_elems, (int)(ee - eb));
+    P.max_nodes = std::max(P.max_nodes, L);
+    lcl.resize((size_t)ne_p * nnpe);
     for (int32_t i = eb; i < ee; ++i) {
       const uint32_t* c = conn + (int64_t)P.elem_order[i] * nnpe;
-      for (int a = 0; a < nnpe; ++a) P.lconn[(size_t)i * nnpe + a] = (uint16_t)lidx[c[a]];
+      for (int a = 0; a < nnpe; ++a) lcl[(size_t)(i - eb) * nnpe + a] = (uint16_t)lidx[c[a]];
     }
-    for (size_t j = 0; j < local.size(); ++j) {
+    pos.assign(L, 0);
+    place_nodes(lcl, ne_p, nnpe, L, pos.data());
+    P.lpos.insert(P.lpos.end(), pos.begin(), pos.end());
+    for (int j = 0; j < L; ++j) {
       const int64_t s = sidx[local[j]];
       P.slot.push_back(s < 0 ? 0xffffffffu : (uint32_t)(P.sptr[s] + sfill[s]++));
     }
-    // chunks: corners sorted by (local node, element, corner); the sort key
-    // orders a node's contributions by ascending element
-    P.chunk_base.push_back((int32_t)P.seg_ptr.size());
-    const size_t seg_first = P.segs.size();
-    for (int32_t c0 = eb; c0 < ee; c0 += kChunk) {
-      const int32_t c1 = std::min(ee, c0 + kChunk);
+    P.chunk_base.push_back((int32_t)P.chunks.size());
+    for (int c0 = 0; c0 < ne_p; c0 += kChunk) {
+      const int nec = std::min(ne_p - c0, kChunk), ncorner = nec * nnpe;
+      // runs: the chunk's corners sorted by (local node, element, corner)
       keyed.clear();
-      for (int32_t i = c0; i < c1; ++i)
-        for (int a = 0; a < nnpe; ++a) {
-          const uint32_t j = P.lconn[(size_t)i * nnpe + a];
-          keyed.push_back(((uint64_t)j << 32) | ((uint64_t)(i - c0) << 8) | (uint64_t)a);
-        }
+      for (int e = 0; e < nec; ++e)
+        for (int a = 0; a < nnpe; ++a)
+          keyed.push_back(((uint64_t)lcl[(size_t)(c0 + e) * nnpe + a] << 32) |
+                          ((uint64_t)e << 8) | (uint64_t)a);
       std::sort(keyed.begin(), keyed.end());
-      P.seg_ptr.push_back((int32_t)P.segs.size());
-      for (size_t k = 0; k < keyed.size(); ++k) {
-        const uint32_t j = (uint32_t)(keyed[k] >> 32);
-        const int32_t le = (int32_t)((keyed[k] >> 8) & 0xffffff), a = (int32_t)(keyed[k] & 0xff);
-        P.cslot[(size_t)(c0 + le) * nnpe + a] = (uint16_t)k;
-        if (k + 1 == keyed.size() || (uint32_t)(keyed[k + 1] >> 32) != j)
-          P.segs.push_back((j << 16) | (uint32_t)(k + 1));
+      runs.clear();
+      for (int k = 0; k < ncorner; ++k) {
+        const int32_t j = (int32_t)(keyed[k] >> 32);
+        if (runs.empty() || runs.back().node != j) runs.push_back({j, k, 0});
+        ++runs.back().len;
       }
+      // pieces: runs cut into pieces of at most `piece` entries, by
+      // descending length; G consecutive pieces are summed together
+      pieces.clear();
+      run_piece0.assign(runs.size(), 0);
+      for (int r = 0; r < (int)runs.size(); ++r) {
+        run_piece0[r] = (int)pieces.size();
+        for (int t0 = 0; t0 < runs[r].len; t0 += piece)
+          pieces.push_back({r, runs[r].first + t0, std::min(piece, runs[r].len - t0), t0 / piece});
+      }
+      std::stable_sort(pieces.begin(), pieces.end(), [&](const Piece& x, const Piece& y) {
+        if (x.len != y.len) return x.len > y.len;
+        const int px = pos[runs[x.run].node], py = pos[runs[y.run].node];
+        return px != py ? px < py : x.j < y.j;
+      });
+      const int R1 = (int)pieces.size(), R1p = (R1 + 31) / 32 * 32, nh1 = R1p / G;
+      // sum groups: entry t of G consecutive pieces is one instruction
+      P.max_pieces = std::max(P.max_pieces, R1p);
+      qof.assign(R1, 0);  // sorted index of piece j of run r at run_piece0[r] + j
+      for (int q = 0; q < R1; ++q) qof[run_piece0[pieces[q].run] + pieces[q].j] = q;
+      hlen.assign(nh1, 0);
+      for (int h = 0; h < nh1; ++h) hlen[h] = h * G < R1 ? pieces[h * G].len : 0;
+      rgbase.assign(nh1 + 1, 0);
+      for (int h = 0; h < nh1; ++h) rgbase[h + 1] = rgbase[h] + hlen[h];
+      // colour the (scatter group, sum group) graph: corner a of G
+      // consecutive elements is one scatter instruction, entry t of G
+      // consecutive pieces one sum instruction; a colour is a slot residue
+      const int nsg = (nec + G - 1) / G * nnpe;
+      BipartiteColouring bc(nsg, std::max(rgbase[nh1], 1), G);
+      std::vector<int32_t> edge_of(ncorner);
+      int ne_ = 0;
+      for (int q = 0; q < R1; ++q)
+        for (int t = 0; t < pieces[q].len; ++t) {
+          const uint64_t kk = keyed[pieces[q].first + t];
+          const int e = (int)((kk >> 8) & 0xffffff), a = (int)(kk & 0xff);
+          bc.add((e / G) * nnpe + a, rgbase[q / G] + t);
+          edge_of[e * nnpe + a] = ne_++;
+        }
+      cls.assign(G, 0);
+      eslot.assign(ncorner, 0);
+      for (int k = 0; k < ncorner; ++k) {
+        const int c = bc.colour(edge_of[k]);
+        eslot[k] = c + G * cls[c]++;
+      }
+      int maxcls = 0;
+      for (int c = 0; c < G; ++c) maxcls = std::max(maxcls, cls[c]);
+      P.contrib_slots = std::max(P.contrib_slots, G * maxcls);
+      auto slot_of = [&](int k) {  // slot of sorted corner k
+        const uint64_t kk = keyed[k];
+        return eslot[((kk >> 8) & 0xffffff) * nnpe + (kk & 0xff)];
+      };
+      // second level: nodes cut into several pieces add the pieces' sums,
+      // left by the first level in the slot of each piece's first entry
+      multi.clear();
+      for (int r = 0; r < (int)runs.size(); ++r)
+        if (runs[r].len > piece) multi.push_back(r);
+      std::stable_sort(multi.begin(), multi.end(), [&](int x, int y) {
+        const int nx = (runs[x].len + piece - 1) / piece, ny = (runs[y].len + piece - 1) / piece;
+        return nx != ny ? nx > ny : pos[runs[x].node] < pos[runs[y].node];
+      });
+      const int R2 = (int)multi.size(), R2p = (R2 + 31) / 32 * 32;
+      // index rows: entry t of piece q at row t, column q (rows1 x R1p);
+      // piece j of second-level node q at row j, column q (rows2 x R2p)
+      const int rows1 = R1 > 0 ? pieces[0].len : 0;
+      const int rows2 = R2 > 0 ? (runs[multi[0]].len + piece - 1) / piece : 0;
+      // the record (akb_patch.cuh), offsets in uint16
+      const int A = (ncorner + 7) / 8 * 8;
+      const int o_lc = 8, o_cs = o_lc + A, o_r1 = o_cs + A;
+      const int o_i1 = o_r1 + 2 * R1p, o_r2 = o_i1 + rows1 * R1p;
+      const int o_i2 = o_r2 + 2 * R2p, o_end = o_i2 + rows2 * R2p;
+      if (o_end * 2 > 65535) throw std::length_error("chunk record above 64 KB");
+      rec.assign(o_end, 0);
+      const int hdr[8] = {R1p, rows1, 2 * o_i1, R2p, rows2, 2 * o_r2, 2 * o_i2, 0};
+      for (int k = 0; k < 8; ++k) rec[k] = (uint16_t)hdr[k];
+      for (int k = 0; k < ncorner; ++k) {
+        rec[o_lc + k] = pos[lcl[(size_t)c0 * nnpe + k]];
+        rec[o_cs + k] = (uint16_t)eslot[k];
+      }
+      auto put32 = [&](int at, uint32_t w) {
+        rec[at] = (uint16_t)(w & 0xffff);
+        rec[at + 1] = (uint16_t)(w >> 16);
+      };
+      for (int q = 0; q < R1; ++q) {
+        const Run& rn = runs[pieces[q].run];
+        put32(o_r1 + 2 * q, (uint32_t)pos[rn.node] | ((uint32_t)pieces[q].len << 16) |
+                                ((rn.len > piece ? 1u : 0u) << 24));
+        for (int t = 0; t < pieces[q].len; ++t)
+          rec[o_i1 + t * R1p + q] = (uint16_t)slot_of(pieces[q].first + t);
+      }
+      for (int q = 0; q < R2; ++q) {
+        const Run& rn = runs[multi[q]];
+        const int np = (rn.len + piece - 1) / piece;
+        put32(o_r2 + 2 * q, (uint32_t)pos[rn.node] | ((uint32_t)np << 16));
+        for (int jj = 0; jj < np; ++jj)
+          rec[o_i2 + jj * R2p + q] =
+              (uint16_t)(by_piece ? qof[run_piece0[multi[q]] + jj] : slot_of(rn.first + jj * piece));
+      }
+      ChunkDesc cd;
+      cd.off16 = (uint32_t)(P.cdata.size() / 8);
+      cd.bytes = (uint32_t)rec.size() * 2;
+      P.chunks.push_back(cd);
+      P.cdata.insert(P.cdata.end(), rec.begin(), rec.end());
+      P.chunk_bytes = std::max(P.chunk_bytes, (int)cd.bytes);
     }
-    P.max_segs = std::max(P.max_segs, (int)(P.segs.size() - seg_first));
     P.lnodes.insert(P.lnodes.end(), local.begin(), local.end());
     P.node_ptr.push_back((int32_t)P.lnodes.size());
   }
-  P.seg_ptr.push_back((int32_t)P.segs.size());
+  P.chunk_base.push_back((int32_t)P.chunks.size());
+  // positions stay below 16 * ceil(L / 16); a stride of 5 mod 16 puts the
+  // components of a node in different bank pairs
+  P.node_stride = (P.max_nodes + kBankPairs - 1) / kBankPairs * kBankPairs + 5;
   return P;
 }
 
