@@ -65,10 +65,19 @@ struct akb_model {
   double* d_inst_dt = nullptr;
   const int64_t* d_node_off = nullptr;
   const int64_t* d_elem_off = nullptr;
-  // staging of akb_apply_dirichlet
-  uint32_t* d_bc_nodes = nullptr;
-  double* d_bc_values = nullptr;
-  int64_t bc_capacity = 0;
+  // staging of akb_apply_dirichlet: a ring of pinned host / device buffer
+  // pairs (node ids padded to 8 bytes, then values); a slot is refilled only
+  // once the kernel that read its previous contents has run
+  struct BcSlot {
+    unsigned char* host = nullptr;
+    unsigned char* dev = nullptr;
+    int64_t capacity = 0;  // nodes
+    cudaEvent_t done = nullptr;
+    bool pending = false;
+  };
+  static constexpr int kBcSlots = 4;
+  BcSlot bc[kBcSlots];
+  int bc_next = 0;
 };
 
 namespace {
@@ -608,6 +617,10 @@ akb_status akb_model_destroy(akb_model* m) {
   destroy_graphs(m);
   for (void* p : m->allocations) cudaFree(p);
   if (m->h_result) cudaFreeHost(m->h_result);
+  for (auto& b : m->bc) {
+    if (b.host) cudaFreeHost(b.host);
+    if (b.done) cudaEventDestroy(b.done);
+  }
   if (m->owns_stream) cudaStreamDestroy(m->stream);
   delete m;
   return AKB_OK;
@@ -879,27 +892,36 @@ akb_status akb_apply_dirichlet(akb_model* m, const uint32_t* nodes, int64_t nb_n
     return fail(AKB_ERR_INVALID_ARGUMENT, "component out of range");
   if (nb_nodes == 0) return AKB_OK;
   AKB_CUDA_TRY(cudaSetDevice(m->device));
-  if (nb_nodes > m->bc_capacity) {
-    AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
-    dfree(m, m->d_bc_nodes);
-    dfree(m, m->d_bc_values);
-    m->d_bc_nodes = nullptr;
-    m->d_bc_values = nullptr;
-    m->bc_capacity = 0;
-    if ((st = dalloc(m, &m->d_bc_nodes, nb_nodes)) != AKB_OK) return st;
-    if ((st = dalloc(m, &m->d_bc_values, nb_nodes)) != AKB_OK) return st;
-    m->bc_capacity = nb_nodes;
+  // the caller's arrays are copied to a pinned staging slot on the host, so
+  // they may be reused as soon as the call returns; the upload and the kernel
+  // are queued on the model's stream without waiting for them
+  akb_model::BcSlot& b = m->bc[m->bc_next];
+  m->bc_next = (m->bc_next + 1) % akb_model::kBcSlots;
+  if (!b.done) AKB_CUDA_TRY(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+  if (b.pending) AKB_CUDA_TRY(cudaEventSynchronize(b.done));
+  b.pending = false;
+  const size_t nbytes = ((size_t)nb_nodes * sizeof(uint32_t) + 7) & ~size_t(7);
+  const size_t bytes = nbytes + (size_t)nb_nodes * sizeof(double);
+  if (nb_nodes > b.capacity) {
+    if (b.host) cudaFreeHost(b.host);
+    dfree(m, b.dev);
+    b.host = nullptr;
+    b.dev = nullptr;
+    b.capacity = 0;
+    AKB_CUDA_TRY(cudaMallocHost((void**)&b.host, bytes));
+    if ((st = dalloc(m, &b.dev, bytes)) != AKB_OK) return st;
+    b.capacity = nb_nodes;
   }
-  AKB_CUDA_TRY(cudaMemcpyAsync(m->d_bc_nodes, nodes, nb_nodes * sizeof(uint32_t),
-                               cudaMemcpyHostToDevice, m->stream));
-  AKB_CUDA_TRY(cudaMemcpyAsync(m->d_bc_values, values, nb_nodes * sizeof(double),
-                               cudaMemcpyHostToDevice, m->stream));
-  AKB_CUDA_TRY(apply_dirichlet(m->dm, m->d_bc_nodes, nb_nodes, component, m->d_bc_values,
-                               m->stream));
+  std::memcpy(b.host, nodes, (size_t)nb_nodes * sizeof(uint32_t));
+  std::memcpy(b.host + nbytes, values, (size_t)nb_nodes * sizeof(double));
+  AKB_CUDA_TRY(cudaMemcpyAsync(b.dev, b.host, bytes, cudaMemcpyHostToDevice, m->stream));
+  AKB_CUDA_TRY(apply_dirichlet(m->dm, reinterpret_cast<const uint32_t*>(b.dev), nb_nodes, component,
+                               reinterpret_cast<const double*>(b.dev + nbytes), m->stream));
+  AKB_CUDA_TRY(cudaEventRecord(b.done, m->stream));
+  b.pending = true;
   m->fint_valid = false;
   m->stresses_valid = false;
-  // the caller's host arrays may be reused as soon as the call returns
-  return sync(m);
+  return AKB_OK;
 }
 
 akb_status akb_time_kernels(akb_model* m, int64_t nb_steps, double* ms_per_launch,

@@ -202,7 +202,9 @@ akb_status akb_get_energy(akb_model* model, int32_t kind, double* value);
  * (boundary_condition_functor_inline_impl.hh:85-93, boundary_condition_tmpl.hh:63-88):
  * for each listed node, blocks DOF (node, component) and sets its
  * displacement to values[k]. nodes and values are host arrays of nb_nodes
- * entries (pinned memory makes the copy asynchronous-capable). */
+ * entries; they are copied before the call returns (and may be reused
+ * then), while the upload and the update are queued on the model's stream:
+ * an error of the update is reported by the next call that synchronises. */
 akb_status akb_apply_dirichlet(akb_model* model, const uint32_t* nodes,
                                int64_t nb_nodes, int32_t component,
                                const double* values);
