@@ -20,7 +20,7 @@
 // Every wait on a chunk copy is bounded: past it the CTA flags the error
 // (P.err, read by the host on its next synchronisation), waits again (bounded)
 // for the copies it issued and stops.
-// k_shared_nodes: one thread per shared node adds its partials in patch order
+// k_shared_nodes: one thread per shared DOF adds its partials in patch order
 // and applies the same predictor/corrector arithmetic.
 #include <mutex>
 
@@ -399,29 +399,35 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
 
 template <int D, bool FEXT>
 __global__ void k_shared_nodes(DevModel m, DevPatches P, double dt0) {
-  const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (s >= P.nshared) return;
+  // one thread per (shared node, component): neighbouring threads touch
+  // neighbouring words of the partials and of u, v, a
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t ns = P.nshared;
+  if (t >= ns * D) return;
+  const int64_t s = t / D;
+  const int i = (int)(t - s * D);
   const int64_t g = P.snodes[s];
-  const double dt = P.inst_dt ? P.inst_dt[P.snode_inst[s]] : dt0;
-  const int k0 = P.sptr[s], k1 = P.sptr[s + 1];
-  double f[3] = {0, 0, 0};
-  for (int k = k0; k < k1; ++k)
-#pragma unroll
-    for (int i = 0; i < D; ++i) f[i] += P.partial[(int64_t)k * D + i];
+  const int64_t k = g * D + i;
+  // every load that depends on the node id is issued before the blocked
+  // flag is tested
+  const uint8_t bl = m.blocked[k];
   const double im = m.inv_mass[g];
-#pragma unroll
-  for (int i = 0; i < D; ++i) {
-    const int64_t k = g * D + i;
-    if (m.blocked[k]) continue;
-    double u = m.u[k], v = m.v[k], a = m.a[k];
-    fast::predict(dt, u, v, a);
-    double r = f[i];
-    if (FEXT) r += m.fext[k];
-    fast::correct(dt, r, im, u, v, a);
-    m.u[k] = u;
-    m.v[k] = v;
-    m.a[k] = a;
-  }
+  double u = m.u[k], v = m.v[k], a = m.a[k];
+  const double fx = FEXT ? m.fext[k] : 0.0;
+  const double dt = P.inst_dt ? P.inst_dt[P.snode_inst[s]] : dt0;
+  // partials in patch order: the first two in the dense rows, the others
+  // after them (zero for a node of no element)
+  const int k0 = P.sptr[s], k1 = P.sptr[s + 1];
+  double f = 0.0 + P.partial[s * D + i];
+  f += P.partial[(ns + s) * D + i];
+  for (int q = k0; q < k1; ++q) f += P.partial[(2 * ns + q) * D + i];
+  if (bl) return;
+  fast::predict(dt, u, v, a);
+  if (FEXT) f += fx;
+  fast::correct(dt, f, im, u, v, a);
+  m.u[k] = u;
+  m.v[k] = v;
+  m.a[k] = a;
 }
 
 // grid of the patch kernel: one CTA per patch, or a persistent grid of
@@ -530,7 +536,7 @@ cudaError_t patch_step(const DevModel& m, const DevPatches& p, double dt, bool f
 cudaError_t patch_shared_nodes(const DevModel& m, const DevPatches& p, double dt, bool fext,
                                cudaStream_t s) {
   if (p.nshared == 0) return cudaSuccess;
-  const int blocks = (int)((p.nshared + kThreads - 1) / kThreads);
+  const int blocks = (int)((p.nshared * m.dim + kThreads - 1) / kThreads);
   switch (m.dim) {
   case 1: fext ? k_shared_nodes<1, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
                : k_shared_nodes<1, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;

@@ -9,9 +9,9 @@
 // at build time so that the corner gathers, the contribution scatter and the
 // per-node sums are (nearly) free of bank conflicts.
 // Nodes touched by one patch only ("interior") are finished by that CTA;
-// nodes shared by several patches write one FP64 partial per (node, patch) to
-// slots laid out node-major, and a second kernel adds them in patch order and
-// finishes those nodes.
+// nodes shared by several patches write one FP64 partial per (node, patch)
+// (the first two of every node in two dense rows, the others node-major), and
+// a second kernel adds them in patch order and finishes those nodes.
 #pragma once
 
 #include <stdint.h>
@@ -78,7 +78,7 @@ struct PatchHost {
   std::vector<uint16_t> cdata;     // chunk records (multiple of 8 uint16 each)
   std::vector<uint32_t> slot;      // per local node: partial slot (0xffffffff if interior)
   std::vector<uint32_t> snodes;    // shared nodes, ascending
-  std::vector<int32_t> sptr;       // nshared + 1, partial slots of each shared node
+  std::vector<int32_t> sptr;       // nshared + 1, partial slots of each shared node (CSR)
   int64_t nslots = 0;
 };
 
@@ -106,6 +106,8 @@ struct DevPatches {
   const uint16_t* cdata;   // chunk records (16-byte aligned)
   const uint32_t* slot;
   const uint32_t* snodes;
+  // partial slots: shared node s has its first two at s and nshared + s, the
+  // others at 2 nshared + [sptr[s], sptr[s + 1])
   const int32_t* sptr;
   const uint32_t* emat;  // material of each patch-ordered element, or null
   int* err;              // set when a bounded wait gave up
