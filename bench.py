@@ -326,7 +326,7 @@ def run_ours(args, dist):
                          # (dram__bytes_read.sum + dram__bytes_write.sum) of the
                          # 90^3-cell cube (4.374 M elements, 201.4 MB), scaled by
                          # elements; the capture is not taken inside this run
-                         "traffic": 201.4e6 * E / 4.374e6,
+                         "traffic": 281.9e6 * E / 4.374e6,
                          "traffic_kernel": "k_patch_step (ncu, 90^3 cells, scaled by elements)",
                          "kernels_ms": {n: t for n, t in ktimes},
                          "dominant": top[0]},
