@@ -212,18 +212,25 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
   //    to their contribution slots, then one thread per node run adds the
   //    run (ascending element order) to that node
   for (int c = 0; c < nchunks; ++c) {
-    const int ahead = two ? 1 : 0;  // chunks in flight beyond this one
-    if (tid == 0 && c > 0 && c + ahead < nchunks) issue(c + ahead);  // into chunk c-1's buffer
+    // one buffer: chunk c's record goes where chunk c-1's was, once every
+    // thread is done with it
+    if (!two && c > 0) {
+      __syncthreads();
+      if (tid == 0) issue(c);
+    }
+    // with two buffers this barrier also ends chunk c-1: past it no thread
+    // reads chunk c-1's record or contributions any more
     const uint32_t b = buffer(uses + c);
     const bool ok = mbar_wait(mb0 + 8 * b, phase(uses + c));
     if (__syncthreads_or(!ok)) {  // bounded: flag, drain what was issued, stop
       if (tid == 0) {
         atomicExch(P.err, 1);
-        for (int k = c; k <= c + ahead && k < nchunks; ++k)
-          mbar_wait(mb0 + 8 * buffer(uses + k), phase(uses + k));
+        const int last = min(nchunks - 1, (two && c == 0) ? 1 : c);
+        for (int k = c; k <= last; ++k) mbar_wait(mb0 + 8 * buffer(uses + k), phase(uses + k));
       }
       return false;
     }
+    if (two && tid == 0 && c > 0 && c + 1 < nchunks) issue(c + 1);  // into chunk c-1's buffer
     const int c0 = c * kChunk, nec = min(kChunk, ne - c0);
     const uint32_t A = (uint32_t)align16((size_t)nec * n * 2);
     if (tid < nec) {
@@ -320,8 +327,8 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
         for (int i = 0; i < d; ++i) fs[i * LM + jp] -= f[i];
       }
     }
-    __syncthreads();
   }
+  __syncthreads();  // the sums of the last chunk are in
   uses += nchunks;
 
   // 3. finish the nodes of this patch (state re-read, predictor recomputed
