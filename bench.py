@@ -676,6 +676,8 @@ def main():
     ap.add_argument("--fe2-heldout", type=int, default=4096)
     ap.add_argument("--fe2-check-cells", type=int, default=8)
     ap.add_argument("--no-fe2", action="store_true")
+    ap.add_argument("--workload", default="", choices=["", "plate_tri3", "block_hex8", "plates_batch"],
+                    help="run only this secondary workload (1 GPU) and print its result")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -691,6 +693,14 @@ def main():
         d.rank, d.world = rank, world
         res = run_reference(args, d)
         print(json.dumps(res), flush=True)
+        return
+    if args.workload:  # one secondary workload alone, for profiling
+        import torch
+        torch.cuda.set_device(0)
+        peak, _ = load_peaks()
+        fn = {"plate_tri3": lambda: run_plate(args, 0), "block_hex8": lambda: run_hex8(args, 0, peak),
+              "plates_batch": lambda: run_batch(args, 0)}[args.workload]
+        print(json.dumps({"workloads": {args.workload: fn()}}), flush=True)
         return
     dist = Dist(args.gpus)
     try:
