@@ -1,7 +1,8 @@
 // akb_patch.cuh -- element patches of the fused explicit step.
 //
-// The mesh is cut into patches of spatially close elements (Morton order of
-// element centroids). One CTA owns one patch: it stages the patch's nodes in
+// The mesh is cut into patches of spatially close elements (recursive
+// coordinate bisection of the element centroids, Morton order inside a
+// patch). One CTA owns one patch: it stages the patch's nodes in
 // shared memory, applies the central-difference predictor there, computes
 // the element forces and adds them per node in ascending local element order
 // (static per-chunk runs, so the sum is deterministic without atomics).
