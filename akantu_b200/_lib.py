@@ -55,6 +55,14 @@ SIGNATURES = {
     "akb_batch_get_energies": (I32, [P, I32, PD]),
     "akb_kinetic_energy_static": (I32, [P, P, I64, I32, P, P]),
     "akb_synchronize": (I32, [P]),
+    "akb_model_create_part": (I32, [C.POINTER(_abi.MeshDesc), I32, C.POINTER(_abi.MaterialDesc),
+                                    PU32, C.POINTER(_abi.ModelOptions), PU32, I64,
+                                    C.POINTER(P)]),
+    "akb_part_step_begin": (I32, [P]),
+    "akb_part_export_forces": (I32, [P, P]),
+    "akb_part_step_end": (I32, [P, P]),
+    "akb_part_export_mass": (I32, [P, P]),
+    "akb_part_import_mass": (I32, [P, P]),
     # include/akb_fe2.h
     "akb_step_begin": (I32, [P]),
     "akb_step_end": (I32, [P]),

@@ -78,6 +78,19 @@ struct akb_model {
   static constexpr int kBcSlots = 4;
   BcSlot bc[kBcSlots];
   int bc_next = 0;
+  // part of a partitioned mesh (akb_model_create_part): its interface nodes,
+  // finished only once their forces are summed over all parts
+  bool part = false;
+  bool part_in_step = false;
+  int64_t n_iface = 0;
+  const uint32_t* d_iface_s = nullptr;  // shared-node index of each interface node
+  const uint32_t* d_iface_g = nullptr;  // node id of each interface node
+};
+
+// Interface nodes of a part, in the caller's order.
+struct PartLayout {
+  const uint32_t* nodes = nullptr;
+  int64_t n = 0;
 };
 
 namespace {
@@ -201,7 +214,8 @@ template <typename T>
 akb_status upload(akb_model* m, const std::vector<T>& v, const T** out);
 
 akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
-                                const uint32_t* element_material, const BatchLayout* batch) {
+                                const uint32_t* element_material, const BatchLayout* batch,
+                                const PartLayout* part) {
   int target, max_nodes, piece;
   patch_params(m->dm.type, &target, &max_nodes, &piece);
   if (fp32(m) && m->dm.type == AKB_TETRAHEDRON_4) {
@@ -236,8 +250,14 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
   std::vector<uint32_t> patch_inst, snode_inst;
   try {
     if (!batch) {
+      std::vector<uint8_t> force;
+      if (part) {
+        force.assign(mesh->nb_nodes, 0);
+        for (int64_t i = 0; i < part->n; ++i) force[part->nodes[i]] = 1;
+      }
       P = build_patches(mesh->nodes, mesh->connectivity, mesh->nb_nodes, mesh->nb_elements,
-                        m->dm.dim, m->dm.nnpe, target, max_nodes, cbytes, piece);
+                        m->dm.dim, m->dm.nnpe, target, max_nodes, cbytes, piece,
+                        part ? force.data() : nullptr);
     } else {
       // one instance at a time, so no patch spans two instances; the union is
       // the concatenation of the instances' patches
@@ -335,6 +355,20 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
   }
   if ((st = upload(m, P.slot, &d.slot)) != AKB_OK) return st;
   if ((st = upload(m, P.snodes, &d.snodes)) != AKB_OK) return st;
+  if (part) {  // each interface node's index among the shared nodes
+    std::vector<uint32_t> is(part->n), ig(part->n);
+    for (int64_t i = 0; i < part->n; ++i) {
+      const auto it = std::lower_bound(P.snodes.begin(), P.snodes.end(), part->nodes[i]);
+      if (it == P.snodes.end() || *it != part->nodes[i])
+        return fail(AKB_ERR_INVALID_ARGUMENT, "interface node is not a shared node");
+      is[i] = (uint32_t)(it - P.snodes.begin());
+      ig[i] = part->nodes[i];
+    }
+    if ((st = upload(m, is, &m->d_iface_s)) != AKB_OK) return st;
+    if ((st = upload(m, ig, &m->d_iface_g)) != AKB_OK) return st;
+    m->n_iface = part->n;
+    m->part = true;
+  }
   if ((st = upload(m, P.sptr, &d.sptr)) != AKB_OK) return st;
   {
     int* e;
@@ -454,7 +488,7 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
                                const akb_material_desc* materials,
                                const uint32_t* element_material,
                                const akb_model_options* options, const BatchLayout* batch,
-                               akb_model** out);
+                               akb_model** out, const PartLayout* part = nullptr);
 
 extern "C" {
 
@@ -471,6 +505,21 @@ akb_status akb_model_create(const akb_mesh_desc* mesh, int32_t nb_materials,
   return create_model(mesh, nb_materials, materials, element_material, options, nullptr, out);
 }
 
+akb_status akb_model_create_part(const akb_mesh_desc* mesh, int32_t nb_materials,
+                                 const akb_material_desc* materials,
+                                 const uint32_t* element_material,
+                                 const akb_model_options* options,
+                                 const uint32_t* interface_nodes, int64_t nb_interface,
+                                 akb_model** out) {
+  if (!out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output handle");
+  *out = nullptr;
+  PartLayout part;
+  part.nodes = interface_nodes;
+  part.n = nb_interface;
+  return create_model(mesh, nb_materials, materials, element_material, options, nullptr, out,
+                      &part);
+}
+
 }  // extern "C"
 
 // Shared by akb_model_create and akb_batch_create. batch (may be null) gives
@@ -481,7 +530,7 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
                                const akb_material_desc* materials,
                                const uint32_t* element_material,
                                const akb_model_options* options, const BatchLayout* batch,
-                               akb_model** out) {
+                               akb_model** out, const PartLayout* part) {
   if (!out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output handle");
   *out = nullptr;
   if (!mesh || !materials || nb_materials < 1 || nb_materials > (1 << 24))
@@ -521,6 +570,17 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
   if (nb_user && (nb_user != nb_materials || opt.precision_mode != AKB_MODE_FP64 || batch))
     return fail(AKB_ERR_UNSUPPORTED,
                 "user materials: every material of the model, AKB_MODE_FP64, no batch");
+  if (part) {
+    if (opt.precision_mode == AKB_MODE_FP64_REFERENCE || nb_user || batch || ne == 0)
+      return fail(AKB_ERR_UNSUPPORTED,
+                  "partitioned mesh: AKB_MODE_FP64 or AKB_MODE_FP32_BULK, built-in materials, "
+                  "elements");
+    if (part->n < 0 || (part->n > 0 && !part->nodes))
+      return fail(AKB_ERR_INVALID_ARGUMENT, "null interface node array");
+    for (int64_t i = 0; i < part->n; ++i)
+      if (part->nodes[i] >= (uint64_t)nn)
+        return fail(AKB_ERR_INVALID_ARGUMENT, "interface node out of range");
+  }
 
   auto m = std::make_unique<akb_model>();
   m->mode = opt.precision_mode;
@@ -634,7 +694,8 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
     if ((st = ensure_stress_arrays(m.get())) != AKB_OK) return st;
     AKB_CUDA_TRY(cudaMemsetAsync(dm.stress, 0, (size_t)ne * q * d * d * sizeof(double), m->stream));
   } else if (m->mode != AKB_MODE_FP64_REFERENCE && ne > 0) {
-    if ((st = build_device_patches(m.get(), mesh, element_material, batch)) != AKB_OK) return st;
+    if ((st = build_device_patches(m.get(), mesh, element_material, batch, part)) != AKB_OK)
+      return st;
   }
   if (batch) {
     m->ninst = batch->ninst;
@@ -842,6 +903,8 @@ akb_status akb_solve_steps(akb_model* m, int64_t nb_steps) {
   if ((st = check_model(m)) != AKB_OK) return st;
   if (m->user)
     return fail(AKB_ERR_STATE, "user material: step with akb_step_begin / akb_step_end");
+  if (m->part)
+    return fail(AKB_ERR_STATE, "partitioned mesh: step with akb_part_step_begin / akb_part_step_end");
   if (nb_steps < 0) return fail(AKB_ERR_INVALID_ARGUMENT, "negative step count");
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   if (nb_steps == 0) return AKB_OK;
@@ -868,6 +931,8 @@ akb_status akb_time_solve_steps(akb_model* m, int64_t nb_steps, double* elapsed_
   if ((st = check_model(m)) != AKB_OK) return st;
   if (m->user)
     return fail(AKB_ERR_STATE, "user material: step with akb_step_begin / akb_step_end");
+  if (m->part)
+    return fail(AKB_ERR_STATE, "partitioned mesh: step with akb_part_step_begin / akb_part_step_end");
   if (!elapsed_ms) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
@@ -980,6 +1045,8 @@ akb_status akb_time_kernels(akb_model* m, int64_t nb_steps, double* ms_per_launc
     return fail(AKB_ERR_INVALID_ARGUMENT, "bad timing arguments");
   if (m->user)
     return fail(AKB_ERR_STATE, "user material: step with akb_step_begin / akb_step_end");
+  if (m->part)
+    return fail(AKB_ERR_STATE, "partitioned mesh: step with akb_part_step_begin / akb_part_step_end");
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   StepTimer t;
@@ -1155,6 +1222,76 @@ akb_status akb_step_end(akb_model* m) {
   AKB_CUDA_TRY(fast_gather_correct(m->dm, m->dt, false, true, m->has_fext, m->stream));
   m->in_step = false;
   m->fint_valid = true;
+  return AKB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Parts of a partitioned mesh (one process and GPU each): the step is split
+// around the sum of the interface nodes' forces over all parts.
+extern "C" {
+
+static akb_status check_part(akb_model* m) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!m->part) return fail(AKB_ERR_STATE, "not a partitioned model (akb_model_create_part)");
+  return AKB_OK;
+}
+
+akb_status akb_part_step_begin(akb_model* m) {
+  akb_status st;
+  if ((st = check_part(m)) != AKB_OK) return st;
+  if (m->part_in_step) return fail(AKB_ERR_STATE, "step already begun");
+  if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(patch_step(m->dm, m->patches, m->dt, fp32(m), m->has_fext, m->stream));
+  m->part_in_step = true;
+  return AKB_OK;
+}
+
+akb_status akb_part_export_forces(akb_model* m, double* device_out) {
+  akb_status st;
+  if ((st = check_part(m)) != AKB_OK) return st;
+  if (!m->part_in_step) return fail(AKB_ERR_STATE, "no step begun");
+  if (m->n_iface > 0 && !device_out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(patch_iface_export(m->dm, m->patches, m->d_iface_s, m->n_iface, device_out,
+                                  m->stream));
+  return AKB_OK;
+}
+
+akb_status akb_part_step_end(akb_model* m, const double* device_in) {
+  akb_status st;
+  if ((st = check_part(m)) != AKB_OK) return st;
+  if (!m->part_in_step) return fail(AKB_ERR_STATE, "no step begun");
+  if (m->n_iface > 0 && !device_in) return fail(AKB_ERR_INVALID_ARGUMENT, "null input");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(patch_iface_import(m->dm, m->patches, m->d_iface_s, m->n_iface, device_in,
+                                  m->stream));
+  AKB_CUDA_TRY(patch_shared_nodes(m->dm, m->patches, m->dt, m->has_fext, m->stream));
+  m->part_in_step = false;
+  m->fint_valid = false;
+  m->stresses_valid = false;
+  return AKB_OK;
+}
+
+akb_status akb_part_export_mass(akb_model* m, double* device_out) {
+  akb_status st;
+  if ((st = check_part(m)) != AKB_OK) return st;
+  if (m->n_iface > 0 && !device_out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(mass_export(m->dm, m->d_iface_g, m->n_iface, device_out, m->stream));
+  return AKB_OK;
+}
+
+akb_status akb_part_import_mass(akb_model* m, const double* device_in) {
+  akb_status st;
+  if ((st = check_part(m)) != AKB_OK) return st;
+  if (m->part_in_step) return fail(AKB_ERR_STATE, "inside a step");
+  if (m->n_iface > 0 && !device_in) return fail(AKB_ERR_INVALID_ARGUMENT, "null input");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(mass_import(m->dm, m->d_iface_g, m->n_iface, device_in, m->stream));
   return AKB_OK;
 }
 

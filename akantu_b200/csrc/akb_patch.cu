@@ -437,6 +437,49 @@ __global__ void k_shared_nodes(DevModel m, DevPatches P, double dt0) {
   m.a[k] = a;
 }
 
+// Interface nodes of a partitioned mesh, one thread per (interface node,
+// component): the sum of the node's partials in patch order (export), or the
+// total over all parts written as its only partial (import).
+__global__ void k_iface_export(DevPatches P, const uint32_t* iface, int64_t n, int d,
+                               double* out) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n * d) return;
+  const int64_t q = t / d;
+  const int i = (int)(t - q * d);
+  const int64_t ns = P.nshared, s = iface[q];
+  double f = 0.0 + P.partial[s * d + i];
+  f += P.partial[(ns + s) * d + i];
+  for (int k = P.sptr[s]; k < P.sptr[s + 1]; ++k) f += P.partial[(2 * ns + k) * d + i];
+  out[t] = f;
+}
+
+__global__ void k_iface_import(DevPatches P, const uint32_t* iface, int64_t n, int d,
+                               const double* in) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n * d) return;
+  const int64_t q = t / d;
+  const int i = (int)(t - q * d);
+  const int64_t ns = P.nshared, s = iface[q];
+  P.partial[s * d + i] = in[t];
+  P.partial[(ns + s) * d + i] = 0.0;
+  for (int k = P.sptr[s]; k < P.sptr[s + 1]; ++k) P.partial[(2 * ns + k) * d + i] = 0.0;
+}
+
+__global__ void k_mass_export(DevModel m, const uint32_t* nodes, int64_t n, double* out) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  out[t] = m.mass[(int64_t)nodes[t] * m.dim];
+}
+
+__global__ void k_mass_import(DevModel m, const uint32_t* nodes, int64_t n, const double* in) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int64_t g = nodes[t];
+  const double M = in[t];
+  for (int c = 0; c < m.dim; ++c) m.mass[g * m.dim + c] = M;
+  m.inv_mass[g] = 1. / M;
+}
+
 // grid of the patch kernel: one CTA per patch, or a persistent grid of
 // P.grid CTAs that stride over the patches
 inline int grid_of(const DevPatches& p) {
@@ -538,6 +581,36 @@ cudaError_t patch_step(const DevModel& m, const DevPatches& p, double dt, bool f
     return fp32 ? launch_patch<AKB_HEXAHEDRON_8, float>(m, p, dt, fext, s)
                 : launch_patch<AKB_HEXAHEDRON_8, double>(m, p, dt, fext, s);
   }
+}
+
+cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* iface,
+                               int64_t n, double* out, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int blocks = (int)((n * m.dim + kThreads - 1) / kThreads);
+  k_iface_export<<<blocks, kThreads, 0, s>>>(p, iface, n, m.dim, out);
+  return cudaGetLastError();
+}
+
+cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* iface,
+                               int64_t n, const double* in, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int blocks = (int)((n * m.dim + kThreads - 1) / kThreads);
+  k_iface_import<<<blocks, kThreads, 0, s>>>(p, iface, n, m.dim, in);
+  return cudaGetLastError();
+}
+
+cudaError_t mass_export(const DevModel& m, const uint32_t* nodes, int64_t n, double* out,
+                        cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_mass_export<<<(int)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(m, nodes, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t mass_import(const DevModel& m, const uint32_t* nodes, int64_t n, const double* in,
+                        cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  k_mass_import<<<(int)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(m, nodes, n, in);
+  return cudaGetLastError();
 }
 
 cudaError_t patch_shared_nodes(const DevModel& m, const DevPatches& p, double dt, bool fext,

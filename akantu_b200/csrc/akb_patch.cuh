@@ -85,10 +85,12 @@ struct PatchHost {
 
 // Builds the patches. target_elems: elements per patch; max_nodes: local node
 // cap (<= 60000); contrib_bytes: element vector precision (8: FP64, 4:
-// FP32); piece: contributions one thread adds (<= kMaxPiece).
+// FP32); piece: contributions one thread adds (<= kMaxPiece); force_shared
+// (per node, or null): nodes finished by the shared-node pass even when one
+// patch holds them (the interface nodes of a partitioned mesh).
 PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64_t ne, int dim,
                         int nnpe, int target_elems, int max_nodes, int contrib_bytes,
-                        int piece);
+                        int piece, const uint8_t* force_shared = nullptr);
 
 // Device copy of a PatchHost.
 struct DevPatches {
@@ -127,5 +129,16 @@ cudaError_t patch_step(const DevModel& m, const DevPatches& p, double dt, bool f
 cudaError_t patch_shared_nodes(const DevModel& m, const DevPatches& p, double dt,
                                bool has_fext, cudaStream_t s);
 cudaError_t patch_configure(const DevModel& m, const DevPatches& p, bool fp32);
+// Partitioned meshes: out[i] = sum of the partials of shared node iface[i]
+// (per component); import writes in[i] as that node's only partial. Masses:
+// out[i] = lumped mass of node nodes[i]; import sets it (and 1/M).
+cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* iface,
+                               int64_t n, double* out, cudaStream_t s);
+cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* iface,
+                               int64_t n, const double* in, cudaStream_t s);
+cudaError_t mass_export(const DevModel& m, const uint32_t* nodes, int64_t n, double* out,
+                        cudaStream_t s);
+cudaError_t mass_import(const DevModel& m, const uint32_t* nodes, int64_t n, const double* in,
+                        cudaStream_t s);
 
 }  // namespace akb

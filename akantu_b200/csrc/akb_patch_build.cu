@@ -145,7 +145,7 @@ class BipartiteColouring {
 
 PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64_t ne, int dim,
                         int nnpe, int target_elems, int max_nodes, int contrib_bytes,
-                        int piece) {
+                        int piece, const uint8_t* force_shared) {
   PatchHost P;
   // 1. element centroids and their Morton keys
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -261,7 +261,7 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
   std::vector<int64_t> sidx(nn, -1);
   P.sptr.push_back(0);
   for (int64_t i = 0; i < nn; ++i)
-    if (count[i] >= 2 || count[i] == 0) {
+    if (count[i] >= 2 || count[i] == 0 || (force_shared && force_shared[i])) {
       sidx[i] = (int64_t)P.snodes.size();
       P.snodes.push_back((uint32_t)i);
       P.sptr.push_back(P.sptr.back() + count[i]);
@@ -303,14 +303,14 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
         }
     }
     std::sort(local.begin(), local.end(), [&](uint32_t x, uint32_t y) {
-      const bool sx = count[x] >= 2, sy = count[y] >= 2;
+      const bool sx = sidx[x] >= 0, sy = sidx[y] >= 0;
       return sx != sy ? !sx : x < y;
     });
     const int L = (int)local.size();
     int nint = 0;
     for (int j = 0; j < L; ++j) {
       lidx[local[j]] = j;
-      nint += count[local[j]] < 2;
+      nint += sidx[local[j]] < 0;
     }
     P.ninterior.push_back(nint);
     P.max_nodes = std::max(P.max_nodes, L);

@@ -120,8 +120,13 @@ class SolidMechanicsModel:
 
     def __init__(self, mesh, materials=None, element_material=None,
                  precision=_abi.MODE_FP64_REFERENCE, device=0, stream=None,
-                 patch_elements=0, patch_nodes=0):
+                 patch_elements=0, patch_nodes=0, interface_nodes=None):
+        """interface_nodes: this model is one part of a partitioned mesh
+        (akb_model_create_part), these of its nodes are shared with other
+        parts; step it through akantu_b200.decompose.DistributedModel."""
         self.mesh = mesh
+        self._iface = None if interface_nodes is None else \
+            np.ascontiguousarray(interface_nodes, dtype=np.uint32)
         self.dim, self.nnpe, self.nqp = element_properties(mesh.element_type)
         self._materials = list(materials) if materials else []
         self._element_material = element_material
@@ -164,8 +169,14 @@ class SolidMechanicsModel:
             self._stream = torch_stream(self._device)
         opt = _abi.ModelOptions(self._precision, self._device, self._stream, *self._patch)
         h = C.c_void_p()
-        check(L.akb_model_create(C.byref(desc), len(self._materials), mats, em,
-                                 C.byref(opt), C.byref(h)))
+        if self._iface is None:
+            check(L.akb_model_create(C.byref(desc), len(self._materials), mats, em,
+                                     C.byref(opt), C.byref(h)))
+        else:
+            check(L.akb_model_create_part(C.byref(desc), len(self._materials), mats, em,
+                                          C.byref(opt),
+                                          self._iface.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                          self._iface.size, C.byref(h)))
         self._h = h
 
     def __del__(self):

@@ -266,6 +266,39 @@ akb_status akb_kinetic_energy_static(const double* mass, const double* velocity,
 /* Waits for all work queued on the model's stream. */
 akb_status akb_synchronize(akb_model* model);
 
+/* ---- Partitioned meshes (one process and GPU per part) -------------------
+ * The reference distributes a mesh over MPI ranks with ghost elements and
+ * sums the interface nodes' residual contributions across ranks
+ * (solid_mechanics_model.cc:94-100, 395-411; ElementSynchronizer). Here a
+ * part is a model of its own elements and the nodes they touch;
+ * interface_nodes lists its nodes that other parts' elements touch too
+ * (local ids, in an order of the caller's choice). Fast modes only
+ * (AKB_MODE_FP64, AKB_MODE_FP32_BULK), built-in materials; akb_solve_steps
+ * is refused. A step is
+ *   akb_part_step_begin   predictor, element forces, this part's nodes
+ *                         finished, the interface nodes' partial forces kept;
+ *   akb_part_export_forces  out[i*d + c] = this part's internal force on
+ *                         interface node i (device array, nb_interface x d);
+ *   (the caller sums the exported arrays over all parts, e.g. an all-reduce
+ *   on the model's stream, akb_model_get_stream)
+ *   akb_part_step_end     in = the summed forces: lumped solve and corrector
+ *                         of the interface nodes and the other shared nodes.
+ * The lumped mass of an interface node is also a sum over parts: after
+ * creation, export it (out[i], nb_interface doubles), sum over parts and
+ * import the sum; and set one time step for all parts (the minimum of the
+ * parts' stable steps). All calls only queue work on the model's stream. */
+akb_status akb_model_create_part(const akb_mesh_desc* mesh, int32_t nb_materials,
+                                 const akb_material_desc* materials,
+                                 const uint32_t* element_material,
+                                 const akb_model_options* options,
+                                 const uint32_t* interface_nodes, int64_t nb_interface,
+                                 akb_model** model);
+akb_status akb_part_step_begin(akb_model* model);
+akb_status akb_part_export_forces(akb_model* model, double* device_out);
+akb_status akb_part_step_end(akb_model* model, const double* device_in);
+akb_status akb_part_export_mass(akb_model* model, double* device_out);
+akb_status akb_part_import_mass(akb_model* model, const double* device_in);
+
 #ifdef __cplusplus
 }
 #endif
