@@ -324,7 +324,7 @@ def run_ours(args, dist):
                          "algorithmic_bytes_per_step": balg,
                          # DRAM bytes of one k_patch_step launch from an ncu capture
                          # (dram__bytes_read.sum + dram__bytes_write.sum) of the
-                         # 90^3-cell cube (4.374 M elements, 201.4 MB), scaled by
+                         # 90^3-cell cube (4.374 M elements, 281.9 MB), scaled by
                          # elements; the capture is not taken inside this run
                          "traffic": 281.9e6 * E / 4.374e6,
                          "traffic_kernel": "k_patch_step (ncu, 90^3 cells, scaled by elements)",
@@ -338,6 +338,56 @@ def run_ours(args, dist):
         }
     m.close()
     return result
+
+
+def run_decomposed(args, dist):
+    """The headline cube cut into parts, one per rank (or --parts-per-rank on
+    each GPU), stepped as one mesh: per step each part's interface forces go
+    into one array over all interface nodes, all-reduced (NCCL) across ranks.
+    Total work is fixed as N grows (strong scaling)."""
+    import torch
+    from akantu_b200.decompose import DistributedModel
+    device = dist.local_rank
+    torch.cuda.set_device(device)
+    w = configs.cube_tet4(args.cells)
+    E = w["mesh"].getNbElement()
+    ppr = max(1, args.parts_per_rank)
+    nparts = dist.world * ppr
+    dm = DistributedModel(w["mesh"], w["materials"], nparts, precision=_abi.MODE_FP64,
+                          device=device, here=list(range(dist.rank * ppr, (dist.rank + 1) * ppr)))
+    dm.set_blocked(w["blocked"])
+    dm.set_field(_abi.FIELD_DISPLACEMENT, w["u0"])
+    dm.set_field(_abi.FIELD_VELOCITY, w["v0"])
+    dt = w["dt_factor"] * dm.stable_time_step()
+    dm.set_time_step(dt)
+    dm.solve_steps(args.warmup)
+    sampler = ClockSampler(device)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.start()
+    e0.record()
+    dm.solve_steps(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    dist.barrier()
+    ms = dist.max(e0.elapsed_time(e1))
+    iface = dm.n_interface
+    dm.close()
+    if dist.rank != 0:
+        return None
+    return {"metric": METRIC, "value": E * args.steps / (ms / 1e3), "unit": UNIT,
+            "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cube_tet4: %d^3 cells x 6 tetrahedron_4 (%d elements), "
+                                   "linear elastic, FP64, dt = 0.8 x stable" % (args.cells, E),
+                       "parallelism": "mesh cut into %d parts (coordinate bisection), %d per GPU; "
+                                      "%d interface nodes, their forces all-reduced each step"
+                                      % (nparts, ppr, iface),
+                       "time_step": dt},
+            "clocks": clocks, "gpu_launches": args.steps * 4 * nparts}
 
 
 def run_plate(args, device):
@@ -676,6 +726,10 @@ def main():
     ap.add_argument("--fe2-heldout", type=int, default=4096)
     ap.add_argument("--fe2-check-cells", type=int, default=8)
     ap.add_argument("--no-fe2", action="store_true")
+    ap.add_argument("--decompose", action="store_true",
+                    help="the headline cube as one mesh cut over the ranks (strong scaling) "
+                         "instead of one mesh per rank")
+    ap.add_argument("--parts-per-rank", type=int, default=1)
     ap.add_argument("--workload", default="", choices=["", "plate_tri3", "block_hex8", "plates_batch"],
                     help="run only this secondary workload (1 GPU) and print its result")
     args = ap.parse_args()
@@ -703,6 +757,14 @@ def main():
         print(json.dumps({"workloads": {args.workload: fn()}}), flush=True)
         return
     dist = Dist(args.gpus)
+    if args.decompose:
+        try:
+            res = run_decomposed(args, dist)
+            if dist.rank == 0:
+                print(json.dumps(res), flush=True)
+        finally:
+            dist.close()
+        return
     try:
         res = run_ours(args, dist)
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
