@@ -303,6 +303,23 @@ def run_ours(args, dist):
         u32 = m32.getDisplacement()
         fp32["rel_err_displacement_vs_fp64"] = float(np.abs(u32 - u64).max() / np.abs(u64).max())
     m32.close()
+    parity = None
+    if dist.rank == 0:
+        # full-size parity: the same K steps in the reference-order GPU mode
+        # (the reference's operation order, bitwise equal to the oracle on
+        # the sizes the oracle runs) against the fused FP64 step
+        mref = make_model(w, _abi.MODE_FP64_REFERENCE, device)
+        configs.setup_model(Facade(mref), w)
+        mref.setTimeStep(dt)
+        reset_state(mref, w)
+        mref.solveSteps(args.steps)
+        uref = mref.getDisplacement()
+        vref = mref.getVelocity()
+        mref.close()
+        v64 = m.getVelocity()
+        parity = {"steps": args.steps, "reference": "AKB_MODE_FP64_REFERENCE on the GPU",
+                  "rel_err_displacement": float(np.abs(u64 - uref).max() / np.abs(uref).max()),
+                  "rel_err_velocity": float(np.abs(v64 - vref).max() / np.abs(vref).max())}
     launches = args.steps * len(ktimes)
     result = None
     if dist.rank == 0:
@@ -335,6 +352,7 @@ def run_ours(args, dist):
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},
             "gpu_launches": launches,
             "fp32_bulk": fp32,
+            "fp64_vs_reference_order": parity,
         }
     m.close()
     return result
