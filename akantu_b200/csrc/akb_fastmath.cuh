@@ -291,6 +291,47 @@ __device__ inline S shape_gradients(const S* dX, int q, S* B) {
   return detJ;
 }
 
+// Hexahedron force at quadrature point q, without forming the shape
+// gradients: with H = du/dxi (H[i*3+k] = sum_a du_a,i dN(k, a, q)) and A the
+// adjugate of J, grad u = H A^T / det J, and the corner forces
+// w det J P grad N_a = (w P A) dN_a: Q = w P A, fe_a,i += sum_k Q_ik dN(k, a, q).
+template <int T, typename S>
+__device__ inline void hex_qp_force(const MatParams& p, const S* du, const S* A, S idet, int q,
+                                    S* fe) {
+  constexpr int d = 3, n = 8;
+  S H[9];
+#pragma unroll
+  for (int i = 0; i < d; ++i)
+#pragma unroll
+    for (int k = 0; k < d; ++k) {
+      S c = 0;
+#pragma unroll
+      for (int a = 1; a < n; ++a) c += du[a * d + i] * dN<T, S>(k, a, q);
+      H[i * d + k] = c;
+    }
+  S g[9];
+#pragma unroll
+  for (int i = 0; i < d; ++i)
+#pragma unroll
+    for (int j = 0; j < d; ++j)
+      g[i * d + j] = (H[i * d] * A[j * d] + H[i * d + 1] * A[j * d + 1] + H[i * d + 2] * A[j * d + 2]) * idet;
+  S P[9];
+  stress_P<d, S>(p, g, P);
+  const S w = S(weight<T>());
+  S Q[9];
+#pragma unroll
+  for (int i = 0; i < d; ++i)
+#pragma unroll
+    for (int k = 0; k < d; ++k)
+      Q[i * d + k] = w * (P[i * d] * A[k] + P[i * d + 1] * A[d + k] + P[i * d + 2] * A[2 * d + k]);
+#pragma unroll
+  for (int a = 0; a < n; ++a)
+#pragma unroll
+    for (int i = 0; i < d; ++i)
+      fe[a * d + i] += Q[i * d] * dN<T, S>(0, a, q) + Q[i * d + 1] * dN<T, S>(1, a, q) +
+                       Q[i * d + 2] * dN<T, S>(2, a, q);
+}
+
 // Element internal force (without the -1 of the assembly):
 // fe[a*d + i] = sum_q w_q det J_q sum_j P_ij dN_a/dx_j.
 // dX[a*d+i] = X_a - X_0, du[a*d+i] = u_a - u_0 (entry a = 0 is zero).
@@ -300,6 +341,69 @@ __device__ inline void element_force(const MatParams& p, const S* dX, const S* d
     simplex_force<T, S>(p, dX, du, fe);
     return;
   }
+  if (T == AKB_HEXAHEDRON_8) {
+    constexpr int d = 3, n = 8, nq = 8;
+#pragma unroll
+    for (int k = 0; k < d * n; ++k) fe[k] = 0;
+    // a parallelepiped (the trilinear terms of x(xi) vanish to 1e-12 of the
+    // element's extent) has one Jacobian at every point: formed once
+    const int sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+    const int sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+    const int sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+    S ext = 0, bend = 0;
+#pragma unroll
+    for (int j = 0; j < d; ++j) {
+      S cxy = 0, cxz = 0, cyz = 0, cxyz = 0;
+#pragma unroll
+      for (int a = 1; a < n; ++a) {
+        const S x = dX[a * d + j];
+        cxy += S(sx[a] * sy[a]) * x;
+        cxz += S(sx[a] * sz[a]) * x;
+        cyz += S(sy[a] * sz[a]) * x;
+        cxyz += S(sx[a] * sy[a] * sz[a]) * x;
+        ext = fmax(ext, fabs(x));
+      }
+      bend = fmax(bend, fmax(fmax(fabs(cxy), fabs(cxz)), fmax(fabs(cyz), fabs(cxyz))));
+    }
+    if (bend <= S(1e-12) * ext) {
+      S J[9];
+#pragma unroll
+      for (int k = 0; k < d; ++k)
+#pragma unroll
+        for (int j = 0; j < d; ++j) {
+          S c = 0;
+#pragma unroll
+          for (int a = 1; a < n; ++a) {
+            const int s = k == 0 ? sx[a] : k == 1 ? sy[a] : sz[a];
+            c += S(0.125 * s) * dX[a * d + j];
+          }
+          J[k * d + j] = c;
+        }
+      S A[9];
+      const S idet = S(1) / adjugate<d, S>(J, A);
+#pragma unroll 1
+      for (int q = 0; q < nq; ++q) hex_qp_force<T, S>(p, du, A, idet, q, fe);
+      return;
+    }
+#pragma unroll 1
+    for (int q = 0; q < nq; ++q) {
+      S J[9];
+#pragma unroll
+      for (int k = 0; k < d; ++k)
+#pragma unroll
+        for (int j = 0; j < d; ++j) {
+          S c = 0;
+#pragma unroll
+          for (int a = 1; a < n; ++a) c += dN<T, S>(k, a, q) * dX[a * d + j];
+          J[k * d + j] = c;
+        }
+      S A[9];
+      const S idet = S(1) / adjugate<d, S>(J, A);
+      hex_qp_force<T, S>(p, du, A, idet, q, fe);
+    }
+    return;
+  }
+  // segment_2: one point, B = +-1 / length
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe, nq = ET<T>::nqp;
 #pragma unroll
   for (int k = 0; k < d * n; ++k) fe[k] = 0;
