@@ -1,0 +1,273 @@
+// Host check of the fused step's patch records (akb_patch_build.cu), no GPU:
+// every shared-memory index the kernel derives from a record stays inside
+// the buffers it addresses, the contribution slots of a chunk are a
+// bijection, the first- and second-level sums reproduce each node's sum of
+// contributions, node positions are distinct, and the coloured accesses (a
+// half-warp's scatter, a half-warp's row of piece sums; 16 bank pairs for
+// 8-byte contributions, 32 banks for 4-byte ones) hit distinct banks.
+// Prints one line per case and exits non-zero on any failure.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <set>
+#include <vector>
+
+#include "akb_patch.cuh"
+
+using namespace akb;
+
+namespace {
+
+struct Mesh {
+  std::vector<double> X;
+  std::vector<uint32_t> C;
+  int dim, nnpe;
+};
+
+Mesh tet_cube(int n) {
+  Mesh m{{}, {}, 3, 4};
+  const int N = n + 1;
+  for (int k = 0; k < N; ++k)
+    for (int j = 0; j < N; ++j)
+      for (int i = 0; i < N; ++i) m.X.insert(m.X.end(), {double(i), double(j), double(k)});
+  auto id = [&](int i, int j, int k) { return (uint32_t)((k * N + j) * N + i); };
+  const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i)
+        for (const auto& p : perm) {
+          int c[3] = {i, j, k};
+          m.C.push_back(id(c[0], c[1], c[2]));
+          for (int s = 0; s < 3; ++s) {
+            c[p[s]]++;
+            m.C.push_back(id(c[0], c[1], c[2]));
+          }
+        }
+  return m;
+}
+
+Mesh hex_cube(int n) {
+  Mesh m{{}, {}, 3, 8};
+  const int N = n + 1;
+  for (int k = 0; k < N; ++k)
+    for (int j = 0; j < N; ++j)
+      for (int i = 0; i < N; ++i) m.X.insert(m.X.end(), {double(i), double(j), double(k)});
+  auto id = [&](int i, int j, int k) { return (uint32_t)((k * N + j) * N + i); };
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i)
+        m.C.insert(m.C.end(), {id(i, j, k), id(i + 1, j, k), id(i + 1, j + 1, k), id(i, j + 1, k),
+                               id(i, j, k + 1), id(i + 1, j, k + 1), id(i + 1, j + 1, k + 1),
+                               id(i, j + 1, k + 1)});
+  return m;
+}
+
+Mesh tri_plate(int nx, int ny) {
+  Mesh m{{}, {}, 2, 3};
+  for (int j = 0; j <= ny; ++j)
+    for (int i = 0; i <= nx; ++i) m.X.insert(m.X.end(), {double(i), double(j)});
+  auto id = [&](int i, int j) { return (uint32_t)(j * (nx + 1) + i); };
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      m.C.insert(m.C.end(), {id(i, j), id(i + 1, j), id(i + 1, j + 1)});
+      m.C.insert(m.C.end(), {id(i, j), id(i + 1, j + 1), id(i, j + 1)});
+    }
+  return m;
+}
+
+Mesh seg_line(int n) {
+  Mesh m{{}, {}, 1, 2};
+  for (int i = 0; i <= n; ++i) m.X.push_back(i);
+  for (int i = 0; i < n; ++i) m.C.insert(m.C.end(), {(uint32_t)i, (uint32_t)i + 1});
+  return m;
+}
+
+// the same mesh with its elements in a scrambled order
+Mesh shuffled(Mesh m, unsigned seed) {
+  srand(seed);
+  const int ne = (int)m.C.size() / m.nnpe;
+  for (int e = ne - 1; e > 0; --e) {
+    const int f = rand() % (e + 1);
+    for (int a = 0; a < m.nnpe; ++a) std::swap(m.C[e * m.nnpe + a], m.C[f * m.nnpe + a]);
+  }
+  return m;
+}
+
+// a star: every element shares node 0 (one node with a long run)
+Mesh star(int k) {
+  Mesh m{{}, {}, 3, 4};
+  m.X.insert(m.X.end(), {0, 0, 0});
+  for (int i = 0; i < k + 2; ++i) m.X.insert(m.X.end(), {std::cos(i * 0.37), std::sin(i * 0.37), i * 0.1});
+  for (int i = 0; i < k; ++i) m.C.insert(m.C.end(), {0u, (uint32_t)i + 1, (uint32_t)i + 2, (uint32_t)i + 3});
+  return m;
+}
+
+size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
+
+int fails = 0;
+#define CHECK(c)                                                                         \
+  do {                                                                                   \
+    if (!(c) && fails++ < 20)                                                            \
+      printf("FAIL %s (line %d, case %s, patch %d, chunk %d)\n", #c, __LINE__, name, p, c_); \
+  } while (0)
+
+long max_group(const std::vector<int>& addr, int banks) {
+  std::vector<std::set<int>> b(banks);
+  for (int x : addr) b[x % banks].insert(x);
+  size_t mx = 0;
+  for (auto& s : b) mx = std::max(mx, s.size());
+  return (long)mx;
+}
+
+void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, int piece) {
+  const int64_t nn = (int64_t)m.X.size() / m.dim, ne = (int64_t)m.C.size() / m.nnpe;
+  PatchHost P = build_patches(m.X.data(), m.C.data(), nn, ne, m.dim, m.nnpe, target, maxn, cbytes,
+                              piece);
+  const int n = m.nnpe, G = cbytes == 8 ? 16 : 32, LM = P.node_stride, CH = P.contrib_slots;
+  long worst_scatter = 0, worst_sum = 0;
+  int p = -1, c_ = -1;
+  std::vector<int> elem_seen(ne, 0);
+  for (p = 0; p < P.npatch; ++p) {
+    c_ = -1;
+    const int nb = P.node_ptr[p], L = P.node_ptr[p + 1] - nb, eb = P.elem_ptr[p];
+    const int nep = P.elem_ptr[p + 1] - eb;
+    CHECK(L <= P.max_nodes && nep > 0);
+    for (int i = eb; i < eb + nep; ++i) elem_seen[P.elem_order[i]]++;
+    std::set<int> ps;
+    for (int j = 0; j < L; ++j) {
+      const int q = P.lpos[nb + j];
+      CHECK(q < 16 * ((L + 15) / 16) && q < LM);
+      ps.insert(q);
+    }
+    CHECK((int)ps.size() == L);
+    const int nch = (nep + kChunk - 1) / kChunk;
+    CHECK(P.chunk_base[p + 1] - P.chunk_base[p] == nch);
+    for (int c = 0; c < nch; ++c) {
+      c_ = c;
+      const ChunkDesc& cd = P.chunks[P.chunk_base[p] + c];
+      CHECK((int)cd.bytes <= P.chunk_bytes && cd.bytes % 16 == 0);
+      CHECK((size_t)cd.off16 * 8 + cd.bytes / 2 <= P.cdata.size());
+      const uint16_t* rec = &P.cdata[(size_t)cd.off16 * 8];
+      const char* rb = (const char*)rec;
+      const int nec = std::min(kChunk, nep - c * kChunk);
+      const size_t A = a16((size_t)nec * n * 2);
+      const uint16_t* lcs = rec + 8;
+      const uint16_t* sl = (const uint16_t*)(rb + 16 + A);
+      const int R1 = rec[0], rows1 = rec[1], ix1 = rec[2], R2 = rec[3], rows2 = rec[4], r2 = rec[5],
+                ix2 = rec[6];
+      CHECK(R1 % 32 == 0 && R2 % 32 == 0 && rows1 <= kMaxPiece && R1 <= P.max_pieces);
+      CHECK(16 + 2 * A + 4 * (size_t)R1 <= (size_t)ix1 && ix1 + 2 * rows1 * R1 <= r2 &&
+            r2 + 4 * R2 <= ix2 && ix2 + 2 * rows2 * R2 <= (int)cd.bytes);
+      const uint32_t* s1 = (const uint32_t*)(rb + 16 + 2 * A);
+      const uint16_t* i1 = (const uint16_t*)(rb + ix1);
+      const uint32_t* s2 = (const uint32_t*)(rb + r2);
+      const uint16_t* i2 = (const uint16_t*)(rb + ix2);
+      // slots: a bijection onto the chunk's corners
+      std::vector<int> owner(CH, -1);
+      for (int k = 0; k < nec * n; ++k) {
+        CHECK(sl[k] < CH && lcs[k] < LM);
+        if (sl[k] < CH) {
+          CHECK(owner[sl[k]] < 0);
+          owner[sl[k]] = k;
+        }
+      }
+      // sums: contribution k = k + 1; the two levels must give every node
+      // the sum of its corners, each contribution read once
+      std::map<int, long> expect, got;
+      for (int k = 0; k < nec * n; ++k) expect[lcs[k]] += k + 1;
+      std::vector<long> val(CH, 0), scratch(std::max(R1, 1), 0);
+      for (int s = 0; s < CH; ++s)
+        if (owner[s] >= 0) val[s] = owner[s] + 1;
+      std::vector<int> reads(CH, 0);
+      for (int q = 0; q < R1; ++q) {
+        const uint32_t w = s1[q];
+        const int len = (w >> 16) & 0xff, jp = w & 0xffff;
+        if (!len) continue;
+        CHECK(len <= rows1 && jp < LM);
+        long f = 0;
+        int prev = -1, first = -1;
+        for (int t = 0; t < len; ++t) {
+          const int s = i1[t * R1 + q];
+          CHECK(s < CH && owner[s] >= 0);
+          if (s >= CH || owner[s] < 0) continue;
+          CHECK(lcs[owner[s]] == jp);       // the run's node
+          CHECK(owner[s] / n >= prev);      // ascending element order
+          prev = owner[s] / n;
+          reads[s]++;
+          f += val[s];
+          if (t == 0) first = s;
+        }
+        if (w >> 24) {
+          if (G == 16)
+            val[first] = f;  // FP64: the piece's sum over its first slot
+          else
+            scratch[q] = f;  // FP32: by piece
+        } else {
+          got[jp] += f;
+        }
+      }
+      for (int s = 0; s < CH; ++s)
+        if (owner[s] >= 0) CHECK(reads[s] == 1);
+      for (int q = 0; q < R2; ++q) {
+        const uint32_t w = s2[q];
+        const int np = w >> 16, jp = w & 0xffff;
+        if (!np) continue;
+        CHECK(np <= rows2 && got.count(jp) == 0);
+        long f = 0;
+        for (int j = 0; j < np; ++j) {
+          const int k = i2[j * R2 + q];
+          if (G == 16) {
+            CHECK(k < CH);
+            if (k < CH) f += val[k];
+          } else {
+            CHECK(k < R1 && (s1[k] >> 24) && (int)(s1[k] & 0xffff) == jp);
+            if (k < R1) f += scratch[k];
+          }
+        }
+        got[jp] += f;
+      }
+      CHECK(got == expect);
+      // colouring: one scatter instruction (corner a of G elements), one row
+      // of G pieces: distinct banks
+      for (int h = 0; h * G < nec; ++h)
+        for (int a = 0; a < n; ++a) {
+          std::vector<int> ad;
+          for (int e = h * G; e < std::min(nec, h * G + G); ++e) ad.push_back(sl[e * n + a]);
+          worst_scatter = std::max(worst_scatter, max_group(ad, G));
+        }
+      for (int h = 0; h * G < R1; ++h)
+        for (int t = 0; t < rows1; ++t) {
+          std::vector<int> ad;
+          for (int q = h * G; q < h * G + G; ++q)
+            if (t < (int)((s1[q] >> 16) & 0xff)) ad.push_back(i1[t * R1 + q]);
+          worst_sum = std::max(worst_sum, max_group(ad, G));
+        }
+    }
+  }
+  p = c_ = -1;
+  for (int64_t e = 0; e < ne; ++e) CHECK(elem_seen[e] == 1);  // every element in one patch
+  CHECK(worst_scatter <= 1 && worst_sum <= 1);
+  printf("%-28s patches %5d max_nodes %4d contrib %4d chunk_bytes %5d worst bank group %ld/%ld\n",
+         name, P.npatch, P.max_nodes, CH, P.chunk_bytes, worst_scatter, worst_sum);
+}
+
+}  // namespace
+
+int main() {
+  check("tet4 cube 20 fp64", tet_cube(20), 1024, 400, 8, 6);
+  check("tet4 cube 20 fp32", tet_cube(20), 768, 320, 4, 6);
+  check("tet4 shuffled fp64", shuffled(tet_cube(12), 1), 1024, 400, 8, 6);
+  check("tet4 shuffled fp32 piece 2", shuffled(tet_cube(12), 2), 1024, 400, 4, 2);
+  check("tet4 odd sizes", tet_cube(7), 300, 150, 8, 6);
+  check("tet4 star", star(300), 1024, 400, 8, 6);
+  check("hex8 cube fp64", hex_cube(16), 512, 800, 8, 8);
+  check("hex8 cube fp32 piece 3", hex_cube(16), 512, 800, 4, 3);
+  check("tri3 plate", tri_plate(200, 20), 1024, 640, 8, 6);
+  check("tri3 plate small patches", tri_plate(200, 20), 256, 200, 8, 6);
+  check("seg2 line fp64", seg_line(3000), 1024, 1100, 8, 2);
+  check("seg2 line fp32 piece 1", seg_line(3000), 1024, 1100, 4, 1);
+  printf("fails %d\n", fails);
+  return fails != 0;
+}
