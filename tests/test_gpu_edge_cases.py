@@ -65,3 +65,38 @@ def test_mesh_without_elements():
     m.setTimeStep(1e-3)
     m.solveSteps(3)
     m.close()
+
+
+def test_dirichlet_arrays_reusable_on_return():
+    """akb_apply_dirichlet queues its update without waiting for it: the
+    caller's arrays are copied before the call returns, so overwriting them
+    at once changes nothing; more calls than staging slots, of growing sizes,
+    in a row."""
+    import ctypes as C
+
+    from akantu_b200._lib import check, lib
+    from akantu_b200.model import SolidMechanicsModel, material_from_dict
+    w = configs.plate_tri3(nx=40, ny=8, lx=1.0, ly=0.2)
+    m = SolidMechanicsModel(w["mesh"], [material_from_dict(mm) for mm in w["materials"]],
+                            precision=_abi.MODE_FP64)
+    m.initFull()
+    nn = w["mesh"].nodes.shape[0]
+    rng = np.random.default_rng(3)
+    expect_u = np.zeros((nn, 2))
+    expect_b = np.zeros((nn, 2), dtype=np.uint8)
+    for call in range(11):
+        nodes = rng.choice(nn, size=5 + 20 * call, replace=False).astype(np.uint32)
+        vals = rng.normal(size=nodes.size)
+        comp = call % 2
+        expect_u[nodes, comp] = vals
+        expect_b[nodes, comp] = 1
+        check(lib().akb_apply_dirichlet(m.handle, nodes.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                        nodes.size, comp,
+                                        vals.ctypes.data_as(C.POINTER(C.c_double))))
+        nodes[:] = 0            # the caller reuses its arrays right away
+        vals[:] = np.nan
+    u = np.array(m.getDisplacement())
+    b = np.array(m.getBlockedDOFs(), dtype=np.uint8).reshape(-1, 2)
+    assert np.array_equal(b, expect_b)
+    assert np.array_equal(u[expect_b.astype(bool)], expect_u[expect_b.astype(bool)])
+    m.close()
