@@ -32,6 +32,7 @@ SIGNATURES = {
     "akb_set_field": (I32, [P, I32, PD, I64]),
     "akb_get_field": (I32, [P, I32, PD, I64]),
     "akb_field_device_pointer": (I32, [P, I32, C.POINTER(P)]),
+    "akb_get_node_numbering": (I32, [P, PU32, I64]),
     "akb_set_blocked_dofs": (I32, [P, PU8, I64]),
     "akb_get_blocked_dofs": (I32, [P, PU8, I64]),
     "akb_assemble_mass_lumped": (I32, [P]),

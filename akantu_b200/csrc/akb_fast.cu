@@ -172,21 +172,24 @@ __global__ void k_qp_forces(DevModel m) {
 }
 
 __global__ void k_apply_dirichlet(DevModel m, const uint32_t* nodes, int64_t n, int comp,
-                                  const double* values) {
+                                  const double* values, const uint32_t* perm, double* w) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (k >= n) return;
-  const uint32_t node = nodes[k];
+  uint32_t node = nodes[k];
   if (node >= m.nn) return;  // out-of-range node ids are ignored
+  if (perm) node = perm[node];
   const int64_t i = (int64_t)node * m.dim + comp;
   m.blocked[i] = 1;
   m.u[i] = values[k];
+  if (w) w[i] = values[k];  // a blocked DOF's predicted displacement is its u
 }
 
 }  // namespace
 
 cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n, int comp,
-                            const double* values, cudaStream_t s) {
-  k_apply_dirichlet<<<blocks_for(n), kThreads, 0, s>>>(m, nodes, n, comp, values);
+                            const double* values, const uint32_t* perm, double* w,
+                            cudaStream_t s) {
+  k_apply_dirichlet<<<blocks_for(n), kThreads, 0, s>>>(m, nodes, n, comp, values, perm, w);
   return cudaGetLastError();
 }
 

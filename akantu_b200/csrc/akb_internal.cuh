@@ -83,9 +83,12 @@ cudaError_t fast_gather_correct(const DevModel& m, double dt, bool fp32, bool co
 cudaError_t user_qp_gradients(const DevModel& m, cudaStream_t s);
 cudaError_t user_element_forces(const DevModel& m, cudaStream_t s);
 
-// Dirichlet values (akb_fast.cu): blocked[node][comp] = 1, u[node][comp] = value.
+// Dirichlet values (akb_fast.cu): blocked[node][comp] = 1, u[node][comp] = value
+// (and the predicted displacement w, when the model keeps one); perm (or
+// null) maps the caller's node ids to the model's internal order.
 cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n, int comp,
-                            const double* values, cudaStream_t s);
+                            const double* values, const uint32_t* perm, double* w,
+                            cudaStream_t s);
 
 // Reductions (akb_reduce.cu). Scratch holds per-block partial results.
 cudaError_t stable_dt(const DevModel& m, double* d_scratch, int scratch_len,

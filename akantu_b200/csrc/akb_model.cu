@@ -1,5 +1,6 @@
 // akb_model.cu -- the C ABI of include/akb.h: model lifecycle, fields, the
 // explicit step driver and its CUDA-graph replay.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -78,13 +79,23 @@ struct akb_model {
   static constexpr int kBcSlots = 4;
   BcSlot bc[kBcSlots];
   int bc_next = 0;
-  // part of a partitioned mesh (akb_model_create_part): its interface nodes,
-  // finished only once their forces are summed over all parts
+  // part of a partitioned mesh (akb_model_create_part): its interface nodes
+  // (shared nodes of the patch plan), finished only once their forces are
+  // summed over all parts
   bool part = false;
   bool part_in_step = false;
   int64_t n_iface = 0;
-  const uint32_t* d_iface_s = nullptr;  // shared-node index of each interface node
-  const uint32_t* d_iface_g = nullptr;  // node id of each interface node
+  const uint32_t* d_iface_g = nullptr;     // internal id of each interface node
+  const uint32_t* d_iface_part = nullptr;  // its first partial slot
+  const uint32_t* d_iface_k = nullptr;     // its partial count
+  // internal node order of the fused step (akb_patch.cuh): perm[caller's id]
+  // = internal id; nodal arrays crossing the C ABI are reordered through
+  // d_tmp. Without patches the order is the caller's (d_perm null).
+  const uint32_t* d_perm = nullptr;
+  std::vector<uint32_t> perm;
+  double* d_tmp = nullptr;
+  // the predicted displacement of the fused step is current
+  bool w_valid = false;
 };
 
 // Interface nodes of a part, in the caller's order.
@@ -155,7 +166,7 @@ inline void mark(StepTimer* t, cudaStream_t s) {
 
 const char* const kRefKernels[] = {"ref_predictor", "ref_element_forces", "ref_gather_correct"};
 const char* const kFastKernels[] = {"fast_predictor", "fast_element_forces", "fast_gather_correct"};
-const char* const kPatchKernels[] = {"patch_step", "patch_shared_nodes"};
+const char* const kPatchKernels[] = {"patch_step", "patch_finish_list"};
 
 // One NonLinearSolverLumped::solve.
 cudaError_t enqueue_step(akb_model* m, StepTimer* t = nullptr) {
@@ -176,7 +187,7 @@ cudaError_t enqueue_step(akb_model* m, StepTimer* t = nullptr) {
     if ((e = patch_step(d, m->patches, m->dt, fp32(m), m->has_fext, m->stream)) != cudaSuccess)
       return e;
     mark(t, m->stream);
-    e = patch_shared_nodes(d, m->patches, m->dt, m->has_fext, m->stream);
+    e = patch_finish_list(d, m->patches, m->dt, m->has_fext, m->stream);
     mark(t, m->stream);
     return e;
   }
@@ -213,9 +224,15 @@ void patch_params(int type, int* target, int* max_nodes, int* piece) {
 template <typename T>
 akb_status upload(akb_model* m, const std::vector<T>& v, const T** out);
 
-akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
-                                const uint32_t* element_material, const BatchLayout* batch,
-                                const PartLayout* part) {
+// Patch plan of the fused step on the host (mesh in the caller's node
+// order): a single mesh, a partitioned part (its interface nodes forced to
+// be finished outside the fused step), or a batch (patches built per
+// instance, so that no patch spans two instances, and concatenated).
+// patch_inst / orphan_inst: the instance of each patch and node of no
+// element (batches only).
+akb_status plan_patches(akb_model* m, const akb_mesh_desc* mesh, const BatchLayout* batch,
+                        const PartLayout* part, PatchHost& P, std::vector<uint32_t>& patch_inst,
+                        std::vector<uint32_t>& orphan_inst) {
   int target, max_nodes, piece;
   patch_params(m->dm.type, &target, &max_nodes, &piece);
   if (fp32(m) && m->dm.type == AKB_TETRAHEDRON_4) {
@@ -246,8 +263,6 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
   if (m->opt_patch_elements > 0) target = std::min(m->opt_patch_elements, 8191);
   if (m->opt_patch_nodes > 0) max_nodes = std::min(m->opt_patch_nodes, 60000);
   const int cbytes = fp32(m) ? 4 : 8;  // element vector precision
-  PatchHost P;
-  std::vector<uint32_t> patch_inst, snode_inst;
   try {
     if (!batch) {
       std::vector<uint8_t> force;
@@ -258,73 +273,89 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
       P = build_patches(mesh->nodes, mesh->connectivity, mesh->nb_nodes, mesh->nb_elements,
                         m->dm.dim, m->dm.nnpe, target, max_nodes, cbytes, piece,
                         part ? force.data() : nullptr);
-    } else {
-      // one instance at a time, so no patch spans two instances; the union is
-      // the concatenation of the instances' patches
-      const int dd = m->dm.dim, nn_ = m->dm.nnpe;
-      P.elem_ptr.push_back(0);
-      P.node_ptr.push_back(0);
-      P.sptr.push_back(0);
-      std::vector<uint32_t> lconn;
-      for (int i = 0; i < batch->ninst; ++i) {
-        const int64_t n0 = batch->node_off[i], e0 = batch->elem_off[i];
-        const int64_t nni = batch->node_off[i + 1] - n0, nei = batch->elem_off[i + 1] - e0;
-        lconn.assign(mesh->connectivity + e0 * nn_, mesh->connectivity + (e0 + nei) * nn_);
-        for (auto& c : lconn) c -= (uint32_t)n0;
-        PatchHost Q = build_patches(mesh->nodes + n0 * dd, lconn.data(), nni, nei, dd, nn_,
-                                    target, max_nodes, cbytes, piece);
-        const int64_t lbase = (int64_t)P.lnodes.size(), sbase = P.nslots;
-        const int64_t chbase = (int64_t)P.chunks.size();
-        const uint32_t dbase16 = (uint32_t)(P.cdata.size() / 8);
-        for (int p = 0; p < Q.npatch; ++p) {
-          P.elem_ptr.push_back((int32_t)(e0 + Q.elem_ptr[p + 1]));
-          P.node_ptr.push_back((int32_t)(lbase + Q.node_ptr[p + 1]));
-          P.chunk_base.push_back((int32_t)(chbase + Q.chunk_base[p]));
-          patch_inst.push_back((uint32_t)i);
-        }
-        P.npatch += Q.npatch;
-        P.max_nodes = std::max(P.max_nodes, Q.max_nodes);
-        P.node_stride = std::max(P.node_stride, Q.node_stride);
-        P.contrib_slots = std::max(P.contrib_slots, Q.contrib_slots);
-        P.max_pieces = std::max(P.max_pieces, Q.max_pieces);
-        P.chunk_bytes = std::max(P.chunk_bytes, Q.chunk_bytes);
-        P.ninterior.insert(P.ninterior.end(), Q.ninterior.begin(), Q.ninterior.end());
-        for (auto g : Q.lnodes) P.lnodes.push_back((uint32_t)(g + n0));
-        P.lpos.insert(P.lpos.end(), Q.lpos.begin(), Q.lpos.end());
-        for (auto e : Q.elem_order) P.elem_order.push_back((uint32_t)(e + e0));
-        for (auto c : Q.chunks) {
-          c.off16 += dbase16;
-          P.chunks.push_back(c);
-        }
-        P.cdata.insert(P.cdata.end(), Q.cdata.begin(), Q.cdata.end());
-        for (auto s : Q.slot) P.slot.push_back(s == 0xffffffffu ? s : (uint32_t)(s + sbase));
-        for (auto g : Q.snodes) {
-          P.snodes.push_back((uint32_t)(g + n0));
-          snode_inst.push_back((uint32_t)i);
-        }
-        for (size_t k = 1; k < Q.sptr.size(); ++k) P.sptr.push_back((int32_t)(Q.sptr[k] + sbase));
-        P.nslots += Q.nslots;
-      }
-      P.chunk_base.push_back((int32_t)P.chunks.size());
+      return AKB_OK;
     }
+    const int dd = m->dm.dim, nn_ = m->dm.nnpe;
+    P = PatchHost{};
+    P.elem_ptr.push_back(0);
+    P.sh_ptr.push_back(0);
+    std::vector<uint32_t> lconn;
+    for (int i = 0; i < batch->ninst; ++i) {
+      const int64_t n0 = batch->node_off[i], e0 = batch->elem_off[i];
+      const int64_t nni = batch->node_off[i + 1] - n0, nei = batch->elem_off[i + 1] - e0;
+      lconn.assign(mesh->connectivity + e0 * nn_, mesh->connectivity + (e0 + nei) * nn_);
+      for (auto& c : lconn) c -= (uint32_t)n0;
+      PatchHost Q = build_patches(mesh->nodes + n0 * dd, lconn.data(), nni, nei, dd, nn_, target,
+                                  max_nodes, cbytes, piece);
+      const int64_t ebase = (int64_t)P.sgid.size(), sbase = P.nslots;
+      const int64_t chbase = (int64_t)P.chunks.size();
+      const uint32_t dbase16 = (uint32_t)(P.cdata.size() / 8);
+      for (int p = 0; p < Q.npatch; ++p) {
+        P.elem_ptr.push_back((int32_t)(e0 + Q.elem_ptr[p + 1]));
+        P.ibeg.push_back((int32_t)(n0 + Q.ibeg[p]));
+        P.nint.push_back(Q.nint[p]);
+        P.sh_ptr.push_back((int32_t)(ebase + Q.sh_ptr[p + 1]));
+        P.chunk_base.push_back((int32_t)(chbase + Q.chunk_base[p]));
+        patch_inst.push_back((uint32_t)i);
+      }
+      P.npatch += Q.npatch;
+      P.max_nodes = std::max(P.max_nodes, Q.max_nodes);
+      P.max_interior = std::max(P.max_interior, Q.max_interior);
+      P.max_shared = std::max(P.max_shared, Q.max_shared);
+      P.contrib_slots = std::max(P.contrib_slots, Q.contrib_slots);
+      P.max_pieces = std::max(P.max_pieces, Q.max_pieces);
+      P.chunk_bytes = std::max(P.chunk_bytes, Q.chunk_bytes);
+      for (auto g : Q.perm) P.perm.push_back((uint32_t)(g + n0));
+      for (auto e : Q.elem_order) P.elem_order.push_back((uint32_t)(e + e0));
+      for (auto g : Q.sgid) P.sgid.push_back((uint32_t)(g + n0));
+      for (auto v : Q.sslot) P.sslot.push_back((uint32_t)(v + sbase));
+      for (auto c : Q.chunks) {
+        c.off16 += dbase16;
+        P.chunks.push_back(c);
+      }
+      P.cdata.insert(P.cdata.end(), Q.cdata.begin(), Q.cdata.end());
+      for (auto g : Q.shared_nodes) P.shared_nodes.push_back((uint32_t)(g + n0));
+      for (auto v : Q.shared_part) P.shared_part.push_back((uint32_t)(v + sbase));
+      P.shared_k.insert(P.shared_k.end(), Q.shared_k.begin(), Q.shared_k.end());
+      for (auto g : Q.orphans) {
+        P.orphans.push_back((uint32_t)(g + n0));
+        orphan_inst.push_back((uint32_t)i);
+      }
+      P.nslots += Q.nslots;
+    }
+    P.chunk_base.push_back((int32_t)P.chunks.size());
+    P.node_stride = (P.max_nodes + kBankPairs - 1) / kBankPairs * kBankPairs + 5;
   } catch (const std::exception& ex) {
     return fail(AKB_ERR_UNSUPPORTED, std::string("patch construction: ") + ex.what());
   }
+  return AKB_OK;
+}
+
+// Device copy of a patch plan; the model's arrays are already in the plan's
+// internal node order.
+akb_status build_device_patches(akb_model* m, const PatchHost& P,
+                                const std::vector<uint32_t>& patch_inst,
+                                const std::vector<uint32_t>& orphan_inst,
+                                const uint32_t* element_material, const BatchLayout* batch,
+                                const PartLayout* part) {
   DevPatches& d = m->patches;
+  d = DevPatches{};
   d.npatch = P.npatch;
   d.grid = m->opt_patch_grid > 0 ? m->opt_patch_grid : 0;
   d.max_nodes = P.max_nodes;
+  d.max_shared = P.max_shared;
   d.node_stride = P.node_stride;
   d.contrib_slots = P.contrib_slots;
   d.max_pieces = P.max_pieces;
   d.chunk_bytes = P.chunk_bytes;
-  d.nshared = (int64_t)P.snodes.size();
   akb_status st;
   if ((st = upload(m, P.elem_ptr, &d.elem_ptr)) != AKB_OK) return st;
-  if ((st = upload(m, P.node_ptr, &d.node_ptr)) != AKB_OK) return st;
-  if ((st = upload(m, P.ninterior, &d.ninterior)) != AKB_OK) return st;
-  if ((st = upload(m, P.lnodes, &d.lnodes)) != AKB_OK) return st;
-  if ((st = upload(m, P.lpos, &d.lpos)) != AKB_OK) return st;
+  if ((st = upload(m, P.ibeg, &d.ibeg)) != AKB_OK) return st;
+  if ((st = upload(m, P.nint, &d.nint)) != AKB_OK) return st;
+  if ((st = upload(m, P.sh_ptr, &d.sh_ptr)) != AKB_OK) return st;
+  if ((st = upload(m, P.sgid, &d.sgid)) != AKB_OK) return st;
+  if ((st = upload(m, P.sslot, &d.sslot)) != AKB_OK) return st;
+
   if ((st = upload(m, P.chunk_base, &d.chunk_base)) != AKB_OK) return st;
   if ((st = upload(m, P.cdata, &d.cdata)) != AKB_OK) return st;
   {
@@ -333,43 +364,40 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
     std::memcpy(cd.data(), P.chunks.data(), cd.size() * sizeof(uint2));
     if ((st = upload(m, cd, &d.chunks)) != AKB_OK) return st;
   }
-  // partial slots of the shared nodes: each has at least two partials (an
-  // orphan node none), so the first two of every shared node sit in two dense
-  // rows indexed by shared node, read coalesced by k_shared_nodes, and the
-  // others after them, node-major; sptr becomes the CSR of those others.
-  // Orphan nodes read two partials that stay zero.
-  {
-    const int64_t ns = (int64_t)P.snodes.size();
-    std::vector<int32_t> ovf(ns + 1, 0);
-    for (int64_t q = 0; q < ns; ++q) ovf[q + 1] = ovf[q] + std::max(0, P.sptr[q + 1] - P.sptr[q] - 2);
-    std::vector<int32_t> owner((size_t)P.nslots);
-    for (int64_t q = 0; q < ns; ++q)
-      for (int32_t v = P.sptr[q]; v < P.sptr[q + 1]; ++v) owner[v] = (int32_t)q;
-    for (auto& v : P.slot) {
-      if (v == 0xffffffffu) continue;
-      const int64_t q = owner[v], k = (int64_t)v - P.sptr[q];
-      v = (uint32_t)(k < 2 ? k * ns + q : 2 * ns + ovf[q] + (k - 2));
+  // nodes finished by k_finish_list: the nodes of no element, then the
+  // shared nodes (in internal order: their partial slots are consecutive)
+  std::vector<uint32_t> lg(P.orphans), lp(P.orphans.size(), 0), lk(P.orphans.size(), 0);
+  std::vector<uint32_t> li(orphan_inst);
+  lg.insert(lg.end(), P.shared_nodes.begin(), P.shared_nodes.end());
+  lp.insert(lp.end(), P.shared_part.begin(), P.shared_part.end());
+  lk.insert(lk.end(), P.shared_k.begin(), P.shared_k.end());
+  if (batch) {  // instance of each shared node: instances own contiguous node ranges
+    for (uint32_t g : P.shared_nodes) {
+      const auto it = std::upper_bound(batch->node_off.begin(), batch->node_off.end(), (int64_t)g);
+      li.push_back((uint32_t)(it - batch->node_off.begin() - 1));
     }
-    P.sptr.swap(ovf);
-    P.nslots = 2 * ns + P.sptr[ns];
   }
-  if ((st = upload(m, P.slot, &d.slot)) != AKB_OK) return st;
-  if ((st = upload(m, P.snodes, &d.snodes)) != AKB_OK) return st;
-  if (part) {  // each interface node's index among the shared nodes
-    std::vector<uint32_t> is(part->n), ig(part->n);
+  if (part) {
+    std::vector<uint32_t> ig(part->n), ip(part->n), ik(part->n);
     for (int64_t i = 0; i < part->n; ++i) {
-      const auto it = std::lower_bound(P.snodes.begin(), P.snodes.end(), part->nodes[i]);
-      if (it == P.snodes.end() || *it != part->nodes[i])
-        return fail(AKB_ERR_INVALID_ARGUMENT, "interface node is not a shared node");
-      is[i] = (uint32_t)(it - P.snodes.begin());
-      ig[i] = part->nodes[i];
+      const uint32_t g = P.perm[part->nodes[i]];
+      const int64_t s = (int64_t)g - P.shared_base;
+      if (s < 0 || s >= (int64_t)P.shared_nodes.size() || P.shared_nodes[s] != g)
+        return fail(AKB_ERR_INVALID_ARGUMENT, "interface node is not a node of an element");
+      ig[i] = g;
+      ip[i] = P.shared_part[s];
+      ik[i] = P.shared_k[s];
     }
-    if ((st = upload(m, is, &m->d_iface_s)) != AKB_OK) return st;
     if ((st = upload(m, ig, &m->d_iface_g)) != AKB_OK) return st;
+    if ((st = upload(m, ip, &m->d_iface_part)) != AKB_OK) return st;
+    if ((st = upload(m, ik, &m->d_iface_k)) != AKB_OK) return st;
     m->n_iface = part->n;
     m->part = true;
   }
-  if ((st = upload(m, P.sptr, &d.sptr)) != AKB_OK) return st;
+  d.nlist = (int64_t)lg.size();
+  if ((st = upload(m, lg, &d.list_gid)) != AKB_OK) return st;
+  if ((st = upload(m, lp, &d.list_part)) != AKB_OK) return st;
+  if ((st = upload(m, lk, &d.list_k)) != AKB_OK) return st;
   {
     int* e;
     if ((st = dalloc(m, &e, 1)) != AKB_OK) return st;
@@ -382,21 +410,28 @@ akb_status build_device_patches(akb_model* m, const akb_mesh_desc* mesh,
     for (size_t i = 0; i < em.size(); ++i) em[i] = element_material[P.elem_order[i]];
     if ((st = upload(m, em, &d.emat)) != AKB_OK) return st;
   }
-  if ((st = dalloc(m, &d.partial, (size_t)std::max<int64_t>(P.nslots, 1) * m->dm.dim)) != AKB_OK)
-    return st;
-  AKB_CUDA_TRY(cudaMemsetAsync(d.partial, 0,
-                               (size_t)std::max<int64_t>(P.nslots, 1) * m->dm.dim * sizeof(double),
+  const size_t nsl = (size_t)std::max<int64_t>(P.nslots, 1);
+  if ((st = dalloc(m, &d.partial, nsl * m->dm.dim)) != AKB_OK) return st;
+  AKB_CUDA_TRY(cudaMemsetAsync(d.partial, 0, nsl * m->dm.dim * sizeof(double), m->stream));
+  // predicted displacement, with the slack of the other nodal arrays
+  if ((st = dalloc(m, &d.w, (size_t)m->dm.nn * m->dm.dim + 2)) != AKB_OK) return st;
+  AKB_CUDA_TRY(cudaMemsetAsync(d.w, 0, ((size_t)m->dm.nn * m->dm.dim + 2) * sizeof(double),
                                m->stream));
+  m->w_valid = false;
+  if ((st = upload(m, P.perm, &m->d_perm)) != AKB_OK) return st;
+  m->perm = P.perm;
   d.inst_dt = nullptr;
   d.patch_inst = nullptr;
-  d.snode_inst = nullptr;
+  d.list_inst = nullptr;
+  d.node_off = nullptr;
+  d.ninst = 0;
   if (batch) {
     if ((st = upload(m, patch_inst, &d.patch_inst)) != AKB_OK) return st;
-    if ((st = upload(m, snode_inst, &d.snode_inst)) != AKB_OK) return st;
+    if ((st = upload(m, li, &d.list_inst)) != AKB_OK) return st;
   }
   AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));  // host vectors go out of scope
   d.nbuf = patch_buffers(d, m->dm.type, fp32(m));
-  const size_t smem = patch_smem_bytes(d, m->dm.dim, m->dm.nnpe, fp32(m), d.nbuf);
+  const size_t smem = patch_smem_bytes(d, m->dm.dim, fp32(m), d.nbuf);
   if (smem > 227 * 1024)
     return fail(AKB_ERR_UNSUPPORTED, "patch does not fit in shared memory");
   AKB_CUDA_TRY(patch_configure(m->dm, d, fp32(m)));
@@ -480,6 +515,23 @@ int64_t field_count(const akb_model* m, int32_t field) {
   if (field == AKB_FIELD_GRAD_U || field == AKB_FIELD_STRESS)
     return m->dm.ne * m->dm.nqp * m->dm.dim * m->dm.dim;
   return m->dm.nn * m->dm.dim;
+}
+
+bool nodal(int32_t field) { return field != AKB_FIELD_GRAD_U && field != AKB_FIELD_STRESS; }
+
+// Staging buffer of the reordered copies (nn x dim doubles).
+akb_status ensure_tmp(akb_model* m) {
+  if (m->d_tmp) return AKB_OK;
+  return dalloc(m, &m->d_tmp, (size_t)m->dm.nn * m->dm.dim);
+}
+
+// The predicted displacement w = u + dt v + dt^2/2 a of the fused step,
+// recomputed after the caller changed u, v, a, the blocked DOFs or dt.
+akb_status ensure_w(akb_model* m) {
+  if (!m->use_patches || m->w_valid) return AKB_OK;
+  AKB_CUDA_TRY(patch_refresh_w(m->dm, m->patches, m->dt, m->stream));
+  m->w_valid = true;
+  return AKB_OK;
 }
 
 }  // namespace
@@ -614,19 +666,42 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
   }
 
   const size_t ndof = (size_t)nn * d;
+  // the fused step of the fast modes works on the mesh in its own node order
+  // (akb_patch.cuh): plan the patches first, then store X and the
+  // connectivity renumbered
+  const bool patched = m->mode != AKB_MODE_FP64_REFERENCE && !m->user && ne > 0;
+  PatchHost plan;
+  std::vector<uint32_t> patch_inst, orphan_inst;
+  std::vector<double> Xr;
+  std::vector<uint32_t> Cr;
+  const double* mesh_X = mesh->nodes;
+  const uint32_t* mesh_C = mesh->connectivity;
+  if (patched) {
+    if ((st = plan_patches(m.get(), mesh, batch, part, plan, patch_inst, orphan_inst)) != AKB_OK)
+      return st;
+    Xr.resize(ndof);
+    for (int64_t i = 0; i < nn; ++i)
+      for (int c = 0; c < d; ++c) Xr[(size_t)plan.perm[i] * d + c] = mesh->nodes[i * d + c];
+    Cr.resize((size_t)ne * n);
+    for (int64_t k = 0; k < ne * n; ++k) Cr[k] = plan.perm[mesh->connectivity[k]];
+    mesh_X = Xr.data();
+    mesh_C = Cr.data();
+  }
   double* X;
   uint32_t* conn;
-  if ((st = dalloc(m.get(), &X, ndof)) != AKB_OK) return st;
+  // nodal arrays carry 16 bytes of slack at their end: the fused step's bulk
+  // copies and L2 prefetches round node ranges out to 16 bytes
+  if ((st = dalloc(m.get(), &X, ndof + 2)) != AKB_OK) return st;
   if ((st = dalloc(m.get(), &conn, (size_t)ne * n)) != AKB_OK) return st;
   dm.X = X;
   dm.conn = conn;
   for (double** f : {&dm.u, &dm.v, &dm.a, &dm.fext, &dm.fint, &dm.mass})
-    if ((st = dalloc(m.get(), f, ndof)) != AKB_OK) return st;
-  if ((st = dalloc(m.get(), &dm.inv_mass, nn)) != AKB_OK) return st;
-  if ((st = dalloc(m.get(), &dm.blocked, ndof)) != AKB_OK) return st;
-  AKB_CUDA_TRY(cudaMemcpyAsync(X, mesh->nodes, ndof * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+    if ((st = dalloc(m.get(), f, ndof + 2)) != AKB_OK) return st;
+  if ((st = dalloc(m.get(), &dm.inv_mass, nn + 2)) != AKB_OK) return st;
+  if ((st = dalloc(m.get(), &dm.blocked, ndof + 16)) != AKB_OK) return st;
+  AKB_CUDA_TRY(cudaMemcpyAsync(X, mesh_X, ndof * sizeof(double), cudaMemcpyHostToDevice, m->stream));
   if (ne > 0)
-    AKB_CUDA_TRY(cudaMemcpyAsync(conn, mesh->connectivity, (size_t)ne * n * sizeof(uint32_t),
+    AKB_CUDA_TRY(cudaMemcpyAsync(conn, mesh_C, (size_t)ne * n * sizeof(uint32_t),
                                  cudaMemcpyHostToDevice, m->stream));
   for (double* f : {dm.u, dm.v, dm.a, dm.fext, dm.fint, dm.mass})
     AKB_CUDA_TRY(cudaMemsetAsync(f, 0, ndof * sizeof(double), m->stream));
@@ -642,10 +717,10 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
   // which DOFManager::assembleElementalArrayLocalArray adds element vectors.
   {
     std::vector<int32_t> ptr(nn + 1, 0), ent((size_t)ne * n);
-    for (int64_t k = 0; k < ne * n; ++k) ptr[mesh->connectivity[k] + 1]++;
+    for (int64_t k = 0; k < ne * n; ++k) ptr[mesh_C[k] + 1]++;
     for (int64_t i = 0; i < nn; ++i) ptr[i + 1] += ptr[i];
     std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
-    for (int64_t k = 0; k < ne * n; ++k) ent[fill[mesh->connectivity[k]]++] = (int32_t)k;
+    for (int64_t k = 0; k < ne * n; ++k) ent[fill[mesh_C[k]]++] = (int32_t)k;
     int32_t *dptr, *dent;
     if ((st = dalloc(m.get(), &dptr, nn + 1)) != AKB_OK) return st;
     if ((st = dalloc(m.get(), &dent, (size_t)ne * n)) != AKB_OK) return st;
@@ -693,8 +768,9 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
   if (m->user) {
     if ((st = ensure_stress_arrays(m.get())) != AKB_OK) return st;
     AKB_CUDA_TRY(cudaMemsetAsync(dm.stress, 0, (size_t)ne * q * d * d * sizeof(double), m->stream));
-  } else if (m->mode != AKB_MODE_FP64_REFERENCE && ne > 0) {
-    if ((st = build_device_patches(m.get(), mesh, element_material, batch, part)) != AKB_OK)
+  } else if (patched) {
+    if ((st = build_device_patches(m.get(), plan, patch_inst, orphan_inst, element_material, batch,
+                                   part)) != AKB_OK)
       return st;
   }
   if (batch) {
@@ -706,6 +782,8 @@ static akb_status create_model(const akb_mesh_desc* mesh, int32_t nb_materials,
     if ((st = upload(m.get(), batch->elem_off, &m->d_elem_off)) != AKB_OK) return st;
     if ((st = upload(m.get(), batch->node_off, &m->d_node_off)) != AKB_OK) return st;
     m->patches.inst_dt = m->d_inst_dt;
+    m->patches.node_off = m->d_node_off;
+    m->patches.ninst = batch->ninst;
     m->dt = 1.0;  // the step reads the instances' time steps from the device
     AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
   }
@@ -758,8 +836,17 @@ akb_status akb_set_field(akb_model* m, int32_t field, const double* values, int6
   if (!values || count != field_count(m, field))
     return fail(AKB_ERR_INVALID_ARGUMENT, "wrong number of values");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
-  AKB_CUDA_TRY(cudaMemcpyAsync(field_ptr(m, field), values, count * sizeof(double),
-                               cudaMemcpyHostToDevice, m->stream));
+  if (m->d_perm) {  // into the model's node order
+    if ((st = ensure_tmp(m)) != AKB_OK) return st;
+    AKB_CUDA_TRY(cudaMemcpyAsync(m->d_tmp, values, count * sizeof(double), cudaMemcpyHostToDevice,
+                                 m->stream));
+    AKB_CUDA_TRY(permute_rows(m->d_perm, m->dm.nn, m->dm.dim, m->d_tmp, field_ptr(m, field), true,
+                              m->stream));
+  } else {
+    AKB_CUDA_TRY(cudaMemcpyAsync(field_ptr(m, field), values, count * sizeof(double),
+                                 cudaMemcpyHostToDevice, m->stream));
+  }
+  if (field != AKB_FIELD_EXTERNAL_FORCE) m->w_valid = false;
   if (field == AKB_FIELD_DISPLACEMENT) {
     m->fint_valid = false;
     m->stresses_valid = false;
@@ -787,8 +874,16 @@ akb_status akb_get_field(akb_model* m, int32_t field, double* values, int64_t co
   if ((field == AKB_FIELD_GRAD_U || field == AKB_FIELD_STRESS) && !m->stresses_valid && !m->user) {
     if ((st = akb_compute_stresses(m)) != AKB_OK) return st;
   }
-  AKB_CUDA_TRY(cudaMemcpyAsync(values, field_ptr(m, field), count * sizeof(double),
-                               cudaMemcpyDeviceToHost, m->stream));
+  if (m->d_perm && nodal(field)) {  // back to the caller's node order
+    if ((st = ensure_tmp(m)) != AKB_OK) return st;
+    AKB_CUDA_TRY(permute_rows(m->d_perm, m->dm.nn, m->dm.dim, field_ptr(m, field), m->d_tmp,
+                              false, m->stream));
+    AKB_CUDA_TRY(cudaMemcpyAsync(values, m->d_tmp, count * sizeof(double), cudaMemcpyDeviceToHost,
+                                 m->stream));
+  } else {
+    AKB_CUDA_TRY(cudaMemcpyAsync(values, field_ptr(m, field), count * sizeof(double),
+                                 cudaMemcpyDeviceToHost, m->stream));
+  }
   return sync(m);
 }
 
@@ -804,13 +899,29 @@ akb_status akb_field_device_pointer(akb_model* m, int32_t field, void** dptr) {
   return AKB_OK;
 }
 
+akb_status akb_get_node_numbering(const akb_model* m, uint32_t* row_of_node, int64_t count) {
+  if (!m || !row_of_node) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (count != m->dm.nn) return fail(AKB_ERR_INVALID_ARGUMENT, "wrong number of values");
+  for (int64_t i = 0; i < count; ++i)
+    row_of_node[i] = m->perm.empty() ? (uint32_t)i : m->perm[i];
+  return AKB_OK;
+}
+
 akb_status akb_set_blocked_dofs(akb_model* m, const uint8_t* blocked, int64_t count) {
   akb_status st;
   if ((st = check_model(m)) != AKB_OK) return st;
   if (!blocked || count != m->dm.nn * m->dm.dim)
     return fail(AKB_ERR_INVALID_ARGUMENT, "wrong number of values");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
-  AKB_CUDA_TRY(cudaMemcpyAsync(m->dm.blocked, blocked, count, cudaMemcpyHostToDevice, m->stream));
+  if (m->d_perm) {
+    if ((st = ensure_tmp(m)) != AKB_OK) return st;
+    uint8_t* t = reinterpret_cast<uint8_t*>(m->d_tmp);
+    AKB_CUDA_TRY(cudaMemcpyAsync(t, blocked, count, cudaMemcpyHostToDevice, m->stream));
+    AKB_CUDA_TRY(permute_rows_u8(m->d_perm, m->dm.nn, m->dm.dim, t, m->dm.blocked, true, m->stream));
+  } else {
+    AKB_CUDA_TRY(cudaMemcpyAsync(m->dm.blocked, blocked, count, cudaMemcpyHostToDevice, m->stream));
+  }
+  m->w_valid = false;
   return sync(m);
 }
 
@@ -820,7 +931,14 @@ akb_status akb_get_blocked_dofs(akb_model* m, uint8_t* blocked, int64_t count) {
   if (!blocked || count != m->dm.nn * m->dm.dim)
     return fail(AKB_ERR_INVALID_ARGUMENT, "wrong number of values");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
-  AKB_CUDA_TRY(cudaMemcpyAsync(blocked, m->dm.blocked, count, cudaMemcpyDeviceToHost, m->stream));
+  if (m->d_perm) {
+    if ((st = ensure_tmp(m)) != AKB_OK) return st;
+    uint8_t* t = reinterpret_cast<uint8_t*>(m->d_tmp);
+    AKB_CUDA_TRY(permute_rows_u8(m->d_perm, m->dm.nn, m->dm.dim, m->dm.blocked, t, false, m->stream));
+    AKB_CUDA_TRY(cudaMemcpyAsync(blocked, t, count, cudaMemcpyDeviceToHost, m->stream));
+  } else {
+    AKB_CUDA_TRY(cudaMemcpyAsync(blocked, m->dm.blocked, count, cudaMemcpyDeviceToHost, m->stream));
+  }
   return sync(m);
 }
 
@@ -848,6 +966,7 @@ akb_status akb_set_time_step(akb_model* m, double dt) {
   akb_status st;
   if ((st = check_model(m)) != AKB_OK) return st;
   if (!(dt > 0) || !std::isfinite(dt)) return fail(AKB_ERR_INVALID_ARGUMENT, "time step must be > 0");
+  if (dt != m->dt) m->w_valid = false;
   m->dt = dt;
   return AKB_OK;
 }
@@ -909,6 +1028,7 @@ akb_status akb_solve_steps(akb_model* m, int64_t nb_steps) {
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   if (nb_steps == 0) return AKB_OK;
   AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if ((st = ensure_w(m)) != AKB_OK) return st;
   if (nb_steps == 1) {
     AKB_CUDA_TRY(enqueue_step(m));
   } else {
@@ -936,6 +1056,7 @@ akb_status akb_time_solve_steps(akb_model* m, int64_t nb_steps, double* elapsed_
   if (!elapsed_ms) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if ((st = ensure_w(m)) != AKB_OK) return st;
   if (nb_steps > 1) {  // instantiate the graphs outside the timed region
     cudaGraphExec_t full, rest;
     if ((st = prepare_graphs(m, nb_steps, &full, &rest)) != AKB_OK) return st;
@@ -1029,7 +1150,8 @@ akb_status akb_apply_dirichlet(akb_model* m, const uint32_t* nodes, int64_t nb_n
   std::memcpy(b.host + nbytes, values, (size_t)nb_nodes * sizeof(double));
   AKB_CUDA_TRY(cudaMemcpyAsync(b.dev, b.host, bytes, cudaMemcpyHostToDevice, m->stream));
   AKB_CUDA_TRY(apply_dirichlet(m->dm, reinterpret_cast<const uint32_t*>(b.dev), nb_nodes, component,
-                               reinterpret_cast<const double*>(b.dev + nbytes), m->stream));
+                               reinterpret_cast<const double*>(b.dev + nbytes), m->d_perm,
+                               m->use_patches ? m->patches.w : nullptr, m->stream));
   AKB_CUDA_TRY(cudaEventRecord(b.done, m->stream));
   b.pending = true;
   m->fint_valid = false;
@@ -1049,6 +1171,7 @@ akb_status akb_time_kernels(akb_model* m, int64_t nb_steps, double* ms_per_launc
     return fail(AKB_ERR_STATE, "partitioned mesh: step with akb_part_step_begin / akb_part_step_end");
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if ((st = ensure_w(m)) != AKB_OK) return st;
   StepTimer t;
   for (auto& e : t.ev) AKB_CUDA_TRY(cudaEventCreate(&e));
   double acc[AKB_MAX_KERNEL_SLOTS] = {0};
@@ -1141,6 +1264,7 @@ akb_status akb_batch_set_time_steps(akb_model* m, const double* dt) {
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   AKB_CUDA_TRY(cudaMemcpyAsync(m->d_inst_dt, dt, m->ninst * sizeof(double), cudaMemcpyHostToDevice,
                                m->stream));
+  m->w_valid = false;
   return sync(m);
 }
 
@@ -1245,6 +1369,7 @@ akb_status akb_part_step_begin(akb_model* m) {
   if (m->part_in_step) return fail(AKB_ERR_STATE, "step already begun");
   if (!(m->dt > 0)) return fail(AKB_ERR_STATE, "time step not set");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if ((st = ensure_w(m)) != AKB_OK) return st;
   AKB_CUDA_TRY(patch_step(m->dm, m->patches, m->dt, fp32(m), m->has_fext, m->stream));
   m->part_in_step = true;
   return AKB_OK;
@@ -1256,8 +1381,8 @@ akb_status akb_part_export_forces(akb_model* m, double* device_out) {
   if (!m->part_in_step) return fail(AKB_ERR_STATE, "no step begun");
   if (m->n_iface > 0 && !device_out) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
-  AKB_CUDA_TRY(patch_iface_export(m->dm, m->patches, m->d_iface_s, m->n_iface, device_out,
-                                  m->stream));
+  AKB_CUDA_TRY(patch_iface_export(m->dm, m->patches, m->d_iface_part, m->d_iface_k, m->n_iface,
+                                  device_out, m->stream));
   return AKB_OK;
 }
 
@@ -1267,9 +1392,9 @@ akb_status akb_part_step_end(akb_model* m, const double* device_in) {
   if (!m->part_in_step) return fail(AKB_ERR_STATE, "no step begun");
   if (m->n_iface > 0 && !device_in) return fail(AKB_ERR_INVALID_ARGUMENT, "null input");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
-  AKB_CUDA_TRY(patch_iface_import(m->dm, m->patches, m->d_iface_s, m->n_iface, device_in,
-                                  m->stream));
-  AKB_CUDA_TRY(patch_shared_nodes(m->dm, m->patches, m->dt, m->has_fext, m->stream));
+  AKB_CUDA_TRY(patch_iface_import(m->dm, m->patches, m->d_iface_part, m->d_iface_k, m->n_iface,
+                                  device_in, m->stream));
+  AKB_CUDA_TRY(patch_finish_list(m->dm, m->patches, m->dt, m->has_fext, m->stream));
   m->part_in_step = false;
   m->fint_valid = false;
   m->stresses_valid = false;

@@ -1,27 +1,29 @@
 // akb_patch.cu -- the fused explicit step (AKB_MODE_FP64, AKB_MODE_FP32_BULK).
 //
-// k_patch_step: one CTA per patch.
-//   1. stage the patch's nodes: the threads gather X, u, v, a and blocked
-//      flags to the nodes' planned shared-memory positions and apply the
-//      predictor u+ = u + dt v + dt^2/2 a, v* = v + dt a on free DOFs
-//      (NewmarkBeta::predictor, newmark-beta.cc:60-89), while a TMA bulk copy
-//      brings the first chunk record (corner positions, contribution slots,
-//      runs, index blocks: akb_patch.cuh);
+// k_patch_step: one CTA per patch (akb_patch.cuh for the node order, the
+// predicted displacement w and the shared-node protocol).
+//   1. stage: thread 0 starts TMA bulk copies of the interior nodes' X and w
+//      (two contiguous slices) and of the first chunk records, and prefetches
+//      the interior nodes' v, a, 1/M and blocked flags into L2; every thread
+//      starts cp.async copies of its shared nodes' X and w and zeroes the
+//      force accumulators;
 //   2. element forces in chunks of blockDim elements from shared memory
 //      (akb_fastmath.cuh), each corner vector written to its contribution
 //      slot; one thread per node run adds the run (ascending local element
 //      order) to the node accumulators (the -1 scatter of
 //      dof_manager.cc:83-137, without atomics). The record of the next chunk
 //      is copied while this one is used (two buffers, when they fit);
-//   3. nodes of this patch only: residual, lumped solve and corrector
-//      (non_linear_solver_lumped.cc:85-98, newmark-beta.cc:176-210) on u+
-//      kept in shared memory and v, a re-read, written back; nodes shared
-//      with other patches: FP64 partial force to its slot.
-// Every wait on a chunk copy is bounded: past it the CTA flags the error
+//   3. finish: each shared node's partial force goes to its slot; the
+//      interior nodes get the residual, lumped solve and corrector
+//      (non_linear_solver_lumped.cc:85-98, newmark-beta.cc:176-210) and the
+//      next predictor (newmark-beta.cc:60-89), written back as u, v, a and w.
+// Every wait on a bulk copy is bounded: past it the CTA flags the error
 // (P.err, read by the host on its next synchronisation), waits again (bounded)
 // for the copies it issued and stops.
-// k_shared_nodes: one thread per shared DOF adds its partials in patch order
-// and applies the same predictor/corrector arithmetic.
+// k_finish_list: one thread per (listed node, component) adds the partials
+// of the shared nodes in patch order and finishes them the same way, and the
+// nodes of no element (after the exchange between parts, for a partitioned
+// mesh).
 #include <mutex>
 
 #include "akb_fastmath.cuh"
@@ -33,36 +35,36 @@ namespace {
 constexpr int kThreads = 256;
 
 struct SmemLayout {
-  size_t xs, us, fs, contrib, scratch, buf, buf_stride, flags, mbar, total;
+  size_t xs, ws, fs, contrib, scratch, buf, buf_stride, mbar, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 __host__ __device__ inline size_t align128(size_t x) { return (x + 127) & ~size_t(127); }
 
-// Shared-memory layout: node arrays component-major ([i][position], row
-// stride LM), the chunk's element vectors component-major ([i][slot], CH
-// slots), FP32 only: FP64 piece sums ([i][piece], PM pieces), nbuf chunk
-// record buffers of CB bytes, per-(node, component) blocked flags for up to
-// Lmax nodes, one mbarrier per buffer.
+// Shared-memory layout: node arrays X and w row-major ([position][i], 16
+// bytes of slack in front for the offset of the interior slice), force
+// accumulators component-major ([i][position], row stride LM), the chunk's
+// element vectors component-major ([i][slot], CH slots), FP32 only: FP64
+// piece sums ([i][piece], PM pieces), nbuf chunk record buffers of CB
+// bytes, three mbarriers (two record buffers, the node staging).
 __host__ __device__ inline SmemLayout layout(int LM, int CH, int PM, int CB, int Lmax, int d,
                                              int sbytes, int nbuf) {
   SmemLayout s;
-  const size_t nd = align16((size_t)LM * d * sizeof(double));
+  const size_t nb = align16(16 + (size_t)Lmax * d * sizeof(double));
   s.xs = 0;
-  s.us = s.xs + nd;
-  s.fs = s.us + nd;
-  s.contrib = s.fs + nd;
+  s.ws = s.xs + nb;
+  s.fs = s.ws + nb;
+  s.contrib = s.fs + align16((size_t)LM * d * sizeof(double));
   s.scratch = align16(s.contrib + (size_t)CH * d * sbytes);
   s.buf = align128(s.scratch + (sbytes == 8 ? 0 : (size_t)PM * d * sizeof(double)));
   s.buf_stride = align128((size_t)CB);
-  s.flags = s.buf + nbuf * s.buf_stride;
-  s.mbar = align16(s.flags + (size_t)Lmax * d);
-  s.total = s.mbar + 16;
+  s.mbar = s.buf + nbuf * s.buf_stride;
+  s.total = s.mbar + 24;
   return s;
 }
 __host__ __device__ inline SmemLayout layout(const DevPatches& p, int d, int sbytes, int nbuf) {
-  return layout(p.node_stride, p.contrib_slots, p.max_pieces, p.chunk_bytes, p.max_nodes, d, sbytes,
-                nbuf);
+  return layout(p.node_stride, p.contrib_slots, p.max_pieces, p.chunk_bytes, p.max_nodes, d,
+                sbytes, nbuf);
 }
 
 // The n local indices of element el (uint16, n per element): one vector load
@@ -92,14 +94,48 @@ __device__ inline void load_corners(const uint16_t* base, int el, int* out) {
   }
 }
 
+// Differences of an element's corner coordinates and predicted
+// displacements to its first corner, in FP64 before any rounding to S. Node
+// arrays are row-major; in 2D a node's two components are one 16-byte load.
+template <int d, int n, typename S>
+__device__ inline void gather_differences(const double* xs, const double* ws, const int* lc,
+                                          S* dX, S* du) {
+  if constexpr (d == 2) {
+    const double2 x0 = reinterpret_cast<const double2*>(xs)[lc[0]];
+    const double2 u0 = reinterpret_cast<const double2*>(ws)[lc[0]];
+    dX[0] = dX[1] = du[0] = du[1] = S(0);
+#pragma unroll
+    for (int a = 1; a < n; ++a) {
+      const double2 x = reinterpret_cast<const double2*>(xs)[lc[a]];
+      const double2 u = reinterpret_cast<const double2*>(ws)[lc[a]];
+      dX[a * 2] = S(x.x - x0.x);
+      dX[a * 2 + 1] = S(x.y - x0.y);
+      du[a * 2] = S(u.x - u0.x);
+      du[a * 2 + 1] = S(u.y - u0.y);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < d; ++i) {
+      dX[i] = 0;
+      du[i] = 0;
+      const double x0 = xs[d * lc[0] + i], u0 = ws[d * lc[0] + i];
+#pragma unroll
+      for (int a = 1; a < n; ++a) {
+        dX[a * d + i] = S(xs[d * lc[a] + i] - x0);
+        du[a * d + i] = S(ws[d * lc[a] + i] - u0);
+      }
+    }
+  }
+}
+
 // CTAs per SM each instantiation is built for (register budget).
 template <int T, typename S> struct PatchOccupancy { static constexpr int value = 3; };
 template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, float> { static constexpr int value = 2; };
 template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, double> { static constexpr int value = 1; };
 
-// (node, component) items handled per thread per round of the staging and
-// finishing loops: their global loads are issued together.
-constexpr int kBatch = 5;
+// DOFs handled per thread per round of the finishing loop: their global
+// loads are issued together.
+constexpr int kBatch = 4;
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 __device__ inline uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -107,6 +143,24 @@ __device__ inline void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, 
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(mbar)
                : "memory");
+}
+// L2 prefetch of [lo, hi) rounded out to 16-byte boundaries (inside the
+// allocation: nodal arrays carry 16 bytes of slack at their end).
+__device__ inline void prefetch_l2(const void* base, size_t lo, size_t hi) {
+  const size_t a = lo & ~size_t(15), b = (hi + 15) & ~size_t(15);
+  if (b <= a) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char*)base + a),
+               "r"((uint32_t)(b - a))
+               : "memory");
+}
+__device__ inline void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr(dst)), "l"(src) : "memory");
+}
+__device__ inline void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(dst)), "l"(src) : "memory");
+}
+__device__ inline void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 __device__ inline bool mbar_wait(uint32_t a, uint32_t parity) {
   for (uint32_t it = 0; it < kWaitLimit; ++it) {
@@ -127,36 +181,88 @@ __device__ inline void expect_tx(uint32_t mbar, uint32_t bytes) {
                "r"(bytes)
                : "memory");
 }
+__device__ inline void arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+// Finishing inputs of a patch's interior nodes [ib, ib + nint): v, a (rows
+// of d doubles), 1/M (one double), blocked flags (d bytes), f_ext (d
+// doubles, when used). Each slice is bulk-copied from the 16-byte boundary at
+// or below its start to the one at or above its end (inside the arrays'
+// 16-byte slack); off[k]: where the slice's first item lands, from the
+// buffer's start; returns the bytes of all copies.
+template <int d, bool FEXT>
+__device__ inline uint32_t finish_regions(int ib, int nint, uint32_t* off, uint32_t* lo,
+                                          uint32_t* bytes) {
+  constexpr int nf = FEXT ? 5 : 4;
+  const uint32_t rowb[5] = {8u * d, 8u * d, 8u, (uint32_t)d, 8u * d};
+  uint32_t total = 0;
+#pragma unroll
+  for (int k = 0; k < nf; ++k) {
+    const size_t s0 = (size_t)ib * rowb[k], s1 = (size_t)(ib + nint) * rowb[k];
+    const size_t c0 = s0 & ~size_t(15), c1 = (s1 + 15) & ~size_t(15);
+    off[k] = total + (uint32_t)(s0 - c0);
+    lo[k] = (uint32_t)c0;  // (byte offsets below 4 GB: nn x d doubles < 2^32 bytes)
+    bytes[k] = (uint32_t)(c1 - c0);
+    total += bytes[k];
+  }
+  return total;
+}
+
+// Corrector of one free DOF from its total force r (with f_ext), and the
+// next predictor: u = w (the predicted displacement this step's forces were
+// evaluated at), v* = v + dt a recomputed bit for bit, then
+// x = r / M - a, v = v* + dt/2 x, a += x (u += 0 x only when x is not
+// finite); w' = u + dt v + dt^2/2 a.
+__device__ inline void finish_dof(double dt, double r, double im, double w, double& v, double& a,
+                                  double& u, double& wn) {
+  u = w;
+  v = __dadd_rn(v, __dmul_rn(dt, a));
+  fast::correct(dt, r, im, u, v, a);
+  wn = u;
+  double vn = v;
+  fast::predict(dt, wn, vn, a);
+}
 
 // One patch p, by the whole CTA. uses: chunk records this CTA has consumed
-// before (it picks the buffer and the mbarrier phase). Returns false when a
+// before (it picks the buffer and the mbarrier phase); stages: patches it
+// staged before (the phase of the staging mbarrier). Returns false when a
 // bounded wait gave up.
 template <int T, typename S, bool FEXT>
 __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& P, double dt0,
-                                           int p, unsigned char* smem, uint32_t& uses) {
+                                           int p, unsigned char* smem, uint32_t& uses,
+                                           uint32_t& stages) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe;
   static_assert(kChunk == kThreads, "one element per thread per chunk");
   const double dt = P.inst_dt ? P.inst_dt[P.patch_inst[p]] : dt0;
-  const int nb = P.node_ptr[p];
-  const int L = P.node_ptr[p + 1] - nb;
+  const int ib = P.ibeg[p], nint = P.nint[p];
+  const int s0 = P.sh_ptr[p], nsh = P.sh_ptr[p + 1] - s0;
+  const int L = nint + nsh;
   const int eb = P.elem_ptr[p];
   const int ne = P.elem_ptr[p + 1] - eb;
-  const int nint = P.ninterior[p];
   const int nchunks = (ne + kChunk - 1) / kChunk;
   const int ch0 = P.chunk_base[p];
   const int LM = P.node_stride, CH = P.contrib_slots;
   const bool two = P.nbuf == 2;  // buffers: 1 or 2
   const SmemLayout lay = layout(P, d, sizeof(S), two ? 2 : 1);
-  double* xs = reinterpret_cast<double*>(smem + lay.xs);
-  double* us = reinterpret_cast<double*>(smem + lay.us);
-  double* fs = reinterpret_cast<double*>(smem + lay.fs);
+  // the interior slice [ib, ib + nint) of X and w is bulk-copied from the
+  // 16-byte boundary at or below its start (the bytes before it land in the
+  // slack in front of the array; o: the slice's offset in doubles) to the
+  // boundary at or below its end; the remaining tail (one double at most)
+  // comes by cp.async, so that nothing is written past the slice, where the
+  // shared nodes go
+  const size_t row = (size_t)d * sizeof(double);
+  const size_t s_lo = (size_t)ib * row, s_hi = (size_t)(ib + nint) * row;
+  const size_t c_lo = s_lo & ~size_t(15), c_hi = s_hi & ~size_t(15);
+  const int o = (int)((s_lo - c_lo) / sizeof(double));
+  double* xs = reinterpret_cast<double*>(smem + lay.xs) + o;  // node at position j: xs[d j + i]
+  double* ws = reinterpret_cast<double*>(smem + lay.ws) + o;
+  double* fs = reinterpret_cast<double*>(smem + lay.fs);      // fs[i LM + j]
   S* contrib = reinterpret_cast<S*>(smem + lay.contrib);
   double* scratch = reinterpret_cast<double*>(smem + lay.scratch);  // FP32: piece sums
   const int PM = P.max_pieces;
-  uint8_t* flags = smem + lay.flags;
   const int tid = threadIdx.x;
-  const int items = L * d;
-  const uint32_t mb0 = saddr(smem + lay.mbar);
+  const uint32_t mb0 = saddr(smem + lay.mbar), mbs = mb0 + 16;
 
   // record k (counted over the CTA's chunks) uses buffer k % nbuf, and the
   // (k / nbuf)-th phase of that buffer's mbarrier
@@ -168,45 +274,96 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
     expect_tx(bar, cd.y);
     bulk_copy(saddr(smem + lay.buf + b * lay.buf_stride), P.cdata + (size_t)cd.x * 8, cd.y, bar);
   };
-  if (tid == 0) {
-    issue(0);
-    if (two && nchunks > 1) issue(1);
-  }
 
-  // 1. stage the nodes at their positions
-  for (int base = 0; base < items; base += kThreads * kBatch) {
-    int64_t idx[kBatch];
+  // 1. staging
+  // the interior nodes' finishing inputs go to the spare record buffer (the
+  // one the next chunk would use) at the start of the last chunk, when two
+  // buffers are used and they fit; the finish then reads shared memory
+  bool pre;
+  {
+    uint32_t f_off[5], f_lo[5], f_bytes[5];
+    pre = two && nint > 0 &&
+          finish_regions<d, FEXT>(ib, nint, f_off, f_lo, f_bytes) <= lay.buf_stride;
+  }
+  const uint32_t spare = buffer(uses + nchunks);
+  auto issue_finish = [&]() {  // by thread 0
+    const void* src[5] = {m.v, m.a, m.inv_mass, m.blocked, m.fext};
+    uint32_t f_off[5], f_lo[5], f_bytes[5];
+    const uint32_t total = finish_regions<d, FEXT>(ib, nint, f_off, f_lo, f_bytes);
+    const uint32_t dst = saddr(smem + lay.buf + spare * lay.buf_stride);
+    expect_tx(mbs, total);
+    uint32_t at = 0;
 #pragma unroll
-    for (int b = 0; b < kBatch; ++b) {
-      const int k = base + b * kThreads + tid;
-      const int j = k / d, i = k - j * d;
-      idx[b] = k < items ? (int64_t)P.lnodes[nb + j] * d + i : -1;
+    for (int k = 0; k < (FEXT ? 5 : 4); ++k) {
+      bulk_copy(dst + at, reinterpret_cast<const char*>(src[k]) + f_lo[k], f_bytes[k], mbs);
+      at += f_bytes[k];
     }
-    double x[kBatch], u[kBatch], v[kBatch], a[kBatch];
-    uint8_t bl[kBatch];
-#pragma unroll
-    for (int b = 0; b < kBatch; ++b)
-      if (idx[b] >= 0) {
-        x[b] = __ldg(&m.X[idx[b]]);
-        u[b] = m.u[idx[b]];
-        v[b] = m.v[idx[b]];
-        a[b] = m.a[idx[b]];
-        bl[b] = m.blocked[idx[b]];
-      }
-#pragma unroll
-    for (int b = 0; b < kBatch; ++b) {
-      const int k = base + b * kThreads + tid;
-      if (k >= items) continue;
-      const int j = k / d, i = k - j * d;
-      const int pj = P.lpos[nb + j];
-      double uu = u[b], vv = v[b];
-      if (!bl[b]) fast::predict(dt, uu, vv, a[b]);
-      xs[i * LM + pj] = x[b];
-      us[i * LM + pj] = uu;
-      fs[i * LM + pj] = 0.0;
-      flags[k] = bl[b];
+  };
+  if (tid == 0) {
+    // the previous patch's generic-proxy accesses of these buffers (ordered
+    // before this point by the CTA barrier) come before the bulk copies
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (nint > 0 && c_hi > c_lo) {
+      const uint32_t bytes = (uint32_t)(c_hi - c_lo);
+      expect_tx(mbs, 2 * bytes);
+      bulk_copy(saddr(smem + lay.xs), reinterpret_cast<const char*>(m.X) + c_lo, bytes, mbs);
+      bulk_copy(saddr(smem + lay.ws), reinterpret_cast<const char*>(P.w) + c_lo, bytes, mbs);
+    } else {
+      arrive(mbs);
+    }
+    if (nchunks > 0) issue(0);
+    if (two && nchunks > 1) issue(1);
+    if (nint > 0 && !pre) {  // inputs of the interior nodes' finish
+      prefetch_l2(m.v, s_lo, s_hi);
+      prefetch_l2(m.a, s_lo, s_hi);
+      prefetch_l2(m.inv_mass, (size_t)ib * 8, (size_t)(ib + nint) * 8);
+      prefetch_l2(m.blocked, (size_t)ib * d, (size_t)(ib + nint) * d);
+      if (FEXT) prefetch_l2(m.fext, s_lo, s_hi);
     }
   }
+  if (tid == kThreads - 1 && nint > 0 && c_hi < s_hi && c_hi >= s_lo) {  // the tail double
+    const size_t k = (c_hi - s_lo) / sizeof(double);
+    cp_async8(xs + k, m.X + (size_t)ib * d + k);
+    cp_async8(ws + k, P.w + (size_t)ib * d + k);
+  } else if (tid == kThreads - 1 && nint > 0 && c_hi < s_lo) {  // slice within one 16 bytes
+    for (size_t k = 0; k < (size_t)nint * d; ++k) {
+      cp_async8(xs + k, m.X + (size_t)ib * d + k);
+      cp_async8(ws + k, P.w + (size_t)ib * d + k);
+    }
+  }
+  for (int t = tid; t < nsh; t += kThreads) {
+    const int64_t g = P.sgid[s0 + t];
+    const int j = nint + t;
+    if constexpr (d == 2) {
+      cp_async16(xs + 2 * j, m.X + g * 2);
+      cp_async16(ws + 2 * j, P.w + g * 2);
+    } else {
+#pragma unroll
+      for (int i = 0; i < d; ++i) {
+        cp_async8(xs + d * j + i, m.X + g * d + i);
+        cp_async8(ws + d * j + i, P.w + g * d + i);
+      }
+    }
+  }
+  for (int k = tid; k < L * d; k += kThreads) {
+    const int i = k / L, j = k - i * L;
+    fs[i * LM + j] = 0.0;
+  }
+  cp_async_wait_all();
+  {
+    const bool ok = mbar_wait(mbs, stages & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(P.err, 1);
+        mbar_wait(mbs, stages & 1u);
+        for (int k = 0; k < min(nchunks, two ? 2 : 1); ++k)
+          mbar_wait(mb0 + 8 * buffer(uses + k), phase(uses + k));
+      }
+      return false;
+    }
+  }
+  ++stages;
+  if (pre && nchunks <= 1 && tid == 0) issue_finish();  // the second buffer is free already
 
   // 2. element forces chunk by chunk: each element writes its corner vectors
   //    to their contribution slots, then one thread per node run adds the
@@ -227,10 +384,12 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
         atomicExch(P.err, 1);
         const int last = min(nchunks - 1, (two && c == 0) ? 1 : c);
         for (int k = c; k <= last; ++k) mbar_wait(mb0 + 8 * buffer(uses + k), phase(uses + k));
+        if (pre && nchunks <= 1) mbar_wait(mbs, stages & 1u);  // the finishing inputs
       }
       return false;
     }
     if (two && tid == 0 && c > 0 && c + 1 < nchunks) issue(c + 1);  // into chunk c-1's buffer
+    if (pre && tid == 0 && c > 0 && c + 1 == nchunks) issue_finish();  // ditto
     const int c0 = c * kChunk, nec = min(kChunk, ne - c0);
     const uint32_t A = (uint32_t)align16((size_t)nec * n * 2);
     if (tid < nec) {
@@ -240,17 +399,7 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
       load_corners<n>(lcs + A / 2, tid, sl);
       const MatParams& mp = (P.emat ? m.mat_table[P.emat[(size_t)eb + c0 + tid]] : m.mats[0]);
       S dX[3 * 8], du[3 * 8];
-#pragma unroll
-      for (int i = 0; i < d; ++i) {
-        dX[i] = 0;
-        du[i] = 0;
-        const double x0 = xs[i * LM + lc[0]], u0 = us[i * LM + lc[0]];
-#pragma unroll
-        for (int a = 1; a < n; ++a) {
-          dX[a * d + i] = S(xs[i * LM + lc[a]] - x0);
-          du[a * d + i] = S(us[i * LM + lc[a]] - u0);
-        }
-      }
+      gather_differences<d, n, S>(xs, ws, lc, dX, du);
       S fe[3 * 8];
       fast::element_force<T, S>(mp, dX, du, fe);
 #pragma unroll
@@ -271,17 +420,23 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
       const uint16_t* ixs = reinterpret_cast<const uint16_t*>(buf + (hd.y & 0xffff));
       for (int q = tid; q < R1; q += kThreads) {
         const uint32_t w = sums[q];
+        const int len = (int)((w >> 16) & 0xff), jp = (int)(w & 0xffff);
+        if (len == 0) continue;
+        // pieces are sorted by length, so the loops below end at nearly the
+        // same trip count across a warp
         int k[kMaxPiece];
 #pragma unroll
-        for (int t = 0; t < kMaxPiece; ++t) k[t] = t < rows ? ixs[t * R1 + q] : 0;
-        const int len = (int)((w >> 16) & 0xff), jp = (int)(w & 0xffff);
+        for (int t = 0; t < kMaxPiece; ++t) {
+          if (t >= len || t >= rows) break;
+          k[t] = ixs[t * R1 + q];
+        }
         double f[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int t = 0; t < kMaxPiece; ++t)
-          if (t < len)
+        for (int t = 0; t < kMaxPiece; ++t) {
+          if (t >= len) break;
 #pragma unroll
-            for (int i = 0; i < d; ++i) f[i] += double(contrib[i * CH + k[t]]);
-        if (len == 0) continue;
+          for (int i = 0; i < d; ++i) f[i] += double(contrib[i * CH + k[t]]);
+        }
         if (w >> 24) {  // FP64: over the piece's first slot; FP32: by piece
 #pragma unroll
           for (int i = 0; i < d; ++i) {
@@ -328,49 +483,70 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
       }
     }
   }
-  __syncthreads();  // the sums of the last chunk are in
+  {
+    // the sums of the last chunk are in (and the finishing inputs)
+    const bool ok = !pre || mbar_wait(mbs, stages & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(P.err, 1);
+        mbar_wait(mbs, stages & 1u);
+      }
+      return false;
+    }
+  }
+  if (pre) ++stages;
   uses += nchunks;
+  const unsigned char* fin = smem + lay.buf + spare * lay.buf_stride;
+  uint32_t f_off[5];
+  {
+    uint32_t f_lo[5], f_bytes[5];
+    finish_regions<d, FEXT>(ib, nint, f_off, f_lo, f_bytes);
+  }
 
-  // 3. finish the nodes of this patch (state re-read, predictor recomputed
-  //    bit for bit), hand out the shared ones
+  // 3. finish: the shared nodes' partials to their slots (the second pass
+  //    adds them), the interior nodes finished here, one thread per DOF,
+  //    contiguous in the global arrays
+  for (int k = tid; k < nsh * d; k += kThreads) {
+    const int t = k / d, i = k - t * d;
+    P.partial[(size_t)P.sslot[s0 + t] * d + i] = fs[i * LM + nint + t];
+  }
+  const int items = nint * d;
   for (int base = 0; base < items; base += kThreads * kBatch) {
-    int64_t idx[kBatch];
     double v[kBatch], a[kBatch], im[kBatch], fx[kBatch];
+    uint8_t bl[kBatch];
 #pragma unroll
     for (int b = 0; b < kBatch; ++b) {
       const int k = base + b * kThreads + tid;
-      const int j = k / d, i = k - j * d;
-      idx[b] = -1;
-      if (k < items && j < nint && !flags[k]) {
-        const int64_t g = P.lnodes[nb + j];
-        idx[b] = g * d + i;
-        im[b] = m.inv_mass[g];
+      if (k < items) {
+        if (pre) {
+          v[b] = *reinterpret_cast<const double*>(fin + f_off[0] + 8 * k);
+          a[b] = *reinterpret_cast<const double*>(fin + f_off[1] + 8 * k);
+          im[b] = *reinterpret_cast<const double*>(fin + f_off[2] + 8 * (k / d));
+          bl[b] = fin[f_off[3] + k];
+          fx[b] = FEXT ? *reinterpret_cast<const double*>(fin + f_off[4] + 8 * k) : 0.0;
+        } else {
+          const int64_t q = (int64_t)ib * d + k;
+          bl[b] = m.blocked[q];
+          v[b] = m.v[q];
+          a[b] = m.a[q];
+          im[b] = m.inv_mass[ib + k / d];
+          fx[b] = FEXT ? m.fext[q] : 0.0;
+        }
       }
     }
 #pragma unroll
-    for (int b = 0; b < kBatch; ++b)
-      if (idx[b] >= 0) {
-        v[b] = m.v[idx[b]];
-        a[b] = m.a[idx[b]];
-        fx[b] = FEXT ? m.fext[idx[b]] : 0.0;
-      }
-#pragma unroll
     for (int b = 0; b < kBatch; ++b) {
       const int k = base + b * kThreads + tid;
-      if (k >= items) continue;
+      if (k >= items || bl[b]) continue;  // blocked DOFs keep u, v, a (and w = u)
       const int j = k / d, i = k - j * d;
-      const int pj = P.lpos[nb + j];
-      const double f = fs[i * LM + pj];
-      if (j >= nint) {
-        P.partial[(int64_t)P.slot[nb + j] * d + i] = f;
-      } else if (idx[b] >= 0) {  // blocked DOFs keep u, v, a
-        // u+ from the staging, v* recomputed bit for bit
-        double uu = us[i * LM + pj], vv = __dadd_rn(v[b], __dmul_rn(dt, a[b])), aa = a[b];
-        fast::correct(dt, FEXT ? f + fx[b] : f, im[b], uu, vv, aa);
-        m.u[idx[b]] = uu;
-        m.v[idx[b]] = vv;
-        m.a[idx[b]] = aa;
-      }
+      const int64_t q = (int64_t)ib * d + k;
+      const double f = fs[i * LM + j];
+      double u, wn;
+      finish_dof(dt, FEXT ? f + fx[b] : f, im[b], ws[k], v[b], a[b], u, wn);
+      m.u[q] = u;
+      m.v[q] = v[b];
+      m.a[q] = a[b];
+      P.w[q] = wn;
     }
   }
   return true;
@@ -386,83 +562,100 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
   {
     const SmemLayout lay = layout(P, ET<T>::dim, sizeof(S), P.nbuf);
     if (threadIdx.x == 0) {
-      for (int b = 0; b < P.nbuf; ++b)
+      for (int b = 0; b < 3; ++b)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(smem + lay.mbar + 8 * b))
                      : "memory");
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
   }
-  uint32_t uses = 0;
+  uint32_t uses = 0, stages = 0;
   if constexpr (PERSIST) {
     for (int p = blockIdx.x; p < P.npatch; p += gridDim.x) {
       if (p != (int)blockIdx.x) __syncthreads();  // shared memory of the previous patch is free
-      if (!patch_body<T, S, FEXT>(m, P, dt0, p, smem, uses)) return;
+      if (!patch_body<T, S, FEXT>(m, P, dt0, p, smem, uses, stages)) return;
     }
   } else {
-    patch_body<T, S, FEXT>(m, P, dt0, blockIdx.x, smem, uses);
+    patch_body<T, S, FEXT>(m, P, dt0, blockIdx.x, smem, uses, stages);
   }
 }
 
+// Listed nodes, one thread per (entry, component): the sum of the entry's
+// partials in order (none for a node of no element), then the same finish
+// as in the fused step, from the node's stored w.
 template <int D, bool FEXT>
-__global__ void k_shared_nodes(DevModel m, DevPatches P, double dt0) {
-  // one thread per (shared node, component): neighbouring threads touch
-  // neighbouring words of the partials and of u, v, a
+__global__ void k_finish_list(DevModel m, DevPatches P, double dt0) {
+  constexpr int d = D;
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t ns = P.nshared;
-  if (t >= ns * D) return;
-  const int64_t s = t / D;
-  const int i = (int)(t - s * D);
-  const int64_t g = P.snodes[s];
-  const int64_t k = g * D + i;
-  // every load that depends on the node id is issued before the blocked
-  // flag is tested
-  const uint8_t bl = m.blocked[k];
-  const double im = m.inv_mass[g];
-  double u = m.u[k], v = m.v[k], a = m.a[k];
-  const double fx = FEXT ? m.fext[k] : 0.0;
-  const double dt = P.inst_dt ? P.inst_dt[P.snode_inst[s]] : dt0;
-  // partials in patch order: the first two in the dense rows, the others
-  // after them (zero for a node of no element)
-  const int k0 = P.sptr[s], k1 = P.sptr[s + 1];
-  double f = 0.0 + P.partial[s * D + i];
-  f += P.partial[(ns + s) * D + i];
-  for (int q = k0; q < k1; ++q) f += P.partial[(2 * ns + q) * D + i];
+  if (t >= P.nlist * d) return;
+  const int64_t e = t / d;
+  const int i = (int)(t - e * d);
+  const int64_t g = P.list_gid[e];
+  const int64_t q = g * d + i;
+  const uint32_t part = P.list_part[e], k = P.list_k[e];
+  const double dt = P.inst_dt ? P.inst_dt[P.list_inst[e]] : dt0;
+  // every load that depends on the entry is issued before the blocked flag
+  // is tested
+  const uint8_t bl = m.blocked[q];
+  const double im = m.inv_mass[g], w = P.w[q], fx = FEXT ? m.fext[q] : 0.0;
+  double v = m.v[q], a = m.a[q];
+  double f = 0.0;
+  for (uint32_t r = 0; r < k; ++r) f += P.partial[(size_t)(part + r) * d + i];
   if (bl) return;
-  fast::predict(dt, u, v, a);
-  if (FEXT) f += fx;
-  fast::correct(dt, f, im, u, v, a);
-  m.u[k] = u;
-  m.v[k] = v;
-  m.a[k] = a;
+  double u, wn;
+  finish_dof(dt, FEXT ? f + fx : f, im, w, v, a, u, wn);
+  m.u[q] = u;
+  m.v[q] = v;
+  m.a[q] = a;
+  P.w[q] = wn;
 }
 
-// Interface nodes of a partitioned mesh, one thread per (interface node,
-// component): the sum of the node's partials in patch order (export), or the
-// total over all parts written as its only partial (import).
-__global__ void k_iface_export(DevPatches P, const uint32_t* iface, int64_t n, int d,
-                               double* out) {
+// w = u + dt v + dt^2/2 a on free DOFs, w = u on blocked ones; one thread per
+// DOF (batches: the node's instance by bisection of the node ranges).
+__global__ void k_refresh_w(DevModel m, DevPatches P, double dt0) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= m.nn * m.dim) return;
+  double u = m.u[q];
+  if (!m.blocked[q]) {
+    double dt = dt0;
+    if (P.inst_dt) {
+      const int64_t node = q / m.dim;
+      int lo = 0, hi = P.ninst;  // node_off[lo] <= node < node_off[hi]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (P.node_off[mid] <= node) lo = mid; else hi = mid;
+      }
+      dt = P.inst_dt[lo];
+    }
+    double v = m.v[q];
+    fast::predict(dt, u, v, m.a[q]);
+  }
+  P.w[q] = u;
+}
+
+// Interface nodes of a partitioned mesh, one thread per (node, component):
+// the sum of the node's partials in order (export), or the total over all
+// parts written as its only partial (import).
+__global__ void k_iface_export(DevPatches P, const uint32_t* parts, const uint32_t* ks, int64_t n,
+                               int d, double* out) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= n * d) return;
-  const int64_t q = t / d;
-  const int i = (int)(t - q * d);
-  const int64_t ns = P.nshared, s = iface[q];
-  double f = 0.0 + P.partial[s * d + i];
-  f += P.partial[(ns + s) * d + i];
-  for (int k = P.sptr[s]; k < P.sptr[s + 1]; ++k) f += P.partial[(2 * ns + k) * d + i];
+  const int64_t e = t / d;
+  const int i = (int)(t % d);
+  const uint32_t part = parts[e], k = ks[e];
+  double f = 0.0;
+  for (uint32_t r = 0; r < k; ++r) f += P.partial[(size_t)(part + r) * d + i];
   out[t] = f;
 }
 
-__global__ void k_iface_import(DevPatches P, const uint32_t* iface, int64_t n, int d,
-                               const double* in) {
+__global__ void k_iface_import(DevPatches P, const uint32_t* parts, const uint32_t* ks, int64_t n,
+                               int d, const double* in) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= n * d) return;
-  const int64_t q = t / d;
-  const int i = (int)(t - q * d);
-  const int64_t ns = P.nshared, s = iface[q];
-  P.partial[s * d + i] = in[t];
-  P.partial[(ns + s) * d + i] = 0.0;
-  for (int k = P.sptr[s]; k < P.sptr[s + 1]; ++k) P.partial[(2 * ns + k) * d + i] = 0.0;
+  const int64_t e = t / d;
+  const int i = (int)(t % d);
+  const uint32_t part = parts[e], k = ks[e];
+  for (uint32_t r = 0; r < k; ++r) P.partial[(size_t)(part + r) * d + i] = r == 0 ? in[t] : 0.0;
 }
 
 __global__ void k_mass_export(DevModel m, const uint32_t* nodes, int64_t n, double* out) {
@@ -480,11 +673,27 @@ __global__ void k_mass_import(DevModel m, const uint32_t* nodes, int64_t n, cons
   m.inv_mass[g] = 1. / M;
 }
 
+template <typename V>
+__global__ void k_permute_rows(const uint32_t* perm, int64_t n, int width, const V* in, V* out,
+                               bool scatter) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n * width) return;
+  const int64_t i = t / width;
+  const int c = (int)(t - i * width);
+  const int64_t j = perm[i];
+  if (scatter)
+    out[j * width + c] = in[t];
+  else
+    out[t] = in[j * width + c];
+}
+
 // grid of the patch kernel: one CTA per patch, or a persistent grid of
 // P.grid CTAs that stride over the patches
 inline int grid_of(const DevPatches& p) {
   return (p.grid > 0 && p.grid < p.npatch) ? p.grid : p.npatch;
 }
+
+inline int blocks_of(int64_t n) { return (int)((n + kThreads - 1) / kThreads); }
 
 template <int T, typename S>
 cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool fext,
@@ -533,8 +742,7 @@ cudaError_t configure(const DevPatches& p) {
 
 }  // namespace
 
-size_t patch_smem_bytes(const DevPatches& p, int dim, int nnpe, bool fp32, int nbuf) {
-  (void)nnpe;
+size_t patch_smem_bytes(const DevPatches& p, int dim, bool fp32, int nbuf) {
   return layout(p, dim, fp32 ? 4 : 8, nbuf).total;
 }
 
@@ -583,48 +791,66 @@ cudaError_t patch_step(const DevModel& m, const DevPatches& p, double dt, bool f
   }
 }
 
-cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* iface,
-                               int64_t n, double* out, cudaStream_t s) {
-  if (n == 0) return cudaSuccess;
-  const int blocks = (int)((n * m.dim + kThreads - 1) / kThreads);
-  k_iface_export<<<blocks, kThreads, 0, s>>>(p, iface, n, m.dim, out);
+cudaError_t patch_finish_list(const DevModel& m, const DevPatches& p, double dt, bool fext,
+                              cudaStream_t s) {
+  if (p.nlist <= 0) return cudaSuccess;
+  const int blocks = blocks_of(p.nlist * m.dim);
+  switch (m.dim) {
+  case 1: fext ? k_finish_list<1, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
+               : k_finish_list<1, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
+  case 2: fext ? k_finish_list<2, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
+               : k_finish_list<2, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
+  default: fext ? k_finish_list<3, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
+                : k_finish_list<3, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
+  }
   return cudaGetLastError();
 }
 
-cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* iface,
-                               int64_t n, const double* in, cudaStream_t s) {
-  if (n == 0) return cudaSuccess;
-  const int blocks = (int)((n * m.dim + kThreads - 1) / kThreads);
-  k_iface_import<<<blocks, kThreads, 0, s>>>(p, iface, n, m.dim, in);
+cudaError_t patch_refresh_w(const DevModel& m, const DevPatches& p, double dt, cudaStream_t s) {
+  if (m.nn == 0) return cudaSuccess;
+  k_refresh_w<<<blocks_of(m.nn * m.dim), kThreads, 0, s>>>(m, p, dt);
+  return cudaGetLastError();
+}
+
+cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* part,
+                               const uint32_t* k, int64_t n, double* out, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_iface_export<<<blocks_of(n * m.dim), kThreads, 0, s>>>(p, part, k, n, m.dim, out);
+  return cudaGetLastError();
+}
+
+cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* part,
+                               const uint32_t* k, int64_t n, const double* in, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_iface_import<<<blocks_of(n * m.dim), kThreads, 0, s>>>(p, part, k, n, m.dim, in);
   return cudaGetLastError();
 }
 
 cudaError_t mass_export(const DevModel& m, const uint32_t* nodes, int64_t n, double* out,
                         cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_mass_export<<<(int)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(m, nodes, n, out);
+  k_mass_export<<<blocks_of(n), kThreads, 0, s>>>(m, nodes, n, out);
   return cudaGetLastError();
 }
 
 cudaError_t mass_import(const DevModel& m, const uint32_t* nodes, int64_t n, const double* in,
                         cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  k_mass_import<<<(int)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(m, nodes, n, in);
+  k_mass_import<<<blocks_of(n), kThreads, 0, s>>>(m, nodes, n, in);
   return cudaGetLastError();
 }
 
-cudaError_t patch_shared_nodes(const DevModel& m, const DevPatches& p, double dt, bool fext,
-                               cudaStream_t s) {
-  if (p.nshared == 0) return cudaSuccess;
-  const int blocks = (int)((p.nshared * m.dim + kThreads - 1) / kThreads);
-  switch (m.dim) {
-  case 1: fext ? k_shared_nodes<1, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
-               : k_shared_nodes<1, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
-  case 2: fext ? k_shared_nodes<2, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
-               : k_shared_nodes<2, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
-  default: fext ? k_shared_nodes<3, true><<<blocks, kThreads, 0, s>>>(m, p, dt)
-                : k_shared_nodes<3, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
-  }
+cudaError_t permute_rows(const uint32_t* perm, int64_t n, int width, const double* in,
+                         double* out, bool scatter, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_permute_rows<double><<<blocks_of(n * width), kThreads, 0, s>>>(perm, n, width, in, out, scatter);
+  return cudaGetLastError();
+}
+
+cudaError_t permute_rows_u8(const uint32_t* perm, int64_t n, int width, const uint8_t* in,
+                            uint8_t* out, bool scatter, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_permute_rows<uint8_t><<<blocks_of(n * width), kThreads, 0, s>>>(perm, n, width, in, out, scatter);
   return cudaGetLastError();
 }
 

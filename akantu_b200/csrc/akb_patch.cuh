@@ -2,17 +2,33 @@
 //
 // The mesh is cut into patches of spatially close elements (recursive
 // coordinate bisection of the element centroids, Morton order inside a
-// patch). One CTA owns one patch: it stages the patch's nodes in
-// shared memory, applies the central-difference predictor there, computes
-// the element forces and adds them per node in ascending local element order
-// (static per-chunk runs, so the sum is deterministic without atomics).
-// Where node values and element contributions sit in shared memory is planned
-// at build time so that the corner gathers, the contribution scatter and the
-// per-node sums are (nearly) free of bank conflicts.
-// Nodes touched by one patch only ("interior") are finished by that CTA;
-// nodes shared by several patches write one FP64 partial per (node, patch)
-// (the first two of every node in two dense rows, the others node-major), and
-// a second kernel adds them in patch order and finishes those nodes.
+// patch). One CTA owns one patch: it stages the patch's nodes in shared
+// memory, computes the element forces and adds them per node in a fixed
+// order (static per-chunk runs, so the sum is deterministic without float
+// atomics). Where node values and element contributions sit in shared memory
+// is planned at build time so that the corner gathers, the contribution
+// scatter and the per-node sums are (nearly) free of bank conflicts.
+//
+// Node numbering. The model stores its nodes in an internal order chosen
+// here: the nodes touched by one patch only ("interior" nodes) of patch p
+// are the contiguous range [ibeg[p], ibeg[p] + nint[p]), in the order of
+// their shared-memory positions, so the CTA stages them with bulk copies of
+// contiguous slices; the nodes touched by several patches ("shared") follow
+// all interior nodes, then the nodes of no element. perm maps the caller's
+// node id to the internal one.
+//
+// Predicted displacement. Besides u, v, a the model keeps
+// w = u + dt v + dt^2/2 a (w = u on blocked DOFs), the displacement the next
+// step's forces are evaluated at (NewmarkBeta::predictor, newmark-beta.cc:
+// 60-89); a step only stages X and w, and whoever finishes a node writes its
+// new u, v, a and the next w.
+//
+// Shared nodes. Each patch touching a shared node writes its partial force
+// to the node's slot of rank r (its position among the node's k patches in
+// patch order); a second pass (k_finish_list), one thread per DOF over the
+// shared block, adds the k partials in rank order and finishes the node. The
+// same pass finishes the nodes of no element; for a partitioned mesh the
+// interface nodes' sums are exchanged between parts before it.
 #pragma once
 
 #include <stdint.h>
@@ -23,15 +39,20 @@
 
 namespace akb {
 
-// Shared-memory banks the fused step's layout is planned for: 32 banks of 4
-// bytes. An 8-byte word occupies a bank pair, so 16 threads reading 8-byte
-// words at 16 different pair indices (word index mod 16) take one wavefront.
-constexpr int kBankPairs = 16;
-
 // Elements per chunk: the CTA computes one element per thread per chunk.
 constexpr int kChunk = 256;
 // Largest piece (contributions of one node added by one thread).
 constexpr int kMaxPiece = 8;
+// Shared-memory bank pairs (8-byte words): a half-warp reading 8-byte words
+// at 16 distinct (word index mod 16) takes one wavefront.
+constexpr int kBankPairs = 16;
+
+// Node positions are planned so that the CTA's corner gathers hit distinct
+// banks: for dim 1 and 3 (8-byte loads of one component; node arrays are
+// row-major with an odd row length, so distinct positions mod 16 give
+// distinct bank pairs), 16 elements per group and residues mod 16; for
+// dim 2 (16-byte loads of a node's two components) 8 elements and mod 8.
+inline int place_group(int dim) { return dim == 2 ? 8 : 16; }
 
 // Chunk record: one contiguous, 16-byte aligned block per chunk, staged into
 // shared memory by one TMA bulk copy. Contents (uint16 units unless noted;
@@ -64,30 +85,38 @@ struct ChunkDesc {
 struct PatchHost {
   int npatch = 0;
   int max_nodes = 0;      // largest local node count of a patch
-  int node_stride = 0;    // row stride of the shared-memory node arrays
+  int max_interior = 0;   // largest interior node count of a patch
+  int max_shared = 0;     // largest shared node count of a patch
+  int node_stride = 0;    // row stride of the component-major force accumulators
   int contrib_slots = 0;  // largest contribution array of a chunk (per component)
   int max_pieces = 0;     // largest padded first-level piece count of a chunk
   int chunk_bytes = 0;    // largest chunk record
-  std::vector<int32_t> elem_ptr;   // npatch + 1, into element order
-  std::vector<int32_t> node_ptr;   // npatch + 1, into lnodes
-  std::vector<int32_t> ninterior;  // npatch
-  std::vector<uint32_t> lnodes;    // global node ids: interior first, then shared
-  std::vector<uint16_t> lpos;      // per local node: position in the node arrays
+  std::vector<uint32_t> perm;        // caller's node id -> internal id
+  std::vector<int32_t> elem_ptr;     // npatch + 1, into element order
   std::vector<uint32_t> elem_order;  // patch-ordered position -> original element
-  std::vector<int32_t> chunk_base; // npatch + 1: first chunk of each patch
-  std::vector<ChunkDesc> chunks;   // per chunk
-  std::vector<uint16_t> cdata;     // chunk records (multiple of 8 uint16 each)
-  std::vector<uint32_t> slot;      // per local node: partial slot (0xffffffff if interior)
-  std::vector<uint32_t> snodes;    // shared nodes, ascending
-  std::vector<int32_t> sptr;       // nshared + 1, partial slots of each shared node (CSR)
+  std::vector<int32_t> ibeg;         // npatch: internal id of the first interior node
+  std::vector<int32_t> nint;         // npatch: interior node count
+  std::vector<int32_t> sh_ptr;       // npatch + 1, into the shared entries
+  // shared entries, per patch in position order (entry t <-> position nint + t)
+  std::vector<uint32_t> sgid;        // internal node id
+  std::vector<uint32_t> sslot;       // this patch's partial slot of the node
+  std::vector<int32_t> chunk_base;   // npatch + 1: first chunk of each patch
+  std::vector<ChunkDesc> chunks;     // per chunk
+  std::vector<uint16_t> cdata;       // chunk records (multiple of 8 uint16 each)
+  // per shared node (internal id order of the shared block, which starts at
+  // shared_base): internal id, first slot, k
+  uint32_t shared_base = 0;
+  std::vector<uint32_t> shared_nodes, shared_part, shared_k;
+  std::vector<uint32_t> orphans;     // internal ids of nodes of no element
   int64_t nslots = 0;
 };
 
-// Builds the patches. target_elems: elements per patch; max_nodes: local node
-// cap (<= 60000); contrib_bytes: element vector precision (8: FP64, 4:
-// FP32); piece: contributions one thread adds (<= kMaxPiece); force_shared
-// (per node, or null): nodes finished by the shared-node pass even when one
-// patch holds them (the interface nodes of a partitioned mesh).
+// Builds the patches and the internal node order. target_elems: elements per
+// patch; max_nodes: local node cap (<= 60000); contrib_bytes: element vector
+// precision (8: FP64, 4: FP32); piece: contributions one thread adds (<=
+// kMaxPiece); force_shared (per node, or null): nodes treated as shared
+// (finished by the second pass from their partials) even when one patch holds
+// them (the interface nodes of a partitioned mesh).
 PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64_t ne, int dim,
                         int nnpe, int target_elems, int max_nodes, int contrib_bytes,
                         int piece, const uint8_t* force_shared = nullptr);
@@ -97,48 +126,65 @@ struct DevPatches {
   int npatch;
   int grid;  // 0: one CTA per patch; > 0: persistent grid of that many CTAs
   int nbuf;  // chunk record buffers in shared memory (2: next chunk prefetched)
-  int max_nodes, node_stride, contrib_slots, max_pieces, chunk_bytes;
-  int64_t nshared;
+  int max_nodes, max_shared, node_stride, contrib_slots, max_pieces, chunk_bytes;
   const int32_t* elem_ptr;
-  const int32_t* node_ptr;
-  const int32_t* ninterior;
-  const uint32_t* lnodes;
-  const uint16_t* lpos;
+  const int32_t* ibeg;
+  const int32_t* nint;
+  const int32_t* sh_ptr;
+  const uint32_t* sgid;
+  const uint32_t* sslot;
   const int32_t* chunk_base;
   const uint2* chunks;     // ChunkDesc per chunk
   const uint16_t* cdata;   // chunk records (16-byte aligned)
-  const uint32_t* slot;
-  const uint32_t* snodes;
-  // partial slots: shared node s has its first two at s and nshared + s, the
-  // others at 2 nshared + [sptr[s], sptr[s + 1])
-  const int32_t* sptr;
-  const uint32_t* emat;  // material of each patch-ordered element, or null
-  int* err;              // set when a bounded wait gave up
-  double* partial;       // nslots x dim
-  // batches: per-instance time step, instance of each patch and shared node
+  const uint32_t* emat;    // material of each patch-ordered element, or null
+  int* err;                // set when a bounded wait gave up
+  double* partial;         // nslots x dim
+  double* w;               // nn x dim predicted displacement
+  // nodes finished by k_finish_list: the nodes of no element, then the
+  // shared nodes; entry i: node, first slot, k (0 for a node of no element)
+  int64_t nlist;
+  const uint32_t* list_gid;
+  const uint32_t* list_part;
+  const uint32_t* list_k;
+  // batches: per-instance time step, instance of each patch / list entry
   const double* inst_dt;       // null for a single model (scalar dt)
   const uint32_t* patch_inst;
-  const uint32_t* snode_inst;
+  const uint32_t* list_inst;
+  // batches: instance node ranges (ninst + 1), for the w refresh
+  const int64_t* node_off;
+  int ninst;
 };
 
-size_t patch_smem_bytes(const DevPatches& p, int dim, int nnpe, bool fp32, int nbuf);
+size_t patch_smem_bytes(const DevPatches& p, int dim, bool fp32, int nbuf);
 // Chunk record buffers (1 or 2) that keep the most CTAs per SM.
 int patch_buffers(const DevPatches& p, int type, bool fp32);
+cudaError_t patch_configure(const DevModel& m, const DevPatches& p, bool fp32);
+// The fused step: every interior node finished, the shared nodes' partials
+// written.
 cudaError_t patch_step(const DevModel& m, const DevPatches& p, double dt, bool fp32,
                        bool has_fext, cudaStream_t s);
-cudaError_t patch_shared_nodes(const DevModel& m, const DevPatches& p, double dt,
-                               bool has_fext, cudaStream_t s);
-cudaError_t patch_configure(const DevModel& m, const DevPatches& p, bool fp32);
-// Partitioned meshes: out[i] = sum of the partials of shared node iface[i]
-// (per component); import writes in[i] as that node's only partial. Masses:
-// out[i] = lumped mass of node nodes[i]; import sets it (and 1/M).
-cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* iface,
-                               int64_t n, double* out, cudaStream_t s);
-cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* iface,
-                               int64_t n, const double* in, cudaStream_t s);
+// Finishes the listed nodes from their partials (the step's second pass).
+cudaError_t patch_finish_list(const DevModel& m, const DevPatches& p, double dt, bool has_fext,
+                              cudaStream_t s);
+// w = u + dt v + dt^2/2 a on free DOFs, w = u on blocked ones.
+cudaError_t patch_refresh_w(const DevModel& m, const DevPatches& p, double dt, cudaStream_t s);
+// Partitioned meshes, per interface node i (first slot part[i], k[i] slots):
+// out[i] = the sum of its partials (per component); import writes in[i] as
+// its only partial. Masses: out[i] = lumped mass of internal node nodes[i];
+// import sets it (and 1/M).
+cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* part,
+                               const uint32_t* k, int64_t n, double* out, cudaStream_t s);
+cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* part,
+                               const uint32_t* k, int64_t n, const double* in, cudaStream_t s);
 cudaError_t mass_export(const DevModel& m, const uint32_t* nodes, int64_t n, double* out,
                         cudaStream_t s);
 cudaError_t mass_import(const DevModel& m, const uint32_t* nodes, int64_t n, const double* in,
                         cudaStream_t s);
+// Caller order <-> internal order of nodal arrays (rows of `width` items):
+// gather: out[i] = in[perm[i]]; scatter: out[perm[i]] = in[i].
+cudaError_t permute_rows(const uint32_t* perm, int64_t n, int width, const double* in,
+                         double* out, bool scatter, cudaStream_t s);
+cudaError_t permute_rows_u8(const uint32_t* perm, int64_t n, int width, const uint8_t* in,
+                            uint8_t* out, bool scatter, cudaStream_t s);
 
 }  // namespace akb

@@ -28,15 +28,15 @@ inline uint64_t spread2(uint64_t x) {  // 31 bits -> every second bit
   return x;
 }
 
-// Positions of a patch's L local nodes in the shared-memory node arrays. The
-// CTA reads corner a of 16 consecutive elements (a half-warp) as 8-byte words
-// in one instruction; each distinct node of such a group should sit at its own
-// word index mod 16 (bank pair). Greedy in first-touch order: a node takes the
-// residue least used by the groups it belongs to, then the least filled one;
-// each residue holds at most ceil(L / 16) nodes, so positions stay below
-// 16 * ceil(L / 16).
-void place_nodes(const std::vector<uint16_t>& lc, int ne, int nnpe, int L, uint16_t* pos) {
-  const int G = kBankPairs;
+// Positions of a patch's L local nodes in the shared-memory node arrays:
+// local nodes [0, nint) are the interior ones and take positions [0, nint),
+// the others positions [nint, L). The CTA reads corner a of G consecutive
+// elements in one instruction; each distinct node of such a group should sit
+// at its own position mod G (place_group). Greedy in first-touch order: a
+// node takes, within its range, the residue least used by the groups it
+// belongs to, then the one with the most free positions left.
+void place_nodes(const std::vector<uint16_t>& lc, int ne, int nnpe, int L, int nint, int G,
+                 uint16_t* pos) {
   const int nhalf = (ne + G - 1) / G;
   std::vector<std::pair<int32_t, int32_t>> mem;  // (node, group), each pair once
   mem.reserve((size_t)ne * nnpe);
@@ -68,9 +68,17 @@ void place_nodes(const std::vector<uint16_t>& lc, int ne, int nnpe, int L, uint1
     }
   for (int v = 0; v < L; ++v)
     if (!seen[v]) order.push_back(v);
-  const int cap = (L + G - 1) / G;
-  int fill[kBankPairs] = {0};
+  // free positions per (range, residue): next position and how many are left
+  int next[2][kBankPairs], left[2][kBankPairs];
+  const int lo[2] = {0, nint}, hi[2] = {nint, L};
+  for (int g = 0; g < 2; ++g)
+    for (int r = 0; r < G; ++r) {
+      const int p0 = lo[g] + ((r - lo[g] % G) + G) % G;
+      next[g][r] = p0;
+      left[g][r] = p0 < hi[g] ? (hi[g] - 1 - p0) / G + 1 : 0;
+    }
   for (int v : order) {
+    const int g = v < nint ? 0 : 1;
     int64_t cost[kBankPairs] = {0};
     for (int k = gptr[v]; k < gptr[v + 1]; ++k) {
       const int32_t* u = &used[(size_t)mem[k].second * G];
@@ -78,10 +86,13 @@ void place_nodes(const std::vector<uint16_t>& lc, int ne, int nnpe, int L, uint1
     }
     int best = -1;
     for (int r = 0; r < G; ++r) {
-      if (fill[r] >= cap) continue;
-      if (best < 0 || cost[r] < cost[best] || (cost[r] == cost[best] && fill[r] < fill[best])) best = r;
+      if (left[g][r] == 0) continue;
+      if (best < 0 || cost[r] < cost[best] || (cost[r] == cost[best] && left[g][r] > left[g][best]))
+        best = r;
     }
-    pos[v] = (uint16_t)(best + G * fill[best]++);
+    pos[v] = (uint16_t)next[g][best];
+    next[g][best] += G;
+    --left[g][best];
     for (int k = gptr[v]; k < gptr[v + 1]; ++k) ++used[(size_t)mem[k].second * G + best];
   }
 }
@@ -243,8 +254,10 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
   std::fill(stamp.begin(), stamp.end(), -1);
   P.npatch = (int)P.elem_ptr.size() - 1;
 
-  // 3. patches per node
-  std::fill(stamp.begin(), stamp.end(), -1);
+  // 3. patches per node: a node of one patch is interior to it, a node of
+  //    several (or a forced one) is shared, a node of none is an orphan;
+  //    nodes of no element get the reference's lumped solve with M = 0
+  //    (r / M not finite, solid_mechanics_model_mass.cc:79-95)
   std::vector<int32_t> count(nn, 0);
   for (int p = 0; p < P.npatch; ++p)
     for (int32_t i = P.elem_ptr[p]; i < P.elem_ptr[p + 1]; ++i) {
@@ -255,24 +268,18 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
           ++count[c[a]];
         }
     }
-  // shared nodes and their node-major partial slots; nodes of no element
-  // join them with no slot, so they get the reference's lumped solve with
-  // M = 0 (r / M not finite, solid_mechanics_model_mass.cc:79-95)
-  std::vector<int64_t> sidx(nn, -1);
-  P.sptr.push_back(0);
-  for (int64_t i = 0; i < nn; ++i)
-    if (count[i] >= 2 || count[i] == 0 || (force_shared && force_shared[i])) {
-      sidx[i] = (int64_t)P.snodes.size();
-      P.snodes.push_back((uint32_t)i);
-      P.sptr.push_back(P.sptr.back() + count[i]);
-    }
-  P.nslots = P.sptr.back();
-  std::vector<int32_t> sfill(P.snodes.size(), 0);
+  auto is_shared = [&](int64_t v) {
+    return count[v] >= 2 || (count[v] == 1 && force_shared && force_shared[v]);
+  };
 
-  // 4. per patch: local nodes, their shared-memory positions, chunk records
+  // 4. per patch: local nodes (interior first), their shared-memory
+  //    positions, the internal ids of the interior nodes, the shared entries
+  //    and the chunk records
   std::fill(stamp.begin(), stamp.end(), -1);
-  std::vector<int32_t> lidx(nn, -1);
-  P.node_ptr.push_back(0);
+  P.perm.assign(nn, 0xffffffffu);
+  std::vector<int32_t> lidx(nn, -1), rank_fill(nn, 0);
+  std::vector<uint32_t> entry_user;  // caller's id of each shared entry
+  std::vector<uint32_t> entry_rank;  // the patch's rank among the node's patches
   std::vector<uint32_t> local;
   std::vector<uint16_t> lcl, pos;
   std::vector<uint64_t> keyed;
@@ -288,8 +295,11 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
   // FP64 array indexed by piece, the FP64 one over the piece's first slot
   if (piece < 1 || piece > kMaxPiece) throw std::invalid_argument("piece length out of range");
   const int G = contrib_bytes == 8 ? kBankPairs : 32;
+  const int GP = place_group(dim);
   const bool by_piece = contrib_bytes != 8;
   std::vector<int32_t> run_piece0, qof;
+  uint32_t next_id = 0;
+  P.sh_ptr.push_back(0);
   for (int p = 0; p < P.npatch; ++p) {
     const int32_t eb = P.elem_ptr[p], ee = P.elem_ptr[p + 1];
     const int ne_p = ee - eb;
@@ -303,29 +313,42 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
         }
     }
     std::sort(local.begin(), local.end(), [&](uint32_t x, uint32_t y) {
-      const bool sx = sidx[x] >= 0, sy = sidx[y] >= 0;
+      const bool sx = is_shared(x), sy = is_shared(y);
       return sx != sy ? !sx : x < y;
     });
     const int L = (int)local.size();
     int nint = 0;
     for (int j = 0; j < L; ++j) {
       lidx[local[j]] = j;
-      nint += sidx[local[j]] < 0;
+      nint += !is_shared(local[j]);
     }
-    P.ninterior.push_back(nint);
     P.max_nodes = std::max(P.max_nodes, L);
+    P.max_interior = std::max(P.max_interior, nint);
+    P.max_shared = std::max(P.max_shared, L - nint);
     lcl.resize((size_t)ne_p * nnpe);
     for (int32_t i = eb; i < ee; ++i) {
       const uint32_t* c = conn + (int64_t)P.elem_order[i] * nnpe;
       for (int a = 0; a < nnpe; ++a) lcl[(size_t)(i - eb) * nnpe + a] = (uint16_t)lidx[c[a]];
     }
     pos.assign(L, 0);
-    place_nodes(lcl, ne_p, nnpe, L, pos.data());
-    P.lpos.insert(P.lpos.end(), pos.begin(), pos.end());
+    place_nodes(lcl, ne_p, nnpe, L, nint, GP, pos.data());
+    P.ibeg.push_back((int32_t)next_id);
+    P.nint.push_back(nint);
+    const size_t e0 = entry_user.size();
+    entry_user.resize(e0 + (L - nint));
+    entry_rank.resize(e0 + (L - nint));
     for (int j = 0; j < L; ++j) {
-      const int64_t s = sidx[local[j]];
-      P.slot.push_back(s < 0 ? 0xffffffffu : (uint32_t)(P.sptr[s] + sfill[s]++));
+      const uint32_t v = local[j];
+      if (j < nint) {
+        P.perm[v] = next_id + pos[j];
+      } else {
+        const size_t t = e0 + (pos[j] - nint);
+        entry_user[t] = v;
+        entry_rank[t] = (uint32_t)rank_fill[v]++;
+      }
     }
+    next_id += nint;
+    P.sh_ptr.push_back((int32_t)entry_user.size());
     P.chunk_base.push_back((int32_t)P.chunks.size());
     for (int c0 = 0; c0 < ne_p; c0 += kChunk) {
       const int nec = std::min(ne_p - c0, kChunk), ncorner = nec * nnpe;
@@ -445,12 +468,38 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
       P.cdata.insert(P.cdata.end(), rec.begin(), rec.end());
       P.chunk_bytes = std::max(P.chunk_bytes, (int)cd.bytes);
     }
-    P.lnodes.insert(P.lnodes.end(), local.begin(), local.end());
-    P.node_ptr.push_back((int32_t)P.lnodes.size());
   }
   P.chunk_base.push_back((int32_t)P.chunks.size());
-  // positions stay below 16 * ceil(L / 16); a stride of 5 mod 16 puts the
-  // components of a node in different bank pairs
+
+  // 5. internal ids of the shared nodes (in order of first appearance, so
+  //    that the nodes of neighbouring patches stay close) and their partial
+  //    slots (k consecutive slots, one per patch in patch order), then the
+  //    nodes of no element
+  P.shared_base = next_id;
+  for (size_t t = 0; t < entry_user.size(); ++t) {
+    const uint32_t v = entry_user[t];
+    if (P.perm[v] != 0xffffffffu) continue;
+    P.perm[v] = next_id++;
+    P.shared_nodes.push_back(P.perm[v]);
+    P.shared_part.push_back((uint32_t)P.nslots);
+    P.shared_k.push_back((uint32_t)count[v]);
+    P.nslots += count[v];
+  }
+  for (int64_t v = 0; v < nn; ++v)
+    if (count[v] == 0) {
+      P.perm[v] = next_id++;
+      P.orphans.push_back(P.perm[v]);
+    }
+  if ((int64_t)next_id != nn) throw std::logic_error("node numbering is not a bijection");
+  P.sgid.resize(entry_user.size());
+  P.sslot.resize(entry_user.size());
+  for (size_t t = 0; t < entry_user.size(); ++t) {
+    const uint32_t g = P.perm[entry_user[t]];
+    P.sgid[t] = g;
+    P.sslot[t] = P.shared_part[g - P.shared_base] + entry_rank[t];
+  }
+  // positions stay below L; a stride of 5 mod 16 puts the components of a
+  // node's force accumulator in different bank pairs
   P.node_stride = (P.max_nodes + kBankPairs - 1) / kBankPairs * kBankPairs + 5;
   return P;
 }

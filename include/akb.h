@@ -158,9 +158,22 @@ akb_status akb_set_field(akb_model* model, int32_t field, const double* values,
                          int64_t count);
 akb_status akb_get_field(akb_model* model, int32_t field, double* values,
                          int64_t count);
-/* Device address of a field (N x d doubles), valid until akb_model_destroy. */
+/* Device address of a field, valid until akb_model_destroy. Quadrature-point
+ * fields are in element order. Nodal fields (N x d doubles) are in the
+ * model's own node order: in AKB_MODE_FP64 and AKB_MODE_FP32_BULK the fused
+ * step keeps its nodes renumbered so that the nodes of each element patch are
+ * contiguous; akb_get_node_numbering gives the row of each node. A caller
+ * that writes a nodal field through this address calls akb_set_field (or
+ * akb_apply_dirichlet) before the next step, which resets the state the step
+ * derives from it. */
 akb_status akb_field_device_pointer(akb_model* model, int32_t field,
                                     void** device_pointer);
+/* Row of each node in the device arrays of the nodal fields:
+ * row_of_node[i] for the caller's node i (the identity in
+ * AKB_MODE_FP64_REFERENCE and for user materials). No reference
+ * counterpart: the reference's nodal Arrays are in mesh order. */
+akb_status akb_get_node_numbering(const akb_model* model, uint32_t* row_of_node,
+                                  int64_t count);
 
 /* getBlockedDOFs() (solid_mechanics_model.hh:397): N x d bytes, 0 or 1. */
 akb_status akb_set_blocked_dofs(akb_model* model, const uint8_t* blocked,

@@ -121,27 +121,72 @@ long max_group(const std::vector<int>& addr, int banks) {
   return (long)mx;
 }
 
-void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, int piece) {
+void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, int piece,
+           const std::vector<uint8_t>* force = nullptr) {
   const int64_t nn = (int64_t)m.X.size() / m.dim, ne = (int64_t)m.C.size() / m.nnpe;
   PatchHost P = build_patches(m.X.data(), m.C.data(), nn, ne, m.dim, m.nnpe, target, maxn, cbytes,
-                              piece);
+                              piece, force ? force->data() : nullptr);
   const int n = m.nnpe, G = cbytes == 8 ? 16 : 32, LM = P.node_stride, CH = P.contrib_slots;
-  long worst_scatter = 0, worst_sum = 0;
+  const int GP = place_group(m.dim);
+  long worst_scatter = 0, worst_sum = 0, worst_gather = 0;
   int p = -1, c_ = -1;
   std::vector<int> elem_seen(ne, 0);
+  // the internal numbering is a bijection: interior ranges in patch order,
+  // then the shared block, then the nodes of no element
+  std::vector<int> hit(nn, 0);
+  for (int64_t v = 0; v < nn; ++v) {
+    CHECK(P.perm[v] < (uint64_t)nn);
+    if (P.perm[v] < (uint64_t)nn) hit[P.perm[v]]++;
+  }
+  for (int64_t g = 0; g < nn; ++g) CHECK(hit[g] == 1);
+  std::vector<int64_t> user_of(nn, -1);
+  for (int64_t v = 0; v < nn; ++v)
+    if (P.perm[v] < (uint64_t)nn) user_of[P.perm[v]] = v;
+  int64_t next = 0;
+  for (int q = 0; q < P.npatch; ++q) {
+    CHECK(P.ibeg[q] == next);
+    next += P.nint[q];
+  }
+  CHECK(next == (int64_t)P.shared_base);
+  CHECK((int64_t)P.shared_base + (int64_t)P.shared_nodes.size() + (int64_t)P.orphans.size() == nn);
+  // every shared node: its k patches hold it with ranks 0..k-1 (in patch
+  // order), one slot each
+  std::map<uint32_t, std::vector<int>> ranks;
+  for (int q = 0; q < P.npatch; ++q)
+    for (int t = P.sh_ptr[q]; t < P.sh_ptr[q + 1]; ++t) {
+      const int64_t s = (int64_t)P.sgid[t] - P.shared_base;
+      CHECK(s >= 0 && s < (int64_t)P.shared_nodes.size());
+      if (s < 0 || s >= (int64_t)P.shared_nodes.size()) continue;
+      const int r = (int)P.sslot[t] - (int)P.shared_part[s];
+      CHECK(r >= 0 && r < (int)P.shared_k[s]);
+      CHECK((int)ranks[P.sgid[t]].size() == r);  // patches met in order
+      ranks[P.sgid[t]].push_back(r);
+    }
+  // forced (interface) nodes are shared even in one patch
+  if (force)
+    for (int64_t v = 0; v < nn; ++v)
+      if ((*force)[v] && P.perm[v] < P.shared_base) CHECK(false);
+  int64_t slots = 0;
+  for (size_t s = 0; s < P.shared_nodes.size(); ++s) {
+    std::vector<int> r = ranks[P.shared_nodes[s]];
+    std::sort(r.begin(), r.end());
+    CHECK((int)r.size() == (int)P.shared_k[s]);
+    for (int i = 0; i < (int)r.size(); ++i) CHECK(r[i] == i);
+    CHECK(P.shared_part[s] == slots);
+    slots += P.shared_k[s];
+  }
+  CHECK(slots == P.nslots);
   for (p = 0; p < P.npatch; ++p) {
     c_ = -1;
-    const int nb = P.node_ptr[p], L = P.node_ptr[p + 1] - nb, eb = P.elem_ptr[p];
+    const int nint = P.nint[p], s0 = P.sh_ptr[p], L = nint + (P.sh_ptr[p + 1] - s0);
+    const int eb = P.elem_ptr[p];
     const int nep = P.elem_ptr[p + 1] - eb;
-    CHECK(L <= P.max_nodes && nep > 0);
+    CHECK(L <= P.max_nodes && nint <= P.max_interior && L - nint <= P.max_shared && nep > 0);
+    // internal id of the node at each shared-memory position
+    auto id_at = [&](int pos) -> int64_t {
+      return pos < nint ? (int64_t)P.ibeg[p] + pos : (int64_t)P.sgid[s0 + pos - nint];
+    };
     for (int i = eb; i < eb + nep; ++i) elem_seen[P.elem_order[i]]++;
-    std::set<int> ps;
-    for (int j = 0; j < L; ++j) {
-      const int q = P.lpos[nb + j];
-      CHECK(q < 16 * ((L + 15) / 16) && q < LM);
-      ps.insert(q);
-    }
-    CHECK((int)ps.size() == L);
     const int nch = (nep + kChunk - 1) / kChunk;
     CHECK(P.chunk_base[p + 1] - P.chunk_base[p] == nch);
     for (int c = 0; c < nch; ++c) {
@@ -167,7 +212,9 @@ void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, in
       // slots: a bijection onto the chunk's corners
       std::vector<int> owner(CH, -1);
       for (int k = 0; k < nec * n; ++k) {
-        CHECK(sl[k] < CH && lcs[k] < LM);
+        CHECK(sl[k] < CH && lcs[k] < L && lcs[k] < LM);
+        const uint32_t e = P.elem_order[eb + c * kChunk + k / n];
+        if (lcs[k] < L) CHECK(id_at(lcs[k]) == (int64_t)P.perm[m.C[(size_t)e * n + k % n]]);
         if (sl[k] < CH) {
           CHECK(owner[sl[k]] < 0);
           owner[sl[k]] = k;
@@ -237,6 +284,12 @@ void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, in
           for (int e = h * G; e < std::min(nec, h * G + G); ++e) ad.push_back(sl[e * n + a]);
           worst_scatter = std::max(worst_scatter, max_group(ad, G));
         }
+      for (int h = 0; h * GP < nec; ++h)
+        for (int a = 0; a < n; ++a) {
+          std::vector<int> ad;
+          for (int e = h * GP; e < std::min(nec, h * GP + GP); ++e) ad.push_back(lcs[e * n + a]);
+          worst_gather = std::max(worst_gather, max_group(ad, GP));
+        }
       for (int h = 0; h * G < R1; ++h)
         for (int t = 0; t < rows1; ++t) {
           std::vector<int> ad;
@@ -249,8 +302,9 @@ void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, in
   p = c_ = -1;
   for (int64_t e = 0; e < ne; ++e) CHECK(elem_seen[e] == 1);  // every element in one patch
   CHECK(worst_scatter <= 1 && worst_sum <= 1);
-  printf("%-28s patches %5d max_nodes %4d contrib %4d chunk_bytes %5d worst bank group %ld/%ld\n",
-         name, P.npatch, P.max_nodes, CH, P.chunk_bytes, worst_scatter, worst_sum);
+  printf("%-28s patches %5d max_nodes %4d contrib %4d chunk_bytes %5d worst bank group "
+         "%ld/%ld (node gathers %ld)\n",
+         name, P.npatch, P.max_nodes, CH, P.chunk_bytes, worst_scatter, worst_sum, worst_gather);
 }
 
 }  // namespace
@@ -268,6 +322,19 @@ int main() {
   check("tri3 plate small patches", tri_plate(200, 20), 256, 200, 8, 6);
   check("seg2 line fp64", seg_line(3000), 1024, 1100, 8, 2);
   check("seg2 line fp32 piece 1", seg_line(3000), 1024, 1100, 4, 1);
+  {
+    // interface nodes of a partitioned mesh (every node on the plane x = 6)
+    Mesh c = tet_cube(12);
+    std::vector<uint8_t> force(c.X.size() / 3, 0);
+    for (size_t v = 0; v < force.size(); ++v) force[v] = c.X[v * 3] == 6.0;
+    check("tet4 forced interface", c, 1024, 400, 8, 6, &force);
+  }
+  {
+    // nodes of no element, placed after the others
+    Mesh c = tet_cube(6);
+    c.X.insert(c.X.end(), {50, 50, 50, 60, 60, 60});
+    check("tet4 with orphan nodes", c, 256, 200, 8, 6);
+  }
   printf("fails %d\n", fails);
   return fails != 0;
 }
