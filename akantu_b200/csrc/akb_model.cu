@@ -207,17 +207,15 @@ const char* kernel_name(const akb_model* m, int slot) {
   return (slot >= 0 && slot < 3) ? names[slot] : "";
 }
 
-// Patch sizes per element type: elements per patch and the local node cap,
-// chosen so three 256-thread CTAs (two for hexahedra) fit an SM (measured
-// sweeps on the tet4 cube and the hex8 block).
-// Patch size (elements, local node cap) and piece length (contributions one
-// thread adds per node) of the fused step, per element type.
-void patch_params(int type, int* target, int* max_nodes, int* piece) {
+// Patch size of the fused step per element type: elements per patch and the
+// local node cap, chosen so three 256-thread CTAs (two for hexahedra) fit an
+// SM (measured sweeps on the tet4 cube and the hex8 block).
+void patch_params(int type, int* target, int* max_nodes) {
   switch (type) {
-  case AKB_SEGMENT_2: *target = 1024; *max_nodes = 1100; *piece = 2; break;
-  case AKB_TRIANGLE_3: *target = 1024; *max_nodes = 640; *piece = 6; break;
-  case AKB_TETRAHEDRON_4: *target = 1024; *max_nodes = 400; *piece = 6; break;
-  default: *target = 512; *max_nodes = 800; *piece = 8; break;
+  case AKB_SEGMENT_2: *target = 1024; *max_nodes = 1100; break;
+  case AKB_TRIANGLE_3: *target = 1024; *max_nodes = 640; break;
+  case AKB_TETRAHEDRON_4: *target = 1024; *max_nodes = 400; break;
+  default: *target = 512; *max_nodes = 800; break;
   }
 }
 
@@ -233,8 +231,8 @@ akb_status upload(akb_model* m, const std::vector<T>& v, const T** out);
 akb_status plan_patches(akb_model* m, const akb_mesh_desc* mesh, const BatchLayout* batch,
                         const PartLayout* part, PatchHost& P, std::vector<uint32_t>& patch_inst,
                         std::vector<uint32_t>& orphan_inst) {
-  int target, max_nodes, piece;
-  patch_params(m->dm.type, &target, &max_nodes, &piece);
+  int target, max_nodes;
+  patch_params(m->dm.type, &target, &max_nodes);
   if (fp32(m) && m->dm.type == AKB_TETRAHEDRON_4) {
     // FP32 contributions halve the chunk arrays; smaller patches measured
     // 4 % faster on the 6 M-element cube (0.317 against 0.329 ms per step)
@@ -271,7 +269,7 @@ akb_status plan_patches(akb_model* m, const akb_mesh_desc* mesh, const BatchLayo
         for (int64_t i = 0; i < part->n; ++i) force[part->nodes[i]] = 1;
       }
       P = build_patches(mesh->nodes, mesh->connectivity, mesh->nb_nodes, mesh->nb_elements,
-                        m->dm.dim, m->dm.nnpe, target, max_nodes, cbytes, piece,
+                        m->dm.dim, m->dm.nnpe, target, max_nodes, cbytes,
                         part ? force.data() : nullptr);
       return AKB_OK;
     }
@@ -286,7 +284,7 @@ akb_status plan_patches(akb_model* m, const akb_mesh_desc* mesh, const BatchLayo
       lconn.assign(mesh->connectivity + e0 * nn_, mesh->connectivity + (e0 + nei) * nn_);
       for (auto& c : lconn) c -= (uint32_t)n0;
       PatchHost Q = build_patches(mesh->nodes + n0 * dd, lconn.data(), nni, nei, dd, nn_, target,
-                                  max_nodes, cbytes, piece);
+                                  max_nodes, cbytes);
       const int64_t ebase = (int64_t)P.sgid.size(), sbase = P.nslots;
       const int64_t chbase = (int64_t)P.chunks.size();
       const uint32_t dbase16 = (uint32_t)(P.cdata.size() / 8);
@@ -303,7 +301,7 @@ akb_status plan_patches(akb_model* m, const akb_mesh_desc* mesh, const BatchLayo
       P.max_interior = std::max(P.max_interior, Q.max_interior);
       P.max_shared = std::max(P.max_shared, Q.max_shared);
       P.contrib_slots = std::max(P.contrib_slots, Q.contrib_slots);
-      P.max_pieces = std::max(P.max_pieces, Q.max_pieces);
+      P.max_runs = std::max(P.max_runs, Q.max_runs);
       P.chunk_bytes = std::max(P.chunk_bytes, Q.chunk_bytes);
       for (auto g : Q.perm) P.perm.push_back((uint32_t)(g + n0));
       for (auto e : Q.elem_order) P.elem_order.push_back((uint32_t)(e + e0));
@@ -346,7 +344,7 @@ akb_status build_device_patches(akb_model* m, const PatchHost& P,
   d.max_shared = P.max_shared;
   d.node_stride = P.node_stride;
   d.contrib_slots = P.contrib_slots;
-  d.max_pieces = P.max_pieces;
+  d.max_runs = P.max_runs;
   d.chunk_bytes = P.chunk_bytes;
   akb_status st;
   if ((st = upload(m, P.elem_ptr, &d.elem_ptr)) != AKB_OK) return st;

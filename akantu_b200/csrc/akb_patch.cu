@@ -10,7 +10,7 @@
 //   2. element forces in chunks of blockDim elements from shared memory
 //      (akb_fastmath.cuh), each corner vector written to its contribution
 //      slot; one thread per node run adds the run (ascending local element
-//      order) to the node accumulators (the -1 scatter of
+//      order) to the node's accumulator (the -1 scatter of
 //      dof_manager.cc:83-137, without atomics). The record of the next chunk
 //      is copied while this one is used (two buffers, when they fit);
 //   3. finish: each shared node's partial force goes to its slot; the
@@ -35,7 +35,7 @@ namespace {
 constexpr int kThreads = 256;
 
 struct SmemLayout {
-  size_t xs, ws, fs, contrib, scratch, buf, buf_stride, mbar, total;
+  size_t xs, ws, fs, contrib, buf, buf_stride, mbar, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -44,27 +44,25 @@ __host__ __device__ inline size_t align128(size_t x) { return (x + 127) & ~size_
 // Shared-memory layout: node arrays X and w row-major ([position][i], 16
 // bytes of slack in front for the offset of the interior slice), force
 // accumulators component-major ([i][position], row stride LM), the chunk's
-// element vectors component-major ([i][slot], CH slots), FP32 only: FP64
-// piece sums ([i][piece], PM pieces), nbuf chunk record buffers of CB
-// bytes, three mbarriers (two record buffers, the node staging).
-__host__ __device__ inline SmemLayout layout(int LM, int CH, int PM, int CB, int Lmax, int d,
-                                             int sbytes, int nbuf) {
+// element vectors component-major ([i][slot], CH slots), nbuf chunk record
+// buffers of CB bytes, three mbarriers (two record buffers, the node
+// staging).
+__host__ __device__ inline SmemLayout layout(int LM, int CH, int CB, int Lmax, int d, int sbytes,
+                                             int nbuf) {
   SmemLayout s;
   const size_t nb = align16(16 + (size_t)Lmax * d * sizeof(double));
   s.xs = 0;
   s.ws = s.xs + nb;
   s.fs = s.ws + nb;
   s.contrib = s.fs + align16((size_t)LM * d * sizeof(double));
-  s.scratch = align16(s.contrib + (size_t)CH * d * sbytes);
-  s.buf = align128(s.scratch + (sbytes == 8 ? 0 : (size_t)PM * d * sizeof(double)));
+  s.buf = align128(s.contrib + (size_t)CH * d * sbytes);
   s.buf_stride = align128((size_t)CB);
   s.mbar = s.buf + nbuf * s.buf_stride;
   s.total = s.mbar + 24;
   return s;
 }
 __host__ __device__ inline SmemLayout layout(const DevPatches& p, int d, int sbytes, int nbuf) {
-  return layout(p.node_stride, p.contrib_slots, p.max_pieces, p.chunk_bytes, p.max_nodes, d,
-                sbytes, nbuf);
+  return layout(p.node_stride, p.contrib_slots, p.chunk_bytes, p.max_nodes, d, sbytes, nbuf);
 }
 
 // The n local indices of element el (uint16, n per element): one vector load
@@ -259,8 +257,6 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
   double* ws = reinterpret_cast<double*>(smem + lay.ws) + o;
   double* fs = reinterpret_cast<double*>(smem + lay.fs);      // fs[i LM + j]
   S* contrib = reinterpret_cast<S*>(smem + lay.contrib);
-  double* scratch = reinterpret_cast<double*>(smem + lay.scratch);  // FP32: piece sums
-  const int PM = P.max_pieces;
   const int tid = threadIdx.x;
   const uint32_t mb0 = saddr(smem + lay.mbar), mbs = mb0 + 16;
 
@@ -408,76 +404,30 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
         for (int i = 0; i < d; ++i) contrib[i * CH + sl[a]] = fe[a * d + i];
     }
     __syncthreads();
-    // first level: one thread per piece (up to kMaxPiece contributions of
-    // one node, ascending element order); a node in one piece is done, the
-    // sum of a piece of a node in several is left for the second level. The
-    // index loads depend on the header only, so they issue together.
+    // one thread per run (a node's contributions of this chunk, ascending
+    // element order) adds the run to the node's accumulator; runs are sorted
+    // by length, so a warp's threads loop about as long
     const unsigned char* buf = smem + lay.buf + b * lay.buf_stride;
     const uint4 hd = *reinterpret_cast<const uint4*>(buf);  // header: 8 x uint16
     {
-      const int R1 = (int)(hd.x & 0xffff), rows = (int)(hd.x >> 16);
-      const uint32_t* sums = reinterpret_cast<const uint32_t*>(buf + 16 + 2 * A);
-      const uint16_t* ixs = reinterpret_cast<const uint16_t*>(buf + (hd.y & 0xffff));
-      for (int q = tid; q < R1; q += kThreads) {
-        const uint32_t w = sums[q];
-        const int len = (int)((w >> 16) & 0xff), jp = (int)(w & 0xffff);
+      constexpr int G = sizeof(S) == 8 ? 16 : 32;  // runs per group
+      // header words: x = R | ng << 16, y = runs | goff << 16, z = idx | G << 16
+      const int R = (int)(hd.x & 0xffff);
+      const uint32_t* runs = reinterpret_cast<const uint32_t*>(buf + (hd.y & 0xffff));
+      const uint16_t* goff = reinterpret_cast<const uint16_t*>(buf + (hd.y >> 16));
+      const uint16_t* idx = reinterpret_cast<const uint16_t*>(buf + (hd.z & 0xffff));
+      for (int q = tid; q < R; q += kThreads) {
+        const uint32_t w = runs[q];
+        const int len = (int)(w >> 16), jp = (int)(w & 0xffff);
         if (len == 0) continue;
-        // pieces are sorted by length, so the loops below end at nearly the
-        // same trip count across a warp
-        int k[kMaxPiece];
-#pragma unroll
-        for (int t = 0; t < kMaxPiece; ++t) {
-          if (t >= len || t >= rows) break;
-          k[t] = ixs[t * R1 + q];
-        }
+        const uint16_t* ix = idx + goff[q / G] + (q % G);
         double f[3] = {0.0, 0.0, 0.0};
+#pragma unroll 4
+        for (int t = 0; t < len; ++t) {
+          const int k = ix[t * G];
 #pragma unroll
-        for (int t = 0; t < kMaxPiece; ++t) {
-          if (t >= len) break;
-#pragma unroll
-          for (int i = 0; i < d; ++i) f[i] += double(contrib[i * CH + k[t]]);
+          for (int i = 0; i < d; ++i) f[i] += double(contrib[i * CH + k]);
         }
-        if (w >> 24) {  // FP64: over the piece's first slot; FP32: by piece
-#pragma unroll
-          for (int i = 0; i < d; ++i) {
-            if constexpr (sizeof(S) == 8)
-              contrib[i * CH + k[0]] = f[i];
-            else
-              scratch[i * PM + q] = f[i];
-          }
-        } else {
-#pragma unroll
-          for (int i = 0; i < d; ++i) fs[i * LM + jp] -= f[i];
-        }
-      }
-    }
-    if ((hd.y >> 16) != 0) {  // second level: nodes cut in several pieces
-      __syncthreads();
-      const int R2 = (int)(hd.y >> 16), rows = (int)(hd.z & 0xffff);
-      const uint32_t* sums = reinterpret_cast<const uint32_t*>(buf + (hd.z >> 16));
-      const uint16_t* ixs = reinterpret_cast<const uint16_t*>(buf + (hd.w & 0xffff));
-      for (int q = tid; q < R2; q += kThreads) {
-        const uint32_t w = sums[q];
-        constexpr int kUnroll = 4;  // pieces per node read together
-        int k[kUnroll];
-#pragma unroll
-        for (int j = 0; j < kUnroll; ++j) k[j] = j < rows ? ixs[j * R2 + q] : 0;
-        const int np = (int)(w >> 16), jp = (int)(w & 0xffff);
-        double f[3] = {0.0, 0.0, 0.0};
-        auto add = [&](int kk) {
-#pragma unroll
-          for (int i = 0; i < d; ++i) {
-            if constexpr (sizeof(S) == 8)
-              f[i] += double(contrib[i * CH + kk]);
-            else
-              f[i] += scratch[i * PM + kk];
-          }
-        };
-#pragma unroll
-        for (int j = 0; j < kUnroll; ++j)
-          if (j < np) add(k[j]);
-        for (int j = kUnroll; j < np; ++j) add(ixs[j * R2 + q]);
-        if (np == 0) continue;
 #pragma unroll
         for (int i = 0; i < d; ++i) fs[i * LM + jp] -= f[i];
       }

@@ -41,8 +41,6 @@ namespace akb {
 
 // Elements per chunk: the CTA computes one element per thread per chunk.
 constexpr int kChunk = 256;
-// Largest piece (contributions of one node added by one thread).
-constexpr int kMaxPiece = 8;
 // Shared-memory bank pairs (8-byte words): a half-warp reading 8-byte words
 // at 16 distinct (word index mod 16) takes one wavefront.
 constexpr int kBankPairs = 16;
@@ -57,26 +55,25 @@ inline int place_group(int dim) { return dim == 2 ? 8 : 16; }
 // Chunk record: one contiguous, 16-byte aligned block per chunk, staged into
 // shared memory by one TMA bulk copy. Contents (uint16 units unless noted;
 // every section starts on 16 bytes):
-//   header      8 x uint16: R1, rows1, ix1, R2, rows2, r2, ix2, 0 (R: padded
-//               counts, multiples of 32; ix1, r2, ix2: byte offsets)
+//   header      8 x uint16: R, ng, runs, goff, idx, G, 0, 0 (R: run count
+//               padded to a multiple of G; ng = R / G groups; runs, goff,
+//               idx: byte offsets)
 //   corners     per element, the nnpe shared-memory positions of its corner
 //               nodes (at 16 bytes)
 //   slots       per element corner, its slot in the chunk's contribution
 //               array (after the corners, 16-byte aligned)
-//   sums 1      R1 uint32 (at 16 + 2 align16(2 ne_c nnpe) bytes): per piece,
-//               position | count << 16 | (node cut in several pieces) << 24;
-//               a piece is up to `piece` consecutive contributions of one node
-//               (ascending element order), pieces by descending count
-//   index 1     rows1 x R1 (at ix1): row t, column q = the slot of entry t of
-//               piece q
-//   sums 2      R2 uint32 (at r2): per node cut in several pieces,
-//               position | piece count << 16
-//   index 2     rows2 x R2 (at ix2): row j, column q = where the sum of piece
-//               j of node q is (FP64: its first entry's slot; FP32: the
-//               piece's index in sums 1)
-// The slots are a colouring: corner a of G consecutive elements (one scatter
-// instruction) and row t of G consecutive pieces (one sum instruction) hit G
-// different banks (G = 16 for 8-byte contributions, 32 for 4-byte ones).
+//   runs        R uint32: per run (a node's contributions in ascending
+//               element order), position | length << 16; runs by descending
+//               length, G consecutive runs forming a group
+//   goff        ng uint16: where group g's index block starts (in entries)
+//   idx         per group, Lg rows (its longest run) of G entries: entry t of
+//               the group's run l at goff[g] + t G + l is that contribution's
+//               slot
+// One thread sums one run. The slots are a colouring: corner a of G
+// consecutive elements (one scatter instruction) and entry t of a group's
+// runs (one sum instruction) hit G different banks (G = 16 for 8-byte
+// contributions, 32 for 4-byte ones), and the runs of a group have their
+// nodes at distinct positions mod 16 where the build could arrange it.
 struct ChunkDesc {
   uint32_t off16;  // record start in the chunk data, in 16-byte units
   uint32_t bytes;  // record size (multiple of 16)
@@ -89,7 +86,7 @@ struct PatchHost {
   int max_shared = 0;     // largest shared node count of a patch
   int node_stride = 0;    // row stride of the component-major force accumulators
   int contrib_slots = 0;  // largest contribution array of a chunk (per component)
-  int max_pieces = 0;     // largest padded first-level piece count of a chunk
+  int max_runs = 0;       // largest padded run count of a chunk
   int chunk_bytes = 0;    // largest chunk record
   std::vector<uint32_t> perm;        // caller's node id -> internal id
   std::vector<int32_t> elem_ptr;     // npatch + 1, into element order
@@ -113,20 +110,19 @@ struct PatchHost {
 
 // Builds the patches and the internal node order. target_elems: elements per
 // patch; max_nodes: local node cap (<= 60000); contrib_bytes: element vector
-// precision (8: FP64, 4: FP32); piece: contributions one thread adds (<=
-// kMaxPiece); force_shared (per node, or null): nodes treated as shared
+// precision (8: FP64, 4: FP32); force_shared (per node, or null): nodes treated as shared
 // (finished by the second pass from their partials) even when one patch holds
 // them (the interface nodes of a partitioned mesh).
 PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64_t ne, int dim,
                         int nnpe, int target_elems, int max_nodes, int contrib_bytes,
-                        int piece, const uint8_t* force_shared = nullptr);
+                        const uint8_t* force_shared = nullptr);
 
 // Device copy of a PatchHost.
 struct DevPatches {
   int npatch;
   int grid;  // 0: one CTA per patch; > 0: persistent grid of that many CTAs
   int nbuf;  // chunk record buffers in shared memory (2: next chunk prefetched)
-  int max_nodes, max_shared, node_stride, contrib_slots, max_pieces, chunk_bytes;
+  int max_nodes, max_shared, node_stride, contrib_slots, max_runs, chunk_bytes;
   const int32_t* elem_ptr;
   const int32_t* ibeg;
   const int32_t* nint;

@@ -156,7 +156,7 @@ class BipartiteColouring {
 
 PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64_t ne, int dim,
                         int nnpe, int target_elems, int max_nodes, int contrib_bytes,
-                        int piece, const uint8_t* force_shared) {
+                        const uint8_t* force_shared) {
   PatchHost P;
   // 1. element centroids and their Morton keys
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -284,20 +284,13 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
   std::vector<uint16_t> lcl, pos;
   std::vector<uint64_t> keyed;
   struct Run { int32_t node, first, len; };
-  struct Piece { int32_t run, first, len, j; };
   std::vector<Run> runs;
-  std::vector<Piece> pieces;
-  std::vector<int> multi;
-  std::vector<int32_t> hlen, rgbase, eslot, cls;
+  std::vector<int32_t> order, gbase, eslot, cls;
   std::vector<uint16_t> rec;
   // contribution bank groups: 16 bank pairs for 8-byte contributions, 32
-  // banks for 4-byte ones; the FP32 kernel keeps piece sums in a separate
-  // FP64 array indexed by piece, the FP64 one over the piece's first slot
-  if (piece < 1 || piece > kMaxPiece) throw std::invalid_argument("piece length out of range");
+  // banks for 4-byte ones
   const int G = contrib_bytes == 8 ? kBankPairs : 32;
   const int GP = place_group(dim);
-  const bool by_piece = contrib_bytes != 8;
-  std::vector<int32_t> run_piece0, qof;
   uint32_t next_id = 0;
   P.sh_ptr.push_back(0);
   for (int p = 0; p < P.npatch; ++p) {
@@ -352,7 +345,8 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
     P.chunk_base.push_back((int32_t)P.chunks.size());
     for (int c0 = 0; c0 < ne_p; c0 += kChunk) {
       const int nec = std::min(ne_p - c0, kChunk), ncorner = nec * nnpe;
-      // runs: the chunk's corners sorted by (local node, element, corner)
+      // runs: the chunk's corners sorted by (local node, element, corner);
+      // one run is a node's contributions in ascending element order
       keyed.clear();
       for (int e = 0; e < nec; ++e)
         for (int a = 0; a < nnpe; ++a)
@@ -365,43 +359,65 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
         if (runs.empty() || runs.back().node != j) runs.push_back({j, k, 0});
         ++runs.back().len;
       }
-      // pieces: runs cut into pieces of at most `piece` entries, by
-      // descending length; G consecutive pieces are summed together
-      pieces.clear();
-      run_piece0.assign(runs.size(), 0);
-      for (int r = 0; r < (int)runs.size(); ++r) {
-        run_piece0[r] = (int)pieces.size();
-        for (int t0 = 0; t0 < runs[r].len; t0 += piece)
-          pieces.push_back({r, runs[r].first + t0, std::min(piece, runs[r].len - t0), t0 / piece});
+      // run order: by descending length (a warp's threads loop about as
+      // long), and within 16 consecutive runs (a half-warp) the nodes'
+      // positions at distinct residues mod 16 where possible, so that the
+      // read-modify-write of the node accumulators hits distinct bank pairs;
+      // the pick looks at the next runs of the sorted list only
+      std::vector<int32_t> sorted(runs.size());
+      std::iota(sorted.begin(), sorted.end(), 0);
+      std::stable_sort(sorted.begin(), sorted.end(),
+                       [&](int32_t x, int32_t y) { return runs[x].len > runs[y].len; });
+      order.clear();
+      {
+        std::vector<char> taken(runs.size(), 0);
+        size_t head = 0;
+        int used[kBankPairs] = {0};
+        for (size_t q = 0; q < runs.size(); ++q) {
+          if (q % kBankPairs == 0) std::fill(used, used + kBankPairs, 0);
+          while (taken[sorted[head]]) ++head;
+          size_t pick = head;
+          int seen = 0;
+          for (size_t c = head; c < sorted.size() && seen < 3 * G; ++c) {
+            if (taken[sorted[c]]) continue;
+            ++seen;
+            if (!used[pos[runs[sorted[c]].node] % kBankPairs]) {
+              pick = c;
+              break;
+            }
+          }
+          taken[sorted[pick]] = 1;
+          ++used[pos[runs[sorted[pick]].node] % kBankPairs];
+          order.push_back(sorted[pick]);
+        }
       }
-      std::stable_sort(pieces.begin(), pieces.end(), [&](const Piece& x, const Piece& y) {
-        if (x.len != y.len) return x.len > y.len;
-        const int px = pos[runs[x.run].node], py = pos[runs[y.run].node];
-        return px != py ? px < py : x.j < y.j;
-      });
-      const int R1 = (int)pieces.size(), R1p = (R1 + 31) / 32 * 32, nh1 = R1p / G;
-      // sum groups: entry t of G consecutive pieces is one instruction
-      P.max_pieces = std::max(P.max_pieces, R1p);
-      qof.assign(R1, 0);  // sorted index of piece j of run r at run_piece0[r] + j
-      for (int q = 0; q < R1; ++q) qof[run_piece0[pieces[q].run] + pieces[q].j] = q;
-      hlen.assign(nh1, 0);
-      for (int h = 0; h < nh1; ++h) hlen[h] = h * G < R1 ? pieces[h * G].len : 0;
-      rgbase.assign(nh1 + 1, 0);
-      for (int h = 0; h < nh1; ++h) rgbase[h + 1] = rgbase[h] + hlen[h];
-      // colour the (scatter group, sum group) graph: corner a of G
-      // consecutive elements is one scatter instruction, entry t of G
-      // consecutive pieces one sum instruction; a colour is a slot residue
+      const int R = (int)order.size(), Rp = (R + G - 1) / G * G, ng = Rp / G;
+      P.max_runs = std::max(P.max_runs, Rp);
+      // index blocks: group g holds Lg rows (its longest run) of G entries;
+      // entry t of the group's run l at gbase[g] + t G + l
+      gbase.assign(ng + 1, 0);
+      for (int g = 0; g < ng; ++g) {
+        int Lg = 0;
+        for (int l = 0; l < G && g * G + l < R; ++l) Lg = std::max(Lg, runs[order[g * G + l]].len);
+        gbase[g + 1] = gbase[g] + Lg * G;
+      }
+      // colour the (scatter instruction, sum instruction) graph: corner a of
+      // G consecutive elements is one scatter instruction, entry t of a
+      // group's runs one sum instruction; each has at most G contributions,
+      // so G colours suffice (Koenig); a colour is a slot residue
       const int nsg = (nec + G - 1) / G * nnpe;
-      BipartiteColouring bc(nsg, std::max(rgbase[nh1], 1), G);
+      BipartiteColouring bc(nsg, std::max(gbase[ng] / G, 1), G);
       std::vector<int32_t> edge_of(ncorner);
       int ne_ = 0;
-      for (int q = 0; q < R1; ++q)
-        for (int t = 0; t < pieces[q].len; ++t) {
-          const uint64_t kk = keyed[pieces[q].first + t];
+      for (int q = 0; q < R; ++q) {
+        const Run& rn = runs[order[q]];
+        for (int t = 0; t < rn.len; ++t) {
+          const uint64_t kk = keyed[rn.first + t];
           const int e = (int)((kk >> 8) & 0xffffff), a = (int)(kk & 0xff);
-          bc.add((e / G) * nnpe + a, rgbase[q / G] + t);
+          bc.add((e / G) * nnpe + a, gbase[q / G] / G + t);
           edge_of[e * nnpe + a] = ne_++;
         }
+      }
       cls.assign(G, 0);
       eslot.assign(ncorner, 0);
       for (int k = 0; k < ncorner; ++k) {
@@ -411,56 +427,32 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
       int maxcls = 0;
       for (int c = 0; c < G; ++c) maxcls = std::max(maxcls, cls[c]);
       P.contrib_slots = std::max(P.contrib_slots, G * maxcls);
-      auto slot_of = [&](int k) {  // slot of sorted corner k
-        const uint64_t kk = keyed[k];
-        return eslot[((kk >> 8) & 0xffffff) * nnpe + (kk & 0xff)];
-      };
-      // second level: nodes cut into several pieces add the pieces' sums,
-      // left by the first level in the slot of each piece's first entry
-      multi.clear();
-      for (int r = 0; r < (int)runs.size(); ++r)
-        if (runs[r].len > piece) multi.push_back(r);
-      std::stable_sort(multi.begin(), multi.end(), [&](int x, int y) {
-        const int nx = (runs[x].len + piece - 1) / piece, ny = (runs[y].len + piece - 1) / piece;
-        return nx != ny ? nx > ny : pos[runs[x].node] < pos[runs[y].node];
-      });
-      const int R2 = (int)multi.size(), R2p = (R2 + 31) / 32 * 32;
-      // index rows: entry t of piece q at row t, column q (rows1 x R1p);
-      // piece j of second-level node q at row j, column q (rows2 x R2p)
-      const int rows1 = R1 > 0 ? pieces[0].len : 0;
-      const int rows2 = R2 > 0 ? (runs[multi[0]].len + piece - 1) / piece : 0;
       // the record (akb_patch.cuh), offsets in uint16
       const int A = (ncorner + 7) / 8 * 8;
-      const int o_lc = 8, o_cs = o_lc + A, o_r1 = o_cs + A;
-      const int o_i1 = o_r1 + 2 * R1p, o_r2 = o_i1 + rows1 * R1p;
-      const int o_i2 = o_r2 + 2 * R2p, o_end = o_i2 + rows2 * R2p;
-      if (o_end * 2 > 65535) throw std::length_error("chunk record above 64 KB");
+      const int o_lc = 8, o_cs = o_lc + A, o_runs = o_cs + A;
+      const int o_goff = o_runs + 2 * Rp, o_idx = o_goff + (ng + 7) / 8 * 8;
+      const int o_end = o_idx + (gbase[ng] + 7) / 8 * 8;
+      if (o_end * 2 > 65535 || gbase[ng] > 65535)
+        throw std::length_error("chunk record above 64 KB");
       rec.assign(o_end, 0);
-      const int hdr[8] = {R1p, rows1, 2 * o_i1, R2p, rows2, 2 * o_r2, 2 * o_i2, 0};
+      const int hdr[8] = {Rp, ng, 2 * o_runs, 2 * o_goff, 2 * o_idx, G, 0, 0};
       for (int k = 0; k < 8; ++k) rec[k] = (uint16_t)hdr[k];
       for (int k = 0; k < ncorner; ++k) {
         rec[o_lc + k] = pos[lcl[(size_t)c0 * nnpe + k]];
         rec[o_cs + k] = (uint16_t)eslot[k];
       }
-      auto put32 = [&](int at, uint32_t w) {
-        rec[at] = (uint16_t)(w & 0xffff);
-        rec[at + 1] = (uint16_t)(w >> 16);
-      };
-      for (int q = 0; q < R1; ++q) {
-        const Run& rn = runs[pieces[q].run];
-        put32(o_r1 + 2 * q, (uint32_t)pos[rn.node] | ((uint32_t)pieces[q].len << 16) |
-                                ((rn.len > piece ? 1u : 0u) << 24));
-        for (int t = 0; t < pieces[q].len; ++t)
-          rec[o_i1 + t * R1p + q] = (uint16_t)slot_of(pieces[q].first + t);
+      for (int q = 0; q < R; ++q) {
+        const Run& rn = runs[order[q]];
+        const uint32_t w = (uint32_t)pos[rn.node] | ((uint32_t)rn.len << 16);
+        rec[o_runs + 2 * q] = (uint16_t)(w & 0xffff);
+        rec[o_runs + 2 * q + 1] = (uint16_t)(w >> 16);
+        for (int t = 0; t < rn.len; ++t) {
+          const uint64_t kk = keyed[rn.first + t];
+          rec[o_idx + gbase[q / G] + t * G + q % G] =
+              (uint16_t)eslot[((kk >> 8) & 0xffffff) * nnpe + (kk & 0xff)];
+        }
       }
-      for (int q = 0; q < R2; ++q) {
-        const Run& rn = runs[multi[q]];
-        const int np = (rn.len + piece - 1) / piece;
-        put32(o_r2 + 2 * q, (uint32_t)pos[rn.node] | ((uint32_t)np << 16));
-        for (int jj = 0; jj < np; ++jj)
-          rec[o_i2 + jj * R2p + q] =
-              (uint16_t)(by_piece ? qof[run_piece0[multi[q]] + jj] : slot_of(rn.first + jj * piece));
-      }
+      for (int g = 0; g < ng; ++g) rec[o_goff + g] = (uint16_t)gbase[g];
       ChunkDesc cd;
       cd.off16 = (uint32_t)(P.cdata.size() / 8);
       cd.bytes = (uint32_t)rec.size() * 2;

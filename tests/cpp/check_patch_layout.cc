@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <set>
 #include <vector>
@@ -121,14 +122,14 @@ long max_group(const std::vector<int>& addr, int banks) {
   return (long)mx;
 }
 
-void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, int piece,
+void check(const char* name, const Mesh& m, int target, int maxn, int cbytes,
            const std::vector<uint8_t>* force = nullptr) {
   const int64_t nn = (int64_t)m.X.size() / m.dim, ne = (int64_t)m.C.size() / m.nnpe;
   PatchHost P = build_patches(m.X.data(), m.C.data(), nn, ne, m.dim, m.nnpe, target, maxn, cbytes,
-                              piece, force ? force->data() : nullptr);
+                              force ? force->data() : nullptr);
   const int n = m.nnpe, G = cbytes == 8 ? 16 : 32, LM = P.node_stride, CH = P.contrib_slots;
   const int GP = place_group(m.dim);
-  long worst_scatter = 0, worst_sum = 0, worst_gather = 0;
+  long worst_scatter = 0, worst_sum = 0, worst_gather = 0, acc_conflicts = 0, acc_groups = 0;
   int p = -1, c_ = -1;
   std::vector<int> elem_seen(ne, 0);
   // the internal numbering is a bijection: interior ranges in patch order,
@@ -200,15 +201,20 @@ void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, in
       const size_t A = a16((size_t)nec * n * 2);
       const uint16_t* lcs = rec + 8;
       const uint16_t* sl = (const uint16_t*)(rb + 16 + A);
-      const int R1 = rec[0], rows1 = rec[1], ix1 = rec[2], R2 = rec[3], rows2 = rec[4], r2 = rec[5],
-                ix2 = rec[6];
-      CHECK(R1 % 32 == 0 && R2 % 32 == 0 && rows1 <= kMaxPiece && R1 <= P.max_pieces);
-      CHECK(16 + 2 * A + 4 * (size_t)R1 <= (size_t)ix1 && ix1 + 2 * rows1 * R1 <= r2 &&
-            r2 + 4 * R2 <= ix2 && ix2 + 2 * rows2 * R2 <= (int)cd.bytes);
-      const uint32_t* s1 = (const uint32_t*)(rb + 16 + 2 * A);
-      const uint16_t* i1 = (const uint16_t*)(rb + ix1);
-      const uint32_t* s2 = (const uint32_t*)(rb + r2);
-      const uint16_t* i2 = (const uint16_t*)(rb + ix2);
+      const int R = rec[0], ng = rec[1], o_runs = rec[2], o_goff = rec[3], o_idx = rec[4];
+      {
+        // the kernel reads the header as four little-endian 32-bit words
+        uint32_t hd[4];
+        std::memcpy(hd, rec, 16);
+        CHECK((int)(hd[0] & 0xffff) == R && (int)(hd[1] & 0xffff) == o_runs &&
+              (int)(hd[1] >> 16) == o_goff && (int)(hd[2] & 0xffff) == o_idx);
+      }
+      CHECK(rec[5] == G && R % G == 0 && ng * G == R && R <= P.max_runs);
+      CHECK(16 + 2 * A <= (size_t)o_runs && o_runs + 4 * R <= o_goff && o_goff + 2 * ng <= o_idx &&
+            o_idx <= (int)cd.bytes && o_runs % 4 == 0 && o_goff % 2 == 0 && o_idx % 2 == 0);
+      const uint32_t* runs = (const uint32_t*)(rb + o_runs);
+      const uint16_t* goff = (const uint16_t*)(rb + o_goff);
+      const uint16_t* idx = (const uint16_t*)(rb + o_idx);
       // slots: a bijection onto the chunk's corners
       std::vector<int> owner(CH, -1);
       for (int k = 0; k < nec * n; ++k) {
@@ -220,82 +226,66 @@ void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, in
           owner[sl[k]] = k;
         }
       }
-      // sums: contribution k = k + 1; the two levels must give every node
-      // the sum of its corners, each contribution read once
+      // sums: contribution k = k + 1; the runs must give every node the sum
+      // of its corners, each contribution read once, a node in one run
       std::map<int, long> expect, got;
       for (int k = 0; k < nec * n; ++k) expect[lcs[k]] += k + 1;
-      std::vector<long> val(CH, 0), scratch(std::max(R1, 1), 0);
-      for (int s = 0; s < CH; ++s)
-        if (owner[s] >= 0) val[s] = owner[s] + 1;
       std::vector<int> reads(CH, 0);
-      for (int q = 0; q < R1; ++q) {
-        const uint32_t w = s1[q];
-        const int len = (w >> 16) & 0xff, jp = w & 0xffff;
+      for (int q = 0; q < R; ++q) {
+        const int len = runs[q] >> 16, jp = runs[q] & 0xffff;
         if (!len) continue;
-        CHECK(len <= rows1 && jp < LM);
+        CHECK(jp < L && got.count(jp) == 0);
+        const int base = goff[q / G] + q % G;
+        CHECK(q / G + 1 >= ng || base + (len - 1) * G < goff[q / G + 1]);
+        CHECK((size_t)o_idx + 2 * (size_t)(base + (len - 1) * G) < cd.bytes);
         long f = 0;
-        int prev = -1, first = -1;
+        int prev = -1;
         for (int t = 0; t < len; ++t) {
-          const int s = i1[t * R1 + q];
+          const int s = idx[base + t * G];
           CHECK(s < CH && owner[s] >= 0);
           if (s >= CH || owner[s] < 0) continue;
           CHECK(lcs[owner[s]] == jp);       // the run's node
           CHECK(owner[s] / n >= prev);      // ascending element order
           prev = owner[s] / n;
           reads[s]++;
-          f += val[s];
-          if (t == 0) first = s;
+          f += owner[s] + 1;
         }
-        if (w >> 24) {
-          if (G == 16)
-            val[first] = f;  // FP64: the piece's sum over its first slot
-          else
-            scratch[q] = f;  // FP32: by piece
-        } else {
-          got[jp] += f;
-        }
+        got[jp] = f;
       }
       for (int s = 0; s < CH; ++s)
         if (owner[s] >= 0) CHECK(reads[s] == 1);
-      for (int q = 0; q < R2; ++q) {
-        const uint32_t w = s2[q];
-        const int np = w >> 16, jp = w & 0xffff;
-        if (!np) continue;
-        CHECK(np <= rows2 && got.count(jp) == 0);
-        long f = 0;
-        for (int j = 0; j < np; ++j) {
-          const int k = i2[j * R2 + q];
-          if (G == 16) {
-            CHECK(k < CH);
-            if (k < CH) f += val[k];
-          } else {
-            CHECK(k < R1 && (s1[k] >> 24) && (int)(s1[k] & 0xffff) == jp);
-            if (k < R1) f += scratch[k];
-          }
-        }
-        got[jp] += f;
-      }
       CHECK(got == expect);
-      // colouring: one scatter instruction (corner a of G elements), one row
-      // of G pieces: distinct banks
+      // colouring: one scatter instruction (corner a of G elements), entry t
+      // of a group's runs: distinct banks; a group's node accumulators
       for (int h = 0; h * G < nec; ++h)
         for (int a = 0; a < n; ++a) {
           std::vector<int> ad;
           for (int e = h * G; e < std::min(nec, h * G + G); ++e) ad.push_back(sl[e * n + a]);
           worst_scatter = std::max(worst_scatter, max_group(ad, G));
         }
+      for (int g = 0; g < ng; ++g) {
+        int Lg = 0;
+        for (int q = g * G; q < g * G + G; ++q) Lg = std::max(Lg, (int)(runs[q] >> 16));
+        for (int t = 0; t < Lg; ++t) {
+          std::vector<int> ad;
+          for (int q = g * G; q < g * G + G; ++q)
+            if (t < (int)(runs[q] >> 16)) ad.push_back(idx[goff[g] + t * G + q % G]);
+          worst_sum = std::max(worst_sum, max_group(ad, G));
+        }
+        std::vector<int> acc;
+        for (int q = g * G; q < g * G + G; ++q)
+          if (runs[q] >> 16) acc.push_back(runs[q] & 0xffff);
+        for (int hh = 0; hh < (int)acc.size(); hh += 16) {
+          std::vector<int> half(acc.begin() + hh, acc.begin() + std::min((int)acc.size(), hh + 16));
+          acc_conflicts += max_group(half, 16) - 1;
+          acc_groups++;
+        }
+      }
       for (int h = 0; h * GP < nec; ++h)
         for (int a = 0; a < n; ++a) {
           std::vector<int> ad;
           for (int e = h * GP; e < std::min(nec, h * GP + GP); ++e) ad.push_back(lcs[e * n + a]);
           worst_gather = std::max(worst_gather, max_group(ad, GP));
-        }
-      for (int h = 0; h * G < R1; ++h)
-        for (int t = 0; t < rows1; ++t) {
-          std::vector<int> ad;
-          for (int q = h * G; q < h * G + G; ++q)
-            if (t < (int)((s1[q] >> 16) & 0xff)) ad.push_back(i1[t * R1 + q]);
-          worst_sum = std::max(worst_sum, max_group(ad, G));
         }
     }
   }
@@ -303,37 +293,38 @@ void check(const char* name, const Mesh& m, int target, int maxn, int cbytes, in
   for (int64_t e = 0; e < ne; ++e) CHECK(elem_seen[e] == 1);  // every element in one patch
   CHECK(worst_scatter <= 1 && worst_sum <= 1);
   printf("%-28s patches %5d max_nodes %4d contrib %4d chunk_bytes %5d worst bank group "
-         "%ld/%ld (node gathers %ld)\n",
-         name, P.npatch, P.max_nodes, CH, P.chunk_bytes, worst_scatter, worst_sum, worst_gather);
+         "%ld/%ld (node gathers %ld, accumulator conflicts %.2f per half-warp)\n",
+         name, P.npatch, P.max_nodes, CH, P.chunk_bytes, worst_scatter, worst_sum, worst_gather,
+         acc_groups ? (double)acc_conflicts / acc_groups : 0.0);
 }
 
 }  // namespace
 
 int main() {
-  check("tet4 cube 20 fp64", tet_cube(20), 1024, 400, 8, 6);
-  check("tet4 cube 20 fp32", tet_cube(20), 768, 320, 4, 6);
-  check("tet4 shuffled fp64", shuffled(tet_cube(12), 1), 1024, 400, 8, 6);
-  check("tet4 shuffled fp32 piece 2", shuffled(tet_cube(12), 2), 1024, 400, 4, 2);
-  check("tet4 odd sizes", tet_cube(7), 300, 150, 8, 6);
-  check("tet4 star", star(300), 1024, 400, 8, 6);
-  check("hex8 cube fp64", hex_cube(16), 512, 800, 8, 8);
-  check("hex8 cube fp32 piece 3", hex_cube(16), 512, 800, 4, 3);
-  check("tri3 plate", tri_plate(200, 20), 1024, 640, 8, 6);
-  check("tri3 plate small patches", tri_plate(200, 20), 256, 200, 8, 6);
-  check("seg2 line fp64", seg_line(3000), 1024, 1100, 8, 2);
-  check("seg2 line fp32 piece 1", seg_line(3000), 1024, 1100, 4, 1);
+  check("tet4 cube 20 fp64", tet_cube(20), 1024, 400, 8);
+  check("tet4 cube 20 fp32", tet_cube(20), 768, 320, 4);
+  check("tet4 shuffled fp64", shuffled(tet_cube(12), 1), 1024, 400, 8);
+  check("tet4 shuffled fp32", shuffled(tet_cube(12), 2), 1024, 400, 4);
+  check("tet4 odd sizes", tet_cube(7), 300, 150, 8);
+  check("tet4 star", star(300), 1024, 400, 8);
+  check("hex8 cube fp64", hex_cube(16), 512, 800, 8);
+  check("hex8 cube fp32", hex_cube(16), 512, 800, 4);
+  check("tri3 plate", tri_plate(200, 20), 1024, 640, 8);
+  check("tri3 plate small patches", tri_plate(200, 20), 256, 200, 8);
+  check("seg2 line fp64", seg_line(3000), 1024, 1100, 8);
+  check("seg2 line fp32", seg_line(3000), 1024, 1100, 4);
   {
     // interface nodes of a partitioned mesh (every node on the plane x = 6)
     Mesh c = tet_cube(12);
     std::vector<uint8_t> force(c.X.size() / 3, 0);
     for (size_t v = 0; v < force.size(); ++v) force[v] = c.X[v * 3] == 6.0;
-    check("tet4 forced interface", c, 1024, 400, 8, 6, &force);
+    check("tet4 forced interface", c, 1024, 400, 8, &force);
   }
   {
     // nodes of no element, placed after the others
     Mesh c = tet_cube(6);
     c.X.insert(c.X.end(), {50, 50, 50, 60, 60, 60});
-    check("tet4 with orphan nodes", c, 256, 200, 8, 6);
+    check("tet4 with orphan nodes", c, 256, 200, 8);
   }
   printf("fails %d\n", fails);
   return fails != 0;
