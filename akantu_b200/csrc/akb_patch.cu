@@ -35,7 +35,7 @@ namespace {
 constexpr int kThreads = 256;
 
 struct SmemLayout {
-  size_t xs, ws, fs, contrib, buf, buf_stride, mbar, total;
+  size_t xs, ws, fs, contrib, sslot, buf, buf_stride, mbar, total;
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -44,25 +44,27 @@ __host__ __device__ inline size_t align128(size_t x) { return (x + 127) & ~size_
 // Shared-memory layout: node arrays X and w row-major ([position][i], 16
 // bytes of slack in front for the offset of the interior slice), force
 // accumulators component-major ([i][position], row stride LM), the chunk's
-// element vectors component-major ([i][slot], CH slots), nbuf chunk record
-// buffers of CB bytes, three mbarriers (two record buffers, the node
-// staging).
-__host__ __device__ inline SmemLayout layout(int LM, int CH, int CB, int Lmax, int d, int sbytes,
-                                             int nbuf) {
+// element vectors (CH slots, cidx), the partial slot of each shared node
+// (SHmax uint32), nbuf chunk record buffers of CB bytes, three mbarriers (two
+// record buffers, the node staging).
+__host__ __device__ inline SmemLayout layout(int LM, int CH, int CB, int Lmax, int SHmax, int d,
+                                             int sbytes, int nbuf) {
   SmemLayout s;
   const size_t nb = align16(16 + (size_t)Lmax * d * sizeof(double));
   s.xs = 0;
   s.ws = s.xs + nb;
   s.fs = s.ws + nb;
   s.contrib = s.fs + align16((size_t)LM * d * sizeof(double));
-  s.buf = align128(s.contrib + (size_t)CH * d * sbytes);
+  s.sslot = align16(s.contrib + (size_t)CH * d * sbytes);
+  s.buf = align128(s.sslot + (size_t)SHmax * sizeof(uint32_t));
   s.buf_stride = align128((size_t)CB);
   s.mbar = s.buf + nbuf * s.buf_stride;
   s.total = s.mbar + 24;
   return s;
 }
 __host__ __device__ inline SmemLayout layout(const DevPatches& p, int d, int sbytes, int nbuf) {
-  return layout(p.node_stride, p.contrib_slots, p.chunk_bytes, p.max_nodes, d, sbytes, nbuf);
+  return layout(p.node_stride, p.contrib_slots, p.chunk_bytes, p.max_nodes, p.max_shared, d, sbytes,
+                nbuf);
 }
 
 // The n local indices of element el (uint16, n per element): one vector load
@@ -124,6 +126,16 @@ __device__ inline void gather_differences(const double* xs, const double* ws, co
       }
     }
   }
+}
+
+// Where component i of contribution slot k sits: 3D contributions are rows
+// of three (one address per slot; 3 is invertible mod 16 and mod 32, so
+// slots at distinct residues keep distinct banks), 1D and 2D ones
+// component-major ([i][slot], 16-byte loads in 2D would otherwise pair slots
+// on one bank group).
+template <int d>
+__device__ inline int cidx(int k, int i, int CH) {
+  return d == 3 ? 3 * k + i : i * CH + k;
 }
 
 // CTAs per SM each instantiation is built for (register budget).
@@ -327,8 +339,10 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
       cp_async8(ws + k, P.w + (size_t)ib * d + k);
     }
   }
+  uint32_t* sslot = reinterpret_cast<uint32_t*>(smem + lay.sslot);
   for (int t = tid; t < nsh; t += kThreads) {
     const int64_t g = P.sgid[s0 + t];
+    sslot[t] = P.sslot[s0 + t];  // for the finish
     const int j = nint + t;
     if constexpr (d == 2) {
       cp_async16(xs + 2 * j, m.X + g * 2);
@@ -401,7 +415,7 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
 #pragma unroll
       for (int a = 0; a < n; ++a)
 #pragma unroll
-        for (int i = 0; i < d; ++i) contrib[i * CH + sl[a]] = fe[a * d + i];
+        for (int i = 0; i < d; ++i) contrib[cidx<d>(sl[a], i, CH)] = fe[a * d + i];
     }
     __syncthreads();
     // one thread per run (a node's contributions of this chunk, ascending
@@ -426,7 +440,7 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
         for (int t = 0; t < len; ++t) {
           const int k = ix[t * G];
 #pragma unroll
-          for (int i = 0; i < d; ++i) f[i] += double(contrib[i * CH + k]);
+          for (int i = 0; i < d; ++i) f[i] += double(contrib[cidx<d>(k, i, CH)]);
         }
 #pragma unroll
         for (int i = 0; i < d; ++i) fs[i * LM + jp] -= f[i];
@@ -458,7 +472,7 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
   //    contiguous in the global arrays
   for (int k = tid; k < nsh * d; k += kThreads) {
     const int t = k / d, i = k - t * d;
-    P.partial[(size_t)P.sslot[s0 + t] * d + i] = fs[i * LM + nint + t];
+    P.partial[(size_t)sslot[t] * d + i] = fs[i * LM + nint + t];
   }
   const int items = nint * d;
   for (int base = 0; base < items; base += kThreads * kBatch) {
