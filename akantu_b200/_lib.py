@@ -64,6 +64,14 @@ SIGNATURES = {
     "akb_part_step_end": (I32, [P, P]),
     "akb_part_export_mass": (I32, [P, P]),
     "akb_part_import_mass": (I32, [P, P]),
+    # include/akb_mesh.h
+    "akb_msh_read": (I32, [C.c_char_p, I32, C.POINTER(P)]),
+    "akb_msh_parse": (I32, [C.c_char_p, I64, I32, C.POINTER(P)]),
+    "akb_msh_destroy": (I32, [P]),
+    "akb_msh_get_mesh": (I32, [P, C.POINTER(_abi.MeshDesc)]),
+    "akb_msh_get_nb_groups": (I32, [P, C.POINTER(I32)]),
+    "akb_msh_get_group": (I32, [P, I32, C.POINTER(C.c_char_p), C.POINTER(I64), C.POINTER(PU32),
+                                C.POINTER(I64), C.POINTER(PU32)]),
     # include/akb_fe2.h
     "akb_step_begin": (I32, [P]),
     "akb_step_end": (I32, [P]),

@@ -33,8 +33,8 @@ class BatchModel(SolidMechanicsModel):
                                      for m, o in zip(self.meshes, noff[:-1])]).astype(np.uint32))
         mats = [m if not isinstance(m, dict) else material_from_dict(m) for m in materials]
         super().__init__(union, mats, precision=precision, device=device, stream=stream,
-                         patch_elements=patch_elements, patch_nodes=patch_nodes)
-        self._grid = int(patch_grid)
+                         patch_elements=patch_elements, patch_nodes=patch_nodes,
+                         patch_grid=patch_grid)
         self.node_offsets = noff
         self.element_offsets = eoff
 
@@ -57,8 +57,7 @@ class BatchModel(SolidMechanicsModel):
         mesh_arr = (_abi.MeshDesc * len(descs))(*descs)
         mat_arr = (_abi.MaterialDesc * len(self._materials))(*[m.desc() for m in self._materials])
         bd = _abi.BatchDesc(len(descs), mesh_arr, mat_arr)
-        opt = _abi.ModelOptions(self._precision, self._device, self._stream, *self._patch,
-                                self._grid)
+        opt = _abi.ModelOptions(self._precision, self._device, self._stream, *self._patch)
         h = C.c_void_p()
         check(lib().akb_batch_create(C.byref(bd), C.byref(opt), C.byref(h)))
         self._h = h

@@ -1,4 +1,5 @@
-"""Mesh container, Gmsh v2 reader and structured mesh generators.
+"""Mesh container, Gmsh reader (through libakb.so) and structured mesh
+generators.
 
 Mirrors the subset of akantu::Mesh the explicit path uses (mesh.hh:100):
 nodal coordinates (getNodes, mesh.hh:293), one connectivity array of the
@@ -6,6 +7,9 @@ spatial dimension's element type (getConnectivity, mesh.hh:353) and node
 groups for boundary conditions (GroupManager, group_manager.hh:63).
 """
 from __future__ import annotations
+
+import ctypes as C
+import os
 
 import numpy as np
 
@@ -19,11 +23,6 @@ ELEMENT_TYPES = {
     _abi.HEXAHEDRON_8: ("_hexahedron_8", 3, 8, 8),
 }
 NAME_TO_TYPE = {v[0]: k for k, v in ELEMENT_TYPES.items()}
-
-# gmsh element type -> akantu type (mesh_io_msh.cc: _msh_to_akantu_element_types);
-# no node permutation for these types (mesh_io_msh.cc:224-276).
-_MSH_TYPES = {1: _abi.SEGMENT_2, 2: _abi.TRIANGLE_3, 4: _abi.TETRAHEDRON_4,
-              5: _abi.HEXAHEDRON_8}
 
 # boundary facets of each element type (local node indices)
 _FACETS = {
@@ -52,6 +51,7 @@ class Mesh:
         self.connectivity = np.zeros((0, 0), dtype=np.uint32) if connectivity is None \
             else np.ascontiguousarray(connectivity, dtype=np.uint32)
         self.node_groups: dict[str, np.ndarray] = {}
+        self.element_groups: dict[str, np.ndarray] = {}
 
     # --- reference-style accessors -------------------------------------
     def getNodes(self):
@@ -78,54 +78,54 @@ class Mesh:
 
     # --- Gmsh reader (MeshIOMSH::read, mesh_io_msh.cc) ------------------
     def read(self, filename):
-        with open(filename) as fh:
-            text = fh.read()
-        self.read_msh_text(text)
+        """Mesh::read of a Gmsh ASCII 2.x file through libakb.so
+        (include/akb_mesh.h): the elements of this mesh's spatial dimension,
+        all nodes, and one node group and element group per physical name."""
+        from . import _lib
+        h = C.c_void_p()
+        _lib.check(_lib.lib().akb_msh_read(os.fsencode(filename), self.spatial_dimension,
+                                           C.byref(h)))
+        self._take(h)
 
     def read_msh_text(self, text):
-        """Gmsh ASCII v2 reader: nodes in file order, elements of this mesh's
-        spatial dimension; lower-dimension elements are kept by physical tag
-        as node groups named 'physical_<tag>'."""
-        lines = [ln.strip() for ln in text.splitlines()]
-        i = 0
-        tag_to_index = {}
-        nodes = []
-        blocks: dict[int, list] = {}
-        groups: dict[str, set] = {}
-        while i < len(lines):
-            ln = lines[i]
-            if ln == "$Nodes":
-                n = int(lines[i + 1])
-                for k in range(n):
-                    parts = lines[i + 2 + k].split()
-                    tag_to_index[int(parts[0])] = k
-                    nodes.append([float(x) for x in parts[1:1 + self.spatial_dimension]])
-                i += n + 2
-                continue
-            if ln == "$Elements":
-                n = int(lines[i + 1])
-                for k in range(n):
-                    parts = [int(x) for x in lines[i + 2 + k].split()]
-                    etype, ntags = parts[1], parts[2]
-                    tags = parts[3:3 + ntags]
-                    conn = [tag_to_index[t] for t in parts[3 + ntags:]]
-                    akt = _MSH_TYPES.get(etype)
-                    if akt is not None and ELEMENT_TYPES[akt][1] == self.spatial_dimension:
-                        blocks.setdefault(akt, []).append(conn)
-                    elif tags:
-                        groups.setdefault("physical_%d" % tags[0], set()).update(conn)
-                i += n + 2
-                continue
-            i += 1
-        if len(blocks) != 1:
-            raise ValueError("expected one element type of dimension %d, found %s"
-                             % (self.spatial_dimension, list(blocks)))
-        (akt, conn), = blocks.items()
-        self.element_type = akt
-        self.nodes = np.asarray(nodes, dtype=np.float64).reshape(-1, self.spatial_dimension)
-        self.connectivity = np.asarray(conn, dtype=np.uint32)
-        for name, s in groups.items():
-            self.node_groups[name] = np.array(sorted(s), dtype=np.int64)
+        """The same from the text of a Gmsh file."""
+        from . import _lib
+        data = text.encode() if isinstance(text, str) else bytes(text)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().akb_msh_parse(data, len(data), self.spatial_dimension, C.byref(h)))
+        self._take(h)
+
+    def _take(self, h):
+        from . import _abi, _lib
+        L = _lib.lib()
+        try:
+            desc = _abi.MeshDesc()
+            _lib.check(L.akb_msh_get_mesh(h, C.byref(desc)))
+            d = desc.spatial_dimension
+            n = ELEMENT_TYPES[desc.element_type][2]
+            self.element_type = desc.element_type
+            self.nodes = np.ctypeslib.as_array(desc.nodes, (desc.nb_nodes * d,)).reshape(-1, d).copy()
+            self.connectivity = np.ctypeslib.as_array(
+                desc.connectivity, (desc.nb_elements * n,)).reshape(-1, n).copy()
+            ng = C.c_int32()
+            _lib.check(L.akb_msh_get_nb_groups(h, C.byref(ng)))
+            self.node_groups, self.element_groups = {}, {}
+            for k in range(ng.value):
+                name = C.c_char_p()
+                nn, ne = C.c_int64(), C.c_int64()
+                pn, pe = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
+                _lib.check(L.akb_msh_get_group(h, k, C.byref(name), C.byref(nn), C.byref(pn),
+                                               C.byref(ne), C.byref(pe)))
+                key = name.value.decode()
+                self.node_groups[key] = (np.ctypeslib.as_array(pn, (nn.value,)).astype(np.int64)
+                                         if nn.value else np.zeros(0, np.int64))
+                self.element_groups[key] = (np.ctypeslib.as_array(pe, (ne.value,)).astype(np.int64)
+                                            if ne.value else np.zeros(0, np.int64))
+        finally:
+            L.akb_msh_destroy(h)
+
+    def getElementGroup(self, name):
+        return self.element_groups[name]
 
     # --- boundary groups (Mesh::createBoundaryGroupFromGeometry) ---------
     def boundary_nodes(self):

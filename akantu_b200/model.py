@@ -120,10 +120,12 @@ class SolidMechanicsModel:
 
     def __init__(self, mesh, materials=None, element_material=None,
                  precision=_abi.MODE_FP64_REFERENCE, device=0, stream=None,
-                 patch_elements=0, patch_nodes=0, interface_nodes=None):
+                 patch_elements=0, patch_nodes=0, interface_nodes=None, patch_grid=0):
         """interface_nodes: this model is one part of a partitioned mesh
         (akb_model_create_part), these of its nodes are shared with other
-        parts; step it through akantu_b200.decompose.DistributedModel."""
+        parts; step it through akantu_b200.decompose.DistributedModel.
+        patch_elements, patch_nodes, patch_grid: the fused step's patch shape
+        and schedule (akb_model_options; 0 = defaults)."""
         self.mesh = mesh
         self._iface = None if interface_nodes is None else \
             np.ascontiguousarray(interface_nodes, dtype=np.uint32)
@@ -133,7 +135,7 @@ class SolidMechanicsModel:
         self._precision = precision
         self._device = device
         self._stream = stream
-        self._patch = (int(patch_elements), int(patch_nodes))
+        self._patch = (int(patch_elements), int(patch_nodes), int(patch_grid))
         self._h = None
         self._user = []
         self._mirrors = {}

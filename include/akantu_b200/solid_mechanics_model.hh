@@ -21,6 +21,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -28,6 +29,7 @@
 
 #include "../akb.h"
 #include "../akb_fe2.h"
+#include "../akb_mesh.h"
 
 namespace akantu_b200 {
 
@@ -84,9 +86,57 @@ class Array {
   std::vector<T> v_;
 };
 
+// A named group of nodes and of the mesh's elements (GroupManager,
+// group_manager.hh:63), as Mesh::read builds them from physical names.
+struct NodeGroup {
+  std::string name;
+  std::vector<uint32_t> nodes;
+  std::vector<uint32_t> elements;
+  UInt size() const { return (UInt)nodes.size(); }
+  std::vector<uint32_t>::const_iterator begin() const { return nodes.begin(); }
+  std::vector<uint32_t>::const_iterator end() const { return nodes.end(); }
+};
+
 class Mesh {
  public:
   explicit Mesh(UInt spatial_dimension) : dim_(spatial_dimension), nodes_(0, spatial_dimension) {}
+  // Mesh::read (mesh.hh:133) of a Gmsh ASCII 2.x file (include/akb_mesh.h):
+  // elements of the spatial dimension, nodes, and one group per physical name.
+  void read(const std::string& filename) {
+    akb_msh* m = nullptr;
+    check(akb_msh_read(filename.c_str(), (int32_t)dim_, &m));
+    akb_mesh_desc d;
+    akb_status st = akb_msh_get_mesh(m, &d);
+    int32_t ng = 0;
+    if (st == AKB_OK) st = akb_msh_get_nb_groups(m, &ng);
+    if (st != AKB_OK) {
+      akb_msh_destroy(m);
+      check(st);
+    }
+    setElementType((ElementType)d.element_type);
+    nodes_.resize((UInt)d.nb_nodes, dim_);
+    std::copy(d.nodes, d.nodes + d.nb_nodes * dim_, nodes_.storage());
+    const UInt n = conn_.getNbComponent();
+    conn_.resize((UInt)d.nb_elements, n);
+    std::copy(d.connectivity, d.connectivity + d.nb_elements * n, conn_.storage());
+    groups_.clear();
+    for (int32_t k = 0; k < ng; ++k) {
+      const char* name;
+      int64_t nn, ne;
+      const uint32_t *pn, *pe;
+      check(akb_msh_get_group(m, k, &name, &nn, &pn, &ne, &pe));
+      NodeGroup g{name, std::vector<uint32_t>(pn, pn + nn), std::vector<uint32_t>(pe, pe + ne)};
+      groups_[g.name] = std::move(g);
+    }
+    akb_msh_destroy(m);
+  }
+  const NodeGroup& getNodeGroup(const std::string& name) const {
+    auto it = groups_.find(name);
+    if (it == groups_.end()) throw Exception(AKB_ERR_INVALID_ARGUMENT, "no group " + name);
+    return it->second;
+  }
+  const NodeGroup& getElementGroup(const std::string& name) const { return getNodeGroup(name); }
+  const std::map<std::string, NodeGroup>& iterateNodeGroups() const { return groups_; }
   Array<Real>& getNodes() { return nodes_; }
   const Array<Real>& getNodes() const { return nodes_; }
   Array<uint32_t>& getConnectivity() { return conn_; }
@@ -105,6 +155,7 @@ class Mesh {
   ElementType type_ = _triangle_3;
   Array<Real> nodes_;
   Array<uint32_t> conn_;
+  std::map<std::string, NodeGroup> groups_;
 };
 
 // material elastic [ rho, E, nu, Plane_Stress, finite_deformation ]
@@ -225,11 +276,15 @@ class SolidMechanicsModel {
     return blocked_;
   }
 
-  // applyBC(FixedValue, group): the group is given as its node list
+  // applyBC(FixedValue, group) (boundary_condition_tmpl.hh:186-200): by the
+  // group's name, or by its node list
   void applyBC(const BC::Dirichlet::FixedValue& f, const std::vector<uint32_t>& nodes) {
     sync_in();
     std::vector<Real> vals(nodes.size(), f.value);
     check(akb_apply_dirichlet(h_, nodes.data(), (int64_t)nodes.size(), f.axis, vals.data()));
+  }
+  void applyBC(const BC::Dirichlet::FixedValue& f, const std::string& group) {
+    applyBC(f, mesh_.getNodeGroup(group).nodes);
   }
 
   Real getEnergy(const std::string& id) {

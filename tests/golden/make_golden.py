@@ -12,12 +12,22 @@ committed so the tests never read the reference at run time).
       tetrahedron_4,hexahedron_8}.msh (Gmsh v2, parsed by akantu_b200.mesh)
       and the material sections of material_check_stress_plane_strain.dat and
       material_lumped.dat.
+  msh/*.msh
+      the Gmsh files themselves, as text, for the mesh reader's tests: the
+      three patch-test meshes, test_materials/1_tetrahedron.msh (finite
+      deformation test), material_selector.msh (named 1D groups) and
+      test_cohesive/data/cohesive_strait_2D.msh (named 2D groups).
+  reference_materials.json
+      the material sections of test_materials/material_finite_deformation.dat,
+      test_solid_mechanics_model_dynamics_material.dat and
+      test_energies/test_solid_mechanics_model_work_material.dat.
 
-usage: python tests/golden/make_golden.py [reference_root]
+usage: python tests/golden/make_golden.py REFERENCE_ROOT
 """
 import json
 import os
 import re
+import shutil
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -80,8 +90,29 @@ def main(ref):
     }
     with open(os.path.join(HERE, "patch_meshes.json"), "w") as fh:
         json.dump({"meshes": meshes, "materials": materials}, fh, indent=0)
+
+    smm = "test/test_model/test_solid_mechanics_model"
+    msh_dir = os.path.join(HERE, "msh")
+    os.makedirs(msh_dir, exist_ok=True)
+    for src in ("test/test_model/patch_tests/data/_triangle_3.msh",
+                "test/test_model/patch_tests/data/_tetrahedron_4.msh",
+                "test/test_model/patch_tests/data/_hexahedron_8.msh",
+                smm + "/test_materials/1_tetrahedron.msh",
+                smm + "/material_selector.msh",
+                smm + "/test_cohesive/data/cohesive_strait_2D.msh"):
+        shutil.copyfile(os.path.join(ref, src), os.path.join(msh_dir, os.path.basename(src)))
+    mats = {
+        "finite_deformation": smm + "/test_materials/material_finite_deformation.dat",
+        "dynamics": smm + "/test_solid_mechanics_model_dynamics_material.dat",
+        "work": smm + "/test_energies/test_solid_mechanics_model_work_material.dat",
+    }
+    with open(os.path.join(HERE, "reference_materials.json"), "w") as fh:
+        json.dump({k: dict(parse_material_dat(os.path.join(ref, v)), source=v)
+                   for k, v in mats.items()}, fh, indent=1)
     print("wrote fixtures to", HERE)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    main(sys.argv[1])
