@@ -180,19 +180,30 @@ def plate_triangle3(nx, ny, lx, ly, origin=(0.0, 0.0)):
     return Mesh(2, _abi.TRIANGLE_3, nodes, conn)
 
 
-def _grid_nodes_3d(n, length):
-    xs = np.arange(n + 1, dtype=np.float64) * (length / n)
-    Z, Y, X = np.meshgrid(xs, xs, xs, indexing="ij")
+def _grid_nodes_3d(nx, lx, ny=None, ly=None, nz=None, lz=None):
+    ny, nz = ny or nx, nz or nx
+    ly, lz = ly or lx, lz or lx
+    xs = np.arange(nx + 1, dtype=np.float64) * (lx / nx)
+    ys = np.arange(ny + 1, dtype=np.float64) * (ly / ny)
+    zs = np.arange(nz + 1, dtype=np.float64) * (lz / nz)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
     return np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
 
 
 def cube_tetrahedron4(n, length=1.0):
     """n^3 cubes, each split into 6 tetrahedra around the (0,0,0)-(1,1,1)
     diagonal (Kuhn split), all positively oriented; nodes x-fastest."""
-    nodes = _grid_nodes_3d(n, length)
-    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
-    base = (k * (n + 1) * (n + 1) + j * (n + 1) + i).ravel()
-    off = {"x": 1, "y": n + 1, "z": (n + 1) * (n + 1)}
+    return box_tetrahedron4(n, n, n, length, length, length)
+
+
+def box_tetrahedron4(nx, ny, nz, lx, ly, lz):
+    """nx x ny x nz boxes over lx x ly x lz, each split into 6 tetrahedra
+    around its (0,0,0)-(1,1,1) diagonal (Kuhn split), all positively
+    oriented; nodes x-fastest, elements box by box (x-fastest), six per box."""
+    nodes = _grid_nodes_3d(nx, lx, ny, ly, nz, lz)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    base = (k * (ny + 1) * (nx + 1) + j * (nx + 1) + i).ravel()
+    off = {"x": 1, "y": nx + 1, "z": (nx + 1) * (ny + 1)}
     tets = []
     for perm in ("xyz", "xzy", "yxz", "yzx", "zxy", "zyx"):
         a = off[perm[0]]
@@ -210,10 +221,16 @@ def cube_tetrahedron4(n, length=1.0):
 def block_hexahedron8(n, length=1.0):
     """n^3 hexahedron_8 (reference node order: bottom face counter-clockwise,
     then top face); nodes x-fastest, elements x-fastest."""
-    nodes = _grid_nodes_3d(n, length)
-    k, j, i = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
-    p = n + 1
-    b = (k * p * p + j * p + i).ravel()
+    return box_hexahedron8(n, n, n, length, length, length)
+
+
+def box_hexahedron8(nx, ny, nz, lx, ly, lz):
+    """nx x ny x nz hexahedron_8 over lx x ly x lz (reference node order);
+    nodes x-fastest, elements x-fastest."""
+    nodes = _grid_nodes_3d(nx, lx, ny, ly, nz, lz)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    p, q = nx + 1, (nx + 1) * (ny + 1)
+    b = (k * q + j * p + i).ravel()
     conn = np.stack([b, b + 1, b + 1 + p, b + p,
-                     b + p * p, b + 1 + p * p, b + 1 + p + p * p, b + p + p * p], 1)
+                     b + q, b + 1 + q, b + 1 + p + q, b + p + q], 1)
     return Mesh(3, _abi.HEXAHEDRON_8, nodes, conn)

@@ -318,6 +318,10 @@ class OracleAdapter:
     def energy(self, kind):
         return self.m.energy(kind)
 
+    def apply_dirichlet(self, nodes, comp, values):
+        self.m.blocked[nodes, comp] = 1
+        self.m.displacement[nodes, comp] = values
+
 
 class GpuAdapter:
     """The same facade over akantu_b200.SolidMechanicsModel (libakb.so)."""
@@ -367,3 +371,6 @@ class GpuAdapter:
         name = {_abi.ENERGY_KINETIC: "kinetic", _abi.ENERGY_POTENTIAL: "potential",
                 _abi.ENERGY_EXTERNAL_WORK: "external work"}[kind]
         return self.m.getEnergy(name)
+
+    def apply_dirichlet(self, nodes, comp, values):
+        self.m.applyDirichlet(nodes, comp, values)
