@@ -53,6 +53,8 @@ ENERGY_KINETIC = 0
 ENERGY_POTENTIAL = 1
 ENERGY_EXTERNAL_WORK = 2
 
+ALL_COMPONENTS = -1  # akb_apply_dirichlet: every component, values row per node
+
 
 class MeshDesc(C.Structure):
     _fields_ = [

@@ -45,6 +45,7 @@ SIGNATURES = {
     "akb_assemble_internal_forces": (I32, [P]),
     "akb_compute_stresses": (I32, [P]),
     "akb_get_energy": (I32, [P, I32, PD]),
+    "akb_get_energy_async": (I32, [P, I32, P]),
     "akb_apply_dirichlet": (I32, [P, PU32, I64, I32, PD]),
     "akb_time_kernels": (I32, [P, I64, PD, I32]),
     "akb_kernel_name": (C.c_char_p, [P, I32]),

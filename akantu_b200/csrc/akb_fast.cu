@@ -171,14 +171,19 @@ __global__ void k_qp_forces(DevModel m) {
   for (int k = 0; k < d * n; ++k) out[k] = fe[k];
 }
 
+// comp >= 0: one thread per listed node, that component; comp < 0: one
+// thread per (listed node, component), values row per node.
 __global__ void k_apply_dirichlet(DevModel m, const uint32_t* nodes, int64_t n, int comp,
                                   const double* values, const uint32_t* perm, double* w) {
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  uint32_t node = nodes[k];
+  const int ncomp = comp < 0 ? m.dim : 1;
+  if (k >= n * ncomp) return;
+  const int64_t q = k / ncomp;
+  const int c = comp < 0 ? (int)(k - q * ncomp) : comp;
+  uint32_t node = nodes[q];
   if (node >= m.nn) return;  // out-of-range node ids are ignored
   if (perm) node = perm[node];
-  const int64_t i = (int64_t)node * m.dim + comp;
+  const int64_t i = (int64_t)node * m.dim + c;
   m.blocked[i] = 1;
   m.u[i] = values[k];
   if (w) w[i] = values[k];  // a blocked DOF's predicted displacement is its u
@@ -189,7 +194,8 @@ __global__ void k_apply_dirichlet(DevModel m, const uint32_t* nodes, int64_t n, 
 cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n, int comp,
                             const double* values, const uint32_t* perm, double* w,
                             cudaStream_t s) {
-  k_apply_dirichlet<<<blocks_for(n), kThreads, 0, s>>>(m, nodes, n, comp, values, perm, w);
+  k_apply_dirichlet<<<blocks_for(comp < 0 ? n * m.dim : n), kThreads, 0, s>>>(m, nodes, n, comp,
+                                                                              values, perm, w);
   return cudaGetLastError();
 }
 

@@ -84,8 +84,9 @@ cudaError_t user_qp_gradients(const DevModel& m, cudaStream_t s);
 cudaError_t user_element_forces(const DevModel& m, cudaStream_t s);
 
 // Dirichlet values (akb_fast.cu): blocked[node][comp] = 1, u[node][comp] = value
-// (and the predicted displacement w, when the model keeps one); perm (or
-// null) maps the caller's node ids to the model's internal order.
+// (and the predicted displacement w, when the model keeps one); comp < 0:
+// every component, values row per node; perm (or null) maps the caller's
+// node ids to the model's internal order.
 cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n, int comp,
                             const double* values, const uint32_t* perm, double* w,
                             cudaStream_t s);
@@ -96,6 +97,9 @@ cudaError_t stable_dt(const DevModel& m, double* d_scratch, int scratch_len,
 cudaError_t energy(const DevModel& m, int kind, double dt, double* d_scratch,
                    int scratch_len, double* d_out, cudaStream_t s);
 int reduce_blocks(int64_t n);
+// *out = scale * (sum of partial[0, n)), in a fixed order.
+cudaError_t sum_partials(const double* partial, int64_t n, double scale, double* out,
+                         cudaStream_t s);
 // Per-instance reductions of a batch: one block per instance.
 cudaError_t stable_dt_instances(const DevModel& m, const int64_t* elem_off, int ninst,
                                 double* d_out, cudaStream_t s);

@@ -72,13 +72,26 @@ struct akb_model {
   struct BcSlot {
     unsigned char* host = nullptr;
     unsigned char* dev = nullptr;
-    int64_t capacity = 0;  // nodes
-    cudaEvent_t done = nullptr;
+    int64_t capacity = 0;  // bytes
+    cudaEvent_t copied = nullptr;  // the upload (copy stream) is done
+    cudaEvent_t done = nullptr;    // the update kernel (model stream) has run
     bool pending = false;
   };
   static constexpr int kBcSlots = 4;
   BcSlot bc[kBcSlots];
   int bc_next = 0;
+  // host <-> device copies of the per-step calls (Dirichlet uploads, energy
+  // results) run on a stream of their own, ordered against the model's
+  // stream by events, so that they overlap the steps' kernels
+  cudaStream_t copy_stream = nullptr;
+  // akb_get_energy_async: a ring of device result slots; a slot is written
+  // again only once the copy of its previous value is done
+  static constexpr int kEnergySlots = 32;
+  double* d_eres = nullptr;
+  cudaEvent_t eres_ready[kEnergySlots] = {};
+  cudaEvent_t eres_copied[kEnergySlots] = {};
+  bool eres_pending[kEnergySlots] = {};
+  int eres_next = 0;
   // part of a partitioned mesh (akb_model_create_part): its interface nodes
   // (shared nodes of the patch plan), finished only once their forces are
   // summed over all parts
@@ -96,6 +109,9 @@ struct akb_model {
   double* d_tmp = nullptr;
   // the predicted displacement of the fused step is current
   bool w_valid = false;
+  // the kinetic-energy partials the last fused step wrote describe the
+  // current velocities
+  bool ke_valid = false;
 };
 
 // Interface nodes of a part, in the caller's order.
@@ -408,6 +424,11 @@ akb_status build_device_patches(akb_model* m, const PatchHost& P,
     for (size_t i = 0; i < em.size(); ++i) em[i] = element_material[P.elem_order[i]];
     if ((st = upload(m, em, &d.emat)) != AKB_OK) return st;
   }
+  {
+    double* ke;
+    if ((st = dalloc(m, &ke, (size_t)patch_ke_parts(d, m->dm.dim))) != AKB_OK) return st;
+    d.ke_part = ke;
+  }
   const size_t nsl = (size_t)std::max<int64_t>(P.nslots, 1);
   if ((st = dalloc(m, &d.partial, nsl * m->dm.dim)) != AKB_OK) return st;
   AKB_CUDA_TRY(cudaMemsetAsync(d.partial, 0, nsl * m->dm.dim * sizeof(double), m->stream));
@@ -472,6 +493,7 @@ akb_status check_model(const akb_model* m) {
 
 akb_status sync(akb_model* m) {
   cudaError_t e = cudaStreamSynchronize(m->stream);
+  if (e == cudaSuccess && m->copy_stream) e = cudaStreamSynchronize(m->copy_stream);
   if (e != cudaSuccess) return fail(AKB_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
   if (m->use_patches && m->patches.err) {  // a bounded wait of the fused step gave up
     int flag = 0;
@@ -482,6 +504,21 @@ akb_status sync(akb_model* m) {
       return fail(AKB_ERR_TIMEOUT, "fused step: staging copy did not complete in time");
     }
   }
+  return AKB_OK;
+}
+
+// getEnergy into a device double: the kinetic energy right after a fused
+// step sums the partials the step wrote, anything else reduces the fields.
+cudaError_t enqueue_energy(akb_model* m, int32_t kind, double* out) {
+  if (kind == AKB_ENERGY_KINETIC && m->use_patches && m->ke_valid)
+    return sum_partials(m->patches.ke_part, patch_ke_parts(m->patches, m->dm.dim), 0.5, out,
+                        m->stream);
+  return energy(m->dm, kind, m->dt, m->d_scratch, m->scratch_len, out, m->stream);
+}
+
+akb_status ensure_copy_stream(akb_model* m) {
+  if (m->copy_stream) return AKB_OK;
+  AKB_CUDA_TRY(cudaStreamCreateWithFlags(&m->copy_stream, cudaStreamNonBlocking));
   return AKB_OK;
 }
 
@@ -799,13 +836,20 @@ akb_status akb_model_destroy(akb_model* m) {
   if (!m) return AKB_OK;
   cudaSetDevice(m->device);
   cudaStreamSynchronize(m->stream);
+  if (m->copy_stream) cudaStreamSynchronize(m->copy_stream);
   destroy_graphs(m);
   for (void* p : m->allocations) cudaFree(p);
   if (m->h_result) cudaFreeHost(m->h_result);
   for (auto& b : m->bc) {
     if (b.host) cudaFreeHost(b.host);
     if (b.done) cudaEventDestroy(b.done);
+    if (b.copied) cudaEventDestroy(b.copied);
   }
+  for (int k = 0; k < akb_model::kEnergySlots; ++k) {
+    if (m->eres_ready[k]) cudaEventDestroy(m->eres_ready[k]);
+    if (m->eres_copied[k]) cudaEventDestroy(m->eres_copied[k]);
+  }
+  if (m->copy_stream) cudaStreamDestroy(m->copy_stream);
   if (m->owns_stream) cudaStreamDestroy(m->stream);
   delete m;
   return AKB_OK;
@@ -845,6 +889,7 @@ akb_status akb_set_field(akb_model* m, int32_t field, const double* values, int6
                                  cudaMemcpyHostToDevice, m->stream));
   }
   if (field != AKB_FIELD_EXTERNAL_FORCE) m->w_valid = false;
+  if (field == AKB_FIELD_VELOCITY) m->ke_valid = false;
   if (field == AKB_FIELD_DISPLACEMENT) {
     m->fint_valid = false;
     m->stresses_valid = false;
@@ -1041,6 +1086,7 @@ akb_status akb_solve_steps(akb_model* m, int64_t nb_steps) {
   // on demand at the (unchanged) displacement
   m->fint_valid = !m->use_patches;
   m->stresses_valid = false;
+  m->ke_valid = m->use_patches;
   return AKB_OK;
 }
 
@@ -1107,10 +1153,43 @@ akb_status akb_get_energy(akb_model* m, int32_t kind, double* value) {
     AKB_CUDA_TRY(enqueue_internal_forces(m));
     m->fint_valid = true;
   }
-  AKB_CUDA_TRY(energy(m->dm, kind, m->dt, m->d_scratch, m->scratch_len, m->d_result, m->stream));
+  AKB_CUDA_TRY(enqueue_energy(m, kind, m->d_result));
   AKB_CUDA_TRY(cudaMemcpyAsync(m->h_result, m->d_result, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
   if ((st = sync(m)) != AKB_OK) return st;
   *value = *m->h_result;
+  return AKB_OK;
+}
+
+akb_status akb_get_energy_async(akb_model* m, int32_t kind, double* value) {
+  akb_status st;
+  if ((st = check_model(m)) != AKB_OK) return st;
+  if (!value) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  if (kind < AKB_ENERGY_KINETIC || kind > AKB_ENERGY_EXTERNAL_WORK)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "unknown energy");
+  if (m->user && kind == AKB_ENERGY_POTENTIAL)
+    return fail(AKB_ERR_UNSUPPORTED, "user material: no potential energy");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  if (kind == AKB_ENERGY_EXTERNAL_WORK && !m->fint_valid) {
+    AKB_CUDA_TRY(enqueue_internal_forces(m));
+    m->fint_valid = true;
+  }
+  if ((st = ensure_copy_stream(m)) != AKB_OK) return st;
+  if (!m->d_eres && (st = dalloc(m, &m->d_eres, akb_model::kEnergySlots)) != AKB_OK) return st;
+  const int k = m->eres_next;
+  m->eres_next = (k + 1) % akb_model::kEnergySlots;
+  if (!m->eres_ready[k]) {
+    AKB_CUDA_TRY(cudaEventCreateWithFlags(&m->eres_ready[k], cudaEventDisableTiming));
+    AKB_CUDA_TRY(cudaEventCreateWithFlags(&m->eres_copied[k], cudaEventDisableTiming));
+  }
+  // the slot's previous value has been copied out before it is written again
+  if (m->eres_pending[k]) AKB_CUDA_TRY(cudaStreamWaitEvent(m->stream, m->eres_copied[k], 0));
+  AKB_CUDA_TRY(enqueue_energy(m, kind, m->d_eres + k));
+  AKB_CUDA_TRY(cudaEventRecord(m->eres_ready[k], m->stream));
+  AKB_CUDA_TRY(cudaStreamWaitEvent(m->copy_stream, m->eres_ready[k], 0));
+  AKB_CUDA_TRY(cudaMemcpyAsync(value, m->d_eres + k, sizeof(double), cudaMemcpyDefault,
+                               m->copy_stream));
+  AKB_CUDA_TRY(cudaEventRecord(m->eres_copied[k], m->copy_stream));
+  m->eres_pending[k] = true;
   return AKB_OK;
 }
 
@@ -1120,21 +1199,26 @@ akb_status akb_apply_dirichlet(akb_model* m, const uint32_t* nodes, int64_t nb_n
   if ((st = check_model(m)) != AKB_OK) return st;
   if (nb_nodes < 0 || (nb_nodes > 0 && (!nodes || !values)))
     return fail(AKB_ERR_INVALID_ARGUMENT, "null node or value array");
-  if (component < 0 || component >= m->dm.dim)
+  if ((component < 0 && component != AKB_ALL_COMPONENTS) || component >= m->dm.dim)
     return fail(AKB_ERR_INVALID_ARGUMENT, "component out of range");
+  const int64_t nvals = component == AKB_ALL_COMPONENTS ? nb_nodes * m->dm.dim : nb_nodes;
   if (nb_nodes == 0) return AKB_OK;
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   // the caller's arrays are copied to a pinned staging slot on the host, so
   // they may be reused as soon as the call returns; the upload and the kernel
   // are queued on the model's stream without waiting for them
+  if ((st = ensure_copy_stream(m)) != AKB_OK) return st;
   akb_model::BcSlot& b = m->bc[m->bc_next];
   m->bc_next = (m->bc_next + 1) % akb_model::kBcSlots;
-  if (!b.done) AKB_CUDA_TRY(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+  if (!b.done) {
+    AKB_CUDA_TRY(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+    AKB_CUDA_TRY(cudaEventCreateWithFlags(&b.copied, cudaEventDisableTiming));
+  }
   if (b.pending) AKB_CUDA_TRY(cudaEventSynchronize(b.done));
   b.pending = false;
   const size_t nbytes = ((size_t)nb_nodes * sizeof(uint32_t) + 7) & ~size_t(7);
-  const size_t bytes = nbytes + (size_t)nb_nodes * sizeof(double);
-  if (nb_nodes > b.capacity) {
+  const size_t bytes = nbytes + (size_t)nvals * sizeof(double);
+  if ((int64_t)bytes > b.capacity) {
     if (b.host) cudaFreeHost(b.host);
     dfree(m, b.dev);
     b.host = nullptr;
@@ -1142,11 +1226,15 @@ akb_status akb_apply_dirichlet(akb_model* m, const uint32_t* nodes, int64_t nb_n
     b.capacity = 0;
     AKB_CUDA_TRY(cudaMallocHost((void**)&b.host, bytes));
     if ((st = dalloc(m, &b.dev, bytes)) != AKB_OK) return st;
-    b.capacity = nb_nodes;
+    b.capacity = (int64_t)bytes;
   }
   std::memcpy(b.host, nodes, (size_t)nb_nodes * sizeof(uint32_t));
-  std::memcpy(b.host + nbytes, values, (size_t)nb_nodes * sizeof(double));
-  AKB_CUDA_TRY(cudaMemcpyAsync(b.dev, b.host, bytes, cudaMemcpyHostToDevice, m->stream));
+  std::memcpy(b.host + nbytes, values, (size_t)nvals * sizeof(double));
+  // the upload runs on the copy stream (overlapping the kernels queued
+  // before it); the update kernel waits for it on the model's stream
+  AKB_CUDA_TRY(cudaMemcpyAsync(b.dev, b.host, bytes, cudaMemcpyHostToDevice, m->copy_stream));
+  AKB_CUDA_TRY(cudaEventRecord(b.copied, m->copy_stream));
+  AKB_CUDA_TRY(cudaStreamWaitEvent(m->stream, b.copied, 0));
   AKB_CUDA_TRY(apply_dirichlet(m->dm, reinterpret_cast<const uint32_t*>(b.dev), nb_nodes, component,
                                reinterpret_cast<const double*>(b.dev + nbytes), m->d_perm,
                                m->use_patches ? m->patches.w : nullptr, m->stream));
@@ -1189,6 +1277,7 @@ akb_status akb_time_kernels(akb_model* m, int64_t nb_steps, double* ms_per_launc
   for (int k = 0; k < nb_slots; ++k) ms_per_launch[k] = k < nk ? acc[k] / nb_steps : 0.0;
   m->fint_valid = !m->use_patches;
   m->stresses_valid = false;
+  m->ke_valid = m->use_patches;
   return AKB_OK;
 }
 
@@ -1394,6 +1483,7 @@ akb_status akb_part_step_end(akb_model* m, const double* device_in) {
                                   device_in, m->stream));
   AKB_CUDA_TRY(patch_finish_list(m->dm, m->patches, m->dt, m->has_fext, m->stream));
   m->part_in_step = false;
+  m->ke_valid = true;
   m->fint_valid = false;
   m->stresses_valid = false;
   return AKB_OK;
@@ -1415,6 +1505,7 @@ akb_status akb_part_import_mass(akb_model* m, const double* device_in) {
   if (m->n_iface > 0 && !device_in) return fail(AKB_ERR_INVALID_ARGUMENT, "null input");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   AKB_CUDA_TRY(mass_import(m->dm, m->d_iface_g, m->n_iface, device_in, m->stream));
+  m->ke_valid = false;
   return AKB_OK;
 }
 

@@ -24,6 +24,7 @@
 // of the shared nodes in patch order and finishes them the same way, and the
 // nodes of no element (after the exchange between parts, for a partitioned
 // mesh).
+#include <cfloat>
 #include <mutex>
 
 #include "akb_fastmath.cuh"
@@ -224,6 +225,28 @@ __device__ inline uint32_t finish_regions(int ib, int nint, uint32_t* off, uint3
 // evaluated at), v* = v + dt a recomputed bit for bit, then
 // x = r / M - a, v = v* + dt/2 x, a += x (u += 0 x only when x is not
 // finite); w' = u + dt v + dt^2/2 a.
+// M v^2 of one DOF from its inverse lumped mass, for masses above
+// DBL_EPSILON (the test of getKineticEnergy, solid_mechanics_model.cc:547-561).
+__device__ inline double ke_term(double v, double im) {
+  const double M = 1.0 / im;
+  return M > DBL_EPSILON ? v * v * M : 0.0;
+}
+
+// Sum of the CTA's per-thread values in a fixed order (lanes by an xor
+// tree, then warps in order), by thread 0; every thread must call it.
+__device__ inline double cta_sum(double x, double* warp_sums) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();  // warp_sums free (a previous use is read)
+  if ((threadIdx.x & 31) == 0) warp_sums[w] = x;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < nw; ++k) s += warp_sums[k];
+  return s;
+}
+
 __device__ inline void finish_dof(double dt, double r, double im, double w, double& v, double& a,
                                   double& u, double& wn) {
   u = w;
@@ -475,6 +498,7 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
     P.partial[(size_t)sslot[t] * d + i] = fs[i * LM + nint + t];
   }
   const int items = nint * d;
+  double ke = 0.0;  // M v^2 of this thread's DOFs after the step
   for (int base = 0; base < items; base += kThreads * kBatch) {
     double v[kBatch], a[kBatch], im[kBatch], fx[kBatch];
     uint8_t bl[kBatch];
@@ -501,17 +525,25 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
 #pragma unroll
     for (int b = 0; b < kBatch; ++b) {
       const int k = base + b * kThreads + tid;
-      if (k >= items || bl[b]) continue;  // blocked DOFs keep u, v, a (and w = u)
-      const int j = k / d, i = k - j * d;
-      const int64_t q = (int64_t)ib * d + k;
-      const double f = fs[i * LM + j];
-      double u, wn;
-      finish_dof(dt, FEXT ? f + fx[b] : f, im[b], ws[k], v[b], a[b], u, wn);
-      m.u[q] = u;
-      m.v[q] = v[b];
-      m.a[q] = a[b];
-      P.w[q] = wn;
+      if (k >= items) continue;
+      if (!bl[b]) {  // blocked DOFs keep u, v, a (and w = u)
+        const int j = k / d, i = k - j * d;
+        const int64_t q = (int64_t)ib * d + k;
+        const double f = fs[i * LM + j];
+        double u, wn;
+        finish_dof(dt, FEXT ? f + fx[b] : f, im[b], ws[k], v[b], a[b], u, wn);
+        m.u[q] = u;
+        m.v[q] = v[b];
+        m.a[q] = a[b];
+        P.w[q] = wn;
+      }
+      ke += ke_term(v[b], im[b]);
     }
+  }
+  if (P.ke_part) {
+    __shared__ double warp_sums[kThreads / 32];
+    const double s = cta_sum(ke, warp_sums);
+    if (tid == 0) P.ke_part[p] = s;
   }
   return true;
 }
@@ -544,14 +576,13 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
   }
 }
 
-// Listed nodes, one thread per (entry, component): the sum of the entry's
+// One (listed node, component) of k_finish_list: the sum of the entry's
 // partials in order (none for a node of no element), then the same finish
-// as in the fused step, from the node's stored w.
-template <int D, bool FEXT>
-__global__ void k_finish_list(DevModel m, DevPatches P, double dt0) {
-  constexpr int d = D;
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= P.nlist * d) return;
+// as in the fused step, from the node's stored w; returns its M v^2 after
+// the step.
+template <int d, bool FEXT>
+__device__ inline double finish_list_dof(const DevModel& m, const DevPatches& P, double dt0,
+                                         int64_t t) {
   const int64_t e = t / d;
   const int i = (int)(t - e * d);
   const int64_t g = P.list_gid[e];
@@ -565,13 +596,29 @@ __global__ void k_finish_list(DevModel m, DevPatches P, double dt0) {
   double v = m.v[q], a = m.a[q];
   double f = 0.0;
   for (uint32_t r = 0; r < k; ++r) f += P.partial[(size_t)(part + r) * d + i];
-  if (bl) return;
+  if (bl) return ke_term(v, im);
   double u, wn;
   finish_dof(dt, FEXT ? f + fx : f, im, w, v, a, u, wn);
   m.u[q] = u;
   m.v[q] = v;
   m.a[q] = a;
   P.w[q] = wn;
+  return ke_term(v, im);
+}
+
+// Listed nodes, one thread per (entry, component), and the block's sum of
+// M v^2 (a kinetic-energy partial).
+template <int D, bool FEXT>
+__global__ void k_finish_list(DevModel m, DevPatches P, double dt0) {
+  constexpr int d = D;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double ke = 0.0;
+  if (t < P.nlist * d) ke = finish_list_dof<d, FEXT>(m, P, dt0, t);
+  if (P.ke_part) {
+    __shared__ double warp_sums[kThreads / 32];
+    const double s = cta_sum(ke, warp_sums);
+    if (threadIdx.x == 0) P.ke_part[P.npatch + blockIdx.x] = s;
+  }
 }
 
 // w = u + dt v + dt^2/2 a on free DOFs, w = u on blocked ones; one thread per
@@ -768,6 +815,10 @@ cudaError_t patch_finish_list(const DevModel& m, const DevPatches& p, double dt,
                 : k_finish_list<3, false><<<blocks, kThreads, 0, s>>>(m, p, dt); break;
   }
   return cudaGetLastError();
+}
+
+int64_t patch_ke_parts(const DevPatches& p, int dim) {
+  return p.npatch + (p.nlist > 0 ? blocks_of(p.nlist * dim) : 0);
 }
 
 cudaError_t patch_refresh_w(const DevModel& m, const DevPatches& p, double dt, cudaStream_t s) {

@@ -136,6 +136,10 @@ struct DevPatches {
   int* err;                // set when a bounded wait gave up
   double* partial;         // nslots x dim
   double* w;               // nn x dim predicted displacement
+  // per patch, then per finishing-list block: sum over the DOFs finished
+  // there (blocked ones included) of M v^2 after the step, M > DBL_EPSILON
+  // only (getKineticEnergy, solid_mechanics_model.cc:547-561)
+  double* ke_part;
   // nodes finished by k_finish_list: the nodes of no element, then the
   // shared nodes; entry i: node, first slot, k (0 for a node of no element)
   int64_t nlist;
@@ -162,6 +166,8 @@ cudaError_t patch_step(const DevModel& m, const DevPatches& p, double dt, bool f
 // Finishes the listed nodes from their partials (the step's second pass).
 cudaError_t patch_finish_list(const DevModel& m, const DevPatches& p, double dt, bool has_fext,
                               cudaStream_t s);
+// Number of kinetic-energy partials a step writes (patches + list blocks).
+int64_t patch_ke_parts(const DevPatches& p, int dim);
 // w = u + dt v + dt^2/2 a on free DOFs, w = u on blocked ones.
 cudaError_t patch_refresh_w(const DevModel& m, const DevPatches& p, double dt, cudaStream_t s);
 // Partitioned meshes, per interface node i (first slot part[i], k[i] slots):

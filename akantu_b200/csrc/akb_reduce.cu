@@ -268,6 +268,12 @@ cudaError_t stable_dt(const DevModel& m, double* scratch, int scratch_len, doubl
   return cudaGetLastError();
 }
 
+cudaError_t sum_partials(const double* partial, int64_t n, double scale, double* out,
+                         cudaStream_t s) {
+  k_finish<kSum><<<1, kThreads, 0, s>>>(partial, (int)n, scale, out);
+  return cudaGetLastError();
+}
+
 cudaError_t energy(const DevModel& m, int kind, double dt, double* scratch, int scratch_len,
                    double* out, cudaStream_t s) {
   double scale = 1.0;

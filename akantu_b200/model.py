@@ -274,10 +274,12 @@ class SolidMechanicsModel:
     def applyDirichlet(self, nodes, component, values):
         """applyBC(FixedValue(value, axis), group) for a node group
         (boundary_condition_tmpl.hh:63-200): blocks the DOFs and sets their
-        displacement on the device."""
+        displacement on the device. component _abi.ALL_COMPONENTS: every axis
+        at once, values (nb_nodes, dim)."""
         self._sync_in()
         n = np.ascontiguousarray(nodes, dtype=np.uint32)
-        v = np.ascontiguousarray(np.broadcast_to(values, n.shape), dtype=np.float64)
+        shape = n.shape + ((self.dim,) if component == _abi.ALL_COMPONENTS else ())
+        v = np.ascontiguousarray(np.broadcast_to(values, shape), dtype=np.float64)
         check(lib().akb_apply_dirichlet(self.handle, n.ctypes.data_as(C.POINTER(C.c_uint32)),
                                         n.size, int(component),
                                         v.ctypes.data_as(C.POINTER(C.c_double))))
@@ -369,6 +371,16 @@ class SolidMechanicsModel:
         v = C.c_double()
         check(lib().akb_get_energy(self.handle, _ENERGY[energy_id], C.byref(v)))
         return v.value
+
+    def getEnergyAsync(self, energy_id, out):
+        """getEnergy queued on the model's stream: the value lands in out (a
+        pinned host or device float64 buffer of one element, as a pointer or
+        a tensor/array) when the stream reaches it; read it after
+        synchronize()."""
+        self._sync_in()
+        ptr = out if isinstance(out, int) else (out.data_ptr() if hasattr(out, "data_ptr")
+                                                else out.ctypes.data)
+        check(lib().akb_get_energy_async(self.handle, _ENERGY[energy_id], C.c_void_p(ptr)))
 
     def synchronize(self):
         check(lib().akb_synchronize(self.handle))

@@ -210,6 +210,15 @@ akb_status akb_compute_stresses(akb_model* model);
 
 /* SolidMechanicsModel::getEnergy (solid_mechanics_model.cc:665-683). */
 akb_status akb_get_energy(akb_model* model, int32_t kind, double* value);
+/* The same without waiting: the reduction and the copy of its result to
+ * *value are queued on the model's stream, and *value is written when the
+ * stream reaches them; read it after akb_synchronize (the copy itself runs
+ * on a stream of the library's, so an event of the model's stream does not
+ * cover it). value: host memory (pinned, for the copy to run
+ * asynchronously) or device memory. Lets a time loop that records the
+ * energies of every step (examples/explicit/explicit_dynamic.cc:87-99) run
+ * without a host round trip per step. No reference counterpart. */
+akb_status akb_get_energy_async(akb_model* model, int32_t kind, double* value);
 
 /* applyBC(BC::Dirichlet::FixedValue(value, component), group)
  * (boundary_condition_functor_inline_impl.hh:85-93, boundary_condition_tmpl.hh:63-88):
@@ -217,7 +226,11 @@ akb_status akb_get_energy(akb_model* model, int32_t kind, double* value);
  * displacement to values[k]. nodes and values are host arrays of nb_nodes
  * entries; they are copied before the call returns (and may be reused
  * then), while the upload and the update are queued on the model's stream:
- * an error of the update is reported by the next call that synchronises. */
+ * an error of the update is reported by the next call that synchronises.
+ * component AKB_ALL_COMPONENTS: every component of the listed nodes at once,
+ * values then holding nb_nodes x spatial_dimension entries (row per node),
+ * the functor applied to every axis of a group in one call. */
+#define AKB_ALL_COMPONENTS (-1)
 akb_status akb_apply_dirichlet(akb_model* model, const uint32_t* nodes,
                                int64_t nb_nodes, int32_t component,
                                const double* values);

@@ -6,6 +6,9 @@ every GPU mode run the same scenario (test infrastructure).
   elastic_law                    test_elastic_materials.cc:56-290
   plane_wave                     test_solid_mechanics_model_dynamics.cc:39-297
   work_balance                   test_energies/test_solid_mechanics_model_work_dynamics.cc:50-156
+  python_fe_truss                test/python_fe (TrussFE, DynamicSolver): trajectories of
+                                 the reference's own Python restatement, as the explicit
+                                 lumped scheme (tests/golden/make_python_fe.py)
 
 The bar meshes of the last two (patch_tests/data/bar_*.geo: 10 x 1 x 1, mesh
 size 0.6, meshed by Gmsh, which is absent) are generated here as structured
@@ -308,4 +311,32 @@ def work_balance(make, etype):
             W += model.energy(_abi.ENERGY_EXTERNAL_WORK)
         e1 = model.energy(_abi.ENERGY_POTENTIAL) + model.energy(_abi.ENERGY_KINETIC)
         errs.append(abs(W - (e1 - e0)))
+    return errs
+
+
+def python_fe_truss(make):
+    """The bars of tests/golden/python_fe_truss.json (segment_2, node 0
+    fixed, end load, sinusoidal initial displacement) stepped with the
+    stored time step; per case the largest relative difference of the
+    displacement over all stored steps to the reference's Python solver."""
+    from akantu_b200.mesh import bar_segment2
+    g = json.load(open(os.path.join(HERE, "golden", "python_fe_truss.json")))
+    errs = []
+    for c in g["cases"]:
+        mesh = bar_segment2(c["Ne"] + 1, c["L"])
+        model = make(mesh, dict(kind=_abi.MATERIAL_ELASTIC, rho=c["rho"], E=c["E"], nu=0.0))
+        u0 = np.array(c["u0"])[:, None]
+        f = np.zeros_like(u0)
+        f[-1, 0] = c["F"]
+        model.set(_abi.FIELD_DISPLACEMENT, u0)
+        model.set(_abi.FIELD_EXTERNAL_FORCE, f)
+        model.apply_dirichlet(np.array([0]), 0, np.array([0.0]))
+        model.set_time_step(c["dt"])
+        worst = 0.0
+        for ref in c["displacement"]:
+            model.solve_step()
+            ref = np.array(ref)
+            u = model.get(_abi.FIELD_DISPLACEMENT)[:, 0]
+            worst = max(worst, np.abs(u - ref).max() / np.abs(ref).max())
+        errs.append(worst)
     return errs

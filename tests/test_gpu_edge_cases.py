@@ -100,3 +100,42 @@ def test_dirichlet_arrays_reusable_on_return():
     assert np.array_equal(b, expect_b)
     assert np.array_equal(u[expect_b.astype(bool)], expect_u[expect_b.astype(bool)])
     m.close()
+
+
+def test_dirichlet_all_components_and_async_energy():
+    """akb_apply_dirichlet with AKB_ALL_COMPONENTS equals one call per
+    component; akb_get_energy_async gives akb_get_energy's value once the
+    stream is synchronised, for every step of a loop queued without
+    waiting."""
+    import torch
+
+    from akantu_b200.model import SolidMechanicsModel, material_from_dict
+    w = configs.cube_tet4(8)
+    fixed = np.nonzero(w["blocked"][:, 0])[0]
+    vals = np.random.default_rng(5).normal(scale=1e-6, size=(fixed.size, 3))
+    runs = []
+    for all_at_once in (True, False):
+        m = SolidMechanicsModel(w["mesh"], [material_from_dict(mm) for mm in w["materials"]],
+                                precision=_abi.MODE_FP64)
+        m.initFull()
+        m.setField(_abi.FIELD_VELOCITY, w["v0"])
+        m.setTimeStep(0.8 * m.getStableTimeStep())
+        slots = torch.zeros(20, dtype=torch.float64).pin_memory()
+        sync_e = []
+        for s in range(20):
+            if all_at_once:
+                m.applyDirichlet(fixed, _abi.ALL_COMPONENTS, vals * (s + 1))
+            else:
+                for c in range(3):
+                    m.applyDirichlet(fixed, c, vals[:, c] * (s + 1))
+            m.solveStep()
+            if all_at_once:
+                m.getEnergyAsync("kinetic", slots[s:s + 1].data_ptr())
+            else:
+                sync_e.append(m.getEnergy("kinetic"))
+        m.synchronize()
+        runs.append((np.array(m.getDisplacement()), slots.numpy().copy(), sync_e))
+        m.close()
+    (u1, e_async, _), (u2, _, e_sync) = runs
+    assert np.array_equal(u1, u2)
+    assert np.array_equal(e_async, np.array(e_sync))

@@ -66,3 +66,10 @@ def test_plane_wave(mode, etype):
 def test_work_balance(mode, etype):
     errs = rp.work_balance(gpu(mode), etype)
     assert max(errs) < 5e-2  # EXPECT_NEAR(W, Ekin + Epot - Etot0, 5e-2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", MODES)
+def test_python_fe_truss_trajectories(mode):
+    errs = rp.python_fe_truss(gpu(mode))
+    assert max(errs) <= (1e-5 if mode == _abi.MODE_FP32_BULK else 1e-12)
