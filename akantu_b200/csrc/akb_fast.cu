@@ -36,7 +36,8 @@ __global__ void k_element_forces(DevModel m) {
     X0[i] = __ldg(&m.X[(int64_t)nodes[0] * d + i]);
     u0[i] = m.u[(int64_t)nodes[0] * d + i];
   }
-  S dX[3 * 8], du[3 * 8];
+  double dX[3 * 8];
+  S du[3 * 8];
 #pragma unroll
   for (int i = 0; i < d; ++i) {
     dX[i] = 0;
@@ -46,7 +47,7 @@ __global__ void k_element_forces(DevModel m) {
   for (int a = 1; a < n; ++a)
 #pragma unroll
     for (int i = 0; i < d; ++i) {
-      dX[a * d + i] = S(__ldg(&m.X[(int64_t)nodes[a] * d + i]) - X0[i]);
+      dX[a * d + i] = __ldg(&m.X[(int64_t)nodes[a] * d + i]) - X0[i];
       du[a * d + i] = S(m.u[(int64_t)nodes[a] * d + i] - u0[i]);
     }
   S fe[3 * 8];

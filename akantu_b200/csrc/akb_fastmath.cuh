@@ -217,6 +217,172 @@ __device__ inline void stress_P(const MatParams& p, const S* g, S* P) {
     }
 }
 
+// A constant carried as hi + lo in the element precision: for FP32, hi is
+// the constant rounded to float and lo its remainder, so that products with
+// it are as accurate as with the FP64 constant up to the rounding of the
+// result; for FP64, lo is zero and unused.
+template <typename S> struct Split {
+  S hi, lo;
+};
+template <typename S>
+__device__ inline Split<S> split(double x) {
+  if constexpr (sizeof(S) == 8) {
+    return {x, 0.0};
+  } else {
+    const float h = (float)x;
+    return {h, (float)(x - (double)h)};
+  }
+}
+// x c
+template <typename S>
+__device__ inline S mulc(S x, const Split<S>& c) {
+  if constexpr (sizeof(S) == 8)
+    return x * c.hi;
+  else
+    return fmaf(x, c.hi, x * c.lo);
+}
+// acc + x c
+template <typename S>
+__device__ inline S fmac(S x, const Split<S>& c, S acc) {
+  if constexpr (sizeof(S) == 8)
+    return fma(x, c.hi, acc);
+  else
+    return fmaf(x, c.hi, fmaf(x, c.lo, acc));
+}
+
+// Hexahedron force for a parallelepiped (one Jacobian at every point),
+// without rounding any quantity that stays the same from step to step:
+//  - J, its adjugate A and 1 / det J in FP64 from FP64 coordinate
+//    differences, A and 1 / det J then carried as Split constants;
+//  - the Gauss points' shape derivatives (2 x 2 x 2 rule, c = +-1/sqrt(3),
+//    element_class_hexahedron_8_inline_impl.hh:118-215) never formed:
+//    dN_a/dxi_k = 1/8 s_k(a) (1 + s_m(a) c_m) (1 + s_n(a) c_n) ({k, m, n} the
+//    three directions), so at a point
+//      H_ik = du_i/dxi_k = 1/8 (E_k + c_m E_km + c_n E_kn + c_m c_n E_xyz)
+//    with E the signed corner sums of du (once per element), and the corner
+//    forces sum_q Q(q) dN(., a, q) come from four signed sums over the
+//    points of Q = w P A; c = +-g and c_m c_n = +-1/3 enter as Split
+//    constants, once per element.
+// In FP32 the element arithmetic then only rounds quantities that change
+// every step (its errors do not accumulate into a frequency shift); in FP64
+// it takes fewer operations than the point-by-point shape derivatives.
+template <typename S>
+__device__ inline void hex_parallelepiped_force(const MatParams& p, const double* dX, const S* du,
+                                                S* fe) {
+  constexpr int d = 3, n = 8;
+  const int sg[3][8] = {{-1, 1, 1, -1, -1, 1, 1, -1},
+                        {-1, -1, 1, 1, -1, -1, 1, 1},
+                        {-1, -1, -1, -1, 1, 1, 1, 1}};
+  double J[9];
+#pragma unroll
+  for (int k = 0; k < d; ++k)
+#pragma unroll
+    for (int j = 0; j < d; ++j) {
+      double c = 0;
+#pragma unroll
+      for (int a = 1; a < n; ++a) c += (0.125 * sg[k][a]) * dX[a * d + j];
+      J[k * d + j] = c;
+    }
+  double A64[9];
+  const double det = adjugate<d, double>(J, A64);
+  const Split<S> idet = split<S>(1.0 / det);
+  Split<S> A[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) A[t] = split<S>(A64[t] * weight<AKB_HEXAHEDRON_8>());
+  // signed corner sums of du: E0[k] (s_k), Ep[.] (s_x s_y, s_x s_z, s_y s_z),
+  // E3 (s_x s_y s_z); then g Ep and E3 / 3
+  S E0[3][3], Fp[3][3], F3[3];
+  const Split<S> gc = split<S>(0.57735026918962576451), third = split<S>(1.0 / 3.0);
+#pragma unroll
+  for (int i = 0; i < d; ++i) {
+    S e0x = 0, e0y = 0, e0z = 0, exy = 0, exz = 0, eyz = 0, exyz = 0;
+#pragma unroll
+    for (int a = 1; a < n; ++a) {
+      const S v = du[a * d + i];
+      e0x += S(sg[0][a]) * v;
+      e0y += S(sg[1][a]) * v;
+      e0z += S(sg[2][a]) * v;
+      exy += S(sg[0][a] * sg[1][a]) * v;
+      exz += S(sg[0][a] * sg[2][a]) * v;
+      eyz += S(sg[1][a] * sg[2][a]) * v;
+      exyz += S(sg[0][a] * sg[1][a] * sg[2][a]) * v;
+    }
+    E0[0][i] = e0x;
+    E0[1][i] = e0y;
+    E0[2][i] = e0z;
+    Fp[0][i] = mulc(exy, gc);
+    Fp[1][i] = mulc(exz, gc);
+    Fp[2][i] = mulc(eyz, gc);
+    F3[i] = mulc(exyz, third);
+  }
+  // pair index of directions (k, m): xy 0, xz 1, yz 2
+  auto pair = [](int k, int m) { return k + m - 1; };
+  // per (i, k): sums over the points of Q, s_m Q, s_n Q, s_m s_n Q
+  S T0[9], Tm[9], Tn[9], Tmn[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) T0[t] = Tm[t] = Tn[t] = Tmn[t] = 0;
+#pragma unroll 1
+  for (int q = 0; q < 8; ++q) {
+    const S sq[3] = {(q & 1) ? S(1) : S(-1), (q & 2) ? S(1) : S(-1), (q & 4) ? S(1) : S(-1)};
+    S H[9];
+#pragma unroll
+    for (int k = 0; k < d; ++k) {
+      const int m = k == 0 ? 1 : 0, nn = k == 2 ? 1 : 2;
+#pragma unroll
+      for (int i = 0; i < d; ++i)
+        H[i * d + k] = S(0.125) * (E0[k][i] + sq[m] * Fp[pair(k, m)][i] +
+                                   sq[nn] * Fp[pair(k, nn)][i] + (sq[m] * sq[nn]) * F3[i]);
+    }
+    // grad u = H A^T / det J
+    S g[9];
+#pragma unroll
+    for (int i = 0; i < d; ++i)
+#pragma unroll
+      for (int j = 0; j < d; ++j) {
+        S c = 0;
+#pragma unroll
+        for (int k = 0; k < d; ++k) c = fmac(H[i * d + k], A[j * d + k], c);
+        g[i * d + j] = mulc(c, idet);
+      }
+    S P[9];
+    stress_P<d, S>(p, g, P);
+#pragma unroll
+    for (int i = 0; i < d; ++i)
+#pragma unroll
+      for (int k = 0; k < d; ++k) {
+        const int m = k == 0 ? 1 : 0, nn = k == 2 ? 1 : 2;
+        S Q = 0;  // (w P A)_ik
+#pragma unroll
+        for (int j = 0; j < d; ++j) Q = fmac(P[i * d + j], A[j * d + k], Q);
+        const int t = i * d + k;
+        T0[t] += Q;
+        Tm[t] += sq[m] * Q;
+        Tn[t] += sq[nn] * Q;
+        Tmn[t] += (sq[m] * sq[nn]) * Q;
+      }
+  }
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    Tm[t] = mulc(Tm[t], gc);
+    Tn[t] = mulc(Tn[t], gc);
+    Tmn[t] = mulc(Tmn[t], third);
+  }
+#pragma unroll
+  for (int a = 0; a < n; ++a)
+#pragma unroll
+    for (int i = 0; i < d; ++i) {
+      S f = 0;
+#pragma unroll
+      for (int k = 0; k < d; ++k) {
+        const int m = k == 0 ? 1 : 0, nn = k == 2 ? 1 : 2;
+        const int t = i * d + k;
+        const S sm = S(sg[m][a]), sn = S(sg[nn][a]);
+        f += S(sg[k][a]) * (T0[t] + sm * Tm[t] + sn * Tn[t] + (sm * sn) * Tmn[t]);
+      }
+      fe[a * d + i] = S(0.125) * f;
+    }
+}
+
 // Simplex (triangle_3, tetrahedron_4) internal force. The natural
 // derivatives are constant (dN_a/dxi_k = delta(a, k+1) - delta(a, 0)), so the
 // rows of J are X_a - X_0 (a >= 1) and w det J grad N_a = w adj(J)[:, a-1]:
@@ -334,57 +500,48 @@ __device__ inline void hex_qp_force(const MatParams& p, const S* du, const S* A,
 
 // Element internal force (without the -1 of the assembly):
 // fe[a*d + i] = sum_q w_q det J_q sum_j P_ij dN_a/dx_j.
-// dX[a*d+i] = X_a - X_0, du[a*d+i] = u_a - u_0 (entry a = 0 is zero).
+// dX64[a*d+i] = X_a - X_0 in FP64, du[a*d+i] = u_a - u_0 (entry a = 0 is
+// zero).
 template <int T, typename S>
-__device__ inline void element_force(const MatParams& p, const S* dX, const S* du, S* fe) {
+__device__ inline void element_force(const MatParams& p, const double* dX64, const S* du, S* fe) {
+  constexpr int nd = ET<T>::dim * ET<T>::nnpe;
+  S dX[nd];
+#pragma unroll
+  for (int k = 0; k < nd; ++k) dX[k] = S(dX64[k]);
   if (T == AKB_TRIANGLE_3 || T == AKB_TETRAHEDRON_4) {
     simplex_force<T, S>(p, dX, du, fe);
     return;
   }
   if (T == AKB_HEXAHEDRON_8) {
     constexpr int d = 3, n = 8, nq = 8;
-#pragma unroll
-    for (int k = 0; k < d * n; ++k) fe[k] = 0;
     // a parallelepiped (the trilinear terms of x(xi) vanish to 1e-12 of the
     // element's extent) has one Jacobian at every point: formed once
     const int sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
     const int sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
     const int sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
-    S ext = 0, bend = 0;
+    // (tested on the FP64 differences: rounded to FP32 they are not a
+    // parallelepiped to 1e-12)
+    double ext = 0, bend = 0;
 #pragma unroll
     for (int j = 0; j < d; ++j) {
-      S cxy = 0, cxz = 0, cyz = 0, cxyz = 0;
+      double cxy = 0, cxz = 0, cyz = 0, cxyz = 0;
 #pragma unroll
       for (int a = 1; a < n; ++a) {
-        const S x = dX[a * d + j];
-        cxy += S(sx[a] * sy[a]) * x;
-        cxz += S(sx[a] * sz[a]) * x;
-        cyz += S(sy[a] * sz[a]) * x;
-        cxyz += S(sx[a] * sy[a] * sz[a]) * x;
+        const double x = dX64[a * d + j];
+        cxy += double(sx[a] * sy[a]) * x;
+        cxz += double(sx[a] * sz[a]) * x;
+        cyz += double(sy[a] * sz[a]) * x;
+        cxyz += double(sx[a] * sy[a] * sz[a]) * x;
         ext = fmax(ext, fabs(x));
       }
       bend = fmax(bend, fmax(fmax(fabs(cxy), fabs(cxz)), fmax(fabs(cyz), fabs(cxyz))));
     }
-    if (bend <= S(1e-12) * ext) {
-      S J[9];
-#pragma unroll
-      for (int k = 0; k < d; ++k)
-#pragma unroll
-        for (int j = 0; j < d; ++j) {
-          S c = 0;
-#pragma unroll
-          for (int a = 1; a < n; ++a) {
-            const int s = k == 0 ? sx[a] : k == 1 ? sy[a] : sz[a];
-            c += S(0.125 * s) * dX[a * d + j];
-          }
-          J[k * d + j] = c;
-        }
-      S A[9];
-      const S idet = S(1) / adjugate<d, S>(J, A);
-#pragma unroll 1
-      for (int q = 0; q < nq; ++q) hex_qp_force<T, S>(p, du, A, idet, q, fe);
+    if (bend <= 1e-12 * ext) {
+      hex_parallelepiped_force<S>(p, dX64, du, fe);
       return;
     }
+#pragma unroll
+    for (int k = 0; k < d * n; ++k) fe[k] = 0;
 #pragma unroll 1
     for (int q = 0; q < nq; ++q) {
       S J[9];

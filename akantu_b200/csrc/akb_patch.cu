@@ -100,17 +100,18 @@ __device__ inline void load_corners(const uint16_t* base, int el, int* out) {
 // arrays are row-major; in 2D a node's two components are one 16-byte load.
 template <int d, int n, typename S>
 __device__ inline void gather_differences(const double* xs, const double* ws, const int* lc,
-                                          S* dX, S* du) {
+                                          double* dX, S* du) {
   if constexpr (d == 2) {
     const double2 x0 = reinterpret_cast<const double2*>(xs)[lc[0]];
     const double2 u0 = reinterpret_cast<const double2*>(ws)[lc[0]];
-    dX[0] = dX[1] = du[0] = du[1] = S(0);
+    dX[0] = dX[1] = 0.0;
+    du[0] = du[1] = S(0);
 #pragma unroll
     for (int a = 1; a < n; ++a) {
       const double2 x = reinterpret_cast<const double2*>(xs)[lc[a]];
       const double2 u = reinterpret_cast<const double2*>(ws)[lc[a]];
-      dX[a * 2] = S(x.x - x0.x);
-      dX[a * 2 + 1] = S(x.y - x0.y);
+      dX[a * 2] = x.x - x0.x;
+      dX[a * 2 + 1] = x.y - x0.y;
       du[a * 2] = S(u.x - u0.x);
       du[a * 2 + 1] = S(u.y - u0.y);
     }
@@ -122,7 +123,7 @@ __device__ inline void gather_differences(const double* xs, const double* ws, co
       const double x0 = xs[d * lc[0] + i], u0 = ws[d * lc[0] + i];
 #pragma unroll
       for (int a = 1; a < n; ++a) {
-        dX[a * d + i] = S(xs[d * lc[a] + i] - x0);
+        dX[a * d + i] = xs[d * lc[a] + i] - x0;
         du[a * d + i] = S(ws[d * lc[a] + i] - u0);
       }
     }
@@ -431,7 +432,8 @@ __device__ __forceinline__ bool patch_body(const DevModel& m, const DevPatches& 
       load_corners<n>(lcs, tid, lc);
       load_corners<n>(lcs + A / 2, tid, sl);
       const MatParams& mp = (P.emat ? m.mat_table[P.emat[(size_t)eb + c0 + tid]] : m.mats[0]);
-      S dX[3 * 8], du[3 * 8];
+      double dX[3 * 8];
+      S du[3 * 8];
       gather_differences<d, n, S>(xs, ws, lc, dX, du);
       S fe[3 * 8];
       fast::element_force<T, S>(mp, dX, du, fe);

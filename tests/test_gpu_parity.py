@@ -125,9 +125,10 @@ def test_cube_tet4_small(mode):
 def test_block_hex8_neohookean_small(mode):
     w = configs.block_hex8(n=6, length=0.06)
     cpu, dev = run_pair(w, mode, 300)
-    # FP32: the random-velocity field carries ~5e-8 of FP32 rounding per step
-    # into the displacement, which adds up linearly over the 300 steps
-    tol = {0: 1e-12, 1: 1e-10, 2: 5e-5}[mode]
+    # FP32-bulk: the geometry and the constant factors of the hexahedron force
+    # are carried in FP64 / float-float, so the FP32 rounding of the
+    # state-dependent part does not shift the block's frequencies
+    tol = {0: 1e-12, 1: 1e-10, 2: 1e-5}[mode]
     for f in STATE:
         e = rel(dev.get(f), cpu.get(f))
         assert e <= tol, (f, e)
