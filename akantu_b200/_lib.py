@@ -65,6 +65,11 @@ SIGNATURES = {
     "akb_part_step_end": (I32, [P, P]),
     "akb_part_export_mass": (I32, [P, P]),
     "akb_part_import_mass": (I32, [P, P]),
+    "akb_part_set_exchange": (I32, [P, I64, PU32, I64, C.POINTER(I64), C.POINTER(I64)]),
+    "akb_part_pack_forces": (I32, [P, P]),
+    "akb_part_step_end_exchange": (I32, [P, P]),
+    "akb_part_pack_mass": (I32, [P, P]),
+    "akb_part_import_mass_exchange": (I32, [P, P]),
     # include/akb_mesh.h
     "akb_msh_read": (I32, [C.c_char_p, I32, C.POINTER(P)]),
     "akb_msh_parse": (I32, [C.c_char_p, I64, I32, C.POINTER(P)]),

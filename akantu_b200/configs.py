@@ -7,6 +7,10 @@
   cube_tet4      100^3 cubes x 6 tetrahedron_4 (6 M elements, 1 030 301
                  nodes) over a 1 m cube, E = 70 GPa, nu = 0.33, rho = 2700;
                  bottom face fixed, top face v_z = 1 m/s; 1000 steps.
+  bar_tet4       cube_tet4 stacked nslabs times along z: n x n x (n nslabs)
+                 cubes x 6 tetrahedron_4 over 1 m x 1 m x nslabs m, same
+                 material, bottom face fixed, top face v_z = 1 m/s; cut into
+                 its nslabs cubes along z (one part per GPU, weak scaling).
   block_hex8     128^3 hexahedron_8 (2 097 152 elements, 2 146 689 nodes)
                  over a 1.28 m block, neo-Hookean lambda = 1 MPa, mu = 0.4 MPa
                  (E, nu derived), rho = 1100; face x = 0 fixed; v ~ N(0, 0.05)
@@ -22,7 +26,7 @@ import math
 import numpy as np
 
 from . import _abi
-from .mesh import block_hexahedron8, cube_tetrahedron4, plate_triangle3
+from .mesh import Mesh, block_hexahedron8, box_tetrahedron4, cube_tetrahedron4, plate_triangle3
 
 SEED = 20261203
 
@@ -50,6 +54,64 @@ def cube_tet4(n=100, length=1.0):
     mat = dict(kind=_abi.MATERIAL_ELASTIC, rho=2700.0, E=70e9, nu=0.33)
     return dict(name="cube_tet4", mesh=mesh, materials=[mat], blocked=blocked,
                 u0=np.zeros_like(x), v0=v0, dt_factor=0.8, steps=1000)
+
+
+def bar_tet4(n=100, nslabs=1, length=1.0):
+    """The whole bar as one mesh (for sizes a test can hold)."""
+    mesh = box_tetrahedron4(n, n, n * nslabs, length, length, length * nslabs)
+    x = mesh.nodes
+    blocked, v0 = _bar_conditions(x[:, 2], length * nslabs)
+    mat = dict(kind=_abi.MATERIAL_ELASTIC, rho=2700.0, E=70e9, nu=0.33)
+    return dict(name="bar_tet4", mesh=mesh, materials=[mat], blocked=blocked,
+                u0=np.zeros_like(x), v0=v0, dt_factor=0.8, steps=1000)
+
+
+def _bar_conditions(z, top):
+    blocked = np.zeros((len(z), 3), dtype=np.uint8)
+    blocked[np.isclose(z, 0.0)] = 1
+    v0 = np.zeros((len(z), 3))
+    v0[np.isclose(z, top), 2] = 1.0
+    return blocked, v0
+
+
+def bar_tet4_slabs(n, nslabs, here, length=1.0):
+    """The parts of bar_tet4(n, nslabs) cut into its nslabs cubes along z
+    (part r: the cells r n <= k < (r + 1) n), built directly, without the
+    whole mesh: for each part in `here` a decompose.MeshPart with global
+    node ids, its local mesh (node coordinates bit-identical to the whole
+    mesh's), its interface planes (bottom shared with part r - 1, top with
+    part r + 1) and their holders. Also returns the whole mesh's node count
+    and its blocked / initial-velocity arrays (whole-mesh, for set_field)."""
+    from .decompose import MeshPart
+    p = n + 1
+    plane = p * p
+    lz, nz = length * nslabs, n * nslabs
+    h = lz / nz  # the whole mesh's spacing, _grid_nodes_3d
+    xs = np.arange(p, dtype=np.float64) * (length / n)
+    local = box_tetrahedron4(n, n, n, length, length, length)
+    ne = len(local.connectivity)
+    parts = []
+    for r in here:
+        zs = np.arange(r * n, (r + 1) * n + 1, dtype=np.float64) * h
+        Z, Y, X = np.meshgrid(zs, xs, xs, indexing="ij")
+        coords = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+        mesh = Mesh(3, _abi.TETRAHEDRON_4, coords, local.connectivity)
+        nodes = np.arange(r * n * plane, r * n * plane + p * plane, dtype=np.int64)
+        lo = np.arange(plane) if r > 0 else np.zeros(0, np.int64)
+        hi = n * plane + np.arange(plane) if r < nslabs - 1 else np.zeros(0, np.int64)
+        iface = np.concatenate([lo, hi]).astype(np.uint32)
+        holders = np.concatenate([np.repeat([[r - 1, r]], len(lo), 0).ravel(),
+                                  np.repeat([[r, r + 1]], len(hi), 0).ravel()]).astype(np.int64)
+        owned = np.ones(len(nodes), dtype=bool)
+        owned[lo] = False  # the bottom plane belongs to the part below
+        parts.append(MeshPart(r, np.arange(r * ne, (r + 1) * ne, dtype=np.int64), nodes, mesh,
+                              iface, None, owned, np.arange(0, 2 * len(iface) + 1, 2), holders))
+    nb_nodes = plane * (nz + 1)
+    z = np.repeat(np.arange(nz + 1, dtype=np.float64) * h, plane)
+    blocked, v0 = _bar_conditions(z, lz)
+    mat = dict(kind=_abi.MATERIAL_ELASTIC, rho=2700.0, E=70e9, nu=0.33)
+    return dict(name="bar_tet4", parts=parts, nb_nodes=nb_nodes, materials=[mat],
+                blocked=blocked, u0=np.zeros((nb_nodes, 3)), v0=v0, dt_factor=0.8, steps=1000)
 
 
 def neohookean_from_lame(lam, mu, rho):

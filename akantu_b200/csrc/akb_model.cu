@@ -73,17 +73,20 @@ struct akb_model {
     unsigned char* host = nullptr;
     unsigned char* dev = nullptr;
     int64_t capacity = 0;  // bytes
-    cudaEvent_t copied = nullptr;  // the upload (copy stream) is done
+    cudaEvent_t copied = nullptr;  // the upload (upload stream) is done
     cudaEvent_t done = nullptr;    // the update kernel (model stream) has run
     bool pending = false;
   };
   static constexpr int kBcSlots = 4;
   BcSlot bc[kBcSlots];
   int bc_next = 0;
-  // host <-> device copies of the per-step calls (Dirichlet uploads, energy
-  // results) run on a stream of their own, ordered against the model's
-  // stream by events, so that they overlap the steps' kernels
+  // host <-> device copies of the per-step calls run on streams of their own,
+  // ordered against the model's stream by events, so that they overlap the
+  // steps' kernels: Dirichlet uploads on upload_stream, energy results on
+  // copy_stream (one stream for both would queue step s's upload behind step
+  // s-1's result copy, which waits for step s-1's kernels)
   cudaStream_t copy_stream = nullptr;
+  cudaStream_t upload_stream = nullptr;
   // akb_get_energy_async: a ring of device result slots; a slot is written
   // again only once the copy of its previous value is done
   static constexpr int kEnergySlots = 32;
@@ -101,6 +104,8 @@ struct akb_model {
   const uint32_t* d_iface_g = nullptr;     // internal id of each interface node
   const uint32_t* d_iface_part = nullptr;  // its first partial slot
   const uint32_t* d_iface_k = nullptr;     // its partial count
+  akb::ExchangePlan xplan;                 // neighbour exchange (akb_part_set_exchange)
+  bool has_xplan = false;
   // internal node order of the fused step (akb_patch.cuh): perm[caller's id]
   // = internal id; nodal arrays crossing the C ABI are reordered through
   // d_tmp. Without patches the order is the caller's (d_perm null).
@@ -494,6 +499,7 @@ akb_status check_model(const akb_model* m) {
 akb_status sync(akb_model* m) {
   cudaError_t e = cudaStreamSynchronize(m->stream);
   if (e == cudaSuccess && m->copy_stream) e = cudaStreamSynchronize(m->copy_stream);
+  if (e == cudaSuccess && m->upload_stream) e = cudaStreamSynchronize(m->upload_stream);
   if (e != cudaSuccess) return fail(AKB_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
   if (m->use_patches && m->patches.err) {  // a bounded wait of the fused step gave up
     int flag = 0;
@@ -519,6 +525,7 @@ cudaError_t enqueue_energy(akb_model* m, int32_t kind, double* out) {
 akb_status ensure_copy_stream(akb_model* m) {
   if (m->copy_stream) return AKB_OK;
   AKB_CUDA_TRY(cudaStreamCreateWithFlags(&m->copy_stream, cudaStreamNonBlocking));
+  AKB_CUDA_TRY(cudaStreamCreateWithFlags(&m->upload_stream, cudaStreamNonBlocking));
   return AKB_OK;
 }
 
@@ -837,6 +844,7 @@ akb_status akb_model_destroy(akb_model* m) {
   cudaSetDevice(m->device);
   cudaStreamSynchronize(m->stream);
   if (m->copy_stream) cudaStreamSynchronize(m->copy_stream);
+  if (m->upload_stream) cudaStreamSynchronize(m->upload_stream);
   destroy_graphs(m);
   for (void* p : m->allocations) cudaFree(p);
   if (m->h_result) cudaFreeHost(m->h_result);
@@ -850,6 +858,7 @@ akb_status akb_model_destroy(akb_model* m) {
     if (m->eres_copied[k]) cudaEventDestroy(m->eres_copied[k]);
   }
   if (m->copy_stream) cudaStreamDestroy(m->copy_stream);
+  if (m->upload_stream) cudaStreamDestroy(m->upload_stream);
   if (m->owns_stream) cudaStreamDestroy(m->stream);
   delete m;
   return AKB_OK;
@@ -1230,10 +1239,10 @@ akb_status akb_apply_dirichlet(akb_model* m, const uint32_t* nodes, int64_t nb_n
   }
   std::memcpy(b.host, nodes, (size_t)nb_nodes * sizeof(uint32_t));
   std::memcpy(b.host + nbytes, values, (size_t)nvals * sizeof(double));
-  // the upload runs on the copy stream (overlapping the kernels queued
+  // the upload runs on the upload stream (overlapping the kernels queued
   // before it); the update kernel waits for it on the model's stream
-  AKB_CUDA_TRY(cudaMemcpyAsync(b.dev, b.host, bytes, cudaMemcpyHostToDevice, m->copy_stream));
-  AKB_CUDA_TRY(cudaEventRecord(b.copied, m->copy_stream));
+  AKB_CUDA_TRY(cudaMemcpyAsync(b.dev, b.host, bytes, cudaMemcpyHostToDevice, m->upload_stream));
+  AKB_CUDA_TRY(cudaEventRecord(b.copied, m->upload_stream));
   AKB_CUDA_TRY(cudaStreamWaitEvent(m->stream, b.copied, 0));
   AKB_CUDA_TRY(apply_dirichlet(m->dm, reinterpret_cast<const uint32_t*>(b.dev), nb_nodes, component,
                                reinterpret_cast<const double*>(b.dev + nbytes), m->d_perm,
@@ -1486,6 +1495,107 @@ akb_status akb_part_step_end(akb_model* m, const double* device_in) {
   m->ke_valid = true;
   m->fint_valid = false;
   m->stresses_valid = false;
+  return AKB_OK;
+}
+
+akb_status akb_part_set_exchange(akb_model* m, int64_t nb_send, const uint32_t* send_rows,
+                                 int64_t nb_recv, const int64_t* sum_ptr,
+                                 const int64_t* sum_src) {
+  akb_status st;
+  if ((st = check_part(m)) != AKB_OK) return st;
+  if (m->part_in_step) return fail(AKB_ERR_STATE, "inside a step");
+  const int64_t n = m->n_iface;
+  if (nb_send < 0 || nb_recv < 0 || (nb_send > 0 && !send_rows) || !sum_ptr ||
+      (n > 0 && !sum_src))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "exchange plan: null array or negative size");
+  if (nb_send >= INT32_MAX || nb_recv >= INT32_MAX)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "exchange plan: more than 2^31 - 1 rows");
+  for (int64_t k = 0; k < nb_send; ++k)
+    if ((int64_t)send_rows[k] >= n)
+      return fail(AKB_ERR_INVALID_ARGUMENT, "exchange plan: send row out of range");
+  if (sum_ptr[0] != 0) return fail(AKB_ERR_INVALID_ARGUMENT, "exchange plan: sum_ptr[0] != 0");
+  std::vector<uint32_t> ptr(n + 1), rows(send_rows, send_rows + nb_send);
+  std::vector<int32_t> src;
+  for (int64_t i = 0; i < n; ++i) {
+    if (sum_ptr[i + 1] < sum_ptr[i] || sum_ptr[i + 1] >= INT32_MAX)
+      return fail(AKB_ERR_INVALID_ARGUMENT, "exchange plan: sum_ptr not ascending");
+    int own = 0;
+    for (int64_t j = sum_ptr[i]; j < sum_ptr[i + 1]; ++j) {
+      const int64_t v = sum_src[j];
+      if (v < -1 || v >= nb_recv)
+        return fail(AKB_ERR_INVALID_ARGUMENT, "exchange plan: sum term out of range");
+      own += v == -1;
+      src.push_back((int32_t)v);
+    }
+    if (own != 1)
+      return fail(AKB_ERR_INVALID_ARGUMENT,
+                  "exchange plan: every interface row sums its own value exactly once");
+    ptr[i + 1] = (uint32_t)sum_ptr[i + 1];
+  }
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  akb::ExchangePlan x;
+  x.n_send = nb_send;
+  x.n_recv = nb_recv;
+  x.n_rows = n;
+  if (nb_send > 0 && (st = upload(m, rows, &x.send_rows)) != AKB_OK) return st;
+  if ((st = upload(m, ptr, &x.sum_ptr)) != AKB_OK) return st;
+  if (!src.empty() && (st = upload(m, src, &x.sum_src)) != AKB_OK) return st;
+  m->xplan = x;
+  m->has_xplan = true;
+  return AKB_OK;
+}
+
+static akb_status check_xplan(akb_model* m) {
+  akb_status st;
+  if ((st = check_part(m)) != AKB_OK) return st;
+  if (!m->has_xplan) return fail(AKB_ERR_STATE, "no exchange plan (akb_part_set_exchange)");
+  return AKB_OK;
+}
+
+akb_status akb_part_pack_forces(akb_model* m, double* device_send) {
+  akb_status st;
+  if ((st = check_xplan(m)) != AKB_OK) return st;
+  if (!m->part_in_step) return fail(AKB_ERR_STATE, "no step begun");
+  if (m->xplan.n_send > 0 && !device_send) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(patch_iface_pack(m->dm, m->patches, m->d_iface_part, m->d_iface_k, m->xplan,
+                                device_send, m->stream));
+  return AKB_OK;
+}
+
+akb_status akb_part_step_end_exchange(akb_model* m, const double* device_recv) {
+  akb_status st;
+  if ((st = check_xplan(m)) != AKB_OK) return st;
+  if (!m->part_in_step) return fail(AKB_ERR_STATE, "no step begun");
+  if (m->xplan.n_recv > 0 && !device_recv) return fail(AKB_ERR_INVALID_ARGUMENT, "null input");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(patch_iface_sum_import(m->dm, m->patches, m->d_iface_part, m->d_iface_k,
+                                      m->xplan, device_recv, m->stream));
+  AKB_CUDA_TRY(patch_finish_list(m->dm, m->patches, m->dt, m->has_fext, m->stream));
+  m->part_in_step = false;
+  m->ke_valid = true;
+  m->fint_valid = false;
+  m->stresses_valid = false;
+  return AKB_OK;
+}
+
+akb_status akb_part_pack_mass(akb_model* m, double* device_send) {
+  akb_status st;
+  if ((st = check_xplan(m)) != AKB_OK) return st;
+  if (m->xplan.n_send > 0 && !device_send) return fail(AKB_ERR_INVALID_ARGUMENT, "null output");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(mass_pack(m->dm, m->d_iface_g, m->xplan, device_send, m->stream));
+  return AKB_OK;
+}
+
+akb_status akb_part_import_mass_exchange(akb_model* m, const double* device_recv) {
+  akb_status st;
+  if ((st = check_xplan(m)) != AKB_OK) return st;
+  if (m->part_in_step) return fail(AKB_ERR_STATE, "inside a step");
+  if (m->xplan.n_recv > 0 && !device_recv) return fail(AKB_ERR_INVALID_ARGUMENT, "null input");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  AKB_CUDA_TRY(mass_sum_import(m->dm, m->d_iface_g, m->xplan, device_recv, m->stream));
+  m->ke_valid = false;
   return AKB_OK;
 }
 

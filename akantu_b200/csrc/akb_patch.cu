@@ -671,6 +671,61 @@ __global__ void k_iface_import(DevPatches P, const uint32_t* parts, const uint32
   for (uint32_t r = 0; r < k; ++r) P.partial[(size_t)(part + r) * d + i] = r == 0 ? in[t] : 0.0;
 }
 
+// One thread per (packed row, component); the own value of a row is the sum
+// of its partial slots, as k_iface_export forms it.
+__global__ void k_iface_pack(DevPatches P, const uint32_t* parts, const uint32_t* ks,
+                             ExchangePlan x, int d, double* out) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= x.n_send * d) return;
+  const int64_t j = t / d;
+  const int i = (int)(t - j * d);
+  const uint32_t e = x.send_rows[j];
+  const uint32_t part = parts[e], k = ks[e];
+  double f = 0.0;
+  for (uint32_t r = 0; r < k; ++r) f += P.partial[(size_t)(part + r) * d + i];
+  out[t] = f;
+}
+
+// One thread per (interface row, component): the terms in the plan's order,
+// then the total written as the row's only partial.
+__global__ void k_iface_sum_import(DevPatches P, const uint32_t* parts, const uint32_t* ks,
+                                   ExchangePlan x, int d, const double* recv) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= x.n_rows * d) return;
+  const int64_t e = t / d;
+  const int i = (int)(t - e * d);
+  const uint32_t part = parts[e], k = ks[e];
+  double own = 0.0;
+  for (uint32_t r = 0; r < k; ++r) own += P.partial[(size_t)(part + r) * d + i];
+  double acc = 0.0;
+  for (uint32_t j = x.sum_ptr[e]; j < x.sum_ptr[e + 1]; ++j) {
+    const int32_t src = x.sum_src[j];
+    acc += src < 0 ? own : recv[(int64_t)src * d + i];
+  }
+  for (uint32_t r = 0; r < k; ++r) P.partial[(size_t)(part + r) * d + i] = r == 0 ? acc : 0.0;
+}
+
+__global__ void k_mass_pack(DevModel m, const uint32_t* nodes, ExchangePlan x, double* out) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= x.n_send) return;
+  out[t] = m.mass[(int64_t)nodes[x.send_rows[t]] * m.dim];
+}
+
+__global__ void k_mass_sum_import(DevModel m, const uint32_t* nodes, ExchangePlan x,
+                                  const double* recv) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= x.n_rows) return;
+  const int64_t g = nodes[e];
+  const double own = m.mass[g * m.dim];
+  double M = 0.0;
+  for (uint32_t j = x.sum_ptr[e]; j < x.sum_ptr[e + 1]; ++j) {
+    const int32_t src = x.sum_src[j];
+    M += src < 0 ? own : recv[src];
+  }
+  for (int c = 0; c < m.dim; ++c) m.mass[g * m.dim + c] = M;
+  m.inv_mass[g] = 1. / M;
+}
+
 __global__ void k_mass_export(DevModel m, const uint32_t* nodes, int64_t n, double* out) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= n) return;
@@ -854,6 +909,36 @@ cudaError_t mass_import(const DevModel& m, const uint32_t* nodes, int64_t n, con
                         cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   k_mass_import<<<blocks_of(n), kThreads, 0, s>>>(m, nodes, n, in);
+  return cudaGetLastError();
+}
+
+cudaError_t patch_iface_pack(const DevModel& m, const DevPatches& p, const uint32_t* part,
+                             const uint32_t* k, const ExchangePlan& x, double* out,
+                             cudaStream_t s) {
+  if (x.n_send <= 0) return cudaSuccess;
+  k_iface_pack<<<blocks_of(x.n_send * m.dim), kThreads, 0, s>>>(p, part, k, x, m.dim, out);
+  return cudaGetLastError();
+}
+
+cudaError_t patch_iface_sum_import(const DevModel& m, const DevPatches& p, const uint32_t* part,
+                                   const uint32_t* k, const ExchangePlan& x, const double* recv,
+                                   cudaStream_t s) {
+  if (x.n_rows <= 0) return cudaSuccess;
+  k_iface_sum_import<<<blocks_of(x.n_rows * m.dim), kThreads, 0, s>>>(p, part, k, x, m.dim, recv);
+  return cudaGetLastError();
+}
+
+cudaError_t mass_pack(const DevModel& m, const uint32_t* nodes, const ExchangePlan& x,
+                      double* out, cudaStream_t s) {
+  if (x.n_send <= 0) return cudaSuccess;
+  k_mass_pack<<<blocks_of(x.n_send), kThreads, 0, s>>>(m, nodes, x, out);
+  return cudaGetLastError();
+}
+
+cudaError_t mass_sum_import(const DevModel& m, const uint32_t* nodes, const ExchangePlan& x,
+                            const double* recv, cudaStream_t s) {
+  if (x.n_rows <= 0) return cudaSuccess;
+  k_mass_sum_import<<<blocks_of(x.n_rows), kThreads, 0, s>>>(m, nodes, x, recv);
   return cudaGetLastError();
 }
 

@@ -182,6 +182,31 @@ cudaError_t mass_export(const DevModel& m, const uint32_t* nodes, int64_t n, dou
                         cudaStream_t s);
 cudaError_t mass_import(const DevModel& m, const uint32_t* nodes, int64_t n, const double* in,
                         cudaStream_t s);
+// Neighbour exchange of a part. An ExchangePlan lists the interface rows
+// packed for the neighbours (send_rows, the neighbours' blocks concatenated)
+// and, per interface row i, the terms of its sum in ascending part order:
+// sum_src[sum_ptr[i] .. sum_ptr[i+1]), -1 for this part's own value, else a
+// row of the received buffer. Every part holding a node adds the same terms
+// in the same order, so all copies of the sum are equal.
+struct ExchangePlan {
+  int64_t n_send = 0, n_recv = 0, n_rows = 0;
+  const uint32_t* send_rows = nullptr;
+  const uint32_t* sum_ptr = nullptr;
+  const int32_t* sum_src = nullptr;
+};
+// out[k] = this part's force on interface row send_rows[k] (d per row)
+cudaError_t patch_iface_pack(const DevModel& m, const DevPatches& p, const uint32_t* part,
+                             const uint32_t* k, const ExchangePlan& x, double* out,
+                             cudaStream_t s);
+// every interface row's force = its ordered sum, imported as its only partial
+cudaError_t patch_iface_sum_import(const DevModel& m, const DevPatches& p, const uint32_t* part,
+                                   const uint32_t* k, const ExchangePlan& x, const double* recv,
+                                   cudaStream_t s);
+// the same for the lumped masses (one value per row) of internal nodes nodes[i]
+cudaError_t mass_pack(const DevModel& m, const uint32_t* nodes, const ExchangePlan& x,
+                      double* out, cudaStream_t s);
+cudaError_t mass_sum_import(const DevModel& m, const uint32_t* nodes, const ExchangePlan& x,
+                            const double* recv, cudaStream_t s);
 // Caller order <-> internal order of nodal arrays (rows of `width` items):
 // gather: out[i] = in[perm[i]]; scatter: out[perm[i]] = in[i].
 cudaError_t permute_rows(const uint32_t* perm, int64_t n, int width, const double* in,

@@ -18,9 +18,11 @@
 //    last call's partials. Each call overwrites every partial it reads, so
 //    nothing has to start at zero; calls that overlap on the GPU (different
 //    streams, no ordering between them) race on the array;
-//  - the device address of g_partials is looked up once per device, on the
-//    first call made with that device current; make that first call before
-//    any stream capture.
+//  - the device address of g_partials is looked up again on every call made
+//    outside stream capture (so a device reset, which reloads the module,
+//    leaves no stale address behind) and cached per device for calls made
+//    during a capture; make one call with the device current before the
+//    first capture.
 #include <mutex>
 
 #include <cfloat>
@@ -101,10 +103,13 @@ extern "C" akb_status akb_kinetic_energy_static(const double* mass, const double
   AKB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices)
     return fail(AKB_ERR_UNSUPPORTED, "akb_kinetic_energy_static: device ordinal >= 64");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  AKB_CUDA_TRY(cudaStreamIsCapturing(s, &capture));
   double* partials = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_address[dev]) {
+    if (!g_partials_address[dev] || capture == cudaStreamCaptureStatusNone) {
       // host code cannot use &g_partials: it is a host-side stand-in, not the
       // device address; ask the runtime for the address on this device
       void* p = nullptr;
@@ -117,7 +122,6 @@ extern "C" akb_status akb_kinetic_energy_static(const double* mass, const double
   }
   const int per_block = kThreads * kNodesPerThread;
   const int nblocks = (int)((nb_nodes + per_block - 1) / per_block);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   k_kinetic_partials<<<nblocks, kThreads, 0, s>>>(mass, velocity, nb_nodes, spatial_dimension,
                                                   partials);
   k_kinetic_finish<<<1, kThreads, 0, s>>>(partials, nblocks, result);

@@ -9,10 +9,13 @@ whole mesh; the metric counts elements x steps per second.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One process per GPU (torchrun for N > 1); each rank advances its own copy of
-the mesh (the single-mesh path runs as replicas, no data-path collective).
-Device time is measured with CUDA events on the model's stream, max over
-ranks. Prints one JSON line on rank 0.
+One process per GPU (torchrun for N > 1). With N > 1 ranks the workload is
+one mesh cut over the GPUs: the cube stacked N times along z (bar_tet4), one
+100^3 cube per GPU (weak scaling), the forces on the interface planes
+exchanged with the neighbouring GPUs every step (grouped NCCL send/recv);
+--replicas runs one independent cube per rank instead. Device time is
+measured with CUDA events on the model's stream, max over ranks. Prints one
+JSON line on rank 0.
 """
 from __future__ import annotations
 
@@ -365,29 +368,42 @@ def run_ours(args, dist):
 
 
 def run_decomposed(args, dist):
-    """The headline cube cut into parts, one per rank (or --parts-per-rank on
-    each GPU), stepped as one mesh: per step each part's interface forces go
-    into one array over all interface nodes, all-reduced (NCCL) across ranks.
-    Total work is fixed as N grows (strong scaling)."""
+    """bar_tet4: the headline cube stacked N times along z as ONE mesh (N =
+    ranks x --parts-per-rank), cut into its cubes, parts_per_rank slabs per
+    GPU, each slab the 100^3 x 6 cube (weak scaling: the work per GPU is the
+    headline's). Per step each part runs the fused step, packs the forces on
+    its interface planes, exchanges them with its neighbours only (grouped
+    NCCL send/recv on the step's stream, a copy between parts of one GPU),
+    and finishes the planes with the sums in part order."""
     import torch
+    from akantu_b200._lib import check, lib
     from akantu_b200.decompose import DistributedModel
     device = dist.local_rank
     torch.cuda.set_device(device)
-    w = configs.cube_tet4(args.cells)
-    E = w["mesh"].getNbElement()
     ppr = max(1, args.parts_per_rank)
-    nparts = dist.world * ppr
-    dm = DistributedModel(w["mesh"], w["materials"], nparts, precision=_abi.MODE_FP64,
-                          device=device, here=list(range(dist.rank * ppr, (dist.rank + 1) * ppr)))
-    dm.set_blocked(w["blocked"])
-    dm.set_field(_abi.FIELD_DISPLACEMENT, w["u0"])
-    dm.set_field(_abi.FIELD_VELOCITY, w["v0"])
-    dt = w["dt_factor"] * dm.stable_time_step()
+    nslabs = dist.world * ppr
+    here = list(range(dist.rank * ppr, (dist.rank + 1) * ppr))
+    s = configs.bar_tet4_slabs(args.cells, nslabs, here)
+    peak, peak_kind = load_peaks()
+    dm = DistributedModel(None, s["materials"], nslabs, precision=_abi.MODE_FP64, device=device,
+                          parts=s["parts"], nb_nodes=s["nb_nodes"], group=None)
+    E_part = s["parts"][0].mesh.getNbElement()
+    E = E_part * nslabs
+
+    def reset():
+        dm.set_blocked(s["blocked"])
+        dm.set_field(_abi.FIELD_DISPLACEMENT, s["u0"])
+        dm.set_field(_abi.FIELD_VELOCITY, s["v0"])
+        dm.set_field(_abi.FIELD_ACCELERATION, np.zeros_like(s["u0"]))
+
+    reset()
+    dt = s["dt_factor"] * dm.stable_time_step()
     dm.set_time_step(dt)
     dm.solve_steps(args.warmup)
+    reset()
     sampler = ClockSampler(device)
-    dist.barrier()
     torch.cuda.synchronize()
+    dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sampler.start()
     e0.record()
@@ -397,21 +413,72 @@ def run_decomposed(args, dist):
     clocks = sampler.stop()
     dist.barrier()
     ms = dist.max(e0.elapsed_time(e1))
-    iface = dm.n_interface
+    # e2e through the C ABI with host buffers: per step the bottom face's
+    # Dirichlet values (all components, one call, on the part holding it)
+    # from pinned memory, the step, and each part's kinetic energy queued
+    # into its own pinned slot; read after the final synchronisation
+    L = lib()
+    e2e_steps = min(args.steps, 200)
+    fixed_g = np.nonzero(s["blocked"][:, 0])[0]
+    bcs = []
+    for p, b in zip(dm.parts, dm.backends):
+        loc = np.searchsorted(p.nodes, fixed_g)
+        loc = loc[(loc < len(p.nodes)) & (p.nodes[np.minimum(loc, len(p.nodes) - 1)] == fixed_g)]
+        if len(loc):
+            nh = torch.from_numpy(loc.astype(np.uint32)).pin_memory()
+            vh = torch.zeros(len(loc) * 3, dtype=torch.float64).pin_memory()
+            bcs.append((b.m.handle, nh, vh, len(loc)))
+    energies = torch.zeros((e2e_steps, len(dm.backends)), dtype=torch.float64).pin_memory()
+    reset()
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        for h, nh, vh, n in bcs:
+            check(L.akb_apply_dirichlet(h, C.cast(nh.data_ptr(), C.POINTER(C.c_uint32)), n,
+                                        _abi.ALL_COMPONENTS,
+                                        C.cast(vh.data_ptr(), C.POINTER(C.c_double))))
+        dm.solve_step()
+        for j, b in enumerate(dm.backends):
+            check(L.akb_get_energy_async(b.m.handle, _abi.ENERGY_KINETIC,
+                                         C.c_void_p(energies.data_ptr() + 8 * (k * len(dm.backends) + j))))
+    for b in dm.backends:
+        check(L.akb_synchronize(b.m.handle))
+    ek = energies.numpy().sum(axis=1)
+    t1 = time.perf_counter()
+    dist.barrier()
+    assert np.all(np.isfinite(ek))
+    e2e_s = dist.max(t1 - t0)
+    h2d = int(dist.sum(float(sum(n * (4 + 24) for _, _, _, n in bcs))))
+    d2h = 8 * nslabs
+    nbytes = dist.sum(float(dm.bytes_per_step))
+    balg = b_alg_bytes({"mesh": s["parts"][0].mesh}, False) * ppr
     dm.close()
     if dist.rank != 0:
         return None
+    achieved = balg / (ms / args.steps / 1e3) / 1e9
+    n = args.cells
     return {"metric": METRIC, "value": E * args.steps / (ms / 1e3), "unit": UNIT,
             "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "cube_tet4: %d^3 cells x 6 tetrahedron_4 (%d elements), "
-                                   "linear elastic, FP64, dt = 0.8 x stable" % (args.cells, E),
-                       "parallelism": "mesh cut into %d parts (coordinate bisection), %d per GPU; "
-                                      "%d interface nodes, their forces all-reduced each step"
-                                      % (nparts, ppr, iface),
-                       "time_step": dt},
-            "clocks": clocks, "gpu_launches": args.steps * 4 * nparts}
+            "config": {"workload": "bar_tet4: %d x %d x %d cells x 6 tetrahedron_4 (%d elements, "
+                                   "%d nodes), linear elastic, FP64, dt = 0.8 x stable"
+                                   % (n, n, n * nslabs, E, s["nb_nodes"]),
+                       "elements": E, "time_step": dt,
+                       "parallelism": "one mesh cut into %d cubes along z, %d per GPU; "
+                                      "neighbour exchange of the interface planes" % (nslabs, ppr),
+                       "exchange_bytes_per_step": nbytes,
+                       "l2": "no flush: per-GPU working set %.0f MB > 126 MB L2" % (balg / 1e6)},
+            "roofline": {"bound": "hbm", "kernel": "whole step per GPU (fused step, pack, "
+                                                   "exchange, interface sums, shared-node pass)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_step": balg, "traffic": None},
+            "clocks": clocks,
+            "e2e": {"value": E * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "gpu_launches": args.steps * 4 * nslabs}
 
 
 def run_plate(args, device):
@@ -756,8 +823,10 @@ def main():
     ap.add_argument("--fe2-check-cells", type=int, default=8)
     ap.add_argument("--no-fe2", action="store_true")
     ap.add_argument("--decompose", action="store_true",
-                    help="the headline cube as one mesh cut over the ranks (strong scaling) "
-                         "instead of one mesh per rank")
+                    help="one mesh cut over the ranks (the default with several ranks): the "
+                         "headline cube stacked once per part along z, one part per GPU")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with several ranks, one independent headline cube per rank instead")
     ap.add_argument("--parts-per-rank", type=int, default=1)
     ap.add_argument("--workload", default="", choices=["", "plate_tri3", "block_hex8", "plates_batch"],
                     help="run only this secondary workload (1 GPU) and print its result")
@@ -786,7 +855,7 @@ def main():
         print(json.dumps({"workloads": {args.workload: fn()}}), flush=True)
         return
     dist = Dist(args.gpus)
-    if args.decompose:
+    if args.decompose or (dist.world > 1 and not args.replicas):
         try:
             res = run_decomposed(args, dist)
             if dist.rank == 0:

@@ -283,8 +283,9 @@ akb_status akb_batch_get_energies(akb_model* model, int32_t kind, double* values
  * use a fixed 16 KiB array inside the library, held by every GPU that loads
  * it until exit: nb_nodes above 8 388 608 is rejected
  * (AKB_ERR_INVALID_ARGUMENT); calls that overlap on the GPU race on that
- * array; its device address is looked up on the first call per device, which
- * should therefore come before any stream capture. */
+ * array; its device address is looked up again on every call made outside
+ * stream capture and cached per device for calls made during one, so one
+ * call per device should come before the first capture. */
 akb_status akb_kinetic_energy_static(const double* mass, const double* velocity,
                                      int64_t nb_nodes, int32_t spatial_dimension,
                                      double* result, void* stream);
@@ -324,6 +325,32 @@ akb_status akb_part_export_forces(akb_model* model, double* device_out);
 akb_status akb_part_step_end(akb_model* model, const double* device_in);
 akb_status akb_part_export_mass(akb_model* model, double* device_out);
 akb_status akb_part_import_mass(akb_model* model, const double* device_in);
+
+/* Neighbour exchange (the send and receive schemes of the reference's
+ * ElementSynchronizer, element_synchronizer.hh:52, used by the _smm_stress
+ * synchronisation of solid_mechanics_model.cc:395-411): each part sends only
+ * the interface rows it shares with each neighbour and sums what it receives.
+ *   send_rows[k], k < nb_send: the interface row (index into the
+ *       interface_nodes given at creation) of the k-th packed value, the
+ *       blocks for the neighbours concatenated in the caller's order;
+ *   sum_ptr[i] .. sum_ptr[i+1] (nb_interface + 1 entries): the terms of
+ *       interface row i's sum, in the order they are added; sum_src[t] = -1
+ *       for this part's own value (exactly once per row), else a row of the
+ *       received buffer (nb_recv rows, the neighbours' blocks concatenated).
+ * With the terms in ascending part order on every part, all copies of an
+ * interface node's sum are equal. Arrays are host arrays, copied. A step is
+ * then akb_part_step_begin, akb_part_pack_forces (device_send: nb_send x d
+ * doubles), the transfer (e.g. grouped NCCL send/recv on the model's
+ * stream), akb_part_step_end_exchange (device_recv: nb_recv x d doubles);
+ * the masses are summed once by akb_part_pack_mass (nb_send doubles), the
+ * transfer, akb_part_import_mass_exchange (nb_recv doubles). */
+akb_status akb_part_set_exchange(akb_model* model, int64_t nb_send, const uint32_t* send_rows,
+                                 int64_t nb_recv, const int64_t* sum_ptr,
+                                 const int64_t* sum_src);
+akb_status akb_part_pack_forces(akb_model* model, double* device_send);
+akb_status akb_part_step_end_exchange(akb_model* model, const double* device_recv);
+akb_status akb_part_pack_mass(akb_model* model, double* device_send);
+akb_status akb_part_import_mass_exchange(akb_model* model, const double* device_recv);
 
 #ifdef __cplusplus
 }
