@@ -86,6 +86,7 @@ SIGNATURES = {
     "akb_rve_destroy": (I32, [P]),
     "akb_rve_get_info": (I32, [P, C.POINTER(_abi.RveInfo)]),
     "akb_rve_solve": (I32, [P, I64, P, P, P, P, P, P]),
+    "akb_rve_solve_indexed": (I32, [P, I64, P, P, P, P, P, P, P, P]),
     "akb_rve_stress": (I32, [P, I64, P, P, P, P, P]),
     "akb_mlp_create": (I32, [I32, I32, I32, I32, I32, P, C.POINTER(P)]),
     "akb_mlp_destroy": (I32, [P]),
@@ -94,6 +95,7 @@ SIGNATURES = {
     "akb_mlp_get_parameters": (I32, [P, C.POINTER(C.c_float), I64]),
     "akb_mlp_set_scaling": (I32, [P] + [C.POINTER(C.c_float)] * 4),
     "akb_mlp_forward": (I32, [P, I64, P, P, P]),
+    "akb_mlp_stress": (I32, [P, I64, P, P, C.c_double, C.c_double, P, P, P]),
     "akb_mlp_gradients": (I32, [P, I64, P, P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "akb_mlp_train_step": (I32, [P, I64, P, P, C.c_float, C.POINTER(C.c_float)]),
 }

@@ -1,10 +1,15 @@
 """Autotuner of the fused patch step.
 
 Chooses the patch shape (elements per patch, node cap) and the schedule (one
-CTA per patch, or a persistent grid striding over the patches) by timing a
-few steps of each candidate with CUDA events on the model's stream, and
-caches the winner in a JSON file keyed by GPU name, element type, precision
-mode and problem size (log2 bucket of the element count).
+CTA per patch, or a persistent grid of k CTAs per SM striding over the
+patches) by timing a few steps of each candidate with CUDA events on the
+model's stream, in three stages per element type: the patch size at the
+type's usual nodes-per-element ratio, then the node cap around the best
+size, then the persistent schedules of the best shape. Candidates the
+library refuses (a node cap too small for the mesh, shared memory over the
+limit) are skipped. The winner is cached in a JSON file keyed by GPU name,
+element type, precision mode and problem size (log2 bucket of the element
+count).
 """
 from __future__ import annotations
 
@@ -16,13 +21,22 @@ from . import _abi
 
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "akantu_b200", "tuning.json")
 
-# (elements per patch, node cap, persistent CTAs per SM or 0)
-CANDIDATES = {
-    _abi.TRIANGLE_3: [(1024, 640, 0), (512, 320, 0), (2048, 1100, 0), (1024, 640, 3), (768, 480, 0)],
-    _abi.TETRAHEDRON_4: [(1024, 400, 0), (512, 220, 0), (1536, 500, 0), (1024, 400, 3)],
-    _abi.HEXAHEDRON_8: [(512, 800, 0), (256, 448, 0), (384, 640, 0), (512, 800, 2)],
-    _abi.SEGMENT_2: [(1024, 1100, 0), (512, 600, 0)],
+# Search space per element type: patch sizes (elements), node caps as
+# multiples of the patch size (the middle one is the usual ratio of a compact
+# patch of that type), persistent CTAs per SM tried for the best shape.
+SPACE = {
+    _abi.SEGMENT_2: dict(elements=(256, 512, 1024, 2048), ratios=(1.02, 1.08, 1.15), persist=(2, 4)),
+    _abi.TRIANGLE_3: dict(elements=(256, 384, 512, 768, 1024, 1536, 2048),
+                          ratios=(0.56, 0.625, 0.70), persist=(2, 3)),
+    _abi.TETRAHEDRON_4: dict(elements=(256, 384, 512, 768, 1024, 1536),
+                             ratios=(0.33, 0.39, 0.47), persist=(2, 3)),
+    _abi.HEXAHEDRON_8: dict(elements=(128, 192, 256, 384, 512),
+                            ratios=(1.35, 1.56, 1.8), persist=(1, 2)),
 }
+
+
+def _node_cap(elements, ratio):
+    return int(math.ceil(elements * ratio / 16.0)) * 16
 
 
 def _gpu_key():
@@ -66,17 +80,45 @@ def tune(build, element_type, precision, nb_elements, steps=20, warmup=3,
     if key in cache:
         return cache[key], []
     _, sms = _gpu_key()
-    results = []
-    for pe, pn, per_sm in CANDIDATES[element_type]:
-        grid = per_sm * sms if per_sm else 0
-        model = build(pe, pn, grid)
-        model.solveSteps(warmup)
-        ms = model.timeSolveSteps(steps) / steps
-        model.close()
-        opt = dict(patch_elements=pe, patch_nodes=pn, patch_grid=grid)
+    space = SPACE[element_type]
+    results, seen = [], {}
+
+    def trial(pe, pn, per_sm):
+        opt = dict(patch_elements=int(pe), patch_nodes=int(pn),
+                   patch_grid=int(per_sm * sms) if per_sm else 0)
+        key = tuple(opt.values())
+        if key in seen:
+            return seen[key]
+        try:
+            model = build(opt["patch_elements"], opt["patch_nodes"], opt["patch_grid"])
+        except Exception as exc:  # refused shape: skipped
+            if log:
+                log("tune %s: skipped (%s)" % (opt, exc))
+            seen[key] = None
+            return None
+        try:
+            model.solveSteps(warmup)
+            ms = model.timeSolveSteps(steps) / steps
+        finally:
+            model.close()
         results.append((opt, ms))
+        seen[key] = ms
         if log:
             log("tune %s: %.4f ms/step" % (opt, ms))
+        return ms
+
+    def best_of(cands):
+        timed = [(c, trial(*c)) for c in cands]
+        timed = [(c, t) for c, t in timed if t is not None]
+        return min(timed, key=lambda ct: ct[1])[0] if timed else None
+
+    mid = space["ratios"][len(space["ratios"]) // 2]
+    shape = best_of([(pe, _node_cap(pe, mid), 0) for pe in space["elements"]])
+    if shape is None:
+        raise RuntimeError("autotune: no candidate could be built")
+    pe = shape[0]
+    shape = best_of([(pe, _node_cap(pe, r), 0) for r in space["ratios"]])
+    best_of([shape] + [(shape[0], shape[1], k) for k in space["persist"]])
     best = min(results, key=lambda r: r[1])[0]
     cache[key] = best
     if use_cache:

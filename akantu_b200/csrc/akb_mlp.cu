@@ -191,9 +191,18 @@ __device__ inline void tmem_ld16(uint32_t taddr, float* v) {
 
 // SiLU and its derivative (the result is rounded to BF16 anyway: fast
 // division; exp(-z) overflowing gives the limits 0 and 0)
-__device__ inline float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+// The logistic function as 1/2 + tanh(z/2)/2 with the hardware tanh
+// approximation: one special-function operation per element (the exp and
+// reciprocal form takes two), which bounds the epilogue.
+__device__ inline float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ inline float sigmoid(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
+__device__ inline float silu(float z) { return z * sigmoid(z); }
 __device__ inline float dsilu(float z) {
-  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
+  const float s = sigmoid(z);
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -225,35 +234,84 @@ __device__ inline void gemm_kmajor(uint32_t tmem_d, uint32_t a, uint32_t b, int 
 struct Shared {
   unsigned char* act;  // 128 x 256 packed BF16 (64 KB)
   unsigned char* wgt;  // 256 x 256 packed BF16 (128 KB)
-  float* bias;         // 256
+  float* bias;         // forward: every layer's biases (kMaxWidth per layer); backward: 256
   uint64_t* mbar;      // [0] MMA completion, [1] weights landed
   uint32_t* tmem_holder;
+  double* hnorm;       // 128: |H| of each row (stress mode)
 };
 
 constexpr size_t kActBytes = (size_t)kTile * kMaxWidth * 2;
 constexpr size_t kWgtBytes = (size_t)kMaxWidth * kMaxWidth * 2;
-constexpr size_t kFwdSmem = kActBytes + kWgtBytes + kMaxWidth * 4 + 64;
+// The forward pass stages a layer's weights in slices of output rows (a
+// contiguous block of the packed N x K matrix; 64 rows of a 256-wide layer),
+// so that its shared memory (~97 KB) lets two CTAs share an SM: one CTA's
+// epilogue (TMEM -> bias -> SiLU -> BF16) runs while the other's MMAs use
+// the tensor cores.
+constexpr size_t kSliceBytes = (size_t)64 * kMaxWidth * 2;
+constexpr size_t kTail = kMaxLayers * kMaxWidth * 4 + 64 + kTile * 8;  // biases, barriers, |H|
+constexpr size_t kFwdSmem = kActBytes + kSliceBytes + kTail;
+constexpr size_t kBwdSmem = kActBytes + kWgtBytes + kTail;
 
-__device__ inline Shared carve(unsigned char* smem) {
+__device__ inline Shared carve(unsigned char* smem, size_t wgt_bytes) {
   Shared s;
   s.act = smem;
   s.wgt = smem + kActBytes;
-  s.bias = reinterpret_cast<float*>(smem + kActBytes + kWgtBytes);
-  s.mbar = reinterpret_cast<uint64_t*>(smem + kActBytes + kWgtBytes + kMaxWidth * 4);
+  unsigned char* t = smem + kActBytes + wgt_bytes;
+  s.bias = reinterpret_cast<float*>(t);
+  s.mbar = reinterpret_cast<uint64_t*>(t + kMaxLayers * kMaxWidth * 4);
   s.tmem_holder = reinterpret_cast<uint32_t*>(s.mbar + 2);
+  s.hnorm = reinterpret_cast<double*>(t + kMaxLayers * kMaxWidth * 4 + 64);
   return s;
+}
+
+// Stress mode of the forward pass (MaterialFE2 with the surrogate): the
+// inputs are displacement gradients H ([nb][9], column-major per point), the
+// features (H / r, log r) with r = max(|H|, kHMin) are formed in the kernel,
+// the outputs are P = |H| net(.) ([nb][9], column-major), and the points
+// outside the training envelope (max |H_ij| > amplitude or det(I + H) <
+// min_det) are appended to index[] (count[0] entries; the caller zeroes it).
+constexpr double kHMin = 1e-8;
+struct StressArgs {
+  double amplitude = 0.0, min_det = 0.0;
+  int32_t* index = nullptr;
+  int32_t* count = nullptr;
+};
+
+__device__ inline double det_i_plus(const double* H) {  // det(I + H), H column-major
+  const double a = 1.0 + H[0], b = H[3], c = H[6];
+  const double d = H[1], e = 1.0 + H[4], f = H[7];
+  const double g = H[2], h = H[5], i = 1.0 + H[8];
+  return a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
 }
 
 // Forward pass of one tile of 128 samples. x: [nb][nin] FP64 raw inputs.
 // TRAIN stores the packed BF16 input and hidden activations (act[l], tile
 // major), the pre-activations Z (z[l], [nb_pad][N] FP32) and the normalised
 // outputs (ynorm, [nb_pad][16] FP32); otherwise y: [nb][nout] FP64 outputs.
-template <bool TRAIN>
-__global__ void __launch_bounds__(kFwdThreads, 1)
+// Output rows per weight slice of layer l: as many as the buffer holds (a
+// multiple of 16: whole row groups, a valid MMA N), at most the layer's N.
+__device__ inline int slice_rows(const Net& net, int l) {
+  return min(net.N[l], (int)(kSliceBytes / (2 * (size_t)net.K[l])) & ~15);
+}
+// Rows of slice j of layer l, its bytes and its source (rows [rows0 j, ...)
+// of the packed N x K matrix are one contiguous block).
+__device__ inline int slice_n(const Net& net, int l, int j) {
+  return min(slice_rows(net, l), net.N[l] - slice_rows(net, l) * j);
+}
+__device__ inline uint32_t slice_bytes(const Net& net, int l, int j) {
+  return (uint32_t)(slice_n(net, l, j) * net.K[l] * 2);
+}
+__device__ inline const void* slice_src(const Net& net, int l, int j) {
+  return reinterpret_cast<const unsigned char*>(net.W[l]) +
+         (size_t)slice_rows(net, l) * j * net.K[l] * 2;
+}
+
+template <bool TRAIN, bool STRESS = false>
+__global__ void __launch_bounds__(kFwdThreads, 2)
     k_forward(Net net, int64_t nb, const double* __restrict__ x, double* __restrict__ y,
-              Bufs bufs) {
+              Bufs bufs, StressArgs sa = StressArgs{}) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  Shared s = carve(smem);
+  Shared s = carve(smem, kSliceBytes);
   const int tid = threadIdx.x, warp = tid >> 5;
   const int r = tid & (kTile - 1), half = tid >> 7;  // row in the tile, column half
   const int64_t tile = blockIdx.x;
@@ -263,10 +321,43 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
   if (tid == 0) {
     mbar_init(mb_mma);
     mbar_init(mb_w);
-    bulk_load(saddr(s.wgt), net.W[0], (uint32_t)(net.N[0] * net.K[0] * 2), mb_w);
+    bulk_load(saddr(s.wgt), slice_src(net, 0, 0), slice_bytes(net, 0, 0), mb_w);
   }
+  // every layer's biases, once (the first barrier below publishes them)
+  for (int l = 0; l < net.nl; ++l)
+    for (int c = tid; c < net.N[l]; c += kFwdThreads) s.bias[l * kMaxWidth + c] = net.b[l][c];
   // inputs, normalised, padded to 16 columns (8 per thread)
-  {
+  if (STRESS) {
+    double H[9], n2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      H[k] = row < nb ? x[row * 9 + k] : 0.0;
+      n2 += H[k] * H[k];
+    }
+    const double hn = sqrt(n2), rr = fmax(hn, kHMin);
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {  // column j = 8 half + q: H_j / r (j < 9), log r (j = 9)
+      const int j = 8 * half + q;
+      const double f = half == 0 ? H[q] / rr : (q == 0 ? H[8] / rr : (q == 1 ? log(rr) : 0.0));
+      v[q] = (j < net.nin && row < nb) ? (float)((f - net.in_shift[j]) * net.in_scale[j]) : 0.0f;
+    }
+    store8(s.act, r, 8 * half, 16, v);
+    if (half == 0) {  // warps 0-3: one row each lane
+      s.hnorm[r] = hn;
+      if (sa.count) {
+        double hmax = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) hmax = fmax(hmax, fabs(H[k]));
+        const bool out = row < nb && (hmax > sa.amplitude || det_i_plus(H) < sa.min_det);
+        const unsigned mask = __ballot_sync(0xffffffffu, out);
+        int base = 0;
+        if ((tid & 31) == 0 && mask) base = atomicAdd(sa.count, __popc(mask));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (out) sa.index[base + __popc(mask & ((1u << (tid & 31)) - 1u))] = (int32_t)row;
+      }
+    }
+  } else {
     float v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -278,40 +369,48 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
     store8(s.act, r, 8 * half, 16, v);
     if (TRAIN) store8(bufs.act[0] + tile * (size_t)kTile * 16 * 2, r, 8 * half, 16, v);
   }
+  fence_smem_async();  // the A tile, written by this thread, before the MMAs read it
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = *s.tmem_holder;
   const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
-  // the weights of layer l + 1 are copied (TMA bulk) while layer l's
-  // epilogue runs: the copy starts as soon as layer l's MMAs completed
+  // A layer's weights arrive slice by slice (TMA bulk into one buffer):
+  // slice j's MMAs write accumulator columns [kSlice j, ...); the next slice
+  // (or the next layer's first, during this layer's epilogue) is copied as
+  // soon as they completed.
   uint32_t pm = 0, pw = 0;
   bool ok = true, w_pending = true, m_pending = false;
   for (int l = 0; l < net.nl && ok; ++l) {
     const int K = net.K[l], N = net.N[l];
-    for (int c = tid; c < N; c += kFwdThreads) s.bias[c] = net.b[l][c];
-    fence_smem_async();
-    __syncthreads();
-    ok = mbar_wait(mb_w, pw);
-    if (!ok) break;
-    pw ^= 1;
-    w_pending = false;
-    if (tid == 0) {
+    const int rows0 = slice_rows(net, l);
+    const int nslices = (N + rows0 - 1) / rows0;
+    const float* bias = s.bias + l * kMaxWidth;
+    for (int j = 0; j < nslices && ok; ++j) {
+      ok = mbar_wait(mb_w, pw);
+      if (!ok) break;
+      pw ^= 1;
+      w_pending = false;
+      if (tid == 0) {
+        fence_after();
+        gemm_kmajor(tmem + rows0 * j, saddr(s.act), saddr(s.wgt), K, slice_n(net, l, j));
+        mma_commit(mb_mma);
+      }
+      m_pending = true;
+      ok = mbar_wait(mb_mma, pm);
+      if (!ok) break;
+      pm ^= 1;
+      m_pending = false;
       fence_after();
-      gemm_kmajor(tmem, saddr(s.act), saddr(s.wgt), K, N);
-      mma_commit(mb_mma);
+      if (j + 1 < nslices) {
+        if (tid == 0) bulk_load(saddr(s.wgt), slice_src(net, l, j + 1), slice_bytes(net, l, j + 1), mb_w);
+        w_pending = true;
+      } else if (l + 1 < net.nl) {
+        if (tid == 0) bulk_load(saddr(s.wgt), slice_src(net, l + 1, 0), slice_bytes(net, l + 1, 0), mb_w);
+        w_pending = true;
+      }
     }
-    m_pending = true;
-    ok = mbar_wait(mb_mma, pm);
     if (!ok) break;
-    pm ^= 1;
-    m_pending = false;
-    fence_after();
-    if (l + 1 < net.nl) {
-      if (tid == 0)
-        bulk_load(saddr(s.wgt), net.W[l + 1], (uint32_t)(net.N[l + 1] * net.K[l + 1] * 2), mb_w);
-      w_pending = true;
-    }
     const bool last = l == net.nl - 1;
     if (!last) {
       for (int c0 = half * (N >> 1); c0 < (half + 1) * (N >> 1); c0 += 32) {
@@ -319,7 +418,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
         tmem_ld32(tmem + lane_base + c0, v);
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-          const float zz = v[j] + s.bias[c0 + j];
+          const float zz = v[j] + bias[c0 + j];
           if (TRAIN && row < nb) bufs.z[l][row * N + c0 + j] = zz;
           v[j] = silu(zz);
         }
@@ -335,14 +434,16 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
       float v[16];
       tmem_ld16(tmem + lane_base, v);
       if (row < nb) {
+        const double scale = STRESS ? s.hnorm[r] : 1.0;
         for (int j = 0; j < 16; ++j) {
-          const float yy = v[j] + s.bias[j];
+          const float yy = v[j] + bias[j];
           if (TRAIN) bufs.ynorm[row * 16 + j] = yy;
           if (!TRAIN && j < net.nout)
-            y[row * net.nout + j] = (double)yy * net.out_scale[j] + net.out_shift[j];
+            y[row * net.nout + j] = scale * ((double)yy * net.out_scale[j] + net.out_shift[j]);
         }
       }
     }
+    fence_smem_async();  // the next layer's A tile before its MMAs
     fence_before();
     __syncthreads();  // TMEM read and activations written before the next MMA
   }
@@ -362,7 +463,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
 __global__ void __launch_bounds__(kFwdThreads, 1)
     k_backward(Net net, int64_t nb, const double* __restrict__ target, Bufs bufs) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  Shared s = carve(smem);
+  Shared s = carve(smem, kWgtBytes);
   const int tid = threadIdx.x, warp = tid >> 5;
   const int r = tid & (kTile - 1), half = tid >> 7;  // row in the tile, column half
   const int64_t tile = blockIdx.x;
@@ -678,7 +779,7 @@ akb_status gradients(akb_mlp* m, int64_t nb, const double* x, const double* targ
   AKB_CUDA_TRY(cudaMemsetAsync(m->d_error, 0, sizeof(int), m->stream));
   k_forward<true><<<(unsigned)ntiles, kFwdThreads, kFwdSmem, m->stream>>>(n, nb, x, nullptr, m->bufs);
   AKB_CUDA_TRY(cudaGetLastError());
-  k_backward<<<(unsigned)ntiles, kFwdThreads, kFwdSmem, m->stream>>>(n, nb, target, m->bufs);
+  k_backward<<<(unsigned)ntiles, kFwdThreads, kBwdSmem, m->stream>>>(n, nb, target, m->bufs);
   AKB_CUDA_TRY(cudaGetLastError());
   const int tpc = (int)std::max<int64_t>(1, (ntiles + 147) / 148);
   const int nparts = (int)((ntiles + tpc - 1) / tpc);
@@ -781,7 +882,8 @@ akb_status akb_mlp_create(int32_t nb_inputs, int32_t nb_outputs, int32_t width,
   if ((st = repack(m.get())) != AKB_OK) return st;
   AKB_CUDA_TRY(set_smem((const void*)k_forward<true>, kFwdSmem));
   AKB_CUDA_TRY(set_smem((const void*)k_forward<false>, kFwdSmem));
-  AKB_CUDA_TRY(set_smem((const void*)k_backward, kFwdSmem));
+  AKB_CUDA_TRY(set_smem((const void*)k_forward<false, true>, kFwdSmem));
+  AKB_CUDA_TRY(set_smem((const void*)k_backward, kBwdSmem));
   AKB_CUDA_TRY(set_smem((const void*)k_wgrad, kWgradSmem));
   AKB_CUDA_TRY(cudaStreamSynchronize(m->stream));
   *out = m.release();
@@ -857,6 +959,33 @@ akb_status akb_mlp_forward(akb_mlp* m, int64_t nb, const double* x, double* y, v
   AKB_CUDA_TRY(cudaSetDevice(m->device));
   cudaStream_t s = stream ? (cudaStream_t)stream : m->stream;
   k_forward<false><<<(unsigned)ntiles, kFwdThreads, kFwdSmem, s>>>(m->net, nb, x, y, Bufs{});
+  AKB_CUDA_TRY(cudaGetLastError());
+  return AKB_OK;
+}
+
+akb_status akb_mlp_stress(akb_mlp* m, int64_t nb, const double* grad_u, double* stress,
+                          double amplitude, double min_det, int32_t* fallback_index,
+                          int32_t* fallback_count, void* stream) {
+  if (!m) return fail(AKB_ERR_INVALID_ARGUMENT, "null network");
+  if (m->net.nin != 10 || m->net.nout != 9)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "the stress map needs 10 inputs (H / |H|, log |H|) and 9 outputs");
+  if (nb < 0 || (nb > 0 && (!grad_u || !stress)))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "grad_u and stress are required");
+  if ((fallback_index == nullptr) != (fallback_count == nullptr))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "fallback_index and fallback_count go together");
+  const int64_t ntiles = (nb + kTile - 1) / kTile;
+  if (ntiles > INT32_MAX || nb > INT32_MAX) return fail(AKB_ERR_UNSUPPORTED, "too many samples");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : m->stream;
+  if (fallback_count) AKB_CUDA_TRY(cudaMemsetAsync(fallback_count, 0, sizeof(int32_t), s));
+  if (nb == 0) return AKB_OK;
+  StressArgs sa;
+  sa.amplitude = amplitude;
+  sa.min_det = min_det;
+  sa.index = fallback_index;
+  sa.count = fallback_count;
+  k_forward<false, true><<<(unsigned)ntiles, kFwdThreads, kFwdSmem, s>>>(m->net, nb, grad_u,
+                                                                         stress, Bufs{}, sa);
   AKB_CUDA_TRY(cudaGetLastError());
   return AKB_OK;
 }

@@ -21,6 +21,7 @@
 // F shows, so an attempt whose residual turns non-finite or explodes is
 // restarted from its initial state with a 0.6x time step (at most 3 times).
 // The homogenised stress is sum w_q P / L^3.
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <mutex>
@@ -278,14 +279,14 @@ __device__ inline double warp_sum(double x) {
   return x;
 }
 
+// One RVE instance, by the whole CTA: relaxation from the instance's
+// fluctuation (or zero), homogenised stress, state written back.
 template <typename S>
-__global__ void __launch_bounds__(kRveThreads, 1)
-    k_rve(RveArgs R, int64_t nb, const double* __restrict__ grad_u, S* fluct,
-          double* __restrict__ stress, int32_t* iterations, double* residual,
-          double* internal_force) {
+__device__ __forceinline__ void rve_instance(const RveArgs& R, int64_t inst,
+                                             const double* __restrict__ grad_u, S* fluct,
+                                             double* __restrict__ stress, int32_t* iterations,
+                                             double* residual, double* internal_force) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int64_t inst = blockIdx.x;
-  if (inst >= nb) return;
   const int nn = R.nn, tid = threadIdx.x, bs = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nwarps = bs >> 5;
   RveSmem<S> s = carve<S>(smem, nn);
@@ -432,6 +433,34 @@ __global__ void __launch_bounds__(kRveThreads, 1)
   }
 }
 
+template <typename S>
+__global__ void __launch_bounds__(kRveThreads, 1)
+    k_rve(RveArgs R, int64_t nb, const double* __restrict__ grad_u, S* fluct,
+          double* __restrict__ stress, int32_t* iterations, double* residual,
+          double* internal_force) {
+  const int64_t inst = blockIdx.x;
+  if (inst >= nb) return;
+  rve_instance<S>(R, inst, grad_u, fluct, stress, iterations, residual, internal_force);
+}
+
+// The instances index[0 .. min(*count, capacity)) of arrays over all points,
+// the count read on the device (written by an earlier kernel on the same
+// stream): CTAs stride over the list, so a short or empty list costs one
+// small launch and no host round trip.
+template <typename S>
+__global__ void __launch_bounds__(kRveThreads, 1)
+    k_rve_indexed(RveArgs R, int64_t capacity, const int32_t* __restrict__ index,
+                  const int32_t* __restrict__ count, const double* __restrict__ grad_u, S* fluct,
+                  double* __restrict__ stress, int32_t* iterations, double* residual) {
+  const int64_t n = min((int64_t)*count, capacity);
+  for (int64_t b = blockIdx.x; b < n; b += gridDim.x) {
+    const int64_t inst = index[b];
+    if (inst < 0 || inst >= capacity) continue;  // uniform over the CTA
+    rve_instance<S>(R, inst, grad_u, fluct, stress, iterations, residual, nullptr);
+    __syncthreads();  // shared state is reused by the next instance
+  }
+}
+
 std::mutex g_rve_attr_mutex;
 
 template <typename S>
@@ -441,7 +470,10 @@ cudaError_t raise_limit(size_t bytes) {
   cudaError_t e = cudaFuncGetAttributes(&attr, k_rve<S>);
   if (e != cudaSuccess) return e;
   if ((size_t)attr.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
-  return cudaFuncSetAttribute(k_rve<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  e = cudaFuncSetAttribute(k_rve<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_rve_indexed<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)bytes);
 }
 
 RveArgs args_of(const akb_rve* r, int max_it) {
@@ -603,6 +635,33 @@ akb_status akb_rve_solve(akb_rve* r, int64_t nb, const double* grad_u, void* flu
   if (!r) return fail(AKB_ERR_INVALID_ARGUMENT, "null RVE");
   return launch(r, r->max_it, nb, grad_u, fluctuation, stress, iterations, residual, nullptr,
                 stream);
+}
+
+akb_status akb_rve_solve_indexed(akb_rve* r, int64_t capacity, const int32_t* index,
+                                 const int32_t* count, const double* grad_u, void* fluctuation,
+                                 double* stress, int32_t* iterations, double* residual,
+                                 void* stream) {
+  if (!r) return fail(AKB_ERR_INVALID_ARGUMENT, "null RVE");
+  if (capacity < 0 || (capacity > 0 && (!index || !count || !grad_u || !stress)))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "index, count, grad_u and stress are required");
+  if (capacity > INT32_MAX) return fail(AKB_ERR_UNSUPPORTED, "more than 2^31 RVEs in one call");
+  if (capacity == 0) return AKB_OK;
+  AKB_CUDA_TRY(cudaSetDevice(r->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : r->stream;
+  int sms = 0;
+  AKB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, r->device));
+  const unsigned grid = (unsigned)std::min<int64_t>(capacity, std::max(sms, 1));
+  const RveArgs a = args_of(r, r->max_it);
+  if (r->mode == AKB_MODE_FP64)
+    k_rve_indexed<double><<<grid, kRveThreads, r->smem, s>>>(
+        a, capacity, index, count, grad_u, static_cast<double*>(fluctuation), stress, iterations,
+        residual);
+  else
+    k_rve_indexed<float><<<grid, kRveThreads, r->smem, s>>>(
+        a, capacity, index, count, grad_u, static_cast<float*>(fluctuation), stress, iterations,
+        residual);
+  AKB_CUDA_TRY(cudaGetLastError());
+  return AKB_OK;
 }
 
 akb_status akb_rve_stress(akb_rve* r, int64_t nb, const double* grad_u, const void* fluctuation,

@@ -145,7 +145,19 @@ class MaterialFE2:
         self.chunk = chunk
         self.warm_start = warm_start
         self.fluct = None
-        self.stats = dict(rve_solves=0, fallback=0, iterations=0)
+        self._stats = dict(rve_solves=0, fallback=0, iterations=0)
+        self._fb = None  # device buffers of the learned path: index, count, running total
+
+    @property
+    def stats(self):
+        """RVE solves, fallback points (learned path) and RVE updates (plain
+        path) so far; reading it waits for the queued steps."""
+        out = dict(self._stats)
+        if self._fb is not None:
+            n = int(self._fb[2].item())
+            out["fallback"] += n
+            out["rve_solves"] += n
+        return out
 
     def material(self, mats, fractions, rho=1100.0):
         from .model import MaterialUser
@@ -157,41 +169,58 @@ class MaterialFE2:
         d = voigt_material(mats, fractions, rho)
         return _M(rho=d["rho"], E=d["E"], nu=d["nu"], finite_deformation=True)
 
-    def _rve(self, H, idx=None):
-        import torch
-        n = H.shape[0]
+    def _ensure_fluct(self):
         if self.warm_start and (self.fluct is None or self.fluct.shape[0] != self.nq):
             self.fluct = self.rve.zero_fluctuation(self.nq)
+
+    def _rve(self, H):
+        """Plain FE^2: every point's RVE, in chunks; a point's warm start is
+        its row of self.fluct, solved in place."""
+        import torch
+        n = H.shape[0]
+        self._ensure_fluct()
         P = torch.empty((n, 3, 3), dtype=torch.float64, device=H.device)
         for k in range(0, n, self.chunk):
             sl = slice(k, min(n, k + self.chunk))
-            w = None
-            if self.warm_start:
-                rows = torch.arange(sl.start, sl.stop, device=H.device) if idx is None else idx[sl]
-                w = self.fluct[rows].contiguous()
-            out = self.rve.solve(H[sl], w)
-            if self.warm_start:
-                self.fluct[rows] = w
+            out = self.rve.solve(H[sl], self.fluct[sl] if self.warm_start else None)
             P[sl] = out["stress"]
-            self.stats["iterations"] += int(out["iterations"].sum())
-        self.stats["rve_solves"] += n
+            self._stats["iterations"] += int(out["iterations"].sum())
+        self._stats["rve_solves"] += n
         return P
 
     def compute(self, grad_u, stress):
+        """The stresses of every Gauss point. With a surrogate: one kernel
+        forms the features, runs the network, writes |H| net(.) and lists the
+        points outside the envelope; one kernel relaxes the RVEs of the
+        listed points (it reads the list's length on the device, so the step
+        never waits for the host)."""
         import torch
         self.nq = grad_u.shape[0]
         if self.surrogate is None:
             stress.copy_(self._rve(grad_u))
             return
-        P = self.surrogate(grad_u)
-        hmax = grad_u.abs().flatten(1).max(dim=1).values
-        det = torch.linalg.det(torch.eye(3, dtype=grad_u.dtype, device=grad_u.device) + grad_u)
-        out = (hmax > self.amplitude) | (det < self.min_det)
-        idx = torch.nonzero(out).flatten()
-        if idx.numel():
-            P[idx] = self._rve(grad_u[idx].contiguous(), idx)
-            self.stats["fallback"] += int(idx.numel())
-        stress.copy_(P)
+        # [k, i, j] views of column-major storage: transposed back, they are
+        # the (nq, 9) column-major arrays the kernels take
+        H = grad_u.transpose(1, 2).reshape(-1, 9)
+        P = stress.transpose(1, 2).reshape(-1, 9)
+        direct = H.is_contiguous() and P.is_contiguous() and \
+            P.data_ptr() == stress.data_ptr() and H.dtype == P.dtype == torch.float64
+        if not direct:
+            H = H.to(torch.float64).contiguous()
+            P = torch.empty_like(H)
+        if self._fb is None or self._fb[0].shape[0] != self.nq:
+            dev = grad_u.device
+            self._fb = (torch.empty(self.nq, dtype=torch.int32, device=dev),
+                        torch.zeros(1, dtype=torch.int32, device=dev),
+                        torch.zeros(1, dtype=torch.int64, device=dev))
+        idx, cnt, total = self._fb
+        self.surrogate.stress_into(H, P, envelope=(self.amplitude, self.min_det),
+                                   fallback=(idx, cnt))
+        self._ensure_fluct()
+        self.rve.solve_indexed(idx, cnt, H, P, self.fluct if self.warm_start else None)
+        total += cnt
+        if not direct:
+            stress.copy_(P.reshape(-1, 3, 3).transpose(1, 2))
 
 
 def macro_block(material, cells=32, length=1.0, precision=None):

@@ -103,6 +103,28 @@ class SolidMechanicsModelRVE:
         return dict(stress=P.transpose(1, 2), iterations=it, residual=res,
                     fluctuation=fluctuation)
 
+    def solve_indexed(self, index, count, grad_u, stress, fluctuation=None):
+        """Relaxes the RVEs of the points index[:count] (device int32
+        tensors; count is read on the device) of (capacity, 9) column-major
+        FP64 gradient and stress tensors, writing those points' stresses
+        (and fluctuations, warm-started from fluctuation if given)."""
+        torch = _torch()
+        cap = grad_u.shape[0]
+        for t in (grad_u, stress):
+            if t.dtype != torch.float64 or not t.is_contiguous() or tuple(t.shape) != (cap, 9):
+                raise ValueError("grad_u and stress must be contiguous (capacity, 9) float64")
+        if fluctuation is not None and (fluctuation.dtype != self.fluctuation_dtype
+                                        or not fluctuation.is_contiguous()
+                                        or tuple(fluctuation.shape) != (cap, self.nb_nodes, 3)):
+            raise ValueError("fluctuation must be a contiguous (capacity, n^3, 3) %s tensor"
+                             % self.fluctuation_dtype)
+        check(lib().akb_rve_solve_indexed(self._h, cap, index.data_ptr(), count.data_ptr(),
+                                          grad_u.data_ptr(),
+                                          fluctuation.data_ptr() if fluctuation is not None else None,
+                                          stress.data_ptr(), None, None,
+                                          torch_stream(grad_u.device)))
+        return stress
+
     def stress(self, grad_u, fluctuation):
         """Homogenised stress and internal force (nb, n^3, 3) of given states."""
         torch = _torch()

@@ -182,6 +182,26 @@ class MLPSurrogate:
         r = torch.linalg.norm(h, dim=1, keepdim=True)
         return r * self.forward_features(x, stream)
 
+    def stress_into(self, grad_u, stress, envelope=None, fallback=None, stream=None):
+        """MaterialFE2's stress map in one launch (akb_mlp_stress): grad_u and
+        stress are contiguous (nb, 9) FP64 device tensors, column-major per
+        point; stress <- |H| net(H / r, log r). With envelope = (amplitude,
+        min_det) and fallback = (index (nb,) int32, count (1,) int32) device
+        tensors, the points outside the envelope are listed in index[:count]
+        (no host round trip)."""
+        torch = _torch()
+        for t in (grad_u, stress):
+            if t.dtype != torch.float64 or not t.is_contiguous() or t.shape[-1] != 9:
+                raise ValueError("grad_u and stress must be contiguous (nb, 9) float64 tensors")
+        amp, det = envelope if envelope is not None else (0.0, 0.0)
+        idx, cnt = fallback if fallback is not None else (None, None)
+        s = stream if stream is not None else torch_stream(grad_u.device)
+        check(lib().akb_mlp_stress(self._h, grad_u.shape[0], grad_u.data_ptr(), stress.data_ptr(),
+                                   float(amp), float(det),
+                                   idx.data_ptr() if idx is not None else None,
+                                   cnt.data_ptr() if cnt is not None else None, s))
+        return stress
+
     def __call__(self, grad_u, stream=None):
         torch = _torch()
         y = self.predict_flat(_flat(torch.as_tensor(grad_u), torch), stream)

@@ -529,7 +529,9 @@ def run_hex8(args, device, peak):
                        "mu = 0.4 MPa, rho = 1100, face x = 0 fixed, v ~ N(0, 0.05)" % args.hex_cells,
            "elements": E, "steps": steps}
     states = {}
-    for name, mode in (("fp32_bulk", _abi.MODE_FP32_BULK), ("fp64", _abi.MODE_FP64)):
+    modes = [(n, md) for n, md in (("fp32_bulk", _abi.MODE_FP32_BULK), ("fp64", _abi.MODE_FP64))
+             if n in args.hex_modes.split(",")]
+    for name, mode in modes:
         m = make_model(w, mode, device)
         dt = configs.setup_model(Facade(m), w)
         m.solveSteps(3)
@@ -541,9 +543,11 @@ def run_hex8(args, device, peak):
                      "hbm_roofline_frac": fb / (ms / steps / 1e3) / 1e9 / peak,
                      "kernels_ms": dict(kernel_times(m, 10))}
         m.close()
-    (u32, f32), (u64, f64) = states["fp32_bulk"], states["fp64"]
-    out["fp32_vs_fp64"] = {"rel_err_displacement": float(np.abs(u32 - u64).max() / np.abs(u64).max()),
-                           "rel_err_internal_force": float(np.abs(f32 - f64).max() / np.abs(f64).max())}
+    if len(states) == 2:
+        (u32, f32), (u64, f64) = states["fp32_bulk"], states["fp64"]
+        out["fp32_vs_fp64"] = {
+            "rel_err_displacement": float(np.abs(u32 - u64).max() / np.abs(u64).max()),
+            "rel_err_internal_force": float(np.abs(f32 - f64).max() / np.abs(f64).max())}
     out["time_step"] = dt
     # compute roofline of the FP64 launch, from an ncu capture of this
     # workload (sm__inst_executed_pipe_fp64, % of peak; not taken in this run)
@@ -551,6 +555,14 @@ def run_hex8(args, device, peak):
                                "kernel": "k_patch_step<hex8, double>",
                                "source": "ncu capture of the 128^3 block, FP64"}
     return out
+
+
+def batch_alg_bytes(meshes):
+    """b_alg_bytes over the instances of a batch (their union)."""
+    E = sum(m.getNbElement() for m in meshes)
+    N = sum(m.getNbNodes() for m in meshes)
+    n, d = meshes[0].connectivity.shape[1], meshes[0].spatial_dimension
+    return E * n * 4 + N * d * 8 + N * d * 8 * 6 + N * 8 + N * 1
 
 
 def run_batch(args, device, log=None):
@@ -580,11 +592,18 @@ def run_batch(args, device, log=None):
     b.solveSteps(3)
     configs.setup_batch(b, w)
     ms = b.timeSolveSteps(steps)
+    balg = batch_alg_bytes(w["meshes"])
+    peak, peak_kind = load_peaks()
+    achieved = balg / (ms / steps / 1e3) / 1e9
     out = {"workload": "%d triangle_3 plates, %d elements, %d nodes, per-plate E, nu, rho, dt"
                        % (len(w["meshes"]), E, int(b.node_offsets[-1])),
            "elements": E, "steps": steps,
            "batched": {"value": E * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
                        "launches_per_step": len(kernel_times(b, 5)), "tuned": best,
+                       "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                                    "unit": "GB/s", "frac": achieved / peak,
+                                    "peak_source": peak_kind,
+                                    "algorithmic_bytes_per_step": balg},
                        "trials_ms_per_step": [[t[0], t[1]] for t in trials]}}
     b.close()
     # the same sample as separate models (one model per plate, graph replays)
@@ -620,6 +639,61 @@ def run_batch(args, device, log=None):
         m.close()
     bs.close()
     return out
+
+
+def mlp_inference(net, nq, reps=20):
+    """Surrogate inference on nq Gauss points (seeded gradients of the FE^2
+    envelope): the network kernel on ready features, the torch feature path
+    around it, and the macro step's fused form (features, network, |H|
+    rescale and envelope list in one launch, akb_mlp_stress); CUDA events,
+    best of three runs of `reps` calls."""
+    import torch
+    from akantu_b200 import fe2
+    from akantu_b200.surrogate import scaled_features
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        a, b = ev(), ev()
+        torch.cuda.synchronize()
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+    Hq = torch.as_tensor(fe2.sample_gradients(nq, seed=9), device="cuda")
+    Xq = Hq.transpose(1, 2).reshape(-1, 9).contiguous()
+    xq, _ = scaled_features(Xq)
+    Pq = torch.empty_like(Xq)
+    fb = (torch.empty(nq, dtype=torch.int32, device="cuda"),
+          torch.zeros(1, dtype=torch.int32, device="cuda"))
+    for _ in range(5):  # warm every path (allocator, clocks)
+        net.forward_features(xq)
+        net.predict_flat(Xq)
+        net.stress_into(Xq, Pq, envelope=(0.3, 0.5), fallback=fb)
+    ms_k = min(timed(lambda: [net.forward_features(xq) for _ in range(reps)]) for _ in range(3))
+    ms_e = min(timed(lambda: [net.predict_flat(Xq) for _ in range(reps)]) for _ in range(3))
+    ms_f = min(timed(lambda: [net.stress_into(Xq, Pq, envelope=(0.3, 0.5), fallback=fb)
+                              for _ in range(reps)]) for _ in range(3))
+    flop = 2 * sum(max(k, 16) * max(n, 16) for k, n in net.layer_shapes())
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak = float(json.load(fh)["bf16_tflops"])
+    except Exception:
+        peak = 1590.0
+    tf = flop * nq / (ms_k / reps * 1e-3) / 1e12
+    return {"samples": nq, "kernel_ms": ms_k / reps, "with_features_ms": ms_e / reps,
+            "fused_stress_ms": ms_f / reps, "tflops": tf, "flop_per_sample": flop,
+            "tensor_roofline_frac": tf / peak, "peak_tflops": peak}
+
+
+def run_mlp(args, device):
+    """The surrogate's inference alone (akantu_b200/data/rve_surrogate.npz) on one macro
+    step's 262 144 Gauss points."""
+    from akantu_b200.surrogate import MLPSurrogate
+    net = MLPSurrogate.load(os.path.join(ROOT, "akantu_b200", "data", "rve_surrogate.npz"),
+                            device=device)
+    return mlp_inference(net, 8 * args.fe2_cells ** 3)
 
 
 def run_fe2(args, device, log=None):
@@ -664,21 +738,7 @@ def run_fe2(args, device, log=None):
                         "heldout_error_small_strain": fe2.surrogate_error(net, Xs[ok], Ys[ok])}
     # inference throughput over one macro step's Gauss points
     nq = 8 * args.fe2_cells ** 3
-    Hq = torch.as_tensor(fe2.sample_gradients(nq, seed=9), device="cuda")
-    Xq = Hq.transpose(1, 2).reshape(-1, 9).contiguous()
-    from akantu_b200.surrogate import scaled_features
-    xq, _ = scaled_features(Xq)
-    reps = 20
-    for _ in range(5):  # warm both paths (allocator, clocks)
-        net.forward_features(xq)
-        net.predict_flat(Xq)
-    ms_k = min(timed(lambda: [net.forward_features(xq) for _ in range(reps)])[0]
-               for _ in range(3))
-    ms_e = min(timed(lambda: [net.predict_flat(Xq) for _ in range(reps)])[0] for _ in range(3))
-    flop = 2 * sum(max(k, 16) * max(n, 16) for k, n in net.layer_shapes())
-    out["surrogate"]["inference"] = {
-        "samples": nq, "kernel_ms": ms_k / reps, "with_features_ms": ms_e / reps,
-        "tflops": flop * nq / (ms_k / reps * 1e-3) / 1e12, "flop_per_sample": flop}
+    out["surrogate"]["inference"] = mlp_inference(net, nq)
 
     # learned FE^2: the whole ramp on the full block
     learned = fe2.MaterialFE2(rve, surrogate=net)
@@ -815,6 +875,8 @@ def main():
                     help="skip the hexahedron and batch workloads")
     ap.add_argument("--hex-cells", type=int, default=128)
     ap.add_argument("--hex-steps", type=int, default=0, help="0 = the workload's 2000 steps")
+    ap.add_argument("--hex-modes", default="fp32_bulk,fp64",
+                    help="precisions of the hexahedron workload (profiling one alone)")
     ap.add_argument("--batch-instances", type=int, default=4096)
     ap.add_argument("--batch-steps", type=int, default=0, help="0 = the workload's 500 steps")
     ap.add_argument("--fe2-cells", type=int, default=32)
@@ -828,7 +890,8 @@ def main():
     ap.add_argument("--replicas", action="store_true",
                     help="with several ranks, one independent headline cube per rank instead")
     ap.add_argument("--parts-per-rank", type=int, default=1)
-    ap.add_argument("--workload", default="", choices=["", "plate_tri3", "block_hex8", "plates_batch"],
+    ap.add_argument("--workload", default="",
+                    choices=["", "plate_tri3", "block_hex8", "plates_batch", "fe2", "mlp"],
                     help="run only this secondary workload (1 GPU) and print its result")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -851,13 +914,19 @@ def main():
         torch.cuda.set_device(0)
         peak, _ = load_peaks()
         fn = {"plate_tri3": lambda: run_plate(args, 0), "block_hex8": lambda: run_hex8(args, 0, peak),
-              "plates_batch": lambda: run_batch(args, 0)}[args.workload]
+              "plates_batch": lambda: run_batch(args, 0),
+              "fe2": lambda: run_fe2(args, 0, log=lambda s: print(s, file=sys.stderr, flush=True)),
+              "mlp": lambda: run_mlp(args, 0)}[args.workload]
         print(json.dumps({"workloads": {args.workload: fn()}}), flush=True)
         return
     dist = Dist(args.gpus)
     if args.decompose or (dist.world > 1 and not args.replicas):
         try:
             res = run_decomposed(args, dist)
+            if dist.world > 1 and not args.only_headline:
+                sharded = run_batch_sharded(args, dist)  # every rank takes part
+                if dist.rank == 0:
+                    res["workloads"] = {"plates_batch_sharded": sharded}
             if dist.rank == 0:
                 print(json.dumps(res), flush=True)
         finally:

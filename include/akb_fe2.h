@@ -96,6 +96,18 @@ akb_status akb_rve_get_info(const akb_rve* rve, akb_rve_info* info);
 akb_status akb_rve_solve(akb_rve* rve, int64_t nb, const double* grad_u, void* fluctuation,
                          double* stress, int32_t* iterations, double* residual, void* stream);
 
+/* akb_rve_solve for the points index[0 .. min(*count, capacity)) of arrays
+ * over capacity points (grad_u [capacity][9], fluctuation
+ * [capacity][n^3][3] or NULL, stress [capacity][9], iterations / residual
+ * [capacity] or NULL; entries of other points are left alone). index and
+ * count are device arrays read by the kernel (e.g. written by
+ * akb_mlp_stress earlier on the same stream): no host round trip, and an
+ * empty list costs one short launch. */
+akb_status akb_rve_solve_indexed(akb_rve* rve, int64_t capacity, const int32_t* index,
+                                 const int32_t* count, const double* grad_u, void* fluctuation,
+                                 double* stress, int32_t* iterations, double* residual,
+                                 void* stream);
+
 /* Homogenised stress and internal force of given states, no relaxation
  * (internal_force [nb][n^3][3] double, may be NULL). */
 akb_status akb_rve_stress(akb_rve* rve, int64_t nb, const double* grad_u,
@@ -126,6 +138,19 @@ akb_status akb_mlp_set_scaling(akb_mlp* mlp, const float* in_shift, const float*
 /* y[nb][nb_outputs] = network(x[nb][nb_inputs]), device FP64 arrays, queued
  * on stream (NULL = the network's stream). */
 akb_status akb_mlp_forward(akb_mlp* mlp, int64_t nb, const double* x, double* y, void* stream);
+/* The surrogate as MaterialFE2's stress map, in one launch: for nb Gauss
+ * points, grad_u [nb][9] (column-major H = du/dX per point, as
+ * AKB_FIELD_GRAD_U) -> stress [nb][9] (column-major first Piola-Kirchhoff
+ * P = |H| y, y the network's output for the inputs (H / r, log r),
+ * r = max(|H|, 1e-8), |H| the Frobenius norm). Needs 10 inputs and 9
+ * outputs. With fallback_index / fallback_count (device int32, nb entries /
+ * one), the points outside the training envelope (max |H_ij| > amplitude or
+ * det(I + H) < min_det) are listed in fallback_index[0 .. *fallback_count)
+ * (in no particular order; the count is zeroed first), ready for
+ * akb_rve_solve_indexed; both NULL skips the test. Queued on stream. */
+akb_status akb_mlp_stress(akb_mlp* mlp, int64_t nb, const double* grad_u, double* stress,
+                          double amplitude, double min_det, int32_t* fallback_index,
+                          int32_t* fallback_count, void* stream);
 /* Mean squared error of the normalised outputs against target (device FP64
  * [nb][nb_outputs]) and its gradient (host, parameter layout; may be NULL). */
 akb_status akb_mlp_gradients(akb_mlp* mlp, int64_t nb, const double* x, const double* target,
