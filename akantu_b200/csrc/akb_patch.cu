@@ -144,6 +144,10 @@ __device__ inline int cidx(int k, int i, int CH) {
 template <int T, typename S> struct PatchOccupancy { static constexpr int value = 3; };
 template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, float> { static constexpr int value = 2; };
 template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, double> { static constexpr int value = 1; };
+// 2D and 1D patches of <= 1024 elements take <= 56 KB of shared memory:
+// four CTAs per SM when the registers allow it (<= 64 per thread)
+template <typename S> struct PatchOccupancy<AKB_TRIANGLE_3, S> { static constexpr int value = 4; };
+template <typename S> struct PatchOccupancy<AKB_SEGMENT_2, S> { static constexpr int value = 4; };
 
 // DOFs handled per thread per round of the finishing loop: their global
 // loads are issued together.

@@ -350,9 +350,9 @@ def run_ours(args, dist):
                          "algorithmic_bytes_per_step": balg,
                          # DRAM bytes of one k_patch_step launch from an ncu capture
                          # (dram__bytes_read.sum + dram__bytes_write.sum) of the
-                         # 90^3-cell cube (4.374 M elements, 296.6 MB), scaled by
+                         # 90^3-cell cube (4.374 M elements, 232.0 MB), scaled by
                          # elements; the capture is not taken inside this run
-                         "traffic": 296.6e6 * E / 4.374e6,
+                         "traffic": 232.0e6 * E / 4.374e6,
                          "traffic_kernel": "k_patch_step (ncu, 90^3 cells, scaled by elements)",
                          "kernels_ms": {n: t for n, t in ktimes},
                          "dominant": top[0]},
@@ -551,9 +551,11 @@ def run_hex8(args, device, peak):
     out["time_step"] = dt
     # compute roofline of the FP64 launch, from an ncu capture of this
     # workload (sm__inst_executed_pipe_fp64, % of peak; not taken in this run)
-    out["compute_roofline"] = {"bound": "fp64 pipe", "fp64_pipe_active": 0.416,
-                               "kernel": "k_patch_step<hex8, double>",
-                               "source": "ncu capture of the 128^3 block, FP64"}
+    out["compute_roofline"] = {"bound": "fp64 pipe (FP64) / fma pipe (FP32-bulk)",
+                               "fp64_pipe_active": 0.471, "fp32_bulk_fma_pipe_active": 0.432,
+                               "kernel": "k_patch_step<hex8, double> / <hex8, float>",
+                               "source": "ncu captures of the 96^3 block "
+                                         "(profiles/k_patch_step_block_hex8_96.md)"}
     return out
 
 
