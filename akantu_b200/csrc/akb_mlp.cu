@@ -288,6 +288,56 @@ __device__ inline double det_i_plus(const double* H) {  // det(I + H), H column-
 // TRAIN stores the packed BF16 input and hidden activations (act[l], tile
 // major), the pre-activations Z (z[l], [nb_pad][N] FP32) and the normalised
 // outputs (ynorm, [nb_pad][16] FP32); otherwise y: [nb][nout] FP64 outputs.
+// The normalised inputs of row r of a tile (columns 8 half .. 8 half + 7 of
+// 16) into the packed A tile `act`: x's columns, or in stress mode the
+// features (H / r, log r) of the row's displacement gradient, whose |H| goes
+// to hnorm[r] and whose envelope test (by the half-0 threads, whole warps)
+// appends the row to the fallback list.
+template <bool STRESS>
+__device__ inline void stage_inputs(const Net& net, int64_t nb, const double* __restrict__ x,
+                                    unsigned char* act, double* hnorm, int r, int half,
+                                    int64_t row, int tid, const StressArgs& sa, float* v) {
+  if (STRESS) {
+    double H[9], n2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      H[k] = row < nb ? x[row * 9 + k] : 0.0;
+      n2 += H[k] * H[k];
+    }
+    const double hn = sqrt(n2), rr = fmax(hn, kHMin);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {  // column j = 8 half + q: H_j / r (j < 9), log r (j = 9)
+      const int j = 8 * half + q;
+      const double f = half == 0 ? H[q] / rr : (q == 0 ? H[8] / rr : (q == 1 ? log(rr) : 0.0));
+      v[q] = (j < net.nin && row < nb) ? (float)((f - net.in_shift[j]) * net.in_scale[j]) : 0.0f;
+    }
+    store8(act, r, 8 * half, 16, v);
+    if (half == 0) {  // whole warps: one row per lane
+      hnorm[r] = hn;
+      if (sa.count) {
+        double hmax = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) hmax = fmax(hmax, fabs(H[k]));
+        const bool out = row < nb && (hmax > sa.amplitude || det_i_plus(H) < sa.min_det);
+        const unsigned mask = __ballot_sync(0xffffffffu, out);
+        int base = 0;
+        if ((tid & 31) == 0 && mask) base = atomicAdd(sa.count, __popc(mask));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (out) sa.index[base + __popc(mask & ((1u << (tid & 31)) - 1u))] = (int32_t)row;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int j = 8 * half + q;
+      float t = 0.0f;
+      if (j < net.nin && row < nb) t = (float)((x[row * net.nin + j] - net.in_shift[j]) * net.in_scale[j]);
+      v[q] = t;
+    }
+    store8(act, r, 8 * half, 16, v);
+  }
+}
+
 // Output rows per weight slice of layer l: as many as the buffer holds (a
 // multiple of 16: whole row groups, a valid MMA N), at most the layer's N.
 __device__ inline int slice_rows(const Net& net, int l) {
@@ -327,46 +377,9 @@ __global__ void __launch_bounds__(kFwdThreads, 2)
   for (int l = 0; l < net.nl; ++l)
     for (int c = tid; c < net.N[l]; c += kFwdThreads) s.bias[l * kMaxWidth + c] = net.b[l][c];
   // inputs, normalised, padded to 16 columns (8 per thread)
-  if (STRESS) {
-    double H[9], n2 = 0.0;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      H[k] = row < nb ? x[row * 9 + k] : 0.0;
-      n2 += H[k] * H[k];
-    }
-    const double hn = sqrt(n2), rr = fmax(hn, kHMin);
+  {
     float v[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {  // column j = 8 half + q: H_j / r (j < 9), log r (j = 9)
-      const int j = 8 * half + q;
-      const double f = half == 0 ? H[q] / rr : (q == 0 ? H[8] / rr : (q == 1 ? log(rr) : 0.0));
-      v[q] = (j < net.nin && row < nb) ? (float)((f - net.in_shift[j]) * net.in_scale[j]) : 0.0f;
-    }
-    store8(s.act, r, 8 * half, 16, v);
-    if (half == 0) {  // warps 0-3: one row each lane
-      s.hnorm[r] = hn;
-      if (sa.count) {
-        double hmax = 0.0;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) hmax = fmax(hmax, fabs(H[k]));
-        const bool out = row < nb && (hmax > sa.amplitude || det_i_plus(H) < sa.min_det);
-        const unsigned mask = __ballot_sync(0xffffffffu, out);
-        int base = 0;
-        if ((tid & 31) == 0 && mask) base = atomicAdd(sa.count, __popc(mask));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (out) sa.index[base + __popc(mask & ((1u << (tid & 31)) - 1u))] = (int32_t)row;
-      }
-    }
-  } else {
-    float v[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int j = 8 * half + q;
-      float t = 0.0f;
-      if (j < net.nin && row < nb) t = (float)((x[row * net.nin + j] - net.in_shift[j]) * net.in_scale[j]);
-      v[q] = t;
-    }
-    store8(s.act, r, 8 * half, 16, v);
+    stage_inputs<STRESS>(net, nb, x, s.act, s.hnorm, r, half, row, tid, sa, v);
     if (TRAIN) store8(bufs.act[0] + tile * (size_t)kTile * 16 * 2, r, 8 * half, 16, v);
   }
   fence_smem_async();  // the A tile, written by this thread, before the MMAs read it
