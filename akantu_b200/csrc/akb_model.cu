@@ -102,7 +102,7 @@ struct akb_model {
   bool part_in_step = false;
   int64_t n_iface = 0;
   const uint32_t* d_iface_g = nullptr;     // internal id of each interface node
-  const uint32_t* d_iface_part = nullptr;  // its first partial slot
+  const uint32_t* d_iface_part = nullptr;  // its shared node index (partial_slot)
   const uint32_t* d_iface_k = nullptr;     // its partial count
   akb::ExchangePlan xplan;                 // neighbour exchange (akb_part_set_exchange)
   bool has_xplan = false;
@@ -300,7 +300,7 @@ akb_status plan_patches(akb_model* m, const akb_mesh_desc* mesh, const BatchLayo
       for (auto& c : lconn) c -= (uint32_t)n0;
       PatchHost Q = build_patches(mesh->nodes + n0 * dd, lconn.data(), nni, nei, dd, nn_, target,
                                   max_nodes, cbytes);
-      const int64_t ebase = (int64_t)P.sgid.size(), sbase = P.nslots;
+      const int64_t ebase = (int64_t)P.sgid.size();
       const int64_t chbase = (int64_t)P.chunks.size();
       const uint32_t dbase16 = (uint32_t)(P.cdata.size() / 8);
       for (int p = 0; p < Q.npatch; ++p) {
@@ -321,21 +321,20 @@ akb_status plan_patches(akb_model* m, const akb_mesh_desc* mesh, const BatchLayo
       for (auto g : Q.perm) P.perm.push_back((uint32_t)(g + n0));
       for (auto e : Q.elem_order) P.elem_order.push_back((uint32_t)(e + e0));
       for (auto g : Q.sgid) P.sgid.push_back((uint32_t)(g + n0));
-      for (auto v : Q.sslot) P.sslot.push_back((uint32_t)(v + sbase));
+      P.srank.insert(P.srank.end(), Q.srank.begin(), Q.srank.end());
       for (auto c : Q.chunks) {
         c.off16 += dbase16;
         P.chunks.push_back(c);
       }
       P.cdata.insert(P.cdata.end(), Q.cdata.begin(), Q.cdata.end());
       for (auto g : Q.shared_nodes) P.shared_nodes.push_back((uint32_t)(g + n0));
-      for (auto v : Q.shared_part) P.shared_part.push_back((uint32_t)(v + sbase));
       P.shared_k.insert(P.shared_k.end(), Q.shared_k.begin(), Q.shared_k.end());
       for (auto g : Q.orphans) {
         P.orphans.push_back((uint32_t)(g + n0));
         orphan_inst.push_back((uint32_t)i);
       }
-      P.nslots += Q.nslots;
     }
+    assign_partial_slots(P, batch->node_off[batch->ninst]);  // dense rows over all instances
     P.chunk_base.push_back((int32_t)P.chunks.size());
     P.node_stride = (P.max_nodes + kBankPairs - 1) / kBankPairs * kBankPairs + 5;
   } catch (const std::exception& ex) {
@@ -377,19 +376,27 @@ akb_status build_device_patches(akb_model* m, const PatchHost& P,
     std::memcpy(cd.data(), P.chunks.data(), cd.size() * sizeof(uint2));
     if ((st = upload(m, cd, &d.chunks)) != AKB_OK) return st;
   }
-  // nodes finished by k_finish_list: the nodes of no element, then the
-  // shared nodes (in internal order: their partial slots are consecutive)
-  std::vector<uint32_t> lg(P.orphans), lp(P.orphans.size(), 0), lk(P.orphans.size(), 0);
-  std::vector<uint32_t> li(orphan_inst);
-  lg.insert(lg.end(), P.shared_nodes.begin(), P.shared_nodes.end());
-  lp.insert(lp.end(), P.shared_part.begin(), P.shared_part.end());
-  lk.insert(lk.end(), P.shared_k.begin(), P.shared_k.end());
+  // nodes finished by k_finish_list: the shared nodes (entry s: shared node
+  // s, whose ranks 0 and 1 sit in the dense partial rows), then the nodes of
+  // no element
+  std::vector<uint32_t> lg(P.shared_nodes), lp(P.shared_part), lk(P.shared_k);
+  lg.insert(lg.end(), P.orphans.begin(), P.orphans.end());
+  lp.insert(lp.end(), P.orphans.size(), 0);
+  lk.insert(lk.end(), P.orphans.size(), 0);
+  std::vector<uint32_t> li;
   if (batch) {  // instance of each shared node: instances own contiguous node ranges
     for (uint32_t g : P.shared_nodes) {
       const auto it = std::upper_bound(batch->node_off.begin(), batch->node_off.end(), (int64_t)g);
       li.push_back((uint32_t)(it - batch->node_off.begin() - 1));
     }
+    li.insert(li.end(), orphan_inst.begin(), orphan_inst.end());
   }
+  d.nshared = (uint32_t)P.shared_nodes.size();
+  d.shared_base = P.shared_base;
+  // a single mesh numbers its shared nodes as one block (a batch per instance)
+  d.shared_contig = batch ? 0 : 1;
+  for (size_t s = 0; s < P.shared_nodes.size() && d.shared_contig; ++s)
+    if (P.shared_nodes[s] != P.shared_base + s) d.shared_contig = 0;
   if (part) {
     std::vector<uint32_t> ig(part->n), ip(part->n), ik(part->n);
     for (int64_t i = 0; i < part->n; ++i) {
@@ -398,7 +405,7 @@ akb_status build_device_patches(akb_model* m, const PatchHost& P,
       if (s < 0 || s >= (int64_t)P.shared_nodes.size() || P.shared_nodes[s] != g)
         return fail(AKB_ERR_INVALID_ARGUMENT, "interface node is not a node of an element");
       ig[i] = g;
-      ip[i] = P.shared_part[s];
+      ip[i] = (uint32_t)s;  // its shared node index (partial_slot)
       ik[i] = P.shared_k[s];
     }
     if ((st = upload(m, ig, &m->d_iface_g)) != AKB_OK) return st;

@@ -604,17 +604,28 @@ __device__ inline double finish_list_dof(const DevModel& m, const DevPatches& P,
                                          int64_t t) {
   const int64_t e = t / d;
   const int i = (int)(t - e * d);
-  const int64_t g = P.list_gid[e];
+  const bool sh = e < (int64_t)P.nshared;
+  // a single mesh's shared nodes are one block: no index to load
+  const int64_t g = sh && P.shared_contig ? (int64_t)P.shared_base + e : (int64_t)P.list_gid[e];
   const int64_t q = g * d + i;
-  const uint32_t part = P.list_part[e], k = P.list_k[e];
+  const uint32_t k = P.list_k[e];
   const double dt = P.inst_dt ? P.inst_dt[P.list_inst[e]] : dt0;
   // every load that depends on the entry is issued before the blocked flag
-  // is tested
+  // is tested; ranks 0 and 1 are in the dense rows at known addresses
   const uint8_t bl = m.blocked[q];
   const double im = m.inv_mass[g], w = P.w[q], fx = FEXT ? m.fext[q] : 0.0;
   double v = m.v[q], a = m.a[q];
   double f = 0.0;
-  for (uint32_t r = 0; r < k; ++r) f += P.partial[(size_t)(part + r) * d + i];
+  if (sh) {
+    const double p0 = P.partial[(size_t)e * d + i];
+    const double p1 = P.partial[((size_t)P.nshared + e) * d + i];  // zero when k = 1
+    f += p0;
+    if (k > 1) f += p1;
+    if (k > 2) {
+      const uint32_t over = P.list_part[e];
+      for (uint32_t r = 2; r < k; ++r) f += P.partial[(size_t)(over + r - 2) * d + i];
+    }
+  }
   if (bl) return ke_term(v, im);
   double u, wn;
   finish_dof(dt, FEXT ? f + fx : f, im, w, v, a, u, wn);
@@ -668,60 +679,65 @@ __global__ void k_refresh_w(DevModel m, DevPatches P, double dt0) {
 // Interface nodes of a partitioned mesh, one thread per (node, component):
 // the sum of the node's partials in order (export), or the total over all
 // parts written as its only partial (import).
-__global__ void k_iface_export(DevPatches P, const uint32_t* parts, const uint32_t* ks, int64_t n,
+// Component i of the partial of rank r of shared node s.
+__device__ inline double& partial_of(const DevPatches& P, uint32_t s, uint32_t r, int d, int i) {
+  return P.partial[(size_t)partial_slot(P.nshared, s, P.list_part[s], r) * d + i];
+}
+
+__global__ void k_iface_export(DevPatches P, const uint32_t* shared, const uint32_t* ks, int64_t n,
                                int d, double* out) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= n * d) return;
   const int64_t e = t / d;
   const int i = (int)(t % d);
-  const uint32_t part = parts[e], k = ks[e];
+  const uint32_t s = shared[e], k = ks[e];
   double f = 0.0;
-  for (uint32_t r = 0; r < k; ++r) f += P.partial[(size_t)(part + r) * d + i];
+  for (uint32_t r = 0; r < k; ++r) f += partial_of(P, s, r, d, i);
   out[t] = f;
 }
 
-__global__ void k_iface_import(DevPatches P, const uint32_t* parts, const uint32_t* ks, int64_t n,
+__global__ void k_iface_import(DevPatches P, const uint32_t* shared, const uint32_t* ks, int64_t n,
                                int d, const double* in) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= n * d) return;
   const int64_t e = t / d;
   const int i = (int)(t % d);
-  const uint32_t part = parts[e], k = ks[e];
-  for (uint32_t r = 0; r < k; ++r) P.partial[(size_t)(part + r) * d + i] = r == 0 ? in[t] : 0.0;
+  const uint32_t s = shared[e], k = ks[e];
+  for (uint32_t r = 0; r < k; ++r) partial_of(P, s, r, d, i) = r == 0 ? in[t] : 0.0;
 }
 
 // One thread per (packed row, component); the own value of a row is the sum
 // of its partial slots, as k_iface_export forms it.
-__global__ void k_iface_pack(DevPatches P, const uint32_t* parts, const uint32_t* ks,
+__global__ void k_iface_pack(DevPatches P, const uint32_t* shared, const uint32_t* ks,
                              ExchangePlan x, int d, double* out) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= x.n_send * d) return;
   const int64_t j = t / d;
   const int i = (int)(t - j * d);
   const uint32_t e = x.send_rows[j];
-  const uint32_t part = parts[e], k = ks[e];
+  const uint32_t s = shared[e], k = ks[e];
   double f = 0.0;
-  for (uint32_t r = 0; r < k; ++r) f += P.partial[(size_t)(part + r) * d + i];
+  for (uint32_t r = 0; r < k; ++r) f += partial_of(P, s, r, d, i);
   out[t] = f;
 }
 
 // One thread per (interface row, component): the terms in the plan's order,
 // then the total written as the row's only partial.
-__global__ void k_iface_sum_import(DevPatches P, const uint32_t* parts, const uint32_t* ks,
+__global__ void k_iface_sum_import(DevPatches P, const uint32_t* shared, const uint32_t* ks,
                                    ExchangePlan x, int d, const double* recv) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= x.n_rows * d) return;
   const int64_t e = t / d;
   const int i = (int)(t - e * d);
-  const uint32_t part = parts[e], k = ks[e];
+  const uint32_t s = shared[e], k = ks[e];
   double own = 0.0;
-  for (uint32_t r = 0; r < k; ++r) own += P.partial[(size_t)(part + r) * d + i];
+  for (uint32_t r = 0; r < k; ++r) own += partial_of(P, s, r, d, i);
   double acc = 0.0;
   for (uint32_t j = x.sum_ptr[e]; j < x.sum_ptr[e + 1]; ++j) {
     const int32_t src = x.sum_src[j];
     acc += src < 0 ? own : recv[(int64_t)src * d + i];
   }
-  for (uint32_t r = 0; r < k; ++r) P.partial[(size_t)(part + r) * d + i] = r == 0 ? acc : 0.0;
+  for (uint32_t r = 0; r < k; ++r) partial_of(P, s, r, d, i) = r == 0 ? acc : 0.0;
 }
 
 __global__ void k_mass_pack(DevModel m, const uint32_t* nodes, ExchangePlan x, double* out) {
@@ -911,17 +927,17 @@ cudaError_t patch_refresh_w(const DevModel& m, const DevPatches& p, double dt, c
   return cudaGetLastError();
 }
 
-cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* part,
+cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* shared,
                                const uint32_t* k, int64_t n, double* out, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_iface_export<<<blocks_of(n * m.dim), kThreads, 0, s>>>(p, part, k, n, m.dim, out);
+  k_iface_export<<<blocks_of(n * m.dim), kThreads, 0, s>>>(p, shared, k, n, m.dim, out);
   return cudaGetLastError();
 }
 
-cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* part,
+cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* shared,
                                const uint32_t* k, int64_t n, const double* in, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_iface_import<<<blocks_of(n * m.dim), kThreads, 0, s>>>(p, part, k, n, m.dim, in);
+  k_iface_import<<<blocks_of(n * m.dim), kThreads, 0, s>>>(p, shared, k, n, m.dim, in);
   return cudaGetLastError();
 }
 
@@ -939,19 +955,19 @@ cudaError_t mass_import(const DevModel& m, const uint32_t* nodes, int64_t n, con
   return cudaGetLastError();
 }
 
-cudaError_t patch_iface_pack(const DevModel& m, const DevPatches& p, const uint32_t* part,
+cudaError_t patch_iface_pack(const DevModel& m, const DevPatches& p, const uint32_t* shared,
                              const uint32_t* k, const ExchangePlan& x, double* out,
                              cudaStream_t s) {
   if (x.n_send <= 0) return cudaSuccess;
-  k_iface_pack<<<blocks_of(x.n_send * m.dim), kThreads, 0, s>>>(p, part, k, x, m.dim, out);
+  k_iface_pack<<<blocks_of(x.n_send * m.dim), kThreads, 0, s>>>(p, shared, k, x, m.dim, out);
   return cudaGetLastError();
 }
 
-cudaError_t patch_iface_sum_import(const DevModel& m, const DevPatches& p, const uint32_t* part,
+cudaError_t patch_iface_sum_import(const DevModel& m, const DevPatches& p, const uint32_t* shared,
                                    const uint32_t* k, const ExchangePlan& x, const double* recv,
                                    cudaStream_t s) {
   if (x.n_rows <= 0) return cudaSuccess;
-  k_iface_sum_import<<<blocks_of(x.n_rows * m.dim), kThreads, 0, s>>>(p, part, k, x, m.dim, recv);
+  k_iface_sum_import<<<blocks_of(x.n_rows * m.dim), kThreads, 0, s>>>(p, shared, k, x, m.dim, recv);
   return cudaGetLastError();
 }
 

@@ -26,9 +26,13 @@
 // Shared nodes. Each patch touching a shared node writes its partial force
 // to the node's slot of rank r (its position among the node's k patches in
 // patch order); a second pass (k_finish_list), one thread per DOF over the
-// shared block, adds the k partials in rank order and finishes the node. The
-// same pass finishes the nodes of no element; for a partitioned mesh the
-// interface nodes' sums are exchanged between parts before it.
+// shared nodes, adds the k partials in rank order and finishes the node. The
+// slots of ranks 0 and 1 form two dense rows indexed by the shared node (s,
+// ns + s; almost every shared node has two patches), ranks 2 and up follow
+// node by node, so the second pass reads a node's first two partials at
+// addresses it knows without loading any index. The same pass finishes the
+// nodes of no element; for a partitioned mesh the interface nodes' sums are
+// exchanged between parts before it.
 #pragma once
 
 #include <stdint.h>
@@ -74,6 +78,13 @@ inline int place_group(int dim) { return dim == 2 ? 8 : 16; }
 // runs (one sum instruction) hit G different banks (G = 16 for 8-byte
 // contributions, 32 for 4-byte ones), and the runs of a group have their
 // nodes at distinct positions mod 16 where the build could arrange it.
+// Partial slot of rank r of shared node s (ns shared nodes; over: the node's
+// first slot for ranks >= 2).
+__host__ __device__ inline uint32_t partial_slot(uint32_t ns, uint32_t s, uint32_t over,
+                                                 uint32_t r) {
+  return r == 0 ? s : (r == 1 ? ns + s : over + r - 2);
+}
+
 struct ChunkDesc {
   uint32_t off16;  // record start in the chunk data, in 16-byte units
   uint32_t bytes;  // record size (multiple of 16)
@@ -96,12 +107,13 @@ struct PatchHost {
   std::vector<int32_t> sh_ptr;       // npatch + 1, into the shared entries
   // shared entries, per patch in position order (entry t <-> position nint + t)
   std::vector<uint32_t> sgid;        // internal node id
+  std::vector<uint32_t> srank;       // this patch's rank among the node's patches
   std::vector<uint32_t> sslot;       // this patch's partial slot of the node
   std::vector<int32_t> chunk_base;   // npatch + 1: first chunk of each patch
   std::vector<ChunkDesc> chunks;     // per chunk
   std::vector<uint16_t> cdata;       // chunk records (multiple of 8 uint16 each)
-  // per shared node (internal id order of the shared block, which starts at
-  // shared_base): internal id, first slot, k
+  // per shared node s (internal id order; one block starting at shared_base
+  // for a single mesh): internal id, first slot of its ranks >= 2, k
   uint32_t shared_base = 0;
   std::vector<uint32_t> shared_nodes, shared_part, shared_k;
   std::vector<uint32_t> orphans;     // internal ids of nodes of no element
@@ -140,9 +152,13 @@ struct DevPatches {
   // there (blocked ones included) of M v^2 after the step, M > DBL_EPSILON
   // only (getKineticEnergy, solid_mechanics_model.cc:547-561)
   double* ke_part;
-  // nodes finished by k_finish_list: the nodes of no element, then the
-  // shared nodes; entry i: node, first slot, k (0 for a node of no element)
+  // nodes finished by k_finish_list: the shared nodes (entry s: shared node
+  // s), then the nodes of no element; entry i: node, first slot of its ranks
+  // >= 2, k (0 for a node of no element)
   int64_t nlist;
+  uint32_t nshared;      // shared nodes (the dense partial rows' length)
+  uint32_t shared_base;  // with shared_contig: shared node s is node shared_base + s
+  int shared_contig;
   const uint32_t* list_gid;
   const uint32_t* list_part;
   const uint32_t* list_k;
@@ -154,6 +170,12 @@ struct DevPatches {
   const int64_t* node_off;
   int ninst;
 };
+
+// Partial slots of a plan's shared entries (sslot), its shared nodes' first
+// overflow slots (shared_part) and nslots, from sgid, srank, shared_nodes and
+// shared_k (run after building, and again after merging the plans of a
+// batch).
+void assign_partial_slots(PatchHost& P, int64_t nn);
 
 size_t patch_smem_bytes(const DevPatches& p, int dim, bool fp32, int nbuf);
 // Chunk record buffers (1 or 2) that keep the most CTAs per SM.
@@ -170,13 +192,13 @@ cudaError_t patch_finish_list(const DevModel& m, const DevPatches& p, double dt,
 int64_t patch_ke_parts(const DevPatches& p, int dim);
 // w = u + dt v + dt^2/2 a on free DOFs, w = u on blocked ones.
 cudaError_t patch_refresh_w(const DevModel& m, const DevPatches& p, double dt, cudaStream_t s);
-// Partitioned meshes, per interface node i (first slot part[i], k[i] slots):
-// out[i] = the sum of its partials (per component); import writes in[i] as
-// its only partial. Masses: out[i] = lumped mass of internal node nodes[i];
+// Partitioned meshes, per interface node i (shared node shared[i], k[i]
+// partials): out[i] = the sum of its partials (per component); import writes
+// in[i] as its only partial. Masses: out[i] = lumped mass of internal node nodes[i];
 // import sets it (and 1/M).
-cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* part,
+cudaError_t patch_iface_export(const DevModel& m, const DevPatches& p, const uint32_t* shared,
                                const uint32_t* k, int64_t n, double* out, cudaStream_t s);
-cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* part,
+cudaError_t patch_iface_import(const DevModel& m, const DevPatches& p, const uint32_t* shared,
                                const uint32_t* k, int64_t n, const double* in, cudaStream_t s);
 cudaError_t mass_export(const DevModel& m, const uint32_t* nodes, int64_t n, double* out,
                         cudaStream_t s);
@@ -195,11 +217,11 @@ struct ExchangePlan {
   const int32_t* sum_src = nullptr;
 };
 // out[k] = this part's force on interface row send_rows[k] (d per row)
-cudaError_t patch_iface_pack(const DevModel& m, const DevPatches& p, const uint32_t* part,
+cudaError_t patch_iface_pack(const DevModel& m, const DevPatches& p, const uint32_t* shared,
                              const uint32_t* k, const ExchangePlan& x, double* out,
                              cudaStream_t s);
 // every interface row's force = its ordered sum, imported as its only partial
-cudaError_t patch_iface_sum_import(const DevModel& m, const DevPatches& p, const uint32_t* part,
+cudaError_t patch_iface_sum_import(const DevModel& m, const DevPatches& p, const uint32_t* shared,
                                    const uint32_t* k, const ExchangePlan& x, const double* recv,
                                    cudaStream_t s);
 // the same for the lumped masses (one value per row) of internal nodes nodes[i]

@@ -465,17 +465,15 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
 
   // 5. internal ids of the shared nodes (in order of first appearance, so
   //    that the nodes of neighbouring patches stay close) and their partial
-  //    slots (k consecutive slots, one per patch in patch order), then the
-  //    nodes of no element
+  //    slots (one per patch in patch order: partial_slot), then the nodes of
+  //    no element
   P.shared_base = next_id;
   for (size_t t = 0; t < entry_user.size(); ++t) {
     const uint32_t v = entry_user[t];
     if (P.perm[v] != 0xffffffffu) continue;
     P.perm[v] = next_id++;
     P.shared_nodes.push_back(P.perm[v]);
-    P.shared_part.push_back((uint32_t)P.nslots);
     P.shared_k.push_back((uint32_t)count[v]);
-    P.nslots += count[v];
   }
   for (int64_t v = 0; v < nn; ++v)
     if (count[v] == 0) {
@@ -484,16 +482,36 @@ PatchHost build_patches(const double* X, const uint32_t* conn, int64_t nn, int64
     }
   if ((int64_t)next_id != nn) throw std::logic_error("node numbering is not a bijection");
   P.sgid.resize(entry_user.size());
-  P.sslot.resize(entry_user.size());
+  P.srank.resize(entry_user.size());
   for (size_t t = 0; t < entry_user.size(); ++t) {
-    const uint32_t g = P.perm[entry_user[t]];
-    P.sgid[t] = g;
-    P.sslot[t] = P.shared_part[g - P.shared_base] + entry_rank[t];
+    P.sgid[t] = P.perm[entry_user[t]];
+    P.srank[t] = (uint32_t)entry_rank[t];
   }
+  assign_partial_slots(P, nn);
   // positions stay below L; a stride of 5 mod 16 puts the components of a
   // node's force accumulator in different bank pairs
   P.node_stride = (P.max_nodes + kBankPairs - 1) / kBankPairs * kBankPairs + 5;
   return P;
+}
+
+void assign_partial_slots(PatchHost& P, int64_t nn) {
+  const uint32_t ns = (uint32_t)P.shared_nodes.size();
+  std::vector<int32_t> sidx((size_t)nn, -1);  // internal id -> shared node
+  for (uint32_t s = 0; s < ns; ++s) sidx[P.shared_nodes[s]] = (int32_t)s;
+  P.shared_part.assign(ns, 0);
+  int64_t slots = 2 * (int64_t)ns;  // the dense rows of ranks 0 and 1
+  for (uint32_t s = 0; s < ns; ++s) {
+    P.shared_part[s] = (uint32_t)slots;
+    slots += P.shared_k[s] > 2 ? P.shared_k[s] - 2 : 0;
+  }
+  if (slots >= (int64_t)UINT32_MAX) throw std::length_error("too many partial slots");
+  P.nslots = slots;
+  P.sslot.resize(P.sgid.size());
+  for (size_t t = 0; t < P.sgid.size(); ++t) {
+    const int32_t s = sidx[P.sgid[t]];
+    if (s < 0 || P.srank[t] >= P.shared_k[s]) throw std::logic_error("shared entry without its node");
+    P.sslot[t] = partial_slot(ns, (uint32_t)s, P.shared_part[s], P.srank[t]);
+  }
 }
 
 }  // namespace akb

@@ -158,25 +158,34 @@ void check(const char* name, const Mesh& m, int target, int maxn, int cbytes,
       const int64_t s = (int64_t)P.sgid[t] - P.shared_base;
       CHECK(s >= 0 && s < (int64_t)P.shared_nodes.size());
       if (s < 0 || s >= (int64_t)P.shared_nodes.size()) continue;
-      const int r = (int)P.sslot[t] - (int)P.shared_part[s];
+      const int r = (int)P.srank[t];
       CHECK(r >= 0 && r < (int)P.shared_k[s]);
       CHECK((int)ranks[P.sgid[t]].size() == r);  // patches met in order
+      // ranks 0 and 1 in the dense rows, the others after them node by node
+      CHECK(P.sslot[t] == akb::partial_slot((uint32_t)P.shared_nodes.size(), (uint32_t)s,
+                                            P.shared_part[s], (uint32_t)r));
       ranks[P.sgid[t]].push_back(r);
     }
   // forced (interface) nodes are shared even in one patch
   if (force)
     for (int64_t v = 0; v < nn; ++v)
       if ((*force)[v] && P.perm[v] < P.shared_base) CHECK(false);
-  int64_t slots = 0;
+  int64_t slots = 2 * (int64_t)P.shared_nodes.size();
   for (size_t s = 0; s < P.shared_nodes.size(); ++s) {
     std::vector<int> r = ranks[P.shared_nodes[s]];
     std::sort(r.begin(), r.end());
     CHECK((int)r.size() == (int)P.shared_k[s]);
     for (int i = 0; i < (int)r.size(); ++i) CHECK(r[i] == i);
     CHECK(P.shared_part[s] == slots);
-    slots += P.shared_k[s];
+    slots += P.shared_k[s] > 2 ? P.shared_k[s] - 2 : 0;
   }
   CHECK(slots == P.nslots);
+  {  // no two entries share a slot
+    std::vector<uint32_t> all(P.sslot);
+    std::sort(all.begin(), all.end());
+    CHECK(std::adjacent_find(all.begin(), all.end()) == all.end());
+    CHECK(all.empty() || (int64_t)all.back() < P.nslots);
+  }
   for (p = 0; p < P.npatch; ++p) {
     c_ = -1;
     const int nint = P.nint[p], s0 = P.sh_ptr[p], L = nint + (P.sh_ptr[p + 1] - s0);
