@@ -129,14 +129,15 @@ __device__ inline void stress_P(const MatParams& p, const S* g, S* P) {
     const S jm1 = t + I2 + dg;
     const S iJ = S(1) / (S(1) + jm1);
     const S a = mu * iJ, b = lam * log1p(jm1) * iJ, c = S(1) + t;
+    // with u = (1 + t) g^T - (g^T)^2: dev = det(g) I + u, adj(F)^T =
+    // (1 + t + I2) I - u, so P = mu g + (a - b) u + (a det g + b (1 + t + I2)) I
+    const S amb = a - b, diag = a * dg + b * (c + I2);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        const S gt = g[j * 3 + i], ggt = gg[j * 3 + i];
-        const S adjT = (i == j ? c + I2 : S(0)) - c * gt + ggt;
-        const S dev = (i == j ? dg : S(0)) + c * gt - ggt;
-        P[i * 3 + j] = mu * g[i * 3 + j] + a * dev + b * adjT;
+        const S u = c * g[j * 3 + i] - gg[j * 3 + i];
+        P[i * 3 + j] = mu * g[i * 3 + j] + amb * u + (i == j ? diag : S(0));
       }
     return;
   }
@@ -307,13 +308,14 @@ __device__ inline void hex_parallelepiped_force(const MatParams& p, const double
       eyz += S(sg[1][a] * sg[2][a]) * v;
       exyz += S(sg[0][a] * sg[1][a] * sg[2][a]) * v;
     }
-    E0[0][i] = e0x;
-    E0[1][i] = e0y;
-    E0[2][i] = e0z;
-    Fp[0][i] = mulc(exy, gc);
-    Fp[1][i] = mulc(exz, gc);
-    Fp[2][i] = mulc(eyz, gc);
-    F3[i] = mulc(exyz, third);
+    // the 1/8 of the trilinear derivatives folded in (exact: a power of two)
+    E0[0][i] = S(0.125) * e0x;
+    E0[1][i] = S(0.125) * e0y;
+    E0[2][i] = S(0.125) * e0z;
+    Fp[0][i] = S(0.125) * mulc(exy, gc);
+    Fp[1][i] = S(0.125) * mulc(exz, gc);
+    Fp[2][i] = S(0.125) * mulc(eyz, gc);
+    F3[i] = S(0.125) * mulc(exyz, third);
   }
   // pair index of directions (k, m): xy 0, xz 1, yz 2
   auto pair = [](int k, int m) { return k + m - 1; };
@@ -330,8 +332,8 @@ __device__ inline void hex_parallelepiped_force(const MatParams& p, const double
       const int m = k == 0 ? 1 : 0, nn = k == 2 ? 1 : 2;
 #pragma unroll
       for (int i = 0; i < d; ++i)
-        H[i * d + k] = S(0.125) * (E0[k][i] + sq[m] * Fp[pair(k, m)][i] +
-                                   sq[nn] * Fp[pair(k, nn)][i] + (sq[m] * sq[nn]) * F3[i]);
+        H[i * d + k] = E0[k][i] + sq[m] * Fp[pair(k, m)][i] + sq[nn] * Fp[pair(k, nn)][i] +
+                       (sq[m] * sq[nn]) * F3[i];
     }
     // grad u = H A^T / det J
     S g[9];
