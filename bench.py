@@ -350,9 +350,9 @@ def run_ours(args, dist):
                          "algorithmic_bytes_per_step": balg,
                          # DRAM bytes of one k_patch_step launch from an ncu capture
                          # (dram__bytes_read.sum + dram__bytes_write.sum) of the
-                         # 90^3-cell cube (4.374 M elements, 232.0 MB), scaled by
+                         # 90^3-cell cube (4.374 M elements, 232.7 MB), scaled by
                          # elements; the capture is not taken inside this run
-                         "traffic": 232.0e6 * E / 4.374e6,
+                         "traffic": 232.7e6 * E / 4.374e6,
                          "traffic_kernel": "k_patch_step (ncu, 90^3 cells, scaled by elements)",
                          "kernels_ms": {n: t for n, t in ktimes},
                          "dominant": top[0]},
