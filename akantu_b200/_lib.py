@@ -98,6 +98,9 @@ SIGNATURES = {
     "akb_mlp_stress": (I32, [P, I64, P, P, C.c_double, C.c_double, P, P, P]),
     "akb_mlp_gradients": (I32, [P, I64, P, P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "akb_mlp_train_step": (I32, [P, I64, P, P, C.c_float, C.POINTER(C.c_float)]),
+    "akb_mlp_compute_gradients": (I32, [P, I64, P, P, C.POINTER(C.c_float)]),
+    "akb_mlp_gradient_device_pointer": (I32, [P, C.POINTER(P)]),
+    "akb_mlp_apply_gradients": (I32, [P, C.c_float]),
 }
 
 

@@ -1018,13 +1018,23 @@ akb_status akb_mlp_gradients(akb_mlp* m, int64_t nb, const double* x, const doub
   return AKB_OK;
 }
 
-akb_status akb_mlp_train_step(akb_mlp* m, int64_t nb, const double* x, const double* target,
-                              float learning_rate, float* loss) {
+akb_status akb_mlp_compute_gradients(akb_mlp* m, int64_t nb, const double* x,
+                                     const double* target, float* loss) {
   if (!m) return fail(AKB_ERR_INVALID_ARGUMENT, "null network");
   if (nb < 1 || !x || !target) return fail(AKB_ERR_INVALID_ARGUMENT, "x and target are required");
   AKB_CUDA_TRY(cudaSetDevice(m->device));
-  akb_status st;
-  if ((st = gradients(m, nb, x, target, loss)) != AKB_OK) return st;
+  return gradients(m, nb, x, target, loss);
+}
+
+akb_status akb_mlp_gradient_device_pointer(akb_mlp* m, float** grad) {
+  if (!m || !grad) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  *grad = m->d_grad;
+  return AKB_OK;
+}
+
+akb_status akb_mlp_apply_gradients(akb_mlp* m, float learning_rate) {
+  if (!m) return fail(AKB_ERR_INVALID_ARGUMENT, "null network");
+  AKB_CUDA_TRY(cudaSetDevice(m->device));
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   m->adam_step += 1;
   const float c1 = 1.0f - std::pow(b1, (float)m->adam_step);
@@ -1033,6 +1043,13 @@ akb_status akb_mlp_train_step(akb_mlp* m, int64_t nb, const double* x, const dou
       m->d_params, m->d_grad, m->d_m1, m->d_m2, m->nparams, learning_rate, b1, b2, eps, c1, c2);
   AKB_CUDA_TRY(cudaGetLastError());
   return repack(m);
+}
+
+akb_status akb_mlp_train_step(akb_mlp* m, int64_t nb, const double* x, const double* target,
+                              float learning_rate, float* loss) {
+  akb_status st;
+  if ((st = akb_mlp_compute_gradients(m, nb, x, target, loss)) != AKB_OK) return st;
+  return akb_mlp_apply_gradients(m, learning_rate);
 }
 
 }  // extern "C"

@@ -145,10 +145,43 @@ class MLPSurrogate:
                                        float(lr), C.byref(loss)))
         return loss.value
 
-    def train(self, x, t, epochs=20, batch=4096, lr=1e-3, lr_final=1e-5, seed=0, log=None):
-        """Adam over shuffled minibatches with a cosine-decayed learning
-        rate; x, t device (nb, d) FP64 features. Returns the epoch losses."""
+    # -- data-parallel halves of a training step (akb_mlp_compute_gradients,
+    #    akb_mlp_apply_gradients) ------------------------------------------
+    def compute_gradients(self, x, t):
+        """Gradient of the mean loss over (x, t) into the network's device
+        gradient array (gradient_tensor); returns the loss."""
+        loss = C.c_float()
+        check(lib().akb_mlp_compute_gradients(self._h, x.shape[0], x.data_ptr(), t.data_ptr(),
+                                              C.byref(loss)))
+        return loss.value
+
+    def gradient_tensor(self):
+        """Zero-copy float32 torch view of the device gradient array."""
         torch = _torch()
+        ptr = C.c_void_p()
+        check(lib().akb_mlp_gradient_device_pointer(self._h, C.byref(ptr)))
+
+        class _Cai:
+            __cuda_array_interface__ = dict(shape=(self.nb_parameters,), typestr="<f4",
+                                            data=(int(ptr.value), False), version=3,
+                                            strides=None, stream=None)
+        return torch.as_tensor(_Cai(), device="cuda:%d" % self.device)
+
+    def apply_gradients(self, lr):
+        check(lib().akb_mlp_apply_gradients(self._h, float(lr)))
+
+    def train(self, x, t, epochs=20, batch=4096, lr=1e-3, lr_final=1e-5, seed=0, log=None,
+              group=None):
+        """Adam over shuffled minibatches with a cosine-decayed learning
+        rate; x, t device (nb, d) FP64 features. Returns the epoch losses.
+        With a torch.distributed group of several processes (one GPU each,
+        every rank holding the same x and t), each minibatch is split over
+        the ranks and their gradients averaged (data_parallel_train)."""
+        torch = _torch()
+        import torch.distributed as dist
+        if group is not None or (dist.is_available() and dist.is_initialized()
+                                 and dist.get_world_size() > 1):
+            return data_parallel_train(self, x, t, epochs, batch, lr, lr_final, seed, log, group)
         torch.cuda.synchronize()
         n = x.shape[0]
         g = torch.Generator(device=x.device)
@@ -218,3 +251,51 @@ class MLPSurrogate:
         m.set_parameters(d["params"])
         m.set_scaling(d["in_shift"], d["in_scale"], d["out_shift"], d["out_scale"])
         return m
+
+
+def data_parallel_train(model, x, t, epochs=20, batch=4096, lr=1e-3, lr_final=1e-5, seed=0,
+                        log=None, group=None):
+    """Data-parallel Adam (SURVEY's MLP-training case): every rank draws the
+    same shuffled minibatches (same seed), takes its share (rank r: samples
+    r, r + world, ... of each minibatch; batch must be a multiple of the
+    world size), computes its gradient on its GPU, and the gradients are
+    averaged by one all-reduce per step (NCCL on the network's stream, or
+    gloo), so every rank applies the same Adam step and the replicas stay
+    equal. model: compute_gradients(x, t) -> loss, gradient_tensor() (reduced
+    in place), apply_gradients(lr). Returns the epoch losses (averaged over
+    ranks)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    if batch % world:
+        raise ValueError("batch (%d) must be a multiple of the world size (%d)" % (batch, world))
+    n = x.shape[0]
+    g = torch.Generator(device=x.device)
+    g.manual_seed(seed)
+    nbat = max(1, n // batch)
+    steps = epochs * nbat
+    k = 0
+    losses = []
+    grad = model.gradient_tensor()
+    loss_t = torch.zeros(1, dtype=torch.float64, device=grad.device)
+    for ep in range(epochs):
+        perm = torch.randperm(n, device=x.device, generator=g)
+        tot = 0.0
+        for b in range(nbat):
+            idx = perm[b * batch:(b + 1) * batch][rank::world]
+            loss = model.compute_gradients(x[idx].contiguous(), t[idx].contiguous())
+            if world > 1:
+                dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+                grad.div_(world)
+                loss_t.fill_(loss)
+                dist.all_reduce(loss_t, op=dist.ReduceOp.SUM, group=group)
+                loss = float(loss_t.item()) / world
+            lr_k = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / steps))
+            model.apply_gradients(lr_k)
+            tot += loss
+            k += 1
+        losses.append(tot / nbat)
+        if log:
+            log("epoch %d loss %.3e" % (ep, losses[-1]))
+    return losses

@@ -158,6 +158,18 @@ akb_status akb_mlp_gradients(akb_mlp* mlp, int64_t nb, const double* x, const do
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on that loss. */
 akb_status akb_mlp_train_step(akb_mlp* mlp, int64_t nb, const double* x, const double* target,
                               float learning_rate, float* loss);
+/* The same step in two halves, for data-parallel training (one process and
+ * GPU per rank, each with its share of the minibatch): compute_gradients
+ * leaves the gradient of the mean loss over its nb samples in a device array
+ * of nb_parameters floats (parameter layout, gradient_device_pointer; valid
+ * until the next call on this network), which the caller may average over
+ * ranks in place (e.g. an all-reduce on the network's stream), then
+ * apply_gradients takes one Adam step with it. compute + apply is
+ * akb_mlp_train_step. */
+akb_status akb_mlp_compute_gradients(akb_mlp* mlp, int64_t nb, const double* x,
+                                     const double* target, float* loss);
+akb_status akb_mlp_gradient_device_pointer(akb_mlp* mlp, float** grad);
+akb_status akb_mlp_apply_gradients(akb_mlp* mlp, float learning_rate);
 
 #ifdef __cplusplus
 }

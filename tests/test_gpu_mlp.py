@@ -67,3 +67,32 @@ def test_training_reduces_loss():
     losses = net.train(X, T, epochs=60, batch=1024, lr=2e-3, lr_final=1e-4)
     l1, _ = net.gradients_features(X, T)
     assert l1 <= 0.05 * l0 and losses[-1] < losses[0]
+
+
+def test_compute_then_apply_is_the_train_step():
+    """akb_mlp_compute_gradients + akb_mlp_apply_gradients (the halves a
+    data-parallel step all-reduces between) equal akb_mlp_train_step bit for
+    bit, and the gradient view is the array the library reads."""
+    import torch
+    from akantu_b200.surrogate import MLPSurrogate
+    rng = np.random.default_rng(12)
+    x = torch.as_tensor(rng.normal(size=(1000, 10)), device="cuda")
+    t = torch.as_tensor(rng.normal(size=(1000, 9)), device="cuda")
+    a, b = MLPSurrogate(seed=4), MLPSurrogate(seed=4)
+    for step in range(3):
+        la = a.train_step_features(x, t, 1e-3)
+        lb = b.compute_gradients(x, t)
+        g = b.gradient_tensor()
+        assert g.shape == (b.nb_parameters,) and bool(torch.isfinite(g).all())
+        b.apply_gradients(1e-3)
+        assert la == lb
+    assert np.array_equal(a.get_parameters(), b.get_parameters())
+    # a gradient scaled in place before the step changes it (the step reads the view)
+    c = MLPSurrogate(seed=4)
+    c.compute_gradients(x, t)
+    c.gradient_tensor().mul_(0.0)
+    p0 = c.get_parameters()
+    c.apply_gradients(1e-3)
+    torch.cuda.synchronize()
+    assert np.array_equal(c.get_parameters(), p0)  # Adam with zero gradient: no move
+    a.close(), b.close(), c.close()
