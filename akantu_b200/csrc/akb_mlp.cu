@@ -430,11 +430,15 @@ __global__ void __launch_bounds__(kFwdThreads, 2)
         float v[32];
         tmem_ld32(tmem + lane_base + c0, v);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const float zz = v[j] + bias[c0 + j];
-          if (TRAIN && row < nb) bufs.z[l][row * N + c0 + j] = zz;
-          v[j] = silu(zz);
+        for (int j = 0; j < 32; ++j) v[j] += bias[c0 + j];
+        if (TRAIN && row < nb) {  // the pre-activations: eight 16-byte stores
+          float4* z4 = reinterpret_cast<float4*>(bufs.z[l] + (size_t)row * N + c0);
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            z4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
         }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = silu(v[j]);
 #pragma unroll
         for (int q = 0; q < 4; ++q) store8(s.act, r, c0 + 8 * q, N, v + 8 * q);
         if (TRAIN) {
@@ -551,11 +555,21 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
     }
     unsigned char* g = bufs.dz[l - 1] + tile * (size_t)kTile * N * 2;
     for (int c0 = half * (N >> 1); c0 < (half + 1) * (N >> 1); c0 += 32) {
-      float v[32];
+      float v[32], zz[32];
       tmem_ld32(tmem + lane_base + c0, v);
+      if (row < nb) {  // the row's 32 pre-activations: eight 16-byte loads
+        const float4* z4 = reinterpret_cast<const float4*>(bufs.z[l - 1] + (size_t)row * N + c0);
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
-        v[j] = row < nb ? v[j] * dsilu(bufs.z[l - 1][row * N + c0 + j]) : 0.0f;
+        for (int q = 0; q < 8; ++q) {
+          const float4 z = z4[q];
+          zz[4 * q] = z.x;
+          zz[4 * q + 1] = z.y;
+          zz[4 * q + 2] = z.z;
+          zz[4 * q + 3] = z.w;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = row < nb ? v[j] * dsilu(zz[j]) : 0.0f;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         store8(s.act, r, c0 + 8 * q, N, v + 8 * q);
@@ -637,7 +651,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         float v[16];
         tmem_ld16(tmem + lane_base + h * cb + c0, v);
         const int m = h * kTile + tid;
-        for (int j = 0; j < 16; ++j) out[(size_t)m * cb + c0 + j] = v[j];
+        float4* o4 = reinterpret_cast<float4*>(out + (size_t)m * cb + c0);  // four 16-byte stores
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          o4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
       }
   } else if (t1 <= t0) {
     float* out = part + (size_t)blockIdx.x * ca * cb;
@@ -794,7 +811,9 @@ akb_status gradients(akb_mlp* m, int64_t nb, const double* x, const double* targ
   AKB_CUDA_TRY(cudaGetLastError());
   k_backward<<<(unsigned)ntiles, kFwdThreads, kBwdSmem, m->stream>>>(n, nb, target, m->bufs);
   AKB_CUDA_TRY(cudaGetLastError());
-  const int tpc = (int)std::max<int64_t>(1, (ntiles + 147) / 148);
+  // at least four tiles per CTA: each CTA writes a whole ca x cb partial,
+  // so a few more tiles per CTA cost less than more partials to write and sum
+  const int tpc = (int)std::min<int64_t>(ntiles, std::max<int64_t>(4, (ntiles + 147) / 148));
   const int nparts = (int)((ntiles + tpc - 1) / tpc);
   for (int l = 0; l < n.nl; ++l) {
     const bool last = l == n.nl - 1;
