@@ -471,7 +471,7 @@ def run_decomposed(args, dist):
                        "exchange_bytes_per_step": nbytes,
                        "l2": "no flush: per-GPU working set %.0f MB > 126 MB L2" % (balg / 1e6)},
             "roofline": {"bound": "hbm", "kernel": "whole step per GPU (fused step, pack, "
-                                                   "exchange, interface sums, shared-node pass)",
+                                                   "exchange, interface sums, k_finish_list)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "algorithmic_bytes_per_step": balg, "traffic": None},
