@@ -255,7 +255,7 @@ class MLPSurrogate:
 
 def data_parallel_train(model, x, t, epochs=20, batch=4096, lr=1e-3, lr_final=1e-5, seed=0,
                         log=None, group=None):
-    """Data-parallel Adam (SURVEY's MLP-training case): every rank draws the
+    """Data-parallel Adam (one process and GPU per rank): every rank draws the
     same shuffled minibatches (same seed), takes its share (rank r: samples
     r, r + world, ... of each minibatch; batch must be a multiple of the
     world size), computes its gradient on its GPU, and the gradients are
