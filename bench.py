@@ -453,6 +453,10 @@ def run_decomposed(args, dist):
     d2h = 8 * nslabs
     nbytes = dist.sum(float(dm.bytes_per_step))
     balg = b_alg_bytes({"mesh": s["parts"][0].mesh}, False) * ppr
+    # per step and part: the fused step, the pack (rows to send), the ordered
+    # sums (interface rows), the shared-node pass
+    launches = int(dist.sum(float(sum(2 + (x.n_send > 0) + (x.sum_ptr.size > 1)
+                                      for x in dm.plans))))
     dm.close()
     if dist.rank != 0:
         return None
@@ -478,7 +482,7 @@ def run_decomposed(args, dist):
             "clocks": clocks,
             "e2e": {"value": E * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},
-            "gpu_launches": args.steps * 4 * nslabs}
+            "gpu_launches": args.steps * launches}
 
 
 def run_plate(args, device):
