@@ -197,9 +197,19 @@ def test_exchange_plans(nparts):
     assert total == 2 * 8 * 3 * sum(x.n_send for x in plans)
 
 
-@pytest.mark.parametrize("nparts", [2, 3, 4])
-def test_parts_in_one_process_match_whole_mesh(nparts):
-    w = _workload()
+def _plate():
+    w = configs.plate_tri3(nx=40, ny=8, lx=4.0, ly=0.8)
+    rng = np.random.default_rng(9)
+    v0 = rng.normal(0.0, 0.1, w["u0"].shape)
+    v0[w["blocked"].astype(bool)] = 0.0
+    w["v0"] = v0
+    return w
+
+
+@pytest.mark.parametrize("nparts,work", [(2, _workload), (3, _workload), (4, _workload),
+                                         (3, _plate), (5, _plate)])
+def test_parts_in_one_process_match_whole_mesh(nparts, work):
+    w = work()
     dt_w, u_w, v_w = _run_whole(w)
     dt_d, u_d, v_d, copies, nbytes = _run_distributed(w, nparts, copies=True)
     assert dt_d == dt_w
