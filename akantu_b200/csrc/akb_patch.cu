@@ -144,8 +144,11 @@ __device__ inline int cidx(int k, int i, int CH) {
 template <int T, typename S> struct PatchOccupancy { static constexpr int value = 3; };
 template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, float> { static constexpr int value = 2; };
 template <> struct PatchOccupancy<AKB_HEXAHEDRON_8, double> { static constexpr int value = 1; };
-// 2D and 1D patches of <= 1024 elements take <= 56 KB of shared memory:
-// four CTAs per SM when the registers allow it (<= 64 per thread)
+// FP32-bulk tetrahedra (FP32 contributions, 768-element patches, one record
+// buffer: <= 56 KB), 2D and 1D patches of <= 1024 elements take <= 56 KB of
+// shared memory: four CTAs per SM when the registers allow it (<= 64 per
+// thread; the FP64 tetrahedron at 64 registers measured slower)
+template <> struct PatchOccupancy<AKB_TETRAHEDRON_4, float> { static constexpr int value = 4; };
 template <typename S> struct PatchOccupancy<AKB_TRIANGLE_3, S> { static constexpr int value = 4; };
 template <typename S> struct PatchOccupancy<AKB_SEGMENT_2, S> { static constexpr int value = 4; };
 
@@ -865,7 +868,12 @@ int patch_buffers(const DevPatches& p, int type, bool fp32) {
   switch (type) {
   case AKB_HEXAHEDRON_8: regs = fp32 ? PatchOccupancy<AKB_HEXAHEDRON_8, float>::value
                                      : PatchOccupancy<AKB_HEXAHEDRON_8, double>::value; break;
-  default: regs = PatchOccupancy<AKB_TETRAHEDRON_4, double>::value; break;
+  case AKB_TETRAHEDRON_4: regs = fp32 ? PatchOccupancy<AKB_TETRAHEDRON_4, float>::value
+                                      : PatchOccupancy<AKB_TETRAHEDRON_4, double>::value; break;
+  case AKB_TRIANGLE_3: regs = fp32 ? PatchOccupancy<AKB_TRIANGLE_3, float>::value
+                                   : PatchOccupancy<AKB_TRIANGLE_3, double>::value; break;
+  default: regs = fp32 ? PatchOccupancy<AKB_SEGMENT_2, float>::value
+                       : PatchOccupancy<AKB_SEGMENT_2, double>::value; break;
   }
   const int dim = type == AKB_SEGMENT_2 ? 1 : type == AKB_TRIANGLE_3 ? 2 : 3;
   auto ctas = [&](int nbuf) {
