@@ -139,6 +139,7 @@ class SolidMechanicsModel:
         self._h = None
         self._user = []
         self._mirrors = {}
+        self._views = {}
         self._checked_out = set()
         self._blocked = None
 
@@ -185,6 +186,7 @@ class SolidMechanicsModel:
         self.close()
 
     def close(self):
+        self._views = {}  # views of the device arrays about to be freed
         if getattr(self, "_h", None):
             lib().akb_model_destroy(self._h)
             self._h = None
@@ -343,13 +345,20 @@ class SolidMechanicsModel:
 
     def deviceTensor(self, field):
         """Zero-copy torch view of a device field: (N, d) nodal fields, or
-        (E*q, d, d) [k, i, j] quadrature fields (column-major storage)."""
+        (E*q, d, d) [k, i, j] quadrature fields (column-major storage). The
+        views are cached per field while the field's device address stays
+        the same (a user material's step asks for two every step)."""
         ptr = self.devicePointer(field)
+        cached = self._views.get(field)
+        if cached is not None and cached[0] == ptr:
+            return cached[1]
         if field in (_abi.FIELD_GRAD_U, _abi.FIELD_STRESS):
             n = self.mesh.getNbElement() * self.nqp
-            t = _device_tensor(ptr, (n, self.dim, self.dim), self._device)
-            return t.transpose(1, 2)
-        return _device_tensor(ptr, (self.mesh.getNbNodes(), self.dim), self._device)
+            t = _device_tensor(ptr, (n, self.dim, self.dim), self._device).transpose(1, 2)
+        else:
+            t = _device_tensor(ptr, (self.mesh.getNbNodes(), self.dim), self._device)
+        self._views[field] = (ptr, t)
+        return t
 
     def timeSolveSteps(self, nb_steps):
         """Device time (ms) of nb_steps steps, CUDA events on the model's stream."""
