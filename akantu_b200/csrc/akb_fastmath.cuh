@@ -323,7 +323,7 @@ __device__ inline void hex_parallelepiped_force(const MatParams& p, const double
   S T0[9], Tm[9], Tn[9], Tmn[9];
 #pragma unroll
   for (int t = 0; t < 9; ++t) T0[t] = Tm[t] = Tn[t] = Tmn[t] = 0;
-#pragma unroll 1
+#pragma unroll 2  // two points in flight: independent FP64 chains hide each other's latency
   for (int q = 0; q < 8; ++q) {
     const S sq[3] = {(q & 1) ? S(1) : S(-1), (q & 2) ? S(1) : S(-1), (q & 4) ? S(1) : S(-1)};
     S H[9];
