@@ -556,7 +556,7 @@ def run_hex8(args, device, peak):
     # compute roofline of the FP64 launch, from an ncu capture of this
     # workload (sm__inst_executed_pipe_fp64, % of peak; not taken in this run)
     out["compute_roofline"] = {"bound": "fp64 pipe (FP64) / fma pipe (FP32-bulk)",
-                               "fp64_pipe_active": 0.471, "fp32_bulk_fma_pipe_active": 0.432,
+                               "fp64_pipe_active": 0.445, "fp32_bulk_fma_pipe_active": 0.413,
                                "kernel": "k_patch_step<hex8, double> / <hex8, float>",
                                "source": "ncu captures of the 96^3 block "
                                          "(profiles/k_patch_step_block_hex8_96.md)"}
