@@ -100,12 +100,15 @@ cudaError_t launch_elements(const DevModel& m, cudaStream_t s) {
 }
 
 // User materials: displacement gradient at every quadrature point (FP64,
-// column-major per point, like Material::gradu) ...
+// column-major per point, like Material::gradu), one thread per point (the
+// points of an element are consecutive threads: their corner loads coincide) ...
 template <int T>
 __global__ void k_qp_gradu(DevModel m) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe, nq = ET<T>::nqp;
-  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (e >= m.ne) return;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= m.ne * nq) return;
+  const int64_t e = t / nq;
+  const int q = (int)(t - e * nq);
   double dX[3 * 8], du[3 * 8];
   uint32_t nodes[8];
 #pragma unroll
@@ -117,43 +120,45 @@ __global__ void k_qp_gradu(DevModel m) {
       dX[a * d + i] = m.X[(int64_t)nodes[a] * d + i] - m.X[(int64_t)nodes[0] * d + i];
       du[a * d + i] = m.u[(int64_t)nodes[a] * d + i] - m.u[(int64_t)nodes[0] * d + i];
     }
-#pragma unroll 1
-  for (int q = 0; q < nq; ++q) {
-    double B[3 * 8];
-    fast::shape_gradients<T, double>(dX, q, B);
-    double* g = m.gradu + (e * nq + q) * d * d;
+  double B[3 * 8];
+  fast::shape_gradients<T, double>(dX, q, B);
+  double* g = m.gradu + (e * nq + q) * d * d;
 #pragma unroll
-    for (int i = 0; i < d; ++i)
+  for (int i = 0; i < d; ++i)
 #pragma unroll
-      for (int j = 0; j < d; ++j) {
-        double c = 0;
+    for (int j = 0; j < d; ++j) {
+      double c = 0;
 #pragma unroll
-        for (int a = 1; a < n; ++a) c += du[a * d + i] * B[a * d + j];
-        g[i + j * d] = c;
-      }
-  }
+      for (int a = 1; a < n; ++a) c += du[a * d + i] * B[a * d + j];
+      g[i + j * d] = c;
+    }
 }
 
 // ... and the element force vectors sum_q w_q det J_q stress_q grad N_a from
-// the stresses the caller wrote.
+// the stresses the caller wrote: one thread per point, the nq points of an
+// element in consecutive lanes of one warp, their vectors added by a fixed
+// butterfly over those lanes (the element's first lane writes the sum).
 template <int T>
 __global__ void k_qp_forces(DevModel m) {
   constexpr int d = ET<T>::dim, n = ET<T>::nnpe, nq = ET<T>::nqp;
-  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (e >= m.ne) return;
-  double dX[3 * 8], fe[3 * 8];
-  uint32_t nodes[8];
+  static_assert((nq & (nq - 1)) == 0 && nq <= 32, "points per element: a power of two <= 32");
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool valid = t < m.ne * nq;  // every lane takes part in the shuffles
+  const int64_t e = t / nq;
+  const int q = (int)(t - e * nq);
+  double fe[3 * 8];
 #pragma unroll
-  for (int a = 0; a < n; ++a) nodes[a] = m.conn[e * n + a];
+  for (int k = 0; k < d * n; ++k) fe[k] = 0.0;
+  if (valid) {
+    double dX[3 * 8];
+    uint32_t nodes[8];
 #pragma unroll
-  for (int a = 0; a < n; ++a)
+    for (int a = 0; a < n; ++a) nodes[a] = m.conn[e * n + a];
 #pragma unroll
-    for (int i = 0; i < d; ++i) {
-      dX[a * d + i] = m.X[(int64_t)nodes[a] * d + i] - m.X[(int64_t)nodes[0] * d + i];
-      fe[a * d + i] = 0.0;
-    }
-#pragma unroll 1
-  for (int q = 0; q < nq; ++q) {
+    for (int a = 0; a < n; ++a)
+#pragma unroll
+      for (int i = 0; i < d; ++i)
+        dX[a * d + i] = m.X[(int64_t)nodes[a] * d + i] - m.X[(int64_t)nodes[0] * d + i];
     double B[3 * 8];
     const double wq = fast::weight<T>() * fast::shape_gradients<T, double>(dX, q, B);
     const double* P = m.stress + (e * nq + q) * d * d;
@@ -164,12 +169,18 @@ __global__ void k_qp_forces(DevModel m) {
         double c = 0;
 #pragma unroll
         for (int j = 0; j < d; ++j) c += P[i + j * d] * B[a * d + j];
-        fe[a * d + i] += wq * c;
+        fe[a * d + i] = wq * c;
       }
   }
-  double* out = static_cast<double*>(m.fe) + e * d * n;
 #pragma unroll
-  for (int k = 0; k < d * n; ++k) out[k] = fe[k];
+  for (int off = 1; off < nq; off <<= 1)
+#pragma unroll
+    for (int k = 0; k < d * n; ++k) fe[k] += __shfl_xor_sync(0xffffffffu, fe[k], off);
+  if (valid && q == 0) {
+    double* out = static_cast<double*>(m.fe) + e * d * n;
+#pragma unroll
+    for (int k = 0; k < d * n; ++k) out[k] = fe[k];
+  }
 }
 
 // comp >= 0: one thread per listed node, that component; comp < 0: one
@@ -202,22 +213,22 @@ cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n,
 
 cudaError_t user_qp_gradients(const DevModel& m, cudaStream_t s) {
   if (m.ne == 0) return cudaSuccess;
-  switch (m.type) {
+  switch (m.type) {  // one thread per quadrature point
   case AKB_SEGMENT_2: k_qp_gradu<AKB_SEGMENT_2><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
   case AKB_TRIANGLE_3: k_qp_gradu<AKB_TRIANGLE_3><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
   case AKB_TETRAHEDRON_4: k_qp_gradu<AKB_TETRAHEDRON_4><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
-  default: k_qp_gradu<AKB_HEXAHEDRON_8><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  default: k_qp_gradu<AKB_HEXAHEDRON_8><<<blocks_for(m.ne * 8), kThreads, 0, s>>>(m); break;
   }
   return cudaGetLastError();
 }
 
 cudaError_t user_element_forces(const DevModel& m, cudaStream_t s) {
   if (m.ne == 0) return cudaSuccess;
-  switch (m.type) {
+  switch (m.type) {  // one thread per quadrature point
   case AKB_SEGMENT_2: k_qp_forces<AKB_SEGMENT_2><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
   case AKB_TRIANGLE_3: k_qp_forces<AKB_TRIANGLE_3><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
   case AKB_TETRAHEDRON_4: k_qp_forces<AKB_TETRAHEDRON_4><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
-  default: k_qp_forces<AKB_HEXAHEDRON_8><<<blocks_for(m.ne), kThreads, 0, s>>>(m); break;
+  default: k_qp_forces<AKB_HEXAHEDRON_8><<<blocks_for(m.ne * 8), kThreads, 0, s>>>(m); break;
   }
   return cudaGetLastError();
 }
