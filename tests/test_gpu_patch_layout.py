@@ -144,3 +144,36 @@ def test_scrambled_cube(mode, patch):
     mesh = scrambled_cube(10)
     fixed = mesh.nodes[:, 2] < 0.05
     compare(workload(mesh, fixed), mode, 100, **patch)
+
+
+@pytest.mark.parametrize("mode", [_abi.MODE_FP64, _abi.MODE_FP32_BULK], ids=["fp64", "fp32bulk"])
+def test_single_mesh_schedules_match_a_batch_of_one(mode):
+    """A single mesh against a batch holding only that mesh (same patches,
+    the batch's per-instance time step and instance lookups): u, v and a bit
+    for bit, with one CTA per patch and with a persistent grid of 5 CTAs
+    (several patches per CTA, the chunk-record buffers and mbarrier phases
+    carried from patch to patch), and the kinetic energy to rounding."""
+    from akantu_b200.batch import BatchModel
+    mesh = scrambled_cube(10)
+    w = workload(mesh, mesh.nodes[:, 2] < 0.05)
+    patch = dict(patch_elements=256, patch_nodes=160)
+    state = (_abi.FIELD_DISPLACEMENT, _abi.FIELD_VELOCITY, _abi.FIELD_ACCELERATION)
+    ref = BatchModel([mesh], w["materials"], precision=mode, **patch)
+    ref.initFull()
+    ref.setBlockedDOFs(w["blocked"])
+    ref.setField(_abi.FIELD_DISPLACEMENT, w["u0"])
+    ref.setField(_abi.FIELD_VELOCITY, w["v0"])
+    dt = w["dt_factor"] * ref.getStableTimeSteps()
+    ref.setTimeSteps(dt)
+    ref.solveSteps(100)
+    want = {f: np.array(ref.getField(f)) for f in state}
+    ek = ref.getEnergies("kinetic")[0]
+    ref.close()
+    for grid in (0, 5):
+        dev = Gpu(w, mode, patch_grid=grid, **patch)
+        assert configs.setup_model(dev, w) == dt[0]
+        dev.m.solveSteps(100)
+        for f in state:
+            assert np.array_equal(dev.get(f), want[f]), (grid, f)
+        assert abs(dev.m.getEnergy("kinetic") - ek) <= 1e-13 * ek, grid
+        dev.m.close()
