@@ -184,9 +184,13 @@ __global__ void k_qp_forces(DevModel m) {
 }
 
 // comp >= 0: one thread per listed node, that component; comp < 0: one
-// thread per (listed node, component), values row per node.
+// thread per (listed node, component), values row per node. Launched with
+// programmatic serialization behind the step's last kernel, it waits for
+// that grid before touching the node state.
 __global__ void k_apply_dirichlet(DevModel m, const uint32_t* nodes, int64_t n, int comp,
                                   const double* values, const uint32_t* perm, double* w) {
+  grid_wait();
+  grid_launch_dependents();
   int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int ncomp = comp < 0 ? m.dim : 1;
   if (k >= n * ncomp) return;
@@ -206,9 +210,8 @@ __global__ void k_apply_dirichlet(DevModel m, const uint32_t* nodes, int64_t n, 
 cudaError_t apply_dirichlet(const DevModel& m, const uint32_t* nodes, int64_t n, int comp,
                             const double* values, const uint32_t* perm, double* w,
                             cudaStream_t s) {
-  k_apply_dirichlet<<<blocks_for(comp < 0 ? n * m.dim : n), kThreads, 0, s>>>(m, nodes, n, comp,
-                                                                              values, perm, w);
-  return cudaGetLastError();
+  return launch_pdl(k_apply_dirichlet, blocks_for(comp < 0 ? n * m.dim : n), kThreads, 0, s, m,
+                    nodes, n, comp, values, perm, w);
 }
 
 cudaError_t user_qp_gradients(const DevModel& m, cudaStream_t s) {

@@ -13,6 +13,33 @@ namespace akb {
 
 constexpr int kMaxMaterials = 8;
 
+#ifdef __CUDACC__
+// Programmatic dependent launch: a kernel launched by launch_pdl may start
+// while the kernel before it in the stream is finishing. It waits
+// (grid_wait: until that grid has completed and its writes are visible)
+// before it touches memory that grid may use, and signals
+// (grid_launch_dependents) when the kernel after it may start launching.
+__device__ inline void grid_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ inline void grid_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... K, typename... A>
+cudaError_t launch_pdl(void (*kernel)(K...), int grid, int block, size_t smem, cudaStream_t s,
+                       A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+#endif
+
 // Compile-time element properties (ElementClassProperty, element_class_*.hh).
 template <int T> struct ET;
 template <> struct ET<AKB_SEGMENT_2> { static constexpr int dim = 1, nnpe = 2, nqp = 1; };

@@ -159,16 +159,9 @@ constexpr uint32_t kWaitLimit = 1u << 22;
 
 __device__ inline uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Programmatic dependent launch: the step's kernels are launched with
-// programmatic stream serialization, so a kernel's CTAs may start while the
-// kernel before it is finishing. Each waits (grid_wait: until the previous
-// grid has completed and its writes are visible) before it reads anything
-// that kernel writes, and signals (grid_launch_dependents) when the next
-// kernel may start launching.
-__device__ inline void grid_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ inline void grid_launch_dependents() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
+// The step's kernels are launched with programmatic stream serialization
+// (launch_pdl): k_patch_step waits before its first read of the node state,
+// k_finish_list before its first read of the partials.
 __device__ inline void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(mbar)
@@ -801,32 +794,16 @@ inline int grid_of(const DevPatches& p) {
 
 inline int blocks_of(int64_t n) { return (int)((n + kThreads - 1) / kThreads); }
 
-// A launch with programmatic stream serialization (see grid_wait).
-template <typename... K, typename... A>
-cudaError_t launch_pdl(void (*kernel)(K...), int grid, size_t smem, cudaStream_t s, A... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, args...);
-}
-
 template <int T, typename S>
 cudaError_t launch_patch(const DevModel& m, const DevPatches& p, double dt, bool fext,
                          cudaStream_t s) {
   const SmemLayout lay = layout(p, ET<T>::dim, sizeof(S), p.nbuf);
   const int grid = grid_of(p);
   if (grid < p.npatch)
-    return fext ? launch_pdl(k_patch_step<T, S, true, true>, grid, lay.total, s, m, p, dt)
-                : launch_pdl(k_patch_step<T, S, false, true>, grid, lay.total, s, m, p, dt);
-  return fext ? launch_pdl(k_patch_step<T, S, true, false>, grid, lay.total, s, m, p, dt)
-              : launch_pdl(k_patch_step<T, S, false, false>, grid, lay.total, s, m, p, dt);
+    return fext ? launch_pdl(k_patch_step<T, S, true, true>, grid, kThreads, lay.total, s, m, p, dt)
+                : launch_pdl(k_patch_step<T, S, false, true>, grid, kThreads, lay.total, s, m, p, dt);
+  return fext ? launch_pdl(k_patch_step<T, S, true, false>, grid, kThreads, lay.total, s, m, p, dt)
+              : launch_pdl(k_patch_step<T, S, false, false>, grid, kThreads, lay.total, s, m, p, dt);
 }
 
 // The dynamic shared memory limit is an attribute of the kernel function in
@@ -916,12 +893,12 @@ cudaError_t patch_finish_list(const DevModel& m, const DevPatches& p, double dt,
   if (p.nlist <= 0) return cudaSuccess;
   const int blocks = blocks_of(p.nlist * m.dim);
   switch (m.dim) {
-  case 1: return fext ? launch_pdl(k_finish_list<1, true>, blocks, 0, s, m, p, dt)
-                      : launch_pdl(k_finish_list<1, false>, blocks, 0, s, m, p, dt);
-  case 2: return fext ? launch_pdl(k_finish_list<2, true>, blocks, 0, s, m, p, dt)
-                      : launch_pdl(k_finish_list<2, false>, blocks, 0, s, m, p, dt);
-  default: return fext ? launch_pdl(k_finish_list<3, true>, blocks, 0, s, m, p, dt)
-                       : launch_pdl(k_finish_list<3, false>, blocks, 0, s, m, p, dt);
+  case 1: return fext ? launch_pdl(k_finish_list<1, true>, blocks, kThreads, 0, s, m, p, dt)
+                      : launch_pdl(k_finish_list<1, false>, blocks, kThreads, 0, s, m, p, dt);
+  case 2: return fext ? launch_pdl(k_finish_list<2, true>, blocks, kThreads, 0, s, m, p, dt)
+                      : launch_pdl(k_finish_list<2, false>, blocks, kThreads, 0, s, m, p, dt);
+  default: return fext ? launch_pdl(k_finish_list<3, true>, blocks, kThreads, 0, s, m, p, dt)
+                       : launch_pdl(k_finish_list<3, false>, blocks, kThreads, 0, s, m, p, dt);
   }
 }
 

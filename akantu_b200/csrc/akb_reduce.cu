@@ -35,9 +35,15 @@ __device__ inline double block_reduce(double v) {
   return sh[0];
 }
 
+// One block; launched behind the kernel that wrote the partials with
+// programmatic serialization (sum_partials) it waits for that grid first.
+// Each thread combines its partials in index order, eight loads in flight.
 template <Op op>
 __global__ void k_finish(const double* partial, int n, double scale, double* out) {
+  grid_wait();
+  grid_launch_dependents();
   double acc = op == kSum ? 0.0 : DBL_MAX;
+#pragma unroll 8
   for (int i = threadIdx.x; i < n; i += kThreads) acc = combine<op>(acc, partial[i]);
   acc = block_reduce<op>(acc);
   if (threadIdx.x == 0) *out = op == kSum ? acc * scale : acc;
@@ -270,8 +276,7 @@ cudaError_t stable_dt(const DevModel& m, double* scratch, int scratch_len, doubl
 
 cudaError_t sum_partials(const double* partial, int64_t n, double scale, double* out,
                          cudaStream_t s) {
-  k_finish<kSum><<<1, kThreads, 0, s>>>(partial, (int)n, scale, out);
-  return cudaGetLastError();
+  return launch_pdl(k_finish<kSum>, 1, kThreads, 0, s, partial, (int)n, scale, out);
 }
 
 cudaError_t energy(const DevModel& m, int kind, double dt, double* scratch, int scratch_len,
