@@ -591,57 +591,65 @@ __global__ void __launch_bounds__(kThreads, (PatchOccupancy<T, S>::value))
   }
 }
 
-// One (listed node, component) of k_finish_list: the sum of the entry's
-// partials in order (none for a node of no element), then the same finish
-// as in the fused step, from the node's stored w; returns its M v^2 after
-// the step.
-template <int d, bool FEXT>
-__device__ inline double finish_list_dof(const DevModel& m, const DevPatches& P, double dt0,
-                                         int64_t t) {
-  const int64_t e = t / d;
-  const int i = (int)(t - e * d);
-  const bool sh = e < (int64_t)P.nshared;
-  // a single mesh's shared nodes are one block: no index to load
-  const int64_t g = sh && P.shared_contig ? (int64_t)P.shared_base + e : (int64_t)P.list_gid[e];
-  const int64_t q = g * d + i;
-  const uint32_t k = P.list_k[e];
-  const double dt = P.inst_dt ? P.inst_dt[P.list_inst[e]] : dt0;
-  // every load that depends on the entry is issued before the blocked flag
-  // is tested; ranks 0 and 1 are in the dense rows at known addresses
-  const uint8_t bl = m.blocked[q];
-  const double im = m.inv_mass[g], w = P.w[q], fx = FEXT ? m.fext[q] : 0.0;
-  double v = m.v[q], a = m.a[q];
-  double f = 0.0;
-  if (sh) {
-    const double p0 = P.partial[(size_t)e * d + i];
-    const double p1 = P.partial[((size_t)P.nshared + e) * d + i];  // zero when k = 1
-    f += p0;
-    if (k > 1) f += p1;
-    if (k > 2) {
-      const uint32_t over = P.list_part[e];
-      for (uint32_t r = 2; r < k; ++r) f += P.partial[(size_t)(over + r - 2) * d + i];
-    }
-  }
-  if (bl) return ke_term(v, im);
-  double u, wn;
-  finish_dof(dt, FEXT ? f + fx : f, im, w, v, a, u, wn);
-  m.u[q] = u;
-  m.v[q] = v;
-  m.a[q] = a;
-  P.w[q] = wn;
-  return ke_term(v, im);
-}
-
-// Listed nodes, one thread per (entry, component), and the block's sum of
-// M v^2 (a kinetic-energy partial).
+// Listed nodes, one thread per (entry, component): the sum of the entry's
+// partials in rank order (none for a node of no element), then the same
+// finish as in the fused step, from the node's stored w; and the block's sum
+// of M v^2 after the step (a kinetic-energy partial). The entry's own state
+// (v, a, w, 1/M, blocked flag, f_ext) is not written by the fused step, and
+// every kernel before the fused step has completed when this grid launches
+// (the fused step waited for them before letting it launch): it is loaded
+// before waiting for the fused step, through L2 (no L1 line of an earlier
+// grid), so only the partials wait.
 template <int D, bool FEXT>
 __global__ void k_finish_list(DevModel m, DevPatches P, double dt0) {
   constexpr int d = D;
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool on = t < P.nlist * d;
+  const int64_t e = on ? t / d : 0;
+  const int i = (int)(t - e * d);
+  const bool sh = on && e < (int64_t)P.nshared;
+  int64_t q = 0;
+  uint32_t k = 0;
+  uint8_t bl = 1;
+  double dt = dt0, im = 1.0, w = 0.0, fx = 0.0, v = 0.0, a = 0.0;
+  if (on) {
+    // a single mesh's shared nodes are one block: no index to load
+    const int64_t g = sh && P.shared_contig ? (int64_t)P.shared_base + e : (int64_t)P.list_gid[e];
+    q = g * d + i;
+    k = P.list_k[e];
+    if (P.inst_dt) dt = P.inst_dt[P.list_inst[e]];
+    bl = __ldcg(m.blocked + q);
+    im = __ldcg(m.inv_mass + g);
+    w = __ldcg(P.w + q);
+    if (FEXT) fx = __ldcg(m.fext + q);
+    v = __ldcg(m.v + q);
+    a = __ldcg(m.a + q);
+  }
   grid_wait();               // the fused step's partials
   grid_launch_dependents();  // the next step may start launching (it waits for this grid)
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double ke = 0.0;
-  if (t < P.nlist * d) ke = finish_list_dof<d, FEXT>(m, P, dt0, t);
+  if (on) {
+    double f = 0.0;
+    if (sh) {  // ranks 0 and 1 in the dense rows at known addresses
+      const double p0 = P.partial[(size_t)e * d + i];
+      const double p1 = P.partial[((size_t)P.nshared + e) * d + i];  // zero when k = 1
+      f += p0;
+      if (k > 1) f += p1;
+      if (k > 2) {
+        const uint32_t over = P.list_part[e];
+        for (uint32_t r = 2; r < k; ++r) f += P.partial[(size_t)(over + r - 2) * d + i];
+      }
+    }
+    if (!bl) {
+      double u, wn;
+      finish_dof(dt, FEXT ? f + fx : f, im, w, v, a, u, wn);
+      m.u[q] = u;
+      m.v[q] = v;
+      m.a[q] = a;
+      P.w[q] = wn;
+    }
+    ke = ke_term(v, im);
+  }
   if (P.ke_part) {
     __shared__ double warp_sums[kThreads / 32];
     const double s = cta_sum(ke, warp_sums);
