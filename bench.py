@@ -837,7 +837,7 @@ def SolidMechanicsModel_for(w, i, device, opts):
 def run_reference(args, dist):
     if dist.rank != 0:
         return None
-    w = configs.cube_tet4()
+    w = configs.cube_tet4(args.cells)
     from oracle.oracle import OracleModel, material_desc
     threads = os.cpu_count() or 1
     m = OracleModel(w["mesh"], [material_desc(**mm) for mm in w["materials"]], fast=True)
@@ -846,21 +846,25 @@ def run_reference(args, dist):
     m.velocity[...] = w["v0"]
     dt = w["dt_factor"] * m.stable_time_step()
     m.set_time_step(dt)
-    warm = min(args.warmup, 3)  # at least 3 (main raises W to 3); more only costs time
+    warm = args.warmup  # at least 3 (main raises W to 3)
     m.time_steps(warm)
     steps = min(args.steps, 40)
     t = m.time_steps(steps)
     E = w["mesh"].getNbElement()
+    N = w["mesh"].getNbNodes()
+    c = args.cells
     value = E * steps / t
     if dist.world > 1:  # our arm: the cube stacked once per GPU as one mesh
-        workload = ("bar_tet4: 100 x 100 x %d cells x 6 tetrahedron_4 (%d elements), linear "
-                    "elastic, FP64" % (100 * dist.world, E * dist.world))
-        sample = ("%d of the requested %d steps on one of the bar's %d cubes (6,000,000 "
+        workload = ("bar_tet4: %d x %d x %d cells x 6 tetrahedron_4 (%d elements, %d nodes), "
+                    "linear elastic, FP64, dt = 0.8 x stable"
+                    % (c, c, c * dist.world, E * dist.world, (c + 1) ** 2 * (c * dist.world + 1)))
+        sample = ("%d of the requested %d steps on one of the bar's %d cubes (%d "
                   "elements; every cube has the same CPU rate per element-step; the "
-                  "reference cannot be built: Boost is absent)" % (steps, args.steps, dist.world))
+                  "reference cannot be built: Boost is absent)"
+                  % (steps, args.steps, dist.world, E))
     else:
-        workload = ("cube_tet4: 100^3 cells x 6 tetrahedron_4 (6,000,000 elements, 1,030,301 "
-                    "nodes), linear elastic, FP64")
+        workload = ("cube_tet4: %d^3 cells x 6 tetrahedron_4 (%d elements, %d nodes), "
+                    "linear elastic, FP64, dt = 0.8 x stable" % (c, E, N))
         sample = ("%d of the requested %d steps on the full mesh (the reference cannot be "
                   "built: Boost is absent)" % (steps, args.steps))
     return {
