@@ -115,13 +115,40 @@ def material_from_dict(d):
                        finite_deformation=d.get("finite_deformation", False))))
 
 
+# axes of the Dirichlet functors (BC::Axis, boundary_condition_functor.hh)
+_x, _y, _z = 0, 1, 2
+
+
+class FixedValue:
+    """BC::Dirichlet::FixedValue(value, axis)
+    (boundary_condition_functor_inline_impl.hh:85-93): the axis blocked,
+    the displacement set to value."""
+
+    def __init__(self, value, axis):
+        self.value, self.axis = float(value), int(axis)
+
+
+class FreeBoundary:
+    """BC::Dirichlet::FreeBoundary(axis): the axis unblocked."""
+
+    def __init__(self, axis):
+        self.axis = int(axis)
+
+
 class SolidMechanicsModel:
     """The explicit lumped-mass SolidMechanicsModel on one GPU."""
 
     def __init__(self, mesh, materials=None, element_material=None,
-                 precision=_abi.MODE_FP64_REFERENCE, device=0, stream=None,
+                 precision=None, device=0, stream=None,
                  patch_elements=0, patch_nodes=0, interface_nodes=None, patch_grid=0):
-        """interface_nodes: this model is one part of a partitioned mesh
+        """materials: the model's materials; none given, initFull takes them
+        from the sections of the last parseInput (the reference's
+        SolidMechanicsModel(mesh)), laws written in Python included
+        (akantu_b200.material_plugin). element_material: the material of
+        each element (default: the first material, the reference's default
+        selector). precision: AKB_MODE_*; default AKB_MODE_FP64_REFERENCE,
+        or AKB_MODE_FP64 for laws written in Python (their only mode).
+        interface_nodes: this model is one part of a partitioned mesh
         (akb_model_create_part), these of its nodes are shared with other
         parts; step it through akantu_b200.decompose.DistributedModel.
         patch_elements, patch_nodes, patch_grid: the fused step's patch shape
@@ -142,6 +169,8 @@ class SolidMechanicsModel:
         self._views = {}
         self._checked_out = set()
         self._blocked = None
+        self._laws = None  # material_plugin.LawBridge of laws written in Python
+        self._qp_weights = None
 
     # -- initialisation --------------------------------------------------
     def addMaterial(self, material):
@@ -153,7 +182,9 @@ class SolidMechanicsModel:
         if precision is not None:
             self._precision = precision
         if not self._materials:
-            raise ValueError("no material: add one with addMaterial()")
+            self._materials_from_input()
+        if self._precision is None:
+            self._precision = _abi.MODE_FP64_REFERENCE
         L = lib()
         self._nodes = np.ascontiguousarray(self.mesh.nodes, dtype=np.float64)
         self._conn = np.ascontiguousarray(self.mesh.connectivity, dtype=np.uint32)
@@ -181,6 +212,56 @@ class SolidMechanicsModel:
                                           self._iface.ctypes.data_as(C.POINTER(C.c_uint32)),
                                           self._iface.size, C.byref(h)))
         self._h = h
+
+    def _materials_from_input(self):
+        """The materials of the last parseInput's sections: the laws the
+        library computes become device materials, the others are allocated
+        by MaterialFactory and run in Python (material_plugin.LawBridge)."""
+        from . import material_plugin as mp
+        sections = mp.input_sections()
+        if not sections:
+            raise ValueError("no material: pass materials, addMaterial() or parseInput() first")
+        if self._element_material is None:
+            self._element_material = np.zeros(self.mesh.getNbElement(), dtype=np.uint32)
+        builtin = [law in mp.BUILTIN_LAWS for law, _ in sections]
+        if all(builtin):
+            for law, prm in sections:
+                cls = MaterialNeohookean if law == "neohookean" else MaterialElastic
+                kw = {} if cls is MaterialNeohookean else dict(
+                    Plane_Stress=bool(prm.get("Plane_Stress", False)),
+                    finite_deformation=bool(prm.get("finite_deformation", False)))
+                self._materials.append(cls(rho=prm["rho"], E=prm["E"], nu=prm.get("nu", 0.0),
+                                           name=str(prm.get("name", law)), **kw))
+            return
+        if any(builtin):
+            raise ValueError("laws written in Python and built-in laws in one model: the "
+                             "library steps a model with either kind, not both")
+        laws = [mp.law_from_section(law, prm, k, self.dim, self)
+                for k, (law, prm) in enumerate(sections)]
+        self._laws = mp.LawBridge(laws, self._element_material, self.mesh.element_type,
+                                  self.nqp, self.dim)
+        for law in laws:
+            law.initMaterial()
+            # the library's wave speed sqrt((lambda + 2 mu) / rho) with nu = 0
+            # is sqrt(E / rho): E = rho c^2 carries the law's push wave speed
+            c = float(law.getPushWaveSpeed(None))
+            rho = law.getReal("rho")
+            self._materials.append(MaterialUser(rho=rho, E=rho * c * c, nu=0.0,
+                                                finite_deformation=law.finite_deformation,
+                                                name=law.name))
+        if self._precision is None:
+            self._precision = _abi.MODE_FP64
+
+    def getMaterial(self, key):
+        """The material with this index or name (a law written in Python: its
+        Material object)."""
+        laws = self._laws.laws if self._laws is not None else self._materials
+        if isinstance(key, str):
+            for m in laws:
+                if m.name == key:
+                    return m
+            raise KeyError("no material named %r" % key)
+        return laws[key]
 
     def __del__(self):
         self.close()
@@ -286,6 +367,21 @@ class SolidMechanicsModel:
                                         n.size, int(component),
                                         v.ctypes.data_as(C.POINTER(C.c_double))))
 
+    def applyBC(self, functor, group):
+        """applyBC(functor, group) (py_solid_mechanics_model.cc:58-63,
+        boundary_condition_tmpl.hh:63-200) on the nodes of a mesh group
+        (the node group of a `$PhysicalNames` group, or one created with
+        Mesh.createNodeGroup): FixedValue(value, axis) blocks the axis and
+        sets the displacement, FreeBoundary(axis) unblocks it."""
+        nodes = self.mesh.getNodeGroup(group) if isinstance(group, str) else np.asarray(group)
+        if isinstance(functor, FixedValue):
+            self.applyDirichlet(nodes, functor.axis, functor.value)
+        elif isinstance(functor, FreeBoundary):
+            b = self.getBlockedDOFs()
+            b[np.asarray(nodes, dtype=np.int64), functor.axis] = False
+        else:
+            raise TypeError("applyBC takes FixedValue or FreeBoundary")
+
     def getGradU(self):
         return self.getField(_abi.FIELD_GRAD_U)
 
@@ -314,8 +410,11 @@ class SolidMechanicsModel:
         self._sync_in()
         if self._user:
             self.stepBegin()
-            self._user[0].computeStress(self.deviceTensor(_abi.FIELD_GRAD_U),
-                                        self.deviceTensor(_abi.FIELD_STRESS))
+            G, S = self.deviceTensor(_abi.FIELD_GRAD_U), self.deviceTensor(_abi.FIELD_STRESS)
+            if self._laws is not None:
+                self._laws.stresses(G, S)
+            else:
+                self._user[0].computeStress(G, S)
             self.stepEnd()
             return
         check(lib().akb_solve_step(self.handle))
@@ -377,6 +476,11 @@ class SolidMechanicsModel:
 
     def getEnergy(self, energy_id):
         self._sync_in()
+        if self._laws is not None and energy_id == "potential":
+            from .material_plugin import qp_weights
+            if self._qp_weights is None:
+                self._qp_weights = qp_weights(self.mesh)
+            return self._laws.potential_energy(self._qp_weights)
         v = C.c_double()
         check(lib().akb_get_energy(self.handle, _ENERGY[energy_id], C.byref(v)))
         return v.value
