@@ -8,9 +8,9 @@ Material::computeStress) on one GPU. The compute runs in libakb.so
 from . import _abi
 from ._abi import (MODE_FP32_BULK, MODE_FP64, MODE_FP64_REFERENCE, HEXAHEDRON_8,
                    SEGMENT_2, TETRAHEDRON_4, TRIANGLE_3)
-from .material_plugin import (Material, MaterialFactory, _ghost, _not_ghost, _pat_internal,
-                              _pat_modifiable, _pat_parsable, _pat_parsmod, _pat_readable,
-                              _pat_writable, parseInput)
+from .material_plugin import (Material, MaterialFactory, MeshDataMaterialSelectorString, _ghost,
+                              _not_ghost, _pat_internal, _pat_modifiable, _pat_parsable,
+                              _pat_parsmod, _pat_readable, _pat_writable, parseInput)
 from .mesh import Mesh
 from .model import (FixedValue, FreeBoundary, MaterialElastic, MaterialNeohookean, MaterialUser,
                     SolidMechanicsModel, _explicit_lumped_mass, _x, _y, _z)
@@ -21,6 +21,7 @@ _tetrahedron_4 = TETRAHEDRON_4
 _hexahedron_8 = HEXAHEDRON_8
 
 __all__ = ["Mesh", "SolidMechanicsModel", "MaterialElastic", "MaterialNeohookean", "MaterialUser",
-           "Material", "MaterialFactory", "parseInput", "FixedValue", "FreeBoundary",
+           "Material", "MaterialFactory", "MeshDataMaterialSelectorString", "parseInput",
+           "FixedValue", "FreeBoundary",
            "_explicit_lumped_mass", "_x", "_y", "_z", "_not_ghost", "_ghost",
            "MODE_FP64_REFERENCE", "MODE_FP64", "MODE_FP32_BULK"]

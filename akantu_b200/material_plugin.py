@@ -227,10 +227,11 @@ class Material:
     @property
     def element_filter(self):
         """Callable (type, ghost_type) -> indices of the material's elements."""
-        def f(type, ghost_type=_not_ghost):
-            self._check(type, ghost_type)
-            return self._elements
-        return f
+        return self.getElementFilter
+
+    def getElementFilter(self, type, ghost_type=_not_ghost):
+        self._check(type, ghost_type)
+        return self._elements
 
     # -- to override --------------------------------------------------------
     def initMaterial(self):
@@ -266,6 +267,35 @@ class Material:
         self._grad_u = np.zeros((self._npoints, dim * dim))
         self._stress = np.zeros((self._npoints, dim * dim))
         self._energy = np.zeros((self._npoints, 1))
+
+
+class MeshDataMaterialSelectorString:
+    """MeshDataMaterialSelector<std::string>("physical_names", model)
+    (material_selector.hh:151, material_selector_tmpl.hh): an element whose
+    physical group (`$PhysicalNames`) names a material of the model takes
+    that material, any other element the fallback (material 0 unless
+    setFallback says otherwise)."""
+
+    def __init__(self, name, model, first_index=1):
+        if name != "physical_names":
+            raise ValueError("mesh data '%s': the meshes here carry physical_names only" % name)
+        self.model = model
+        self.first_index = first_index
+        self.fallback = 0
+
+    def setFallback(self, fallback):
+        self.fallback = int(fallback)
+
+    def select(self, material_names):
+        """The material index of every element, for materials with these
+        names in model order."""
+        mesh = self.model.mesh
+        index = {n: k for k, n in enumerate(material_names)}
+        em = np.full(mesh.getNbElement(), self.fallback, dtype=np.uint32)
+        for group, elements in mesh.element_groups.items():
+            if group in index:
+                em[np.asarray(elements, dtype=np.int64)] = index[group]
+        return em
 
 
 def law_from_section(law, params, index, dim, model):

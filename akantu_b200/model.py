@@ -50,6 +50,20 @@ class Material:
     def getReal(self, key):
         return self.params[key]
 
+    def getElementFilter(self, el_type, ghost_type=0):
+        """Indices of the elements of this material (set by the model's
+        initFull; Material::getElementFilter)."""
+        if ghost_type != 0:
+            raise ValueError("a single GPU holds no ghost elements")
+        elements = getattr(self, "_elements", None)
+        if elements is None:
+            raise RuntimeError("the material belongs to no initialised model")
+        return elements
+
+    @property
+    def element_filter(self):
+        return self.getElementFilter
+
     def desc(self):
         p = self.params
         return _abi.MaterialDesc(self.kind, int(p["Plane_Stress"]),
@@ -171,10 +185,17 @@ class SolidMechanicsModel:
         self._blocked = None
         self._laws = None  # material_plugin.LawBridge of laws written in Python
         self._qp_weights = None
+        self._selector = None
 
     # -- initialisation --------------------------------------------------
     def addMaterial(self, material):
         self._materials.append(material)
+
+    def setMaterialSelector(self, selector):
+        """setMaterialSelector (solid_mechanics_model.hh): the element ->
+        material map initFull takes, e.g. a
+        material_plugin.MeshDataMaterialSelectorString."""
+        self._selector = selector
 
     def initFull(self, _analysis_method=_explicit_lumped_mass, precision=None):
         if _analysis_method != _explicit_lumped_mass:
@@ -183,8 +204,14 @@ class SolidMechanicsModel:
             self._precision = precision
         if not self._materials:
             self._materials_from_input()
+        elif self._selector is not None and self._element_material is None:
+            self._element_material = self._selector.select([m.name for m in self._materials])
         if self._precision is None:
             self._precision = _abi.MODE_FP64_REFERENCE
+        em = (np.zeros(self.mesh.getNbElement(), dtype=np.int64) if self._element_material is None
+              else np.asarray(self._element_material, dtype=np.int64))
+        for k, m in enumerate(self._materials):
+            m._elements = np.nonzero(em == k)[0]
         L = lib()
         self._nodes = np.ascontiguousarray(self.mesh.nodes, dtype=np.float64)
         self._conn = np.ascontiguousarray(self.mesh.connectivity, dtype=np.uint32)
@@ -222,7 +249,12 @@ class SolidMechanicsModel:
         if not sections:
             raise ValueError("no material: pass materials, addMaterial() or parseInput() first")
         if self._element_material is None:
-            self._element_material = np.zeros(self.mesh.getNbElement(), dtype=np.uint32)
+            if self._selector is not None:
+                names = [str(prm.get("name", "%s_%d" % (law, k)))
+                         for k, (law, prm) in enumerate(sections)]
+                self._element_material = self._selector.select(names)
+            else:  # the default selector: every element takes the first material
+                self._element_material = np.zeros(self.mesh.getNbElement(), dtype=np.uint32)
         builtin = [law in mp.BUILTIN_LAWS for law, _ in sections]
         if all(builtin):
             for law, prm in sections:
@@ -230,7 +262,8 @@ class SolidMechanicsModel:
                 kw = {} if cls is MaterialNeohookean else dict(
                     Plane_Stress=bool(prm.get("Plane_Stress", False)),
                     finite_deformation=bool(prm.get("finite_deformation", False)))
-                self._materials.append(cls(rho=prm["rho"], E=prm["E"], nu=prm.get("nu", 0.0),
+                self._materials.append(cls(rho=prm.get("rho", 0.0), E=prm.get("E", 0.0),
+                                           nu=prm.get("nu", 0.5),  # the reference's default
                                            name=str(prm.get("name", law)), **kw))
             return
         if any(builtin):
@@ -251,6 +284,13 @@ class SolidMechanicsModel:
                                                 name=law.name))
         if self._precision is None:
             self._precision = _abi.MODE_FP64
+
+    def getMaterialIndex(self, name):
+        laws = self._laws.laws if self._laws is not None else self._materials
+        for k, m in enumerate(laws):
+            if m.name == name:
+                return k
+        raise KeyError("no material named %r" % name)
 
     def getMaterial(self, key):
         """The material with this index or name (a law written in Python: its

@@ -137,3 +137,27 @@ def test_distorted_hexahedra():
     assert got[0] == pytest.approx(want[0], rel=1e-14)
     assert rel(got[1], want[1]) <= 1e-10 and rel(got[2], want[2]) <= 1e-10
     assert np.abs(got[3] - want[3]).max() <= 1e-10 * np.abs(want[3]).max()
+
+
+def test_material_selector_in_a_model():
+    """setMaterialSelector with the physical names, as
+    test_material_selector.cc (with the densities the library needs): each
+    segment of material_selector.msh takes the built-in elastic material of
+    its group's name, seen through getMaterial(name).getElementFilter."""
+    mesh = aka.Mesh(1)
+    mesh.read(os.path.join(os.path.dirname(__file__), "golden", "msh", "material_selector.msh"))
+    mp.parse_input_text("material elastic [ name = chocolate\n rho = 1\n E = 2\n nu = 0 ]\n"
+                        "material elastic [ name = chewing-gum\n rho = 1\n E = 1\n nu = 0 ]\n"
+                        "material elastic [ name = candy\n rho = 1\n E = 3\n nu = 0 ]\n")
+    model = aka.SolidMechanicsModel(mesh)
+    model.setMaterialSelector(aka.MeshDataMaterialSelectorString("physical_names", model))
+    model.initFull(_analysis_method=aka._explicit_lumped_mass)
+    for name, element in (("chocolate", 0), ("chewing-gum", 1), ("candy", 2)):
+        assert model.getMaterial(name).getElementFilter(aka._segment_2).tolist() == [element]
+        assert model.getMaterialIndex(name) == element
+    # the stable step: each segment's length over its own material's wave speed
+    x = mesh.getNodes()[:, 0]
+    lengths = np.abs(x[mesh.connectivity[:, 1]] - x[mesh.connectivity[:, 0]])
+    assert model.getStableTimeStep() == pytest.approx((lengths / np.sqrt([2.0, 1.0, 3.0])).min(),
+                                                      rel=1e-12)
+    model.close()

@@ -188,3 +188,24 @@ def test_quadrature_weights():
     w = mp.qp_weights(Mesh(3, _abi.HEXAHEDRON_8, x, np.arange(8, dtype=np.uint32)[None]))
     assert w.sum() == pytest.approx(hex_volume_3x3x3(x), rel=1e-13)
     assert all(w[q | 1] > w[q & ~1] for q in range(8))
+
+
+def test_material_selector_by_physical_names():
+    """test_material_selector.cc on its own mesh: the segments of the
+    physical groups chocolate, chewing-gum and candy take the materials of
+    those names (material_selector.dat order: chocolate, chewing-gum,
+    candy); an element of no named material takes the fallback."""
+    import os
+
+    class ModelLike:  # the selector reads the model's mesh only
+        mesh = Mesh(1)
+    ModelLike.mesh.read(os.path.join(os.path.dirname(__file__), "golden", "msh",
+                                     "material_selector.msh"))
+    sel = mp.MeshDataMaterialSelectorString("physical_names", ModelLike)
+    em = sel.select(["chocolate", "chewing-gum", "candy"])
+    first = {k: int(np.nonzero(em == k)[0][0]) for k in range(3)}
+    assert first == {0: 0, 1: 1, 2: 2}
+    sel.setFallback(1)
+    assert sel.select(["chocolate"]).tolist() == [0, 1, 1]
+    with pytest.raises(ValueError):
+        mp.MeshDataMaterialSelectorString("tag_0", ModelLike)
