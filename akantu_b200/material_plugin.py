@@ -46,6 +46,8 @@ _sections = []  # [(law, {key: value})] of the last parseInput
 
 def _value(text):
     t = text.strip()
+    if t.startswith("[") and t.endswith("]"):  # a vector parameter
+        return [_value(x) for x in t[1:-1].split(",") if x.strip()]
     if t.lower() in ("true", "false"):
         return t.lower() == "true"
     try:
@@ -54,36 +56,58 @@ def _value(text):
         return t
 
 
+_OPEN = re.compile(r"([A-Za-z_]\w*)(?:[ \t\r\n]+([A-Za-z_][\w:.-]*))?[ \t\r\n]*\[")
+_KEY = re.compile(r"([A-Za-z_]\w*)[ \t]*=[ \t]*")
+
+
 def parse_input_text(text):
     """The `material <law> [ key = value ... ]` sections of an Akantu input
-    file (Parser::parse, src/io/parser/): `#` comments, sections nested in
-    other sections, values read as numbers, true/false or plain strings.
+    file (Parser::parse, src/io/parser/): `#` comments, white space and line
+    breaks anywhere between tokens, sections nested in other sections, a
+    value up to the end of its line (or the section's closing bracket) read
+    as a number, true/false, a vector `[a, b, ...]` or a plain string.
     Replaces the sections of an earlier call; returns them."""
     global _sections
+    body = "\n".join(line.split("#", 1)[0] for line in text.splitlines())
     found, stack = [], []  # stack: (kind, law, params) of the open sections
-    for raw in text.splitlines():
-        line = raw.split("#", 1)[0].strip()
-        while line:
-            m = re.match(r"^([A-Za-z_]\w*)(?:\s+([A-Za-z_][\w:.-]*))?\s*\[", line)
-            if m:
-                stack.append((m.group(1), m.group(2) or "", {}))
-                line = line[m.end():].strip()
-                continue
-            if line.startswith("]"):
-                if not stack:
-                    raise ValueError("unbalanced ']' in the input")
-                kind, law, params = stack.pop()
-                if kind == "material":
-                    if not law:
-                        raise ValueError("material section without a law")
-                    found.append((law, params))
-                line = line[1:].strip()
-                continue
-            m = re.match(r"^([A-Za-z_]\w*)\s*=\s*([^\]]*)", line)
-            if not m or not stack:
-                raise ValueError("cannot read input line: %r" % raw)
-            stack[-1][2][m.group(1)] = _value(m.group(2))
-            line = line[m.end():].strip()
+    pos, n = 0, len(body)
+    while True:
+        while pos < n and body[pos].isspace():
+            pos += 1
+        if pos >= n:
+            break
+        if body[pos] == "]":
+            if not stack:
+                raise ValueError("unbalanced ']' in the input")
+            kind, law, params = stack.pop()
+            if kind == "material":
+                if not law:
+                    raise ValueError("material section without a law")
+                found.append((law, params))
+            pos += 1
+            continue
+        m = _KEY.match(body, pos)
+        if m and stack:
+            start = m.end()
+            if body.startswith("[", start):  # a vector value: to its bracket
+                end = body.find("]", start)
+                if end < 0:
+                    raise ValueError("unterminated vector value of '%s'" % m.group(1))
+                end += 1
+            else:
+                end = start
+                while end < n and body[end] not in "\n]":
+                    end += 1
+            stack[-1][2][m.group(1)] = _value(body[start:end])
+            pos = end
+            continue
+        m = _OPEN.match(body, pos)
+        if m:
+            stack.append((m.group(1), m.group(2) or "", {}))
+            pos = m.end()
+            continue
+        line = body[pos:].split("\n", 1)[0]
+        raise ValueError("cannot read the input at: %r" % line)
     if stack:
         raise ValueError("unterminated section '%s %s'" % stack[-1][:2])
     _sections = found

@@ -34,6 +34,11 @@ def test_input_sections():
                                     Plane_Stress=True)),
                    ("my_law", dict(name="soft", rho=1.0))]
     assert mp.input_sections() == got
+    # brackets on their own lines, a vector value, a value closed by the bracket
+    got = mp.parse_input_text("material neohookean\n[\n  name = rubber\n  rho = 1100\n"
+                              "  direction = [1, 0, -2.5]\n  E = 1e6 ]\n")
+    assert got == [("neohookean", dict(name="rubber", rho=1100.0, direction=[1.0, 0.0, -2.5],
+                                       E=1e6))]
     assert mp.parse_input_text("") == [] and mp.input_sections() == []  # replaced, and cleared
     for bad in ("material elastic [ rho = 1", "]", "material [ rho = 1 ]", "rho = 1"):
         with pytest.raises(ValueError):
