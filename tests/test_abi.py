@@ -50,3 +50,22 @@ def test_null_arguments_are_rejected_without_gpu():
     assert L.akb_model_create(None, 1, None, None, None, None) == _abi.AKB_ERR_INVALID_ARGUMENT
     assert L.akb_solve_steps(None, 3) == _abi.AKB_ERR_INVALID_ARGUMENT
     assert b"null" in L.akb_last_error()
+
+
+@pytest.mark.parametrize("header", ["akb.h", "akb_fe2.h", "akb_mesh.h"])
+@pytest.mark.parametrize("lang", [("gcc", "-std=c99", "c"), ("g++", "-std=c++11", "c++")],
+                         ids=["c99", "c++11"])
+def test_header_compiles_as_c_and_cpp(header, lang, tmp_path):
+    """Each C-ABI header stands alone as pedantic C99 (what a cgo, JNI or
+    ctypes binding parses) and C++11, without warnings."""
+    import shutil
+    import subprocess
+    cc, std, xlang = lang
+    if shutil.which(cc) is None:
+        pytest.skip(cc + " not found")
+    src = tmp_path / "use.c"
+    src.write_text('#include "%s"\nint main(void) { return 0; }\n' % header)
+    r = subprocess.run([cc, std, "-x", xlang, "-Wall", "-Wextra", "-pedantic", "-Werror",
+                        "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
