@@ -69,3 +69,18 @@ def test_header_compiles_as_c_and_cpp(header, lang, tmp_path):
                         "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_integration_guide_matches_the_headers():
+    """INTEGRATION.md names every entry point the headers declare, and no
+    akb_ name the headers do not have (globs like akb_mlp_* aside)."""
+    import glob
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    headers = "".join(open(f).read() for f in sorted(glob.glob(os.path.join(ROOT, "include",
+                                                                          "*.h"))))
+    in_headers = set(re.findall(r"\b(akb_[a-z0-9_]+)\b", headers))
+    mentioned = {n for n in re.findall(r"\b(akb_[a-z0-9_]+)(?!\*)\b", doc)
+                 if not n.endswith("_")}
+    mentioned -= {"akb_fe2", "akb_mesh", "akb_msh", "akb_model"}  # file and type stems
+    assert sorted(mentioned - in_headers) == []
+    assert sorted(set(declared_symbols()) - mentioned) == []
