@@ -21,6 +21,7 @@ point order, for the material's own elements only; getPotentialEnergy is
 (points, 1).
 """
 import re
+import weakref
 
 import numpy as np
 
@@ -181,7 +182,9 @@ class Material:
     getPushWaveSpeed as the reference's Python materials do."""
 
     def __init__(self, model, _id):
-        self._model = model
+        # the model holds its laws: a weak reference back avoids a cycle that
+        # would delay freeing the model's device memory
+        self._model = weakref.ref(model) if model is not None else None
         self.id = _id
         self.name = str(_id)
         self._params = {}
@@ -217,7 +220,7 @@ class Material:
         self._params[name] = float(value)
 
     def getModel(self):
-        return self._model
+        return self._model() if self._model is not None else None
 
     # -- the fields of the material's quadrature points --------------------
     def _check(self, el_type, ghost_type):

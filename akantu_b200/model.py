@@ -11,6 +11,7 @@ in-place edits of the returned arrays reach the model as in the reference.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -63,6 +64,29 @@ class Material:
     @property
     def element_filter(self):
         return self.getElementFilter
+
+    def getGradU(self, el_type, ghost_type=0):
+        """The displacement gradient at this material's quadrature points
+        (Material::getGradU): (points, d*d), rows of column-major matrices
+        as the reference's bindings hand them out, the material's elements
+        in order; a copy of the model's field at the current displacement."""
+        return self._rows(_abi.FIELD_GRAD_U, el_type, ghost_type)
+
+    def getStress(self, el_type, ghost_type=0):
+        """The stress at this material's quadrature points (Material::getStress),
+        laid out as getGradU."""
+        return self._rows(_abi.FIELD_STRESS, el_type, ghost_type)
+
+    def _rows(self, field, el_type, ghost_type):
+        ref = getattr(self, "_model", None)
+        model = ref() if ref is not None else None  # a weak reference: no cycle
+        if model is None:
+            raise RuntimeError("the material belongs to no initialised model")
+        if el_type != model.mesh.element_type:
+            raise ValueError("the material has no elements of type %r" % (el_type,))
+        elements = self.getElementFilter(el_type, ghost_type)
+        rows = (elements[:, None] * model.nqp + np.arange(model.nqp)[None, :]).reshape(-1)
+        return model.getField(field)[rows]
 
     def desc(self):
         p = self.params
@@ -212,6 +236,7 @@ class SolidMechanicsModel:
               else np.asarray(self._element_material, dtype=np.int64))
         for k, m in enumerate(self._materials):
             m._elements = np.nonzero(em == k)[0]
+            m._model = weakref.ref(self)
         L = lib()
         self._nodes = np.ascontiguousarray(self.mesh.nodes, dtype=np.float64)
         self._conn = np.ascontiguousarray(self.mesh.connectivity, dtype=np.uint32)

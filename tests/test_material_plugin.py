@@ -214,3 +214,30 @@ def test_material_selector_by_physical_names():
     assert sel.select(["chocolate"]).tolist() == [0, 1, 1]
     with pytest.raises(ValueError):
         mp.MeshDataMaterialSelectorString("tag_0", ModelLike)
+
+
+def test_builtin_material_views():
+    """getGradU / getStress of a built-in material: the rows of the model's
+    quadrature field (column-major matrices) that belong to its elements,
+    every Gauss point of each, in element order."""
+    from akantu_b200.model import MaterialElastic
+
+    class ModelLike:
+        mesh = Mesh(3, _abi.HEXAHEDRON_8, np.zeros((8, 3)), np.zeros((3, 8), dtype=np.uint32))
+        nqp, dim = 8, 3
+
+        @staticmethod
+        def getField(field):
+            base = 1000.0 if field == _abi.FIELD_STRESS else 0.0
+            return base + np.arange(3 * 8 * 9, dtype=float).reshape(3 * 8, 9)
+
+    m = MaterialElastic(rho=1.0, E=1.0, nu=0.3)
+    with pytest.raises(RuntimeError):
+        m.getGradU(_abi.HEXAHEDRON_8)
+    m._model, m._elements = (lambda: ModelLike), np.array([0, 2])  # as the weak reference
+    g = m.getGradU(_abi.HEXAHEDRON_8)
+    assert g.shape == (16, 9)
+    assert np.array_equal(g, ModelLike.getField(_abi.FIELD_GRAD_U)[list(range(8)) + list(range(16, 24))])
+    assert np.array_equal(m.getStress(_abi.HEXAHEDRON_8), 1000.0 + g)
+    with pytest.raises(ValueError):
+        m.getStress(_abi.TETRAHEDRON_4)
