@@ -15,6 +15,19 @@ from .mesh import Mesh
 from .model import (FixedValue, FreeBoundary, MaterialElastic, MaterialNeohookean, MaterialUser,
                     SolidMechanicsModel, _explicit_lumped_mass, _x, _y, _z)
 
+
+
+def initialize(*args, **kwargs):
+    """Kept for scripts written against older interfaces: as in the
+    reference's Python package, there is nothing to initialise; an input
+    file is read with parseInput."""
+    raise RuntimeError("initialize is not needed: read an input file with parseInput")
+
+
+def finalize(*args, **kwargs):
+    raise RuntimeError("finalize is not needed")
+
+
 _segment_2 = SEGMENT_2
 _triangle_3 = TRIANGLE_3
 _tetrahedron_4 = TETRAHEDRON_4

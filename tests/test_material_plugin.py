@@ -241,3 +241,10 @@ def test_builtin_material_views():
     assert np.array_equal(m.getStress(_abi.HEXAHEDRON_8), 1000.0 + g)
     with pytest.raises(ValueError):
         m.getStress(_abi.TETRAHEDRON_4)
+
+
+def test_initialize_points_to_parse_input():
+    import akantu_b200 as aka
+    for f in (aka.initialize, aka.finalize):
+        with pytest.raises(RuntimeError):
+            f("material.dat")
