@@ -129,3 +129,7 @@ class RveOptions(C.Structure):
 class RveInfo(C.Structure):
     _fields_ = [("cells", C.c_int32), ("precision_mode", C.c_int32), ("nb_nodes", C.c_int64),
                 ("volume_fraction", C.c_double * 8), ("shared_bytes", C.c_int64)]
+
+# Neumann condition kinds (akb_neumann_kind)
+NEUMANN_TRACTION = 0
+NEUMANN_STRESS = 1

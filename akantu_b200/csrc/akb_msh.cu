@@ -1,5 +1,6 @@
 // akb_msh.cu -- the Gmsh reader of include/akb_mesh.h (host code only).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <fstream>
 #include <iomanip>
@@ -23,6 +24,8 @@ struct akb_msh {
   struct Group {
     std::string name;
     std::vector<uint32_t> nodes, elements;
+    int32_t facet_nodes = 0;        // nodes per facet (0: no facet)
+    std::vector<uint32_t> facets;   // elements of dimension dim - 1
   };
   std::vector<Group> groups;
 };
@@ -30,7 +33,8 @@ struct akb_msh {
 namespace {
 
 // Gmsh element types read here: number of nodes, dimension, library type
-// (0: carries groups only).
+// (0: carries groups only -- points, and quadrangle_4 as the facet of a 3D
+// mesh).
 struct MshType {
   int nodes, dim, type;
 };
@@ -38,6 +42,7 @@ bool msh_type(int t, MshType* out) {
   switch (t) {
   case 1: *out = {2, 1, AKB_SEGMENT_2}; return true;
   case 2: *out = {3, 2, AKB_TRIANGLE_3}; return true;
+  case 3: *out = {4, 2, 0}; return true;
   case 4: *out = {4, 3, AKB_TETRAHEDRON_4}; return true;
   case 5: *out = {8, 3, AKB_HEXAHEDRON_8}; return true;
   case 15: *out = {1, 0, 0}; return true;
@@ -164,7 +169,7 @@ akb_status parse(const std::string& text, int32_t dim, akb_msh** out) {
   // the mesh: the elements of the requested dimension, of one type
   int type = 0;
   for (const auto& e : elems)
-    if (e.type_dim == dim) {
+    if (e.type_dim == dim && e.type != 0) {  // (a quadrangle of a 2D mesh: skipped)
       if (type && e.type != type)
         return fail(AKB_ERR_UNSUPPORTED, "elements of several types in the mesh's dimension");
       type = e.type;
@@ -172,10 +177,11 @@ akb_status parse(const std::string& text, int32_t dim, akb_msh** out) {
   if (!type) return fail(AKB_ERR_BAD_MESH, "no element of the mesh's dimension");
   m->type = type;
   std::map<std::string, size_t> gidx;
-  std::vector<std::vector<uint32_t>> gnodes, gelems;
+  std::vector<std::vector<uint32_t>> gnodes, gelems, gfacets;
+  std::vector<int32_t> gfnodes;
   uint32_t ecount = 0;
   for (const auto& e : elems) {
-    const bool in_mesh = e.type_dim == dim;
+    const bool in_mesh = e.type_dim == dim && e.type != 0;
     if (in_mesh) m->conn.insert(m->conn.end(), e.nodes.begin(), e.nodes.end());
     if (has_names) {
       const auto it = names.find(e.phys);
@@ -185,9 +191,18 @@ akb_status parse(const std::string& text, int32_t dim, akb_msh** out) {
         g = gidx.emplace(name, gnodes.size()).first;
         gnodes.emplace_back();
         gelems.emplace_back();
+        gfacets.emplace_back();
+        gfnodes.push_back(0);
       }
       gnodes[g->second].insert(gnodes[g->second].end(), e.nodes.begin(), e.nodes.end());
       if (in_mesh) gelems[g->second].push_back(ecount);
+      if (dim >= 2 && e.type_dim == dim - 1) {  // a facet of the group
+        const int32_t nf = (int32_t)e.nodes.size();
+        if (gfnodes[g->second] && gfnodes[g->second] != nf)
+          return fail(AKB_ERR_UNSUPPORTED, "group '" + name + "' has facets of two kinds");
+        gfnodes[g->second] = nf;
+        gfacets[g->second].insert(gfacets[g->second].end(), e.nodes.begin(), e.nodes.end());
+      }
     }
     if (in_mesh) ++ecount;
   }
@@ -198,6 +213,8 @@ akb_status parse(const std::string& text, int32_t dim, akb_msh** out) {
     std::sort(g.nodes.begin(), g.nodes.end());
     g.nodes.erase(std::unique(g.nodes.begin(), g.nodes.end()), g.nodes.end());
     g.elements = std::move(gelems[kv.second]);
+    g.facet_nodes = gfnodes[kv.second];
+    g.facets = std::move(gfacets[kv.second]);
     m->groups.push_back(std::move(g));
   }
   *out = m.release();
@@ -267,6 +284,98 @@ akb_status akb_msh_get_group(const akb_msh* m, int32_t index, const char** name,
   if (nodes) *nodes = g.nodes.data();
   if (nb_elements) *nb_elements = (int64_t)g.elements.size();
   if (elements) *elements = g.elements.data();
+  return AKB_OK;
+}
+
+akb_status akb_msh_get_group_facets(const akb_msh* m, int32_t index, int64_t* nb_facets,
+                                    int32_t* nodes_per_facet, const uint32_t** facets) {
+  if (!m) return fail(AKB_ERR_INVALID_ARGUMENT, "null mesh");
+  if (index < 0 || index >= (int32_t)m->groups.size())
+    return fail(AKB_ERR_INVALID_ARGUMENT, "group index out of range");
+  const auto& g = m->groups[index];
+  if (nb_facets) *nb_facets = g.facet_nodes ? (int64_t)(g.facets.size() / g.facet_nodes) : 0;
+  if (nodes_per_facet) *nodes_per_facet = g.facet_nodes;
+  if (facets) *facets = g.facets.data();
+  return AKB_OK;
+}
+
+akb_status akb_neumann_forces(int32_t d, int64_t nb_nodes, const double* X, int64_t nb_facets,
+                              int32_t nf, const uint32_t* facets, int32_t kind,
+                              const double* value, double* forces) {
+  if (d != 2 && d != 3)
+    return fail(AKB_ERR_UNSUPPORTED, "Neumann conditions are defined in 2D and 3D");
+  if (nb_facets < 0 || nb_nodes < 0) return fail(AKB_ERR_INVALID_ARGUMENT, "negative count");
+  if (nb_facets == 0) return AKB_OK;
+  if (!X || !facets || !value || !forces) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (kind != AKB_NEUMANN_TRACTION && kind != AKB_NEUMANN_STRESS)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "unknown Neumann kind");
+  if ((d == 2 && nf != 2) || (d == 3 && nf != 3 && nf != 4))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "facets must be segments in 2D, triangles or "
+                                          "quadrangles in 3D");
+  for (int64_t k = 0; k < nb_facets * nf; ++k)
+    if (facets[k] >= (uint64_t)nb_nodes)
+      return fail(AKB_ERR_INVALID_ARGUMENT, "facet refers to a node out of range");
+  // Gauss points of the boundary element in its natural coordinates, with
+  // the weights and shape functions there: segment_2 (N = (1 -+ xi) / 2) and
+  // triangle_3 (N = 1 - xi - eta, xi, eta) one point; quadrangle_4 (corners
+  // (-1,-1), (1,-1), (1,1), (-1,1)) the 2 x 2 rule
+  struct Point {
+    double w, N[4], dN[2][4];  // shape values, derivatives in xi and eta
+  };
+  std::vector<Point> pts;
+  if (nf == 2) {
+    pts.push_back({2.0, {0.5, 0.5}, {{-0.5, 0.5}}});
+  } else if (nf == 3) {
+    const double t = 1.0 / 3.0;
+    pts.push_back({0.5, {t, t, t}, {{-1.0, 1.0, 0.0}, {-1.0, 0.0, 1.0}}});
+  } else {
+    const double g = 1.0 / std::sqrt(3.0);
+    const double cx[4] = {-1, 1, 1, -1}, cy[4] = {-1, -1, 1, 1};
+    for (int q = 0; q < 4; ++q) {
+      const double xi = cx[q] * g, eta = cy[q] * g;
+      Point p{1.0, {}, {}};
+      for (int a = 0; a < 4; ++a) {
+        p.N[a] = 0.25 * (1 + cx[a] * xi) * (1 + cy[a] * eta);
+        p.dN[0][a] = 0.25 * cx[a] * (1 + cy[a] * eta);
+        p.dN[1][a] = 0.25 * cy[a] * (1 + cx[a] * xi);
+      }
+      pts.push_back(p);
+    }
+  }
+  for (int64_t f = 0; f < nb_facets; ++f) {
+    const uint32_t* c = facets + f * nf;
+    for (const Point& p : pts) {
+      // tangents dx/dxi (and dx/deta), the normal and the measure |J| there
+      double t0[3] = {0, 0, 0}, t1[3] = {0, 0, 0}, n[3] = {0, 0, 0}, jac;
+      for (int a = 0; a < nf; ++a)
+        for (int i = 0; i < d; ++i) {
+          t0[i] += p.dN[0][a] * X[(size_t)c[a] * d + i];
+          if (d == 3) t1[i] += p.dN[1][a] * X[(size_t)c[a] * d + i];
+        }
+      if (d == 2) {
+        n[0] = t0[1];
+        n[1] = -t0[0];
+        jac = std::sqrt(t0[0] * t0[0] + t0[1] * t0[1]);
+      } else {
+        n[0] = t0[1] * t1[2] - t0[2] * t1[1];
+        n[1] = t0[2] * t1[0] - t0[0] * t1[2];
+        n[2] = t0[0] * t1[1] - t0[1] * t1[0];
+        jac = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      }
+      if (!(jac > 0)) return fail(AKB_ERR_BAD_MESH, "degenerate facet");
+      for (int i = 0; i < d; ++i) n[i] /= jac;
+      double t[3] = {0, 0, 0};
+      for (int i = 0; i < d; ++i) {
+        if (kind == AKB_NEUMANN_TRACTION) {
+          t[i] = value[i];
+        } else {
+          for (int j = 0; j < d; ++j) t[i] += value[i + j * d] * n[j];
+        }
+      }
+      for (int a = 0; a < nf; ++a)
+        for (int i = 0; i < d; ++i) forces[(size_t)c[a] * d + i] += p.w * jac * p.N[a] * t[i];
+    }
+  }
   return AKB_OK;
 }
 

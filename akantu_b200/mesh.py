@@ -52,6 +52,8 @@ class Mesh:
             else np.ascontiguousarray(connectivity, dtype=np.uint32)
         self.node_groups: dict[str, np.ndarray] = {}
         self.element_groups: dict[str, np.ndarray] = {}
+        # per group, its facets (elements of one dimension less), n x nodes
+        self.facet_groups: dict[str, np.ndarray] = {}
 
     # --- reference-style accessors -------------------------------------
     def getNodes(self):
@@ -109,7 +111,7 @@ class Mesh:
                 desc.connectivity, (desc.nb_elements * n,)).reshape(-1, n).copy()
             ng = C.c_int32()
             _lib.check(L.akb_msh_get_nb_groups(h, C.byref(ng)))
-            self.node_groups, self.element_groups = {}, {}
+            self.node_groups, self.element_groups, self.facet_groups = {}, {}, {}
             for k in range(ng.value):
                 name = C.c_char_p()
                 nn, ne = C.c_int64(), C.c_int64()
@@ -121,11 +123,40 @@ class Mesh:
                                          if nn.value else np.zeros(0, np.int64))
                 self.element_groups[key] = (np.ctypeslib.as_array(pe, (ne.value,)).astype(np.int64)
                                             if ne.value else np.zeros(0, np.int64))
+                nf, npf = C.c_int64(), C.c_int32()
+                pf = C.POINTER(C.c_uint32)()
+                _lib.check(L.akb_msh_get_group_facets(h, k, C.byref(nf), C.byref(npf),
+                                                      C.byref(pf)))
+                if nf.value:  # the group's elements of one dimension less
+                    self.facet_groups[key] = np.ctypeslib.as_array(
+                        pf, (nf.value * npf.value,)).reshape(-1, npf.value).astype(np.uint32)
         finally:
             L.akb_msh_destroy(h)
 
     def getElementGroup(self, name):
         return self.element_groups[name]
+
+    def getFacetGroup(self, name):
+        """The group's facets (its elements of one dimension less, as read
+        from the file): (n, nodes per facet) node indices."""
+        return self.facet_groups[name]
+
+    def neumannForces(self, group, functor):
+        """The nodal forces of a Neumann condition (FromTraction or
+        FromStress) on a group's facets (akb_neumann_forces): (N, d)."""
+        from . import _lib
+        X = np.ascontiguousarray(self.nodes, dtype=np.float64)
+        d = X.shape[1]
+        facets = np.ascontiguousarray(self.facet_groups.get(group, np.zeros((0, d), np.uint32)),
+                                      dtype=np.uint32)
+        value = np.ascontiguousarray(functor.akb_value(d), dtype=np.float64)
+        out = np.zeros((X.shape[0], d))
+        _lib.check(_lib.lib().akb_neumann_forces(
+            d, X.shape[0], X.ctypes.data_as(C.POINTER(C.c_double)), facets.shape[0],
+            facets.shape[1] if facets.ndim == 2 and facets.shape[0] else (2 if d == 2 else 3),
+            facets.ctypes.data_as(C.POINTER(C.c_uint32)), functor.kind,
+            value.ctypes.data_as(C.POINTER(C.c_double)), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
 
     # --- boundary groups (Mesh::createBoundaryGroupFromGeometry) ---------
     def boundary_nodes(self):

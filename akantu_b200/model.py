@@ -173,6 +173,40 @@ class FreeBoundary:
         self.axis = int(axis)
 
 
+class FromTraction:
+    """BC::Neumann::FromSameDim (FromTraction in the reference's Python
+    package): a traction vector on the group's facets, its nodal forces
+    added to the external force."""
+    kind = _abi.NEUMANN_TRACTION
+
+    def __init__(self, traction):
+        self.traction = np.asarray(traction, dtype=np.float64).reshape(-1)
+
+    def akb_value(self, dim):
+        if self.traction.size != dim:
+            raise ValueError("a traction of %d components in %dD" % (self.traction.size, dim))
+        return self.traction
+
+
+class FromStress:
+    """BC::Neumann::FromHigherDim (FromStress in the reference's Python
+    package): a stress tensor, the traction sigma n with n each facet's unit
+    normal as its node order gives it."""
+    kind = _abi.NEUMANN_STRESS
+
+    def __init__(self, stress):
+        self.stress = np.asarray(stress, dtype=np.float64)
+
+    def akb_value(self, dim):
+        if self.stress.shape != (dim, dim):
+            raise ValueError("a %s stress in %dD" % (self.stress.shape, dim))
+        return self.stress.T.reshape(-1)  # column-major
+
+
+FromSameDim = FromTraction
+FromHigherDim = FromStress
+
+
 class SolidMechanicsModel:
     """The explicit lumped-mass SolidMechanicsModel on one GPU."""
 
@@ -437,7 +471,14 @@ class SolidMechanicsModel:
         boundary_condition_tmpl.hh:63-200) on the nodes of a mesh group
         (the node group of a `$PhysicalNames` group, or one created with
         Mesh.createNodeGroup): FixedValue(value, axis) blocks the axis and
-        sets the displacement, FreeBoundary(axis) unblocks it."""
+        sets the displacement, FreeBoundary(axis) unblocks it; FromTraction /
+        FromStress add the nodal forces of a traction on the group's facets
+        to the external force (boundary_condition_tmpl.hh:95-185)."""
+        if isinstance(functor, (FromTraction, FromStress)):
+            # ADDED into the external force, as the reference assembles it
+            f = self.getExternalForce()
+            f += self.mesh.neumannForces(group, functor)
+            return
         nodes = self.mesh.getNodeGroup(group) if isinstance(group, str) else np.asarray(group)
         if isinstance(functor, FixedValue):
             self.applyDirichlet(nodes, functor.axis, functor.value)
@@ -445,7 +486,7 @@ class SolidMechanicsModel:
             b = self.getBlockedDOFs()
             b[np.asarray(nodes, dtype=np.int64), functor.axis] = False
         else:
-            raise TypeError("applyBC takes FixedValue or FreeBoundary")
+            raise TypeError("applyBC takes FixedValue, FreeBoundary, FromTraction or FromStress")
 
     def getGradU(self):
         return self.getField(_abi.FIELD_GRAD_U)

@@ -92,6 +92,10 @@ struct NodeGroup {
   std::string name;
   std::vector<uint32_t> nodes;
   std::vector<uint32_t> elements;
+  // the group's facets (its elements of one dimension less, on which
+  // Neumann conditions act): nodes_per_facet node indices each
+  int32_t nodes_per_facet = 0;
+  std::vector<uint32_t> facets;
   UInt size() const { return (UInt)nodes.size(); }
   std::vector<uint32_t>::const_iterator begin() const { return nodes.begin(); }
   std::vector<uint32_t>::const_iterator end() const { return nodes.end(); }
@@ -125,7 +129,12 @@ class Mesh {
       int64_t nn, ne;
       const uint32_t *pn, *pe;
       check(akb_msh_get_group(m, k, &name, &nn, &pn, &ne, &pe));
-      NodeGroup g{name, std::vector<uint32_t>(pn, pn + nn), std::vector<uint32_t>(pe, pe + ne)};
+      NodeGroup g{name, std::vector<uint32_t>(pn, pn + nn), std::vector<uint32_t>(pe, pe + ne), 0,
+                  {}};
+      int64_t nf;
+      const uint32_t* pf;
+      check(akb_msh_get_group_facets(m, k, &nf, &g.nodes_per_facet, &pf));
+      g.facets.assign(pf, pf + nf * g.nodes_per_facet);
       groups_[g.name] = std::move(g);
     }
     akb_msh_destroy(m);
@@ -196,7 +205,37 @@ struct FixedValue {
   SpatialDirection axis;
 };
 }  // namespace Dirichlet
+namespace Neumann {
+// FromTraction (FromSameDim, boundary_condition_functor.hh): a traction
+// vector (d values) on the group's facets.
+struct FromTraction {
+  explicit FromTraction(const std::vector<Real>& traction) : value(traction) {}
+  static constexpr int32_t kind = AKB_NEUMANN_TRACTION;
+  std::vector<Real> value;
+};
+// FromStress (FromHigherDim): a stress (d x d, column-major like Matrix<Real>),
+// the traction sigma n with n each facet's unit normal from its node order.
+struct FromStress {
+  explicit FromStress(const std::vector<Real>& stress_column_major) : value(stress_column_major) {}
+  static constexpr int32_t kind = AKB_NEUMANN_STRESS;
+  std::vector<Real> value;
+};
+}  // namespace Neumann
 }  // namespace BC
+
+// The nodal forces of a Neumann functor on a group's facets
+// (boundary_condition_tmpl.hh:95-185), added into forces (N x d).
+template <class F>
+void addNeumannForces(const Mesh& mesh, const std::string& group, const F& f, Array<Real>& forces) {
+  const NodeGroup& g = mesh.getNodeGroup(group);
+  const UInt d = mesh.getSpatialDimension();
+  if (f.value.size() != (F::kind == AKB_NEUMANN_TRACTION ? d : d * d))
+    throw Exception(AKB_ERR_INVALID_ARGUMENT, "Neumann value of the wrong size");
+  const int64_t nf = g.nodes_per_facet ? (int64_t)(g.facets.size() / g.nodes_per_facet) : 0;
+  check(akb_neumann_forces((int32_t)d, (int64_t)mesh.getNbNodes(), mesh.getNodes().storage(), nf,
+                           g.nodes_per_facet, g.facets.data(), F::kind, f.value.data(),
+                           forces.storage()));
+}
 
 class SolidMechanicsModel {
  public:
@@ -223,7 +262,7 @@ class SolidMechanicsModel {
     akb_mesh_desc md{(int32_t)mesh_.getSpatialDimension(), (int32_t)mesh_.getElementType(),
                      (int64_t)mesh_.getNbNodes(), (int64_t)mesh_.getNbElement(),
                      mesh_.getNodes().storage(), mesh_.getConnectivity().storage()};
-    akb_model_options opt{precision_, device_, nullptr};
+    akb_model_options opt{precision_, device_, nullptr, 0, 0, 0};  // default patches
     check(akb_model_create(&md, (int32_t)mats_.size(), mats_.data(),
                            element_material_.empty() ? nullptr : element_material_.data(), &opt,
                            &h_));
@@ -285,6 +324,14 @@ class SolidMechanicsModel {
   }
   void applyBC(const BC::Dirichlet::FixedValue& f, const std::string& group) {
     applyBC(f, mesh_.getNodeGroup(group).nodes);
+  }
+  // applyBC(FromTraction / FromStress, group): the nodal forces added to the
+  // external force (pushed before the next call that uses the state)
+  void applyBC(const BC::Neumann::FromTraction& f, const std::string& group) {
+    addNeumannForces(mesh_, group, f, getExternalForce());
+  }
+  void applyBC(const BC::Neumann::FromStress& f, const std::string& group) {
+    addNeumannForces(mesh_, group, f, getExternalForce());
   }
 
   Real getEnergy(const std::string& id) {

@@ -84,3 +84,17 @@ def test_integration_guide_matches_the_headers():
     mentioned -= {"akb_fe2", "akb_mesh", "akb_msh", "akb_model"}  # file and type stems
     assert sorted(mentioned - in_headers) == []
     assert sorted(set(declared_symbols()) - mentioned) == []
+
+
+@pytest.mark.parametrize("program", ["shim_plate.cc", "shim_fe2.cc", "shim_neumann.cc"])
+def test_cpp_shim_programs_compile_without_warnings(program):
+    """The header-only C++ shim and the programs written against it compile
+    with -Wall -Wextra as errors (what a maintainer's build would use)."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not found")
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+                        "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "cpp", program)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

@@ -1,0 +1,205 @@
+"""Neumann conditions on the host (akb_msh_get_group_facets,
+akb_neumann_forces; applyBC(FromTraction / FromStress, group) in the
+reference, boundary_condition_tmpl.hh:95-185): the facets the Gmsh reader
+keeps per group, the nodal forces of a traction or a stress on segments,
+triangles and quadrangles (the Gauss rules of the boundary elements, the
+normals as the reference forms them from the node order) against hand
+integrals, and a closed surface under a uniform stress, whose forces cancel."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from akantu_b200 import _abi
+from akantu_b200._lib import AkbError, check, lib
+from akantu_b200.mesh import Mesh
+from akantu_b200.model import FromStress, FromTraction
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "msh")
+
+
+def forces(X, facets, kind, value):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    facets = np.ascontiguousarray(facets, dtype=np.uint32)
+    value = np.ascontiguousarray(value, dtype=np.float64).reshape(-1)
+    out = np.zeros_like(X)
+    check(lib().akb_neumann_forces(X.shape[1], X.shape[0], X.ctypes.data_as(C.POINTER(C.c_double)),
+                                   facets.shape[0], facets.shape[1],
+                                   facets.ctypes.data_as(C.POINTER(C.c_uint32)), kind,
+                                   value.ctypes.data_as(C.POINTER(C.c_double)),
+                                   out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out
+
+
+def colmajor(s):
+    return np.asarray(s, dtype=float).T.reshape(-1)
+
+
+def test_segments():
+    X = np.array([[0.0, 0.0], [2.0, 0.0], [2.0, 3.0]])
+    f = forces(X, [[0, 1]], _abi.NEUMANN_TRACTION, [1.0, 3.0])
+    assert np.allclose(f, [[1.0, 3.0], [1.0, 3.0], [0.0, 0.0]], rtol=0, atol=1e-15)
+    # normal of the tangent t = x1 - x0: (t_y, -t_x) / |t|; segment 1 -> 2 points up: n = (1, 0)
+    sigma = np.array([[2.0, 0.5], [0.5, 5.0]])
+    f = forces(X, [[1, 2]], _abi.NEUMANN_STRESS, colmajor(sigma))
+    t = sigma @ np.array([1.0, 0.0])
+    assert np.allclose(f[1], 1.5 * t, atol=1e-14) and np.allclose(f[2], 1.5 * t, atol=1e-14)
+    # forces are added to what the array holds
+    out = np.ones_like(X)
+    check(lib().akb_neumann_forces(2, 3, np.ascontiguousarray(X).ctypes.data_as(C.POINTER(C.c_double)),
+                                   1, 2, np.array([0, 1], np.uint32).ctypes.data_as(C.POINTER(C.c_uint32)),
+                                   _abi.NEUMANN_TRACTION,
+                                   np.array([1.0, 0.0]).ctypes.data_as(C.POINTER(C.c_double)),
+                                   out.ctypes.data_as(C.POINTER(C.c_double))))
+    assert np.allclose(out[:2, 0], 2.0) and np.allclose(out[2], 1.0)
+
+
+def test_triangles_and_quadrangles():
+    X = np.array([[0.0, 0, 0], [2, 0, 0], [0, 1, 0], [2, 1, 0], [0, 0, 1]])
+    # triangle 0-1-2 in z = 0, area 1, normal (x1-x0) x (x2-x0) = +z
+    f = forces(X, [[0, 1, 2]], _abi.NEUMANN_TRACTION, [0.0, 0.0, 3.0])
+    assert np.allclose(f[:3, 2], 1.0) and np.allclose(f[3:], 0.0)
+    sigma = np.diag([1.0, 2.0, 7.0])
+    f = forces(X, [[0, 1, 2]], _abi.NEUMANN_STRESS, colmajor(sigma))
+    assert np.allclose(f[:3], [0.0, 0.0, 7.0 / 3.0])
+    f = forces(X, [[0, 2, 1]], _abi.NEUMANN_STRESS, colmajor(sigma))  # reversed: -z
+    assert np.allclose(f[:3], [0.0, 0.0, -7.0 / 3.0])
+    # rectangle 0-1-3-2 (2 x 1): the bilinear shape functions' integrals A / 4
+    f = forces(X, [[0, 1, 3, 2]], _abi.NEUMANN_TRACTION, [1.0, -1.0, 2.0])
+    assert np.allclose(f[:4], 0.5 * np.array([1.0, -1.0, 2.0]))
+    # a planar trapezoid: the forces add up to traction x area, unevenly
+    Y = np.array([[0.0, 0, 0], [4, 0, 0], [3, 2, 0], [1, 2, 0]])
+    f = forces(Y, [[0, 1, 2, 3]], _abi.NEUMANN_TRACTION, [0.0, 0.0, 1.0])
+    assert f[:, 2].sum() == pytest.approx(6.0, rel=1e-14)
+    assert f[0, 2] > f[3, 2]
+
+
+def unit_cube_surface():
+    X = np.array([[x, y, z] for z in (0.0, 1.0) for y in (0.0, 1.0) for x in (0.0, 1.0)])
+    idx = lambda x, y, z: int(x + 2 * y + 4 * z)  # noqa: E731
+    # the six faces, each ordered so that t_xi x t_eta points out of the cube
+    faces = [[idx(0, 0, 0), idx(0, 1, 0), idx(1, 1, 0), idx(1, 0, 0)],   # z = 0, -z
+             [idx(0, 0, 1), idx(1, 0, 1), idx(1, 1, 1), idx(0, 1, 1)],   # z = 1, +z
+             [idx(0, 0, 0), idx(1, 0, 0), idx(1, 0, 1), idx(0, 0, 1)],   # y = 0, -y
+             [idx(0, 1, 0), idx(0, 1, 1), idx(1, 1, 1), idx(1, 1, 0)],   # y = 1, +y
+             [idx(0, 0, 0), idx(0, 0, 1), idx(0, 1, 1), idx(0, 1, 0)],   # x = 0, -x
+             [idx(1, 0, 0), idx(1, 1, 0), idx(1, 1, 1), idx(1, 0, 1)]]   # x = 1, +x
+    return X, faces
+
+
+def test_closed_surface_under_uniform_stress():
+    X, faces = unit_cube_surface()
+    rng = np.random.default_rng(4)
+    s = rng.normal(size=(3, 3))
+    sigma = s + s.T
+    f = forces(X, faces, _abi.NEUMANN_STRESS, colmajor(sigma))
+    assert np.abs(f.sum(axis=0)).max() <= 1e-14
+    # the +x face alone carries sigma e_x over its unit area
+    f = forces(X, [faces[5]], _abi.NEUMANN_STRESS, colmajor(sigma))
+    assert np.allclose(f.sum(axis=0), sigma[:, 0])
+    # the same faces as triangles: the same total on each face
+    tris = [[a, b, c] for a, b, c, d in faces] + [[a, c, d] for a, b, c, d in faces]
+    f = forces(X, tris, _abi.NEUMANN_STRESS, colmajor(sigma))
+    assert np.abs(f.sum(axis=0)).max() <= 1e-14
+
+
+def test_checks():
+    X = np.zeros((2, 2))
+    for args in ((_abi.NEUMANN_TRACTION, [[0, 2]]),      # node out of range
+                 (7, [[0, 1]])):                          # unknown kind
+        kind, facets = args
+        with pytest.raises(AkbError):
+            forces(X, facets, kind, [1.0, 0.0])
+    with pytest.raises(AkbError):  # triangles in 2D
+        forces(np.zeros((3, 2)), [[0, 1, 2]], _abi.NEUMANN_TRACTION, [1.0, 0.0])
+    with pytest.raises(AkbError):  # no 1D Neumann condition in the reference
+        forces(np.zeros((2, 1)), [[0, 1]], _abi.NEUMANN_TRACTION, [1.0])
+    with pytest.raises(AkbError):  # a degenerate facet
+        forces(np.zeros((2, 2)), [[0, 1]], _abi.NEUMANN_TRACTION, [1.0, 0.0])
+
+
+def test_reader_keeps_the_groups_facets():
+    mesh = Mesh(2)
+    mesh.read(os.path.join(GOLDEN, "cohesive_strait_2D.msh"))
+    assert set(mesh.facet_groups) == {"fixed", "loading", "insertion"}
+    for name in ("fixed", "loading"):
+        segs = mesh.getFacetGroup(name)
+        assert segs.shape[1] == 2
+        assert set(segs.reshape(-1).tolist()) == set(mesh.getNodeGroup(name).tolist())
+    # FromTraction on the loading line: the forces add up to traction x length
+    segs = mesh.getFacetGroup("loading")
+    x = mesh.nodes
+    length = np.linalg.norm(x[segs[:, 1]] - x[segs[:, 0]], axis=1).sum()
+    f = mesh.neumannForces("loading", FromTraction([0.0, -2.0]))
+    assert f.sum(axis=0) == pytest.approx([0.0, -2.0 * length], abs=1e-14)
+    assert np.all(f[np.setdiff1d(np.arange(len(x)), mesh.getNodeGroup("loading"))] == 0.0)
+    # the body group has no facets (its elements are of the mesh's dimension)
+    assert "body" not in mesh.facet_groups
+    with pytest.raises(ValueError):
+        FromStress(np.eye(3)).akb_value(2)
+
+
+HEX_WITH_TOP = """$MeshFormat
+2.2 0 8
+$EndMeshFormat
+$PhysicalNames
+2
+2 1 "top"
+3 2 "body"
+$EndPhysicalNames
+$Nodes
+8
+1 0 0 0
+2 1 0 0
+3 1 1 0
+4 0 1 0
+5 0 0 1
+6 1 0 1
+7 1 1 1
+8 0 1 1
+$EndNodes
+$Elements
+2
+1 3 2 1 1 5 6 7 8
+2 5 2 2 2 1 2 3 4 5 6 7 8
+$EndElements
+"""
+
+
+def test_quadrangle_facets_of_a_hexahedral_mesh():
+    mesh = Mesh(3)
+    mesh.read_msh_text(HEX_WITH_TOP)
+    assert mesh.element_type == _abi.HEXAHEDRON_8 and len(mesh.connectivity) == 1
+    assert mesh.getFacetGroup("top").tolist() == [[4, 5, 6, 7]]
+    f = mesh.neumannForces("top", FromStress(np.diag([0.0, 0.0, -3.0])))  # n = +z
+    assert np.allclose(f[4:], [0.0, 0.0, -0.75]) and np.all(f[:4] == 0.0)
+    with pytest.raises(AkbError):  # a 2D mesh of quadrangles: skipped, so no element left
+        Mesh(2).read_msh_text(HEX_WITH_TOP.replace("3 2 \"body\"", "2 2 \"body\"")
+                              .replace("2 5 2 2 2 1 2 3 4 5 6 7 8", "2 3 2 2 2 1 2 3 4"))
+
+
+def test_cpp_shim_neumann_forces(tmp_path):
+    """The C++ shim's Mesh::read keeps the groups' facets and its
+    addNeumannForces (what applyBC(FromTraction / FromStress, group) adds to
+    the external force) gives the same forces as the Python layer."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not found")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "akantu_b200")
+    exe = str(tmp_path / "shim_neumann")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(root, "include"), "-o", exe,
+                    os.path.join(root, "tests", "cpp", "shim_neumann.cc"), "-L", libdir, "-lakb",
+                    "-Wl,-rpath," + libdir], check=True)
+    msh = os.path.join(GOLDEN, "cohesive_strait_2D.msh")
+    out = subprocess.run([exe, msh, "loading"], check=True, capture_output=True, text=True).stdout
+    nf, fx, fy, hx, hy = out.split()
+    mesh = Mesh(2)
+    mesh.read(msh)
+    assert int(nf) == len(mesh.getFacetGroup("loading"))
+    want_f = mesh.neumannForces("loading", FromTraction([0.0, -2.0])).sum(axis=0)
+    want_h = mesh.neumannForces("loading", FromStress(np.eye(2))).sum(axis=0)
+    assert np.allclose([float(fx), float(fy)], want_f, rtol=0, atol=1e-14)
+    assert np.allclose([float(hx), float(hy)], want_h, rtol=0, atol=1e-14)
