@@ -24,7 +24,7 @@ struct akb_msh {
   struct Group {
     std::string name;
     std::vector<uint32_t> nodes, elements;
-    int32_t facet_nodes = 0;        // nodes per facet (0: no facet)
+    int32_t facet_nodes = 0;        // nodes per facet (0: no facet, -1: two kinds)
     std::vector<uint32_t> facets;   // elements of dimension dim - 1
   };
   std::vector<Group> groups;
@@ -196,12 +196,15 @@ akb_status parse(const std::string& text, int32_t dim, akb_msh** out) {
       }
       gnodes[g->second].insert(gnodes[g->second].end(), e.nodes.begin(), e.nodes.end());
       if (in_mesh) gelems[g->second].push_back(ecount);
-      if (dim >= 2 && e.type_dim == dim - 1) {  // a facet of the group
+      if (dim >= 2 && e.type_dim == dim - 1 && gfnodes[g->second] >= 0) {  // a facet
         const int32_t nf = (int32_t)e.nodes.size();
-        if (gfnodes[g->second] && gfnodes[g->second] != nf)
-          return fail(AKB_ERR_UNSUPPORTED, "group '" + name + "' has facets of two kinds");
-        gfnodes[g->second] = nf;
-        gfacets[g->second].insert(gfacets[g->second].end(), e.nodes.begin(), e.nodes.end());
+        if (gfnodes[g->second] && gfnodes[g->second] != nf) {  // two kinds: none kept
+          gfnodes[g->second] = -1;
+          gfacets[g->second].clear();
+        } else {
+          gfnodes[g->second] = nf;
+          gfacets[g->second].insert(gfacets[g->second].end(), e.nodes.begin(), e.nodes.end());
+        }
       }
     }
     if (in_mesh) ++ecount;
@@ -293,6 +296,8 @@ akb_status akb_msh_get_group_facets(const akb_msh* m, int32_t index, int64_t* nb
   if (index < 0 || index >= (int32_t)m->groups.size())
     return fail(AKB_ERR_INVALID_ARGUMENT, "group index out of range");
   const auto& g = m->groups[index];
+  if (g.facet_nodes < 0)
+    return fail(AKB_ERR_UNSUPPORTED, "group '" + g.name + "' has facets of two kinds");
   if (nb_facets) *nb_facets = g.facet_nodes ? (int64_t)(g.facets.size() / g.facet_nodes) : 0;
   if (nodes_per_facet) *nodes_per_facet = g.facet_nodes;
   if (facets) *facets = g.facets.data();

@@ -54,6 +54,7 @@ class Mesh:
         self.element_groups: dict[str, np.ndarray] = {}
         # per group, its facets (elements of one dimension less), n x nodes
         self.facet_groups: dict[str, np.ndarray] = {}
+        self._mixed_facets: set[str] = set()  # groups with facets of two kinds
 
     # --- reference-style accessors -------------------------------------
     def getNodes(self):
@@ -112,6 +113,7 @@ class Mesh:
             ng = C.c_int32()
             _lib.check(L.akb_msh_get_nb_groups(h, C.byref(ng)))
             self.node_groups, self.element_groups, self.facet_groups = {}, {}, {}
+            self._mixed_facets = set()
             for k in range(ng.value):
                 name = C.c_char_p()
                 nn, ne = C.c_int64(), C.c_int64()
@@ -125,8 +127,11 @@ class Mesh:
                                             if ne.value else np.zeros(0, np.int64))
                 nf, npf = C.c_int64(), C.c_int32()
                 pf = C.POINTER(C.c_uint32)()
-                _lib.check(L.akb_msh_get_group_facets(h, k, C.byref(nf), C.byref(npf),
-                                                      C.byref(pf)))
+                st = L.akb_msh_get_group_facets(h, k, C.byref(nf), C.byref(npf), C.byref(pf))
+                if st == _abi.AKB_ERR_UNSUPPORTED:  # facets of two kinds
+                    self._mixed_facets.add(key)
+                    continue
+                _lib.check(st)
                 if nf.value:  # the group's elements of one dimension less
                     self.facet_groups[key] = np.ctypeslib.as_array(
                         pf, (nf.value * npf.value,)).reshape(-1, npf.value).astype(np.uint32)
@@ -145,6 +150,9 @@ class Mesh:
         """The nodal forces of a Neumann condition (FromTraction or
         FromStress) on a group's facets (akb_neumann_forces): (N, d)."""
         from . import _lib
+        if group in self._mixed_facets:
+            raise ValueError("group '%s' has facets of two kinds (triangles and quadrangles)"
+                             % group)
         X = np.ascontiguousarray(self.nodes, dtype=np.float64)
         d = X.shape[1]
         facets = np.ascontiguousarray(self.facet_groups.get(group, np.zeros((0, d), np.uint32)),

@@ -93,7 +93,8 @@ struct NodeGroup {
   std::vector<uint32_t> nodes;
   std::vector<uint32_t> elements;
   // the group's facets (its elements of one dimension less, on which
-  // Neumann conditions act): nodes_per_facet node indices each
+  // Neumann conditions act): nodes_per_facet node indices each (-1: facets
+  // of two kinds, not kept)
   int32_t nodes_per_facet = 0;
   std::vector<uint32_t> facets;
   UInt size() const { return (UInt)nodes.size(); }
@@ -133,8 +134,13 @@ class Mesh {
                   {}};
       int64_t nf;
       const uint32_t* pf;
-      check(akb_msh_get_group_facets(m, k, &nf, &g.nodes_per_facet, &pf));
-      g.facets.assign(pf, pf + nf * g.nodes_per_facet);
+      const akb_status fs = akb_msh_get_group_facets(m, k, &nf, &g.nodes_per_facet, &pf);
+      if (fs == AKB_ERR_UNSUPPORTED) {
+        g.nodes_per_facet = -1;  // facets of two kinds: no Neumann condition on it
+      } else {
+        check(fs);
+        g.facets.assign(pf, pf + nf * g.nodes_per_facet);
+      }
       groups_[g.name] = std::move(g);
     }
     akb_msh_destroy(m);
@@ -228,6 +234,8 @@ struct FromStress {
 template <class F>
 void addNeumannForces(const Mesh& mesh, const std::string& group, const F& f, Array<Real>& forces) {
   const NodeGroup& g = mesh.getNodeGroup(group);
+  if (g.nodes_per_facet < 0)
+    throw Exception(AKB_ERR_UNSUPPORTED, "group " + group + " has facets of two kinds");
   const UInt d = mesh.getSpatialDimension();
   if (f.value.size() != (F::kind == AKB_NEUMANN_TRACTION ? d : d * d))
     throw Exception(AKB_ERR_INVALID_ARGUMENT, "Neumann value of the wrong size");

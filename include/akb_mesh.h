@@ -60,8 +60,9 @@ akb_status akb_msh_get_group(const akb_msh* mesh, int32_t index, const char** na
  * elements of ElementGroup::getElements(facet type), group_manager.hh:63):
  * nb_facets x nodes_per_facet node indices in the file's node order --
  * segment_2 facets (2 nodes) of a 2D mesh, triangle_3 (3) or quadrangle_4
- * (4) facets of a 3D one; nb_facets = 0 when the group has none. A group
- * with facets of two kinds is rejected when the file is read. */
+ * (4) facets of a 3D one; nb_facets = 0 when the group has none. For a
+ * group whose facets are of two kinds (triangles and quadrangles) the call
+ * returns AKB_ERR_UNSUPPORTED; the file itself reads. */
 akb_status akb_msh_get_group_facets(const akb_msh* mesh, int32_t index, int64_t* nb_facets,
                                     int32_t* nodes_per_facet, const uint32_t** facets);
 

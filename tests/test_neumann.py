@@ -203,3 +203,15 @@ def test_cpp_shim_neumann_forces(tmp_path):
     want_h = mesh.neumannForces("loading", FromStress(np.eye(2))).sum(axis=0)
     assert np.allclose([float(fx), float(fy)], want_f, rtol=0, atol=1e-14)
     assert np.allclose([float(hx), float(hy)], want_h, rtol=0, atol=1e-14)
+
+
+def test_group_with_facets_of_two_kinds():
+    """A group mixing triangles and quadrangles: the file reads, its nodes and
+    elements are kept, and only a Neumann condition on it is refused."""
+    text = HEX_WITH_TOP.replace("$Elements\n2\n", "$Elements\n3\n0 2 2 1 1 1 2 3\n")
+    mesh = Mesh(3)
+    mesh.read_msh_text(text)
+    assert sorted(mesh.getNodeGroup("top").tolist()) == [0, 1, 2, 4, 5, 6, 7]
+    assert "top" not in mesh.facet_groups
+    with pytest.raises(ValueError):
+        mesh.neumannForces("top", FromTraction([0.0, 0.0, 1.0]))
