@@ -12,9 +12,10 @@ from .material_plugin import (Material, MaterialFactory, MeshDataMaterialSelecto
                               _not_ghost, _pat_internal, _pat_modifiable, _pat_parsable,
                               _pat_parsmod, _pat_readable, _pat_writable, parseInput)
 from .mesh import Mesh
-from .model import (FixedValue, FreeBoundary, FromHigherDim, FromSameDim, FromStress,
-                    FromTraction, MaterialElastic, MaterialNeohookean, MaterialUser,
-                    SolidMechanicsModel, _explicit_lumped_mass, _x, _y, _z)
+from .model import (DirichletFunctor, FixedValue, FreeBoundary, FromHigherDim, FromSameDim,
+                    FromStress, FromTraction, Increment, IncrementValue, MaterialElastic,
+                    MaterialNeohookean, MaterialUser, NeumannFunctor, SolidMechanicsModel,
+                    _explicit_lumped_mass, _x, _y, _z)
 
 
 
@@ -36,6 +37,7 @@ _hexahedron_8 = HEXAHEDRON_8
 
 __all__ = ["Mesh", "SolidMechanicsModel", "MaterialElastic", "MaterialNeohookean", "MaterialUser",
            "Material", "MaterialFactory", "MeshDataMaterialSelectorString", "parseInput",
-           "FixedValue", "FreeBoundary", "FromTraction", "FromStress",
+           "FixedValue", "FreeBoundary", "FromTraction", "FromStress", "IncrementValue",
+           "Increment", "DirichletFunctor", "NeumannFunctor",
            "_explicit_lumped_mass", "_x", "_y", "_z", "_not_ghost", "_ghost",
            "MODE_FP64_REFERENCE", "MODE_FP64", "MODE_FP32_BULK"]

@@ -81,6 +81,10 @@ SIGNATURES = {
     "akb_msh_get_group_facets": (I32, [P, I32, C.POINTER(I64), C.POINTER(I32), C.POINTER(PU32)]),
     "akb_neumann_forces": (I32, [I32, I64, C.POINTER(C.c_double), I64, I32, C.POINTER(C.c_uint32),
                                  I32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "akb_facet_points": (I32, [I32]),
+    "akb_facet_quadrature": (I32, [I32, I64, C.POINTER(C.c_double), I64, I32,
+                                   C.POINTER(C.c_uint32), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     # include/akb_fe2.h
     "akb_step_begin": (I32, [P]),
     "akb_step_end": (I32, [P]),

@@ -304,30 +304,19 @@ akb_status akb_msh_get_group_facets(const akb_msh* m, int32_t index, int64_t* nb
   return AKB_OK;
 }
 
-akb_status akb_neumann_forces(int32_t d, int64_t nb_nodes, const double* X, int64_t nb_facets,
-                              int32_t nf, const uint32_t* facets, int32_t kind,
-                              const double* value, double* forces) {
-  if (d != 2 && d != 3)
-    return fail(AKB_ERR_UNSUPPORTED, "Neumann conditions are defined in 2D and 3D");
-  if (nb_facets < 0 || nb_nodes < 0) return fail(AKB_ERR_INVALID_ARGUMENT, "negative count");
-  if (nb_facets == 0) return AKB_OK;
-  if (!X || !facets || !value || !forces) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
-  if (kind != AKB_NEUMANN_TRACTION && kind != AKB_NEUMANN_STRESS)
-    return fail(AKB_ERR_INVALID_ARGUMENT, "unknown Neumann kind");
-  if ((d == 2 && nf != 2) || (d == 3 && nf != 3 && nf != 4))
-    return fail(AKB_ERR_INVALID_ARGUMENT, "facets must be segments in 2D, triangles or "
-                                          "quadrangles in 3D");
-  for (int64_t k = 0; k < nb_facets * nf; ++k)
-    if (facets[k] >= (uint64_t)nb_nodes)
-      return fail(AKB_ERR_INVALID_ARGUMENT, "facet refers to a node out of range");
-  // Gauss points of the boundary element in its natural coordinates, with
-  // the weights and shape functions there: segment_2 (N = (1 -+ xi) / 2) and
-  // triangle_3 (N = 1 - xi - eta, xi, eta) one point; quadrangle_4 (corners
-  // (-1,-1), (1,-1), (1,1), (-1,1)) the 2 x 2 rule
-  struct Point {
-    double w, N[4], dN[2][4];  // shape values, derivatives in xi and eta
-  };
-  std::vector<Point> pts;
+}  // extern "C"
+
+namespace {
+
+// Gauss points of a boundary element in its natural coordinates, with the
+// weights and shape functions there: segment_2 (N = (1 -+ xi) / 2) and
+// triangle_3 (N = 1 - xi - eta, xi, eta) one point; quadrangle_4 (corners
+// (-1,-1), (1,-1), (1,1), (-1,1)) the 2 x 2 rule.
+struct FacetPoint {
+  double w, N[4], dN[2][4];  // shape values, derivatives in xi and eta
+};
+std::vector<FacetPoint> facet_rule(int nf) {
+  std::vector<FacetPoint> pts;
   if (nf == 2) {
     pts.push_back({2.0, {0.5, 0.5}, {{-0.5, 0.5}}});
   } else if (nf == 3) {
@@ -338,7 +327,7 @@ akb_status akb_neumann_forces(int32_t d, int64_t nb_nodes, const double* X, int6
     const double cx[4] = {-1, 1, 1, -1}, cy[4] = {-1, -1, 1, 1};
     for (int q = 0; q < 4; ++q) {
       const double xi = cx[q] * g, eta = cy[q] * g;
-      Point p{1.0, {}, {}};
+      FacetPoint p{1.0, {}, {}};
       for (int a = 0; a < 4; ++a) {
         p.N[a] = 0.25 * (1 + cx[a] * xi) * (1 + cy[a] * eta);
         p.dN[0][a] = 0.25 * cx[a] * (1 + cy[a] * eta);
@@ -347,28 +336,73 @@ akb_status akb_neumann_forces(int32_t d, int64_t nb_nodes, const double* X, int6
       pts.push_back(p);
     }
   }
+  return pts;
+}
+
+akb_status check_facets(int32_t d, int64_t nb_nodes, const double* X, int64_t nb_facets, int32_t nf,
+                        const uint32_t* facets) {
+  if (d != 2 && d != 3)
+    return fail(AKB_ERR_UNSUPPORTED, "Neumann conditions are defined in 2D and 3D");
+  if (nb_facets < 0 || nb_nodes < 0) return fail(AKB_ERR_INVALID_ARGUMENT, "negative count");
+  if (nb_facets > 0 && (!X || !facets)) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (nb_facets > 0 && ((d == 2 && nf != 2) || (d == 3 && nf != 3 && nf != 4)))
+    return fail(AKB_ERR_INVALID_ARGUMENT, "facets must be segments in 2D, triangles or "
+                                          "quadrangles in 3D");
+  for (int64_t k = 0; k < nb_facets * nf; ++k)
+    if (facets[k] >= (uint64_t)nb_nodes)
+      return fail(AKB_ERR_INVALID_ARGUMENT, "facet refers to a node out of range");
+  return AKB_OK;
+}
+
+// At point p of facet c: its coordinates x, unit normal n (the reference's:
+// (t_y, -t_x) of a segment's tangent, t_xi x t_eta of a surface facet) and
+// w |J|; false for a degenerate facet.
+bool facet_point(int d, int nf, const double* X, const uint32_t* c, const FacetPoint& p,
+                 double* x, double* n, double* wj) {
+  double t0[3] = {0, 0, 0}, t1[3] = {0, 0, 0};
+  for (int i = 0; i < d; ++i) x[i] = 0.0;
+  for (int a = 0; a < nf; ++a)
+    for (int i = 0; i < d; ++i) {
+      const double xa = X[(size_t)c[a] * d + i];
+      x[i] += p.N[a] * xa;
+      t0[i] += p.dN[0][a] * xa;
+      if (d == 3) t1[i] += p.dN[1][a] * xa;
+    }
+  double jac;
+  if (d == 2) {
+    n[0] = t0[1];
+    n[1] = -t0[0];
+    jac = std::sqrt(t0[0] * t0[0] + t0[1] * t0[1]);
+  } else {
+    n[0] = t0[1] * t1[2] - t0[2] * t1[1];
+    n[1] = t0[2] * t1[0] - t0[0] * t1[2];
+    n[2] = t0[0] * t1[1] - t0[1] * t1[0];
+    jac = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  }
+  if (!(jac > 0)) return false;
+  for (int i = 0; i < d; ++i) n[i] /= jac;
+  *wj = p.w * jac;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+akb_status akb_neumann_forces(int32_t d, int64_t nb_nodes, const double* X, int64_t nb_facets,
+                              int32_t nf, const uint32_t* facets, int32_t kind,
+                              const double* value, double* forces) {
+  akb_status st = check_facets(d, nb_nodes, X, nb_facets, nf, facets);
+  if (st != AKB_OK || nb_facets == 0) return st;
+  if (!value || !forces) return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  if (kind != AKB_NEUMANN_TRACTION && kind != AKB_NEUMANN_STRESS)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "unknown Neumann kind");
+  const std::vector<FacetPoint> pts = facet_rule(nf);
   for (int64_t f = 0; f < nb_facets; ++f) {
     const uint32_t* c = facets + f * nf;
-    for (const Point& p : pts) {
-      // tangents dx/dxi (and dx/deta), the normal and the measure |J| there
-      double t0[3] = {0, 0, 0}, t1[3] = {0, 0, 0}, n[3] = {0, 0, 0}, jac;
-      for (int a = 0; a < nf; ++a)
-        for (int i = 0; i < d; ++i) {
-          t0[i] += p.dN[0][a] * X[(size_t)c[a] * d + i];
-          if (d == 3) t1[i] += p.dN[1][a] * X[(size_t)c[a] * d + i];
-        }
-      if (d == 2) {
-        n[0] = t0[1];
-        n[1] = -t0[0];
-        jac = std::sqrt(t0[0] * t0[0] + t0[1] * t0[1]);
-      } else {
-        n[0] = t0[1] * t1[2] - t0[2] * t1[1];
-        n[1] = t0[2] * t1[0] - t0[0] * t1[2];
-        n[2] = t0[0] * t1[1] - t0[1] * t1[0];
-        jac = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-      }
-      if (!(jac > 0)) return fail(AKB_ERR_BAD_MESH, "degenerate facet");
-      for (int i = 0; i < d; ++i) n[i] /= jac;
+    for (const FacetPoint& p : pts) {
+      double x[3], n[3], wj;
+      if (!facet_point(d, nf, X, c, p, x, n, &wj)) return fail(AKB_ERR_BAD_MESH, "degenerate facet");
       double t[3] = {0, 0, 0};
       for (int i = 0; i < d; ++i) {
         if (kind == AKB_NEUMANN_TRACTION) {
@@ -378,9 +412,33 @@ akb_status akb_neumann_forces(int32_t d, int64_t nb_nodes, const double* X, int6
         }
       }
       for (int a = 0; a < nf; ++a)
-        for (int i = 0; i < d; ++i) forces[(size_t)c[a] * d + i] += p.w * jac * p.N[a] * t[i];
+        for (int i = 0; i < d; ++i) forces[(size_t)c[a] * d + i] += wj * p.N[a] * t[i];
     }
   }
+  return AKB_OK;
+}
+
+int32_t akb_facet_points(int32_t nodes_per_facet) {
+  return nodes_per_facet == 2 || nodes_per_facet == 3 ? 1 : nodes_per_facet == 4 ? 4 : 0;
+}
+
+akb_status akb_facet_quadrature(int32_t d, int64_t nb_nodes, const double* X, int64_t nb_facets,
+                                int32_t nf, const uint32_t* facets, double* coords, double* normals,
+                                double* weighted_shapes) {
+  akb_status st = check_facets(d, nb_nodes, X, nb_facets, nf, facets);
+  if (st != AKB_OK || nb_facets == 0) return st;
+  if (!coords || !normals || !weighted_shapes)
+    return fail(AKB_ERR_INVALID_ARGUMENT, "null argument");
+  const std::vector<FacetPoint> pts = facet_rule(nf);
+  const size_t nq = pts.size();
+  for (int64_t f = 0; f < nb_facets; ++f)
+    for (size_t q = 0; q < nq; ++q) {
+      const size_t k = (size_t)f * nq + q;
+      double wj;
+      if (!facet_point(d, nf, X, facets + f * nf, pts[q], coords + k * d, normals + k * d, &wj))
+        return fail(AKB_ERR_BAD_MESH, "degenerate facet");
+      for (int a = 0; a < nf; ++a) weighted_shapes[k * nf + a] = wj * pts[q].N[a];
+    }
   return AKB_OK;
 }
 

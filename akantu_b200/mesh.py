@@ -39,6 +39,21 @@ def element_properties(element_type):
     return dim, nnpe, nqp
 
 
+# facet kinds (the element types of a group's boundary elements); the
+# library has no quadrangle element, so the facet kind has a number of its own
+QUADRANGLE_4 = 5
+FACET_TYPES = {(2, 2): 1, (3, 3): 2, (3, 4): QUADRANGLE_4}  # (dim, nodes) -> type
+
+
+class IntegrationPoint:
+    """IntegrationPoint (element.hh): which Gauss point a NeumannFunctor is
+    called at -- type (the facet kind), element (the facet's index in the
+    group), num_point, ghost_type."""
+
+    def __init__(self, type, element=0, num_point=0, ghost_type=0):
+        self.type, self.element, self.num_point, self.ghost_type = type, element, num_point, ghost_type
+
+
 class Mesh:
     """Nodes (N x d, float64) + connectivity (E x n, uint32) + node groups."""
 
@@ -147,23 +162,47 @@ class Mesh:
         return self.facet_groups[name]
 
     def neumannForces(self, group, functor):
-        """The nodal forces of a Neumann condition (FromTraction or
-        FromStress) on a group's facets (akb_neumann_forces): (N, d)."""
+        """The nodal forces of a Neumann functor on a group's facets, (N, d):
+        FromTraction / FromStress integrated by akb_neumann_forces, any other
+        NeumannFunctor called at the facets' Gauss points
+        (akb_facet_quadrature) as functor(quad_point, dual, coord, normals)."""
         from . import _lib
+        from .model import FromStress, FromTraction
         if group in self._mixed_facets:
             raise ValueError("group '%s' has facets of two kinds (triangles and quadrangles)"
                              % group)
         X = np.ascontiguousarray(self.nodes, dtype=np.float64)
-        d = X.shape[1]
-        facets = np.ascontiguousarray(self.facet_groups.get(group, np.zeros((0, d), np.uint32)),
+        n, d = X.shape
+        facets = np.ascontiguousarray(self.facet_groups.get(group, np.zeros((0, 2), np.uint32)),
                                       dtype=np.uint32)
-        value = np.ascontiguousarray(functor.akb_value(d), dtype=np.float64)
-        out = np.zeros((X.shape[0], d))
-        _lib.check(_lib.lib().akb_neumann_forces(
-            d, X.shape[0], X.ctypes.data_as(C.POINTER(C.c_double)), facets.shape[0],
-            facets.shape[1] if facets.ndim == 2 and facets.shape[0] else (2 if d == 2 else 3),
-            facets.ctypes.data_as(C.POINTER(C.c_uint32)), functor.kind,
-            value.ctypes.data_as(C.POINTER(C.c_double)), out.ctypes.data_as(C.POINTER(C.c_double))))
+        nf, npf = facets.shape
+        xp = X.ctypes.data_as(C.POINTER(C.c_double))
+        fp = facets.ctypes.data_as(C.POINTER(C.c_uint32))
+        out = np.zeros((n, d))
+        if nf == 0:
+            return out
+        L = _lib.lib()
+        if type(functor) in (FromTraction, FromStress):
+            value = np.ascontiguousarray(functor.akb_value(d), dtype=np.float64)
+            _lib.check(L.akb_neumann_forces(d, n, xp, nf, npf, fp, functor.kind,
+                                            value.ctypes.data_as(C.POINTER(C.c_double)),
+                                            out.ctypes.data_as(C.POINTER(C.c_double))))
+            return out
+        nq = L.akb_facet_points(npf)
+        coords, normals = np.zeros((nf * nq, d)), np.zeros((nf * nq, d))
+        shapes = np.zeros((nf * nq, npf))
+        _lib.check(L.akb_facet_quadrature(d, n, xp, nf, npf, fp,
+                                          coords.ctypes.data_as(C.POINTER(C.c_double)),
+                                          normals.ctypes.data_as(C.POINTER(C.c_double)),
+                                          shapes.ctypes.data_as(C.POINTER(C.c_double))))
+        qp = IntegrationPoint(FACET_TYPES[(d, npf)])
+        for f in range(nf):
+            for q in range(nq):
+                k = f * nq + q
+                qp.element, qp.num_point = f, q
+                dual = np.zeros(d)
+                functor(qp, dual, coords[k], normals[k])
+                out[facets[f]] += shapes[k][:, None] * dual[None, :]
         return out
 
     # --- boundary groups (Mesh::createBoundaryGroupFromGeometry) ---------

@@ -157,30 +157,83 @@ def material_from_dict(d):
 _x, _y, _z = 0, 1, 2
 
 
-class FixedValue:
-    """BC::Dirichlet::FixedValue(value, axis)
-    (boundary_condition_functor_inline_impl.hh:85-93): the axis blocked,
-    the displacement set to value."""
+class DirichletFunctor:
+    """BC::Dirichlet::DirichletFunctor (boundary_condition_functor.hh,
+    py_boundary_conditions.cc): applyBC(functor, group) calls it once per
+    node of the group as functor(node, flags, primal, coord) -- flags the
+    node's blocked flags (bool, d) and primal its displacement (d), both
+    writable; coord its coordinates. Subclass it and define __call__."""
 
-    def __init__(self, value, axis):
-        self.value, self.axis = float(value), int(axis)
-
-
-class FreeBoundary:
-    """BC::Dirichlet::FreeBoundary(axis): the axis unblocked."""
-
-    def __init__(self, axis):
+    def __init__(self, axis=_x):
         self.axis = int(axis)
 
+    def __call__(self, node, flags, primal, coord):
+        raise NotImplementedError("a DirichletFunctor defines __call__")
 
-class FromTraction:
+
+class FixedValue(DirichletFunctor):
+    """BC::Dirichlet::FixedValue(value, axis)
+    (boundary_condition_functor_inline_impl.hh:85-93): the axis blocked, the
+    displacement set to value (applied on the device)."""
+
+    def __init__(self, value, axis):
+        super().__init__(axis)
+        self.value = float(value)
+
+    def __call__(self, node, flags, primal, coord):
+        flags[self.axis] = True
+        primal[self.axis] = self.value
+
+
+class IncrementValue(DirichletFunctor):
+    """BC::Dirichlet::IncrementValue(value, axis): the axis blocked, value
+    added to its displacement."""
+
+    def __init__(self, value, axis):
+        super().__init__(axis)
+        self.value = float(value)
+
+    def __call__(self, node, flags, primal, coord):
+        flags[self.axis] = True
+        primal[self.axis] += self.value
+
+
+class Increment(DirichletFunctor):
+    """BC::Dirichlet::Increment(vector): every axis blocked, the vector
+    added to the displacement."""
+
+    def __init__(self, increment):
+        super().__init__(_x)
+        self.increment = np.asarray(increment, dtype=np.float64).reshape(-1)
+
+    def __call__(self, node, flags, primal, coord):
+        flags[:] = True
+        primal += self.increment
+
+
+class NeumannFunctor:
+    """BC::Neumann::NeumannFunctor (boundary_condition_functor.hh,
+    py_boundary_conditions.cc): applyBC(functor, group) calls it at every
+    Gauss point of the group's facets as functor(quad_point, dual, coord,
+    normals) -- dual (d) to receive the traction there, coord the point's
+    coordinates, normals the facet's unit normal -- and adds the integrated
+    nodal forces to the external force. Subclass it and define __call__."""
+
+    def __call__(self, quad_point, dual, coord, normals):
+        raise NotImplementedError("a NeumannFunctor defines __call__")
+
+
+class FromTraction(NeumannFunctor):
     """BC::Neumann::FromSameDim (FromTraction in the reference's Python
-    package): a traction vector on the group's facets, its nodal forces
-    added to the external force."""
+    package): a traction vector on the group's facets (integrated in the
+    library, akb_neumann_forces)."""
     kind = _abi.NEUMANN_TRACTION
 
     def __init__(self, traction):
         self.traction = np.asarray(traction, dtype=np.float64).reshape(-1)
+
+    def __call__(self, quad_point, dual, coord, normals):
+        dual[:] = self.traction
 
     def akb_value(self, dim):
         if self.traction.size != dim:
@@ -188,7 +241,7 @@ class FromTraction:
         return self.traction
 
 
-class FromStress:
+class FromStress(NeumannFunctor):
     """BC::Neumann::FromHigherDim (FromStress in the reference's Python
     package): a stress tensor, the traction sigma n with n each facet's unit
     normal as its node order gives it."""
@@ -197,10 +250,20 @@ class FromStress:
     def __init__(self, stress):
         self.stress = np.asarray(stress, dtype=np.float64)
 
+    def __call__(self, quad_point, dual, coord, normals):
+        dual[:] = self.stress @ normals
+
     def akb_value(self, dim):
         if self.stress.shape != (dim, dim):
             raise ValueError("a %s stress in %dD" % (self.stress.shape, dim))
         return self.stress.T.reshape(-1)  # column-major
+
+
+class FreeBoundary(NeumannFunctor):
+    """BC::Neumann::FreeBoundary: a zero traction (adds nothing)."""
+
+    def __call__(self, quad_point, dual, coord, normals):
+        dual[:] = 0.0
 
 
 FromSameDim = FromTraction
@@ -467,26 +530,36 @@ class SolidMechanicsModel:
                                         v.ctypes.data_as(C.POINTER(C.c_double))))
 
     def applyBC(self, functor, group):
-        """applyBC(functor, group) (py_solid_mechanics_model.cc:58-63,
-        boundary_condition_tmpl.hh:63-200) on the nodes of a mesh group
-        (the node group of a `$PhysicalNames` group, or one created with
-        Mesh.createNodeGroup): FixedValue(value, axis) blocks the axis and
-        sets the displacement, FreeBoundary(axis) unblocks it; FromTraction /
-        FromStress add the nodal forces of a traction on the group's facets
-        to the external force (boundary_condition_tmpl.hh:95-185)."""
-        if isinstance(functor, (FromTraction, FromStress)):
-            # ADDED into the external force, as the reference assembles it
-            f = self.getExternalForce()
-            f += self.mesh.neumannForces(group, functor)
+        """applyBC(functor, group) (py_solid_mechanics_model.cc:58-67,
+        boundary_condition_tmpl.hh) on a mesh group (a `$PhysicalNames`
+        group, or one created with Mesh.createNodeGroup; a Dirichlet functor
+        also takes a node list). A Dirichlet functor acts on the group's
+        nodes: FixedValue on the device, any other (IncrementValue, Increment,
+        a DirichletFunctor written in Python) node by node on the host. A
+        Neumann functor adds the nodal forces of its traction on the group's
+        facets to the external force: FromTraction / FromStress integrated in
+        the library, a NeumannFunctor written in Python at the facets' Gauss
+        points (boundary_condition_tmpl.hh:95-185)."""
+        if isinstance(functor, NeumannFunctor):
+            if not isinstance(group, str):
+                raise TypeError("a Neumann condition acts on a named group's facets")
+            forces = self.mesh.neumannForces(group, functor)
+            f = self.getExternalForce()  # ADDED, as the reference assembles it
+            f += forces
             return
+        if not isinstance(functor, DirichletFunctor):
+            raise TypeError("applyBC takes a DirichletFunctor or a NeumannFunctor")
         nodes = self.mesh.getNodeGroup(group) if isinstance(group, str) else np.asarray(group)
-        if isinstance(functor, FixedValue):
+        if type(functor) is FixedValue:
             self.applyDirichlet(nodes, functor.axis, functor.value)
-        elif isinstance(functor, FreeBoundary):
-            b = self.getBlockedDOFs()
-            b[np.asarray(nodes, dtype=np.int64), functor.axis] = False
-        else:
-            raise TypeError("applyBC takes FixedValue, FreeBoundary, FromTraction or FromStress")
+            return
+        u = np.array(self.getField(_abi.FIELD_DISPLACEMENT))
+        b = self.getBlockedDOFs().copy()
+        X = np.asarray(self.mesh.nodes, dtype=np.float64)
+        for node in np.asarray(nodes, dtype=np.int64):
+            functor(int(node), b[node], u[node], X[node])
+        self.setField(_abi.FIELD_DISPLACEMENT, u)
+        self.setBlockedDOFs(b)
 
     def getGradU(self):
         return self.getField(_abi.FIELD_GRAD_U)

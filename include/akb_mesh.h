@@ -87,6 +87,19 @@ akb_status akb_neumann_forces(int32_t spatial_dimension, int64_t nb_nodes, const
                               int64_t nb_facets, int32_t nodes_per_facet, const uint32_t* facets,
                               int32_t kind, const double* value, double* forces);
 
+/* The Gauss points of the same facets, for a Neumann functor evaluated by
+ * the caller (a NeumannFunctor written in Python, py_boundary_conditions.cc):
+ * akb_facet_points(nodes_per_facet) points per facet (1 or 4; 0 for an
+ * unknown facet), and at facet f, point q (row k = f * points + q) its
+ * coordinates (coords[k][d]), unit normal (normals[k][d]) and w |J| N_a
+ * (weighted_shapes[k][nodes_per_facet]): the force of a functor value t there
+ * on the facet's node a is weighted_shapes[k][a] t. */
+int32_t akb_facet_points(int32_t nodes_per_facet);
+akb_status akb_facet_quadrature(int32_t spatial_dimension, int64_t nb_nodes, const double* nodes,
+                                int64_t nb_facets, int32_t nodes_per_facet,
+                                const uint32_t* facets, double* coords, double* normals,
+                                double* weighted_shapes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -215,3 +215,119 @@ def test_group_with_facets_of_two_kinds():
     assert "top" not in mesh.facet_groups
     with pytest.raises(ValueError):
         mesh.neumannForces("top", FromTraction([0.0, 0.0, 1.0]))
+
+
+class PyTraction(__import__("akantu_b200").NeumannFunctor):
+    """A NeumannFunctor written in Python: a constant traction."""
+
+    def __init__(self, t):
+        self.t = np.asarray(t, dtype=float)
+        self.calls = []
+
+    def __call__(self, quad_point, dual, coord, normals):
+        self.calls.append((quad_point.element, quad_point.num_point))
+        dual[:] = self.t
+
+
+class PyStress(__import__("akantu_b200").NeumannFunctor):
+    def __init__(self, s):
+        self.s = np.asarray(s, dtype=float)
+
+    def __call__(self, quad_point, dual, coord, normals):
+        dual[:] = self.s @ normals
+
+
+class PyLinear(__import__("akantu_b200").NeumannFunctor):
+    """A traction growing with x: evaluated at each Gauss point."""
+
+    def __call__(self, quad_point, dual, coord, normals):
+        dual[:] = 0.0
+        dual[-1] = coord[0]
+
+
+def test_neumann_functors_written_in_python():
+    import akantu_b200 as aka
+    mesh = Mesh(2)
+    mesh.read(os.path.join(GOLDEN, "cohesive_strait_2D.msh"))
+    t = PyTraction([0.5, -2.0])
+    assert np.allclose(mesh.neumannForces("loading", t),
+                       mesh.neumannForces("loading", FromTraction([0.5, -2.0])), rtol=0, atol=1e-15)
+    assert t.calls == [(f, 0) for f in range(len(mesh.getFacetGroup("loading")))]  # one point each
+    sigma = np.array([[1.0, 0.3], [0.3, -2.0]])
+    assert np.allclose(mesh.neumannForces("fixed", PyStress(sigma)),
+                       mesh.neumannForces("fixed", FromStress(sigma)), rtol=0, atol=1e-15)
+    assert np.all(mesh.neumannForces("loading", aka.FreeBoundary()) == 0.0)
+    # 2 x 2 points on a quadrangle: a traction linear in x integrates exactly
+    hexm = Mesh(3)
+    hexm.read_msh_text(HEX_WITH_TOP)
+    f = hexm.neumannForces("top", PyLinear())
+    assert f[:, 2].sum() == pytest.approx(0.5, rel=1e-14)  # integral of x over the unit square
+    assert f[5, 2] > f[4, 2]  # the x = 1 corners carry more
+    assert np.allclose(hexm.neumannForces("top", PyStress(np.diag([0.0, 0.0, -3.0]))),
+                       hexm.neumannForces("top", FromStress(np.diag([0.0, 0.0, -3.0]))))
+
+
+def test_dirichlet_functors():
+    """FixedValue, IncrementValue and Increment act on a node's flags and
+    displacement as boundary_condition_functor_inline_impl.hh states."""
+    import akantu_b200 as aka
+    flags, primal = np.zeros(3, bool), np.array([1.0, 2.0, 3.0])
+    aka.FixedValue(5.0, aka._y)(0, flags, primal, np.zeros(3))
+    assert flags.tolist() == [False, True, False] and primal.tolist() == [1.0, 5.0, 3.0]
+    aka.IncrementValue(0.5, aka._z)(0, flags, primal, np.zeros(3))
+    assert flags.tolist() == [False, True, True] and primal.tolist() == [1.0, 5.0, 3.5]
+    aka.Increment([1.0, 1.0, -1.0])(0, flags, primal, np.zeros(3))
+    assert flags.all() and primal.tolist() == [2.0, 6.0, 2.5]
+    with pytest.raises(NotImplementedError):
+        aka.DirichletFunctor()(0, flags, primal, np.zeros(3))
+
+
+def test_apply_bc_dispatch():
+    """SolidMechanicsModel.applyBC without a device (its field accessors
+    replaced by arrays): FixedValue goes to the device Dirichlet call, other
+    Dirichlet functors run node by node on copies that are written back,
+    Neumann functors add their forces to the external force."""
+    import akantu_b200 as aka
+    from akantu_b200.model import SolidMechanicsModel
+    mesh = Mesh(2)
+    mesh.read(os.path.join(GOLDEN, "cohesive_strait_2D.msh"))
+    n = mesh.getNbNodes()
+
+    class Arrays(SolidMechanicsModel):
+        def __init__(self):
+            super().__init__(mesh, [aka.MaterialElastic(rho=1, E=1, nu=0.3)])
+            self.u, self.b, self.fext = np.zeros((n, 2)), np.zeros((n, 2), bool), np.ones((n, 2))
+            self.dirichlet = []
+
+        def getField(self, field):
+            assert field == _abi.FIELD_DISPLACEMENT
+            return self.u
+
+        def getBlockedDOFs(self):
+            return self.b
+
+        def setField(self, field, values):
+            self.u = np.array(values)
+
+        def setBlockedDOFs(self, blocked):
+            self.b = np.array(blocked, bool)
+
+        def getExternalForce(self):
+            return self.fext
+
+        def applyDirichlet(self, nodes, component, values):
+            self.dirichlet.append((sorted(np.asarray(nodes).tolist()), component, values))
+
+    m = Arrays()
+    fixed = mesh.getNodeGroup("fixed")
+    m.applyBC(aka.FixedValue(0.25, aka._y), "fixed")
+    assert m.dirichlet == [(sorted(fixed.tolist()), aka._y, 0.25)]
+    m.applyBC(aka.IncrementValue(0.5, aka._x), "fixed")
+    m.applyBC(aka.IncrementValue(0.5, aka._x), "fixed")
+    assert np.all(m.u[fixed, 0] == 1.0) and np.all(m.b[fixed, 0])
+    others = np.setdiff1d(np.arange(n), fixed)
+    assert np.all(m.u[others] == 0.0) and not m.b[others].any()
+    m.applyBC(aka.FromTraction([0.0, -2.0]), "loading")
+    assert np.allclose(m.fext, 1.0 + mesh.neumannForces("loading", FromTraction([0.0, -2.0])))
+    with pytest.raises(TypeError):
+        m.applyBC(object(), "fixed")
