@@ -369,7 +369,7 @@ class LawBridge:
         n, d = self.npoints, self.dim
         # the column-major storage: (E*q, d*d), row[i + j*d]
         g = grad_u.transpose(1, 2).reshape(n, d * d).cpu().numpy()
-        s = np.empty((n, d * d))
+        s = np.zeros((n, d * d))
         for law, rows in zip(self.laws, self.rows):
             law._grad_u[...] = g[rows]
             law.computeStress(self.el_type, _not_ghost)
