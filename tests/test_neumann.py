@@ -11,6 +11,7 @@ import os
 import numpy as np
 import pytest
 
+import akantu_b200 as aka
 from akantu_b200 import _abi
 from akantu_b200._lib import AkbError, check, lib
 from akantu_b200.mesh import Mesh
@@ -217,7 +218,7 @@ def test_group_with_facets_of_two_kinds():
         mesh.neumannForces("top", FromTraction([0.0, 0.0, 1.0]))
 
 
-class PyTraction(__import__("akantu_b200").NeumannFunctor):
+class PyTraction(aka.NeumannFunctor):
     """A NeumannFunctor written in Python: a constant traction."""
 
     def __init__(self, t):
@@ -229,7 +230,7 @@ class PyTraction(__import__("akantu_b200").NeumannFunctor):
         dual[:] = self.t
 
 
-class PyStress(__import__("akantu_b200").NeumannFunctor):
+class PyStress(aka.NeumannFunctor):
     def __init__(self, s):
         self.s = np.asarray(s, dtype=float)
 
@@ -237,7 +238,7 @@ class PyStress(__import__("akantu_b200").NeumannFunctor):
         dual[:] = self.s @ normals
 
 
-class PyLinear(__import__("akantu_b200").NeumannFunctor):
+class PyLinear(aka.NeumannFunctor):
     """A traction growing with x: evaluated at each Gauss point."""
 
     def __call__(self, quad_point, dual, coord, normals):
@@ -246,7 +247,6 @@ class PyLinear(__import__("akantu_b200").NeumannFunctor):
 
 
 def test_neumann_functors_written_in_python():
-    import akantu_b200 as aka
     mesh = Mesh(2)
     mesh.read(os.path.join(GOLDEN, "cohesive_strait_2D.msh"))
     t = PyTraction([0.5, -2.0])
@@ -287,7 +287,6 @@ def test_apply_bc_dispatch():
     replaced by arrays): FixedValue goes to the device Dirichlet call, other
     Dirichlet functors run node by node on copies that are written back,
     Neumann functors add their forces to the external force."""
-    import akantu_b200 as aka
     from akantu_b200.model import SolidMechanicsModel
     mesh = Mesh(2)
     mesh.read(os.path.join(GOLDEN, "cohesive_strait_2D.msh"))
