@@ -270,7 +270,6 @@ def test_neumann_functors_written_in_python():
 def test_dirichlet_functors():
     """FixedValue, IncrementValue and Increment act on a node's flags and
     displacement as boundary_condition_functor_inline_impl.hh states."""
-    import akantu_b200 as aka
     flags, primal = np.zeros(3, bool), np.array([1.0, 2.0, 3.0])
     aka.FixedValue(5.0, aka._y)(0, flags, primal, np.zeros(3))
     assert flags.tolist() == [False, True, False] and primal.tolist() == [1.0, 5.0, 3.0]
