@@ -329,3 +329,30 @@ def test_apply_bc_dispatch():
     assert np.allclose(m.fext, 1.0 + mesh.neumannForces("loading", FromTraction([0.0, -2.0])))
     with pytest.raises(TypeError):
         m.applyBC(object(), "fixed")
+
+
+@pytest.mark.parametrize("etype", [_abi.TRIANGLE_3, _abi.TETRAHEDRON_4, _abi.HEXAHEDRON_8],
+                         ids=["triangle_3", "tetrahedron_4", "hexahedron_8"])
+def test_library_matches_the_work_balance_port(etype):
+    """The work-balance port's nodal forces (FromTraction(0.5 e_x) on the
+    bar's face x = max, test_solid_mechanics_model_work_dynamics.cc:84-106,
+    restated there by sharing each facet's measure equally) against
+    akb_neumann_forces on the same facets."""
+    from akantu_b200.mesh import _FACETS
+    from tests.reference_ports import _traction_forces, bar_mesh
+    mesh = bar_mesh(etype)
+    X = mesh.nodes
+    xmax = X[:, 0].max()
+    facets, seen = [], set()
+    for elem in mesh.connectivity:
+        for fc in _FACETS[mesh.element_type]:
+            nodes = [int(elem[k]) for k in fc]
+            key = tuple(sorted(nodes))
+            if all(X[n, 0] > xmax - 1e-6 for n in nodes) and key not in seen:
+                seen.add(key)
+                facets.append(nodes)
+    d = mesh.spatial_dimension
+    got = forces(X, facets, _abi.NEUMANN_TRACTION, [0.5] + [0.0] * (d - 1))
+    want = _traction_forces(mesh, 0.5)
+    assert np.allclose(got, want, rtol=0, atol=1e-15)
+    assert got[:, 0].sum() == pytest.approx(0.5, rel=1e-14)  # the end face's measure is 1
