@@ -219,6 +219,63 @@ class Mesh:
                 nodes.update(key)
         return np.array(sorted(nodes), dtype=np.int64)
 
+    def boundary_facets(self):
+        """The facets that belong to exactly one element, each ordered so that
+        its normal (the reference's: (t_y, -t_x) of a segment's tangent,
+        t_xi x t_eta of a surface facet) points out of its element."""
+        X = np.asarray(self.nodes, dtype=np.float64)
+        owner = {}
+        for e, elem in enumerate(self.connectivity):
+            for f in _FACETS[self.element_type]:
+                nodes = [int(elem[k]) for k in f]
+                key = tuple(sorted(nodes))
+                owner[key] = None if key in owner else (e, nodes)
+        out = []
+        for key, val in owner.items():
+            if val is None:
+                continue
+            e, nodes = val
+            P = X[nodes]
+            if len(nodes) == 2:
+                t = P[1] - P[0]
+                n = np.array([t[1], -t[0]])
+            elif len(nodes) >= 3:
+                n = np.cross(P[1] - P[0], P[-1] - P[0]) if len(nodes) == 4 else \
+                    np.cross(P[1] - P[0], P[2] - P[0])
+            else:
+                continue  # points: no facet orientation in 1D
+            out_dir = P.mean(axis=0) - X[self.connectivity[e]].mean(axis=0)
+            if np.dot(n, out_dir) < 0:
+                nodes = nodes[::-1] if len(nodes) < 4 else [nodes[0]] + nodes[:0:-1]
+            out.append(nodes)
+        return np.array(out, dtype=np.uint32).reshape(len(out), -1 if out else 0)
+
+    def createElementGroupFromNodeGroup(self, name, node_group, dimension=None):
+        """Mesh::createElementGroupFromNodeGroup (group_manager.hh): of the
+        spatial dimension, the elements whose nodes all lie in the node
+        group; of one dimension less, the boundary facets whose nodes all lie
+        in it (outward-oriented, for Neumann conditions). The group's node
+        group is made of its elements' nodes, as an element group's is."""
+        d = self.spatial_dimension
+        dimension = d if dimension is None else int(dimension)
+        inside = np.zeros(len(self.nodes), dtype=bool)
+        inside[self.getNodeGroup(node_group) if isinstance(node_group, str)
+               else np.asarray(node_group, dtype=np.int64)] = True
+        if dimension == d:
+            conn = np.asarray(self.connectivity, dtype=np.int64)
+            elements = np.nonzero(inside[conn].all(axis=1))[0]
+            self.element_groups[name] = elements
+            self.node_groups[name] = np.unique(conn[elements])
+        elif dimension == d - 1 and d >= 2:
+            facets = self.boundary_facets()
+            keep = facets[inside[facets.astype(np.int64)].all(axis=1)]
+            self.facet_groups[name] = keep
+            self.element_groups[name] = np.zeros(0, dtype=np.int64)
+            self.node_groups[name] = np.unique(keep.astype(np.int64))
+        else:
+            raise ValueError("element groups of dimension %d or %d" % (d, d - 1))
+        return self.node_groups[name]
+
     def createBoundaryGroupFromGeometry(self):
         """One node group 'boundary' with every node on a boundary facet
         (the reference splits it into connected surfaces; the explicit path

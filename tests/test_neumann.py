@@ -356,3 +356,34 @@ def test_library_matches_the_work_balance_port(etype):
     want = _traction_forces(mesh, 0.5)
     assert np.allclose(got, want, rtol=0, atol=1e-15)
     assert got[:, 0].sum() == pytest.approx(0.5, rel=1e-14)  # the end face's measure is 1
+
+
+@pytest.mark.parametrize("etype", [_abi.TRIANGLE_3, _abi.TETRAHEDRON_4, _abi.HEXAHEDRON_8],
+                         ids=["triangle_3", "tetrahedron_4", "hexahedron_8"])
+def test_element_groups_from_node_groups(etype):
+    """createElementGroupFromNodeGroup as the work-balance test uses it: the
+    nodes of the face x = max, their facets (dimension d - 1) as a group,
+    FromTraction on it equal to the port's forces; every boundary facet
+    oriented outward (a uniform stress on the closed boundary sums to
+    zero, sigma = I pushes the x = max face towards +x)."""
+    from tests.reference_ports import _traction_forces, bar_mesh
+    mesh = bar_mesh(etype)
+    X = mesh.nodes
+    d = mesh.spatial_dimension
+    end = np.nonzero(X[:, 0] > X[:, 0].max() - 1e-6)[0]
+    mesh.createNodeGroup("apply_force", end)
+    nodes = mesh.createElementGroupFromNodeGroup("el_apply_force", "apply_force", d - 1)
+    assert sorted(nodes.tolist()) == sorted(end.tolist())
+    f = mesh.neumannForces("el_apply_force", FromTraction([0.5] + [0.0] * (d - 1)))
+    assert np.allclose(f, _traction_forces(mesh, 0.5), rtol=0, atol=1e-15)
+    g = mesh.neumannForces("el_apply_force", FromStress(np.eye(d)))
+    assert g[:, 0].sum() == pytest.approx(1.0, rel=1e-14)  # outward: +x, unit face
+    mesh.createNodeGroup("all", np.arange(len(X)))
+    mesh.createElementGroupFromNodeGroup("skin", "all", d - 1)
+    rng = np.random.default_rng(8)
+    s = rng.normal(size=(d, d))
+    h = mesh.neumannForces("skin", FromStress(s + s.T))
+    assert np.abs(h.sum(axis=0)).max() <= 1e-12
+    # of the spatial dimension: the elements whose nodes are all in the group
+    mesh.createElementGroupFromNodeGroup("bulk", "all")
+    assert len(mesh.getElementGroup("bulk")) == len(mesh.connectivity)
