@@ -20,7 +20,6 @@ import os
 import sys
 import time
 
-import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "data", "rve_surrogate.npz")

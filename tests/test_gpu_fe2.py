@@ -3,7 +3,7 @@ path with its envelope fallback, and dataset generation."""
 import numpy as np
 import pytest
 
-from akantu_b200 import _abi, fe2
+from akantu_b200 import fe2
 
 pytestmark = pytest.mark.gpu
 

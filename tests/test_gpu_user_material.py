@@ -1,14 +1,12 @@
 """User materials (AKB_MATERIAL_USER): the step split around
 Material::computeStress, with stresses written by the caller on the device,
 against the built-in laws and against homogeneous RVEs."""
-import ctypes as C
-
 import numpy as np
 import pytest
 
 from akantu_b200 import _abi, configs
 from akantu_b200._lib import AkbError, lib
-from akantu_b200.mesh import block_hexahedron8, cube_tetrahedron4
+from akantu_b200.mesh import block_hexahedron8
 from akantu_b200.model import (MaterialElastic, MaterialNeohookean, MaterialUser,
                                SolidMechanicsModel)
 from tests.fe2_cases import lame
