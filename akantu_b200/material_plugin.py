@@ -20,6 +20,8 @@ d x d matrices (row[i + j*d] = du_i/dX_j), rows in element order then Gauss
 point order, for the material's own elements only; getPotentialEnergy is
 (points, 1).
 """
+import ast
+import math
 import re
 import weakref
 
@@ -43,34 +45,119 @@ _pat_parsmod = _pat_parsable | _pat_modifiable
 BUILTIN_LAWS = ("elastic", "neohookean")
 
 _sections = []  # [(law, {key: value})] of the last parseInput
+_globals = {}    # its global parameters
 
 
-def _value(text):
+_FUNCTIONS = {"max": max, "min": min, "abs": abs, "sqrt": math.sqrt, "exp": math.exp,
+              "log": math.log, "sin": math.sin, "cos": math.cos, "tan": math.tan,
+              "pow": math.pow, "floor": math.floor, "ceil": math.ceil}
+_CONSTANTS = {"pi": math.pi, "e": math.e}
+
+
+class _Scope:
+    """The parameters of a section (raw text), its enclosing scope, and the
+    values already evaluated: a name in an expression is looked up here,
+    then in the enclosing sections, up to the global parameters (the
+    reference's parser resolves them the same way)."""
+
+    def __init__(self, raw, parent=None):
+        self.raw, self.parent, self.values, self.busy = raw, parent, {}, set()
+
+    def lookup(self, name):
+        scope = self
+        while scope is not None:
+            if name in scope.raw:
+                return scope.value(name)
+            scope = scope.parent
+        if name in _CONSTANTS:
+            return _CONSTANTS[name]
+        raise KeyError(name)
+
+    def value(self, name):
+        if name == "name":  # a section's name is text, whatever it reads like
+            return self.raw[name]
+        if name not in self.values:
+            if name in self.busy:
+                raise KeyError(name)  # a cycle: left as text
+            self.busy.add(name)
+            try:
+                self.values[name] = _evaluate(self.raw[name], self)
+            finally:
+                self.busy.discard(name)
+        return self.values[name]
+
+
+def _evaluate(text, scope):
+    """A parameter's value: an arithmetic expression over numbers, the
+    constants pi and e, the parameters in scope and a few functions (max,
+    min, sqrt, ...), a vector [a, b, ...] or a matrix [[...], [...]] of
+    such expressions, true / false; anything else (a name, a random
+    distribution) stays the text it is."""
     t = text.strip()
-    if t.startswith("[") and t.endswith("]"):  # a vector parameter
-        return [_value(x) for x in t[1:-1].split(",") if x.strip()]
     if t.lower() in ("true", "false"):
         return t.lower() == "true"
     try:
-        return float(t)
-    except ValueError:
+        tree = ast.parse(t.replace("^", "**"), mode="eval")
+    except SyntaxError:
         return t
 
+    def ev(node):
+        if isinstance(node, ast.Expression):
+            return ev(node.body)
+        if isinstance(node, ast.Constant) and isinstance(node.value, (int, float)):
+            return float(node.value)
+        if isinstance(node, ast.Name):
+            return scope.lookup(node.id) if scope is not None else _CONSTANTS[node.id]
+        if isinstance(node, ast.UnaryOp) and isinstance(node.op, (ast.USub, ast.UAdd)):
+            v = ev(node.operand)
+            return -v if isinstance(node.op, ast.USub) else v
+        if isinstance(node, ast.BinOp):
+            a, b = ev(node.left), ev(node.right)
+            ops = {ast.Add: lambda: a + b, ast.Sub: lambda: a - b, ast.Mult: lambda: a * b,
+                   ast.Div: lambda: a / b, ast.Pow: lambda: a ** b, ast.Mod: lambda: a % b}
+            if type(node.op) in ops:
+                return ops[type(node.op)]()
+        if (isinstance(node, ast.Call) and isinstance(node.func, ast.Name)
+                and node.func.id in _FUNCTIONS and not node.keywords):
+            return float(_FUNCTIONS[node.func.id](*[ev(a) for a in node.args]))
+        if isinstance(node, ast.List):
+            return [ev(e) for e in node.elts]
+        raise ValueError("not an arithmetic expression")
 
-_OPEN = re.compile(r"([A-Za-z_]\w*)(?:[ \t\r\n]+([A-Za-z_][\w:.-]*))?[ \t\r\n]*\[")
+    try:
+        v = ev(tree)
+    except (KeyError, ValueError, TypeError, ZeroDivisionError, OverflowError):
+        return t
+    if isinstance(v, (float, list)) and not isinstance(v, bool):
+        return v
+    return t
+
+
+def _value(text):
+    """A value with no parameters in scope."""
+    return _evaluate(text, None)
+
+
+_OPEN = re.compile(r"([A-Za-z_]\w*)(?:[ \t]+([A-Za-z_][\w:.-]*))?(?:[ \t]+([A-Za-z_][\w:.-]*))?"
+                   r"[ \t\r\n]*\[")
 _KEY = re.compile(r"([A-Za-z_]\w*)[ \t]*=[ \t]*")
 
 
 def parse_input_text(text):
-    """The `material <law> [ key = value ... ]` sections of an Akantu input
-    file (Parser::parse, src/io/parser/): `#` comments, white space and line
-    breaks anywhere between tokens, sections nested in other sections, a
-    value up to the end of its line (or the section's closing bracket) read
-    as a number, true/false, a vector `[a, b, ...]` or a plain string.
-    Replaces the sections of an earlier call; returns them."""
-    global _sections
-    body = "\n".join(line.split("#", 1)[0] for line in text.splitlines())
-    found, stack = [], []  # stack: (kind, law, params) of the open sections
+    """The sections of an Akantu input file (Parser::parse, src/io/parser/):
+    `type [name [option]] [ ... ]` sections nested at will, `key = value`
+    parameters in them and at the top level (the global section), `#`
+    comments, a value running to the end of its line (or the closing bracket
+    of its section; `\\` continues it on the next line, brackets spanning
+    lines do too), evaluated as _evaluate says with names resolved from the
+    innermost section out to the global parameters. Keeps the material
+    sections (returned, and for the models created after it) and the global
+    parameters (input_parameters). Replaces what an earlier call read."""
+    global _sections, _globals
+    lines = [line.split("#", 1)[0] for line in text.splitlines()]
+    body = "\n".join(lines).replace("\\\n", " ")
+    root = ("global", "", "", {}, [])  # kind, name, option, raw params, children
+    stack = [root]
     pos, n = 0, len(body)
     while True:
         while pos < n and body[pos].isspace():
@@ -78,41 +165,63 @@ def parse_input_text(text):
         if pos >= n:
             break
         if body[pos] == "]":
-            if not stack:
+            if len(stack) == 1:
                 raise ValueError("unbalanced ']' in the input")
-            kind, law, params = stack.pop()
-            if kind == "material":
-                if not law:
-                    raise ValueError("material section without a law")
-                found.append((law, params))
+            sec = stack.pop()
+            if sec[0] == "material" and not sec[1]:
+                raise ValueError("material section without a law")
+            stack[-1][4].append(sec)
             pos += 1
             continue
         m = _KEY.match(body, pos)
-        if m and stack:
-            start = m.end()
-            if body.startswith("[", start):  # a vector value: to its bracket
-                end = body.find("]", start)
-                if end < 0:
-                    raise ValueError("unterminated vector value of '%s'" % m.group(1))
+        if m:
+            start = end = m.end()
+            depth = 0
+            while end < n:
+                ch = body[end]
+                if ch == "[":
+                    depth += 1
+                elif ch == "]":
+                    if depth == 0:
+                        break  # the section's closing bracket
+                    depth -= 1
+                elif ch == "\n" and depth == 0:
+                    break
                 end += 1
-            else:
-                end = start
-                while end < n and body[end] not in "\n]":
-                    end += 1
-            stack[-1][2][m.group(1)] = _value(body[start:end])
+            if depth:
+                raise ValueError("unterminated value of '%s'" % m.group(1))
+            stack[-1][3][m.group(1)] = " ".join(body[start:end].split())
             pos = end
             continue
         m = _OPEN.match(body, pos)
         if m:
-            stack.append((m.group(1), m.group(2) or "", {}))
+            stack.append((m.group(1), m.group(2) or "", m.group(3) or "", {}, []))
             pos = m.end()
             continue
         line = body[pos:].split("\n", 1)[0]
         raise ValueError("cannot read the input at: %r" % line)
-    if stack:
+    if len(stack) > 1:
         raise ValueError("unterminated section '%s %s'" % stack[-1][:2])
+    found = []
+
+    def walk(sec, parent):
+        scope = _Scope(sec[3], parent)
+        if sec[0] == "material":
+            found.append((sec[1], {k: scope.value(k) for k in sec[3]}))
+        for child in sec[4]:
+            walk(child, scope)
+        return scope
+
+    top = walk(root, None)
+    _globals = {k: top.value(k) for k in root[3]}
     _sections = found
     return list(found)
+
+
+def input_parameters():
+    """The global parameters of the last parseInput (Parser::getParameter),
+    evaluated."""
+    return dict(_globals)
 
 
 def parseInput(input_file):

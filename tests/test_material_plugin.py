@@ -40,7 +40,7 @@ def test_input_sections():
     assert got == [("neohookean", dict(name="rubber", rho=1100.0, direction=[1.0, 0.0, -2.5],
                                        E=1e6))]
     assert mp.parse_input_text("") == [] and mp.input_sections() == []  # replaced, and cleared
-    for bad in ("material elastic [ rho = 1", "]", "material [ rho = 1 ]", "rho = 1"):
+    for bad in ("material elastic [ rho = 1", "]", "material [ rho = 1 ]", "material elastic [ = 1 ]"):
         with pytest.raises(ValueError):
             mp.parse_input_text(bad)
 
@@ -87,6 +87,40 @@ def factory():
     f.registerAllocator("transposing", lambda dim, law, model, mid: Transposing(model, mid))
     yield f
     mp.parse_input_text("")
+
+
+def test_input_grammar_of_the_reference_parser():
+    """The constructs of the reference's parser test
+    (test_io/test_parser/test_parser.cc and its verified output), in an
+    input of this test's own: global parameters, expressions over earlier
+    parameters with pi and max, a section option, a nested section, a
+    vector, a matrix continued over two lines, a random distribution kept as
+    text, a name never evaluated."""
+    text = """seed = 42
+    level = 2
+    material elastic opt [
+        name = e        # a name, not the constant
+        E = 1 + 3 * level
+        rho = 2^3
+        nested rules [
+            E = 7
+        ]
+    ]
+    base = 50
+    angle = 2*pi + max(2, base)
+    vect = [ 1, 20+5, angle ]
+    mat = [[ 1, 2 ], \\
+           [ base, 5+8 ]]
+    rand = 10 uniform [0.2, 0.5 ]
+    """
+    got = mp.parse_input_text(text)
+    assert got == [("elastic", dict(name="e", E=7.0, rho=8.0))]
+    g = mp.input_parameters()
+    assert g["seed"] == 42.0 and g["base"] == 50.0
+    assert g["angle"] == 2 * np.pi + 50.0  # bit for bit, as the reference's test checks
+    assert g["vect"] == [1.0, 25.0, 2 * np.pi + 50.0]
+    assert g["mat"] == [[1.0, 2.0], [50.0, 13.0]]
+    assert g["rand"] == "10 uniform [0.2, 0.5 ]"
 
 
 def test_factory_and_parameters(factory):
