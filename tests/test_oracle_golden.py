@@ -101,3 +101,39 @@ def test_energy_conservation_neohookean_block():
     # central differences conserve a shadow energy; at dt = 0.1 dt_crit the
     # kinetic + potential sum stays within half a percent
     assert worst < 5e-3
+
+
+def _oracle_P(H, mat):
+    """The oracle's first Piola-Kirchhoff stress of the neo-Hookean law at
+    F = I + H: one tetrahedron deformed homogeneously (u = H X), its stress
+    field (PK2 S, column-major) times F."""
+    from akantu_b200.mesh import Mesh
+    X = np.array([[0.0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]])
+    mesh = Mesh(3, _abi.TETRAHEDRON_4, X, np.array([[0, 1, 2, 3]], dtype=np.uint32))
+    m = OracleAdapter(mesh, mat)
+    m.set(_abi.FIELD_DISPLACEMENT, X @ H.T)
+    m.assemble_internal_forces()
+    S = np.asarray(m.get(_abi.FIELD_STRESS)).reshape(3, 3).T  # row [i + 3 j] = S_ij
+    return (np.eye(3) + H) @ S
+
+
+def test_neohookean_law_properties():
+    """The oracle's neo-Hookean law (material_neohookean_inline_impl.hh:46-65)
+    against an independent numpy statement of the same law, and its
+    properties: objectivity P(QF) = Q P(F), the small-strain limit (the
+    linear elastic law with the same Lame constants)."""
+    from tests.fe2_cases import lame, neohookean_P, random_rotation
+    mat = dict(kind=_abi.MATERIAL_NEOHOOKEAN, rho=1.0, E=3.0, nu=0.3)
+    lam, mu = lame(mat)
+    rng = np.random.default_rng(21)
+    for _ in range(3):
+        H = rng.uniform(-0.2, 0.2, (3, 3))
+        P = _oracle_P(H, mat)
+        assert np.allclose(P, neohookean_P(H, lam, mu), rtol=0, atol=1e-13 * np.abs(P).max())
+        Q = random_rotation(rng)
+        PQ = _oracle_P(Q @ (np.eye(3) + H) - np.eye(3), mat)
+        assert np.allclose(PQ, Q @ P, rtol=0, atol=1e-12 * np.abs(P).max())
+    H = 1e-7 * rng.normal(size=(3, 3))
+    eps = 0.5 * (H + H.T)
+    lin = lam * np.trace(eps) * np.eye(3) + 2 * mu * eps
+    assert np.abs(_oracle_P(H, mat) - lin).max() <= 1e-5 * np.abs(lin).max()
